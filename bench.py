@@ -1,0 +1,394 @@
+"""Benchmark of the dense lattice-Boltzmann hot path on B200.
+
+Workload: D3Q19 dense flow past a pinned sphere, 256 x 128 x 128 cells,
+sphere r = 16 at (96, 64, 64), inlet/sponge u = 0.05, tau = 0.56, Ladd
+bounce-back with local rho_w, ALBC sponge (width 16) toward the freestream,
+uniform Guo body force F_x = 1e-6, FP32 storage, drag/lift summed in FP64
+every step. A "step" is one fused stream-collide-force pass over the whole
+grid (4,194,304 lattice updates). Inputs are synthetic (uniform freestream
+seed, as the reference's sphere scenario does); f is 2 x 319 MB, larger than
+L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica of the workload on its
+own GPU (weak scaling, no data-path collective); the timed region is
+bracketed by a barrier and a device synchronize, and the reported time is
+the maximum over ranks. `--impl reference` times the CPU restatement of the
+reference's arithmetic (the reference itself is WGSL that cannot run here)
+on this host's cores; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+BYTES_PER_LU = {("d3q19", "fp32"): 152, ("d3q19", "fp16"): 76, ("d3q19", "bf16"): 76}
+DIMS = (256, 128, 128)
+
+
+def load_package():
+    if "getting_air_b200" in sys.modules:
+        return sys.modules["getting_air_b200"]
+    pkg = ROOT / "getting-air_b200"
+    spec = importlib.util.spec_from_file_location("getting_air_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["getting_air_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(storage="fp32", dims=DIMS, n=32):
+    lbm = load_package()
+    from getting_air_b200 import scenarios as sc
+    return sc.sphere(n=n, dims=dims, u0=0.05, tau=0.56, q=19, bounceback=True,
+                     force=(1e-6, 0.0, 0.0), storage=storage)
+
+
+def config_key(storage="fp32"):
+    return {"workload": "D3Q19 dense sphere 256x128x128 r=16 tau=0.56 u0=0.05 bounce-back+sponge+Guo force, "
+                        "FP64 drag/lift every step",
+            "lattice": "D3Q19", "dims": list(DIMS), "cells": int(np.prod(DIMS)), "storage": storage,
+            "l2": "inputs larger than L2 (2 x 319 MB f buffers), no flush"}
+
+
+# ---- clocks ------------------------------------------------------------------
+
+REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x40: "sw_thermal_slowdown",
+           0x80: "hw_thermal_slowdown", 0x100: "hw_power_brake_slowdown", 0x2: "applications_clocks_setting"}
+
+
+class ClockSampler:
+    """Samples the SM clock and clock-event reasons of this rank's GPU via NVML."""
+
+    def __init__(self, torch_dev: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(torch_dev).uuid)
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = u.decode() if isinstance(u, bytes) else u
+                if u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                    self._h = h
+            if self._h is None:
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._nv = pynvml
+        except Exception as e:  # NVML missing: report no clocks rather than guess
+            self.error = repr(e)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+# ---- peaks / profiles -----------------------------------------------------------
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch recorded from an ncu capture, if one is committed."""
+    p = ROOT / "profiles" / f"{kernel}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+# ---- distributed plumbing ----------------------------------------------------
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- our arm -------------------------------------------------------------------
+
+def time_device(lbm, wl, steps, warmup, world):
+    """Device-resident throughput: K fused steps, CUDA events on the session stream."""
+    import torch
+    s = lbm.Solver.create(wl["q"], wl["dims"], **wl["kw"])
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        s.init_macro(wl["mac"])
+        s.step(warmup)
+        s.sync()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(world)
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            start.record(stream)
+            for a, b in evs:
+                a.record(stream)
+                s.step(1)
+                b.record(stream)
+            end.record(stream)
+            torch.cuda.synchronize()
+        barrier(world)
+    total_ms = start.elapsed_time(end)
+    launch_ms = [a.elapsed_time(b) for a, b in evs]
+    forces = s.forces()
+    totals = s.totals()
+    s.close()
+    return total_ms, launch_ms, clk.summary(), forces, totals
+
+
+def time_e2e(lbm, wl, steps, warmup, world):
+    """Through the C ABI with host buffers: upload the seed from pinned host
+    memory, K steps each followed by a 48-byte force readback, and the final
+    macroscopic field read back to pinned host memory."""
+    import torch
+    mac_host = torch.from_numpy(np.ascontiguousarray(wl["mac"], np.float32)).pin_memory()
+    out_host = torch.empty_like(mac_host).pin_memory()
+    mac_np, out_np = mac_host.numpy(), out_host.numpy()
+    s = lbm.Solver.create(wl["q"], wl["dims"], **wl["kw"])
+    s.init_macro(mac_np)
+    s.step(warmup)
+    s.sync()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.init_macro(mac_np)
+    for _ in range(steps):
+        s.step(1)
+        s.forces()
+    s.sync()
+    out_np[:] = s.read_mac()
+    t1 = time.perf_counter()
+    s.close()
+    ms = max_over_ranks((t1 - t0) * 1e3, world)
+    h2d = mac_np.nbytes / steps
+    d2h = (out_np.nbytes + 6 * 8 * steps) / steps
+    return ms, h2d, d2h
+
+
+def cpu_baseline(seconds=10.0):
+    """The oracle's f32 path (a restatement of the reference's shader math) on
+    this host's cores, on a half-scale copy of the workload (same scenario,
+    128 x 64 x 64, r = 8), stepped until `seconds` of CPU time have passed."""
+    import oracle
+    lbm = load_package()
+    wl = workload(dims=(128, 64, 64), n=16)
+    cfg = lbm.default_config(19, wl["dims"])
+    s_kw = wl["kw"]
+    cfg.tau = s_kw["tau"]
+    cfg.has_body, cfg.use_bounceback = 1, 1
+    cfg.body = lbm.make_body(**s_kw["body"])
+    cfg.sponge_w = s_kw["sponge_w"]
+    for j in range(3):
+        cfg.sponge_u[j] = s_kw["sponge_u"][j]
+        cfg.force[j] = s_kw["force"][j]
+    f = oracle.init_eq(19, wl["mac"], fp32=True)
+    cells = int(np.prod(wl["dims"]))
+    done, t_used, chunk = 0, 0.0, 2
+    while t_used < seconds:
+        t0 = time.perf_counter()
+        f, _, _ = oracle.run(cfg, f, chunk, fp32=True)
+        t_used += time.perf_counter() - t0
+        done += chunk
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": cells * done / t_used / 1e6, "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"D3Q19 sphere 128x64x64 r=8 (half-scale workload), {done} steps incl. force pass, "
+                      f"{t_used:.1f} s, oracle f32 mode, OpenMP"}
+
+
+def run_ours(args):
+    import torch
+    lbm = load_package()
+    world, rank, local = dist_setup(args.gpus)
+    wl = workload("fp32")
+    cells = int(np.prod(wl["dims"]))
+    total_ms, launch_ms, clocks, forces, totals = time_device(lbm, wl, args.steps, args.warmup, world)
+    t_max = max_over_ranks(total_ms, world)
+    kern_ms = max_over_ranks(statistics.mean(launch_ms), world)
+    value = cells * args.steps * world / (t_max * 1e-3) / 1e6
+    e2e_ms, h2d, d2h = time_e2e(lbm, wl, args.steps, args.warmup, world)
+    e2e_value = cells * args.steps * world / (e2e_ms * 1e-3) / 1e6
+
+    # Packed storage forms on the same workload (device-resident, same timing).
+    forms = {}
+    if not args.skip_forms:
+        for st in ("fp16", "bf16"):
+            tm, lm, _, fo, _ = time_device(lbm, workload(st), args.steps, args.warmup, world)
+            tm = max_over_ranks(tm, world)
+            forms[st] = {"mlups": cells * args.steps * world / (tm * 1e-3) / 1e6,
+                         "ms_per_step": tm / args.steps,
+                         "gbs": BYTES_PER_LU[("d3q19", st)] * cells / (statistics.mean(lm) * 1e-3) / 1e9,
+                         "fx_last": fo[0]}
+    peak, peak_kind = hbm_peak()
+    achieved = BYTES_PER_LU[("d3q19", "fp32")] * cells / (kern_ms * 1e-3) / 1e9
+    traffic = profiled_traffic("d3q19_sphere_step")
+    line = {
+        "metric": "MLUPS (D3Q19 dense sphere step, FP32) and % of HBM roofline",
+        "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (uniform freestream seed, sphere scenario)",
+        "config": config_key("fp32") | {"parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "algorithmic_bytes_per_lu": 152, "kernel": "d3_step<19,float>",
+                     "kernel_ms": kern_ms},
+        "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms / args.steps},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "forms": forms,
+        "drag_lift_last_step": {"fx": forces[0], "fy": forces[1], "fz": forces[2]},
+        "mass_excess": totals["mass"],
+    }
+    if rank == 0:
+        if world == 1 and not args.skip_cpu:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    lbm = load_package()
+    wl = workload("fp32")
+    cfg = lbm.default_config(19, wl["dims"])
+    kw = wl["kw"]
+    cfg.tau = kw["tau"]
+    cfg.has_body, cfg.use_bounceback = 1, 1
+    cfg.body = lbm.make_body(**kw["body"])
+    cfg.sponge_w = kw["sponge_w"]
+    for j in range(3):
+        cfg.sponge_u[j] = kw["sponge_u"][j]
+        cfg.force[j] = kw["force"][j]
+    cells = int(np.prod(wl["dims"]))
+    f = oracle.init_eq(19, wl["mac"], fp32=True)
+    f, _, _ = oracle.run(cfg, f, args.warmup, fp32=True)
+    t0 = time.perf_counter()
+    f, _, forces = oracle.run(cfg, f, args.steps, fp32=True)
+    dt = time.perf_counter() - t0
+    value = cells * args.steps / dt / 1e6
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {
+        "impl": "reference",
+        "metric": "MLUPS (D3Q19 dense sphere step, FP32) and % of HBM roofline",
+        "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (uniform freestream seed, sphere scenario)",
+        "config": config_key("fp32") | {"parallelism": "host CPU"},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": "port",
+                         "sample": f"full 256x128x128 workload, {args.steps} timed steps incl. the force pass; "
+                                   "the reference's WGSL cannot run here (no WebGPU), so this is the "
+                                   "oracle's f32 restatement of it"},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "drag_lift_last_step": {"fx": float(forces[-1][0]) if len(forces) else None},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--skip-forms", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        # The CPU arm is bounded to a few minutes: its steps are capped.
+        args.steps = min(args.steps, 20)
+        args.warmup = min(args.warmup, 3)
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,56 @@
+// Launch parameters and entry points of the dense-grid kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/lbm.h"
+
+namespace lbm {
+
+// Per-step constants of the fused stream-collide kernels. Mirrors the
+// override constants of common_d3_step.wgsl:125-213 / lbm_step.wgsl:36-135.
+struct StepParams {
+  int nx, ny, nz;
+  int64_t n;            // cells per plane
+  float omega;          // 1 / tau
+  float fx, fy, fz;     // uniform Guo body force
+  int wall_x, wall_y, wall_z;
+  float wall_u0, wall_u1;  // D2Q9 moving y-walls
+  int has_body, bb, solid_eq, rho_w_local, swept;
+  float swept_band;     // |phi| below which a cell can change hands in one step
+  float chi_eps;
+  float sponge_w;
+  int sax, say, saz;
+  float ftarget[27];    // sponge far-field equilibrium per direction (rho = 1)
+  lbm_body body;
+  int write_mac;
+  // Force reduction: the blocks of the launch grid that can see the body.
+  int force_on;
+  int rbx0, rbx1, rby0, rby1, rbz0, rbz1;
+  double *partials;        // 8 doubles per region block
+  unsigned int *counter;   // last-block ticket, returns to 0 after each step
+  double *force_out;       // 8 doubles: fx fy fz tx ty tz nonfinite 0
+};
+
+// Reduction constants.
+constexpr int kStepThreads = 128;
+constexpr int kReduceThreads = 256;
+constexpr int kForceSlots = 8;
+constexpr int kTotalsSlots = 8;
+
+// storage: 0 fp32, 1 fp16 offset, 2 bf16 offset
+cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float *mac,
+                        const StepParams &p, cudaStream_t st);
+cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n,
+                           cudaStream_t st);
+cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n,
+                        cudaStream_t st);
+cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n,
+                          cudaStream_t st);
+// Totals over the current f, FP64; `partials` holds totals_partials() * 8
+// doubles, `counter` one zeroed unsigned int.
+int totals_blocks();
+cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, double *partials,
+                          unsigned int *counter, double *out, cudaStream_t st);
+
+}  // namespace lbm

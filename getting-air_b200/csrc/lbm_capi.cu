@@ -1,0 +1,458 @@
+// C ABI of the dense solver: session lifetime, state transfer, stepping and
+// the FP64 reductions. Host side of the reference's page objects
+// (main-3d.js encodeSteps / debugStepSync / readStats and
+// main-cylinder.js's step loop), without WebGPU: a session owns two f
+// buffers (ping-pong), the mac field and the reduction scratch, and launches
+// on one CUDA stream.
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm.h"
+#include "dense.cuh"
+#include "lattice.cuh"
+
+using namespace lbm;
+
+struct lbm_session {
+  lbm_config cfg{};
+  int q = 0, storage = 0, elem = 4;
+  int64_t n = 0;
+  void *f[2] = {nullptr, nullptr};
+  int cur = 0;
+  float *mac = nullptr;
+  double *force_partials = nullptr;
+  unsigned int *force_counter = nullptr;
+  double *force_out = nullptr;
+  int force_nparts = 0;
+  double *tot_partials = nullptr;
+  unsigned int *tot_counter = nullptr;
+  double *tot_out = nullptr;
+  double *host_out = nullptr;  // pinned, 16 doubles
+  cudaStream_t own = nullptr, stream = nullptr;
+  StepParams sp{};
+  int64_t bytes = 0;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(lbm_session *s, int code, const std::string &msg) {
+  if (s) s->err = msg; else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(lbm_session *s, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return fail(s, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA, m);
+}
+
+#define CK(s, call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, #call); \
+  } while (0)
+
+template <int Q> void tables(int32_t *ex, int32_t *ey, int32_t *ez, float *w, int32_t *opp) {
+  for (int i = 0; i < Q; ++i) {
+    if (ex) ex[i] = Lattice<Q>::ex(i);
+    if (ey) ey[i] = Lattice<Q>::ey(i);
+    if (ez) ez[i] = Lattice<Q>::ez(i);
+    if (w) w[i] = Lattice<Q>::w(i);
+    if (opp) opp[i] = Lattice<Q>::opp(i);
+  }
+}
+
+template <int Q> float weight(int i) { return Lattice<Q>::w(i); }
+float weight_of(int q, int i) {
+  return q == 9 ? weight<9>(i) : (q == 19 ? weight<19>(i) : weight<27>(i));
+}
+void dir_of(int q, int i, int &ex, int &ey, int &ez) {
+  if (q == 9) { ex = Lattice<9>::ex(i); ey = Lattice<9>::ey(i); ez = 0; }
+  else { ex = Lattice<27>::ex(i); ey = Lattice<27>::ey(i); ez = Lattice<27>::ez(i); }
+}
+
+float circumradius(const lbm_body &b) {
+  switch (b.shape) {
+    case LBM_SHAPE_SPHERE: return b.a;
+    case LBM_SHAPE_SPHEROID: return std::fmax(b.a, b.c);
+    case LBM_SHAPE_ELLIPSE: return std::fmax(b.a, b.b);
+    default: return std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c);
+  }
+}
+
+int validate(const lbm_config *c, std::string &why) {
+  if (!c) { why = "config is NULL"; return LBM_EINVAL; }
+  if (c->q != 9 && c->q != 19 && c->q != 27) { why = "q must be 9, 19 or 27"; return LBM_EINVAL; }
+  if (c->nx < 3 || c->ny < 3 || c->nz < 1) { why = "grid must be at least 3 cells per axis"; return LBM_EINVAL; }
+  if (c->q == 9 && c->nz != 1) { why = "D2Q9 requires nz == 1"; return LBM_EINVAL; }
+  if (c->q != 9 && c->nz < 3) { why = "3D lattices need nz >= 3"; return LBM_EINVAL; }
+  if (c->ny > 65535 || c->nz > 65535) { why = "ny and nz are limited to 65535"; return LBM_EINVAL; }
+  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
+  if (n > 0x7fffffffLL) { why = "grid exceeds 2^31-1 cells"; return LBM_EINVAL; }
+  if (!(c->tau > 0.5f) || !std::isfinite(c->tau)) { why = "tau must be finite and > 0.5"; return LBM_EINVAL; }
+  if (c->storage < 0 || c->storage > 2) { why = "unknown storage"; return LBM_EINVAL; }
+  if (c->has_body) {
+    const int sh = c->body.shape;
+    if (c->q == 9 && sh != LBM_SHAPE_ELLIPSE) { why = "D2Q9 bodies are ellipses"; return LBM_EINVAL; }
+    if (c->q != 9 && (sh < 0 || sh > 2)) { why = "3D body shape must be sphere, spheroid or roundbox"; return LBM_EINVAL; }
+    if (!(c->body.a > 0.f)) { why = "body size must be positive"; return LBM_EINVAL; }
+    if (!c->use_bounceback && !(c->chi_eps > 0.f)) { why = "chi_eps must be positive"; return LBM_EINVAL; }
+  }
+  return LBM_OK;
+}
+
+// Which launch blocks can receive a force contribution: cells within the
+// body's circumradius plus the widest band any contribution comes from
+// (|e| for a bounce-back link, the one-step sweep for the swept-cell term,
+// the point where chi drops below 1e-6 for the penalty).
+void set_force_region(lbm_session *s) {
+  StepParams &p = s->sp;
+  const lbm_config &c = s->cfg;
+  p.force_on = c.has_body ? 1 : 0;
+  if (!c.has_body) return;
+  const lbm_body &b = c.body;
+  const float rc = circumradius(b);
+  const float speed = std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
+                      std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc;
+  p.swept = (c.q != 9 && c.use_bounceback && c.swept_force && speed > 0.f) ? 1 : 0;
+  p.swept_band = 2.0f + speed;
+  const float margin = c.use_bounceback ? (3.0f + speed) : (8.0f * c.chi_eps + 2.0f);
+  const float reach = rc + margin;
+  auto range = [&](float centre, int len, bool periodic_image, int &lo, int &hi) {
+    int a = (int)std::floor(centre - reach), e = (int)std::ceil(centre + reach);
+    if (periodic_image && (a < 0 || e > len - 1)) { lo = 0; hi = len - 1; return; }
+    lo = a < 0 ? 0 : a;
+    hi = e > len - 1 ? len - 1 : e;
+  };
+  const bool wrap2d = (c.q == 9);
+  int x0, x1, y0, y1, z0 = 0, z1 = 0;
+  range(b.cx, c.nx, wrap2d, x0, x1);
+  range(b.cy, c.ny, wrap2d, y0, y1);
+  if (c.q != 9) range(b.cz, c.nz, false, z0, z1);
+  if (x0 > x1 || y0 > y1 || z0 > z1) {
+    p.force_on = 0;
+    return;
+  }
+  p.rbx0 = x0 / kStepThreads;
+  p.rbx1 = x1 / kStepThreads + 1;
+  p.rby0 = y0;
+  p.rby1 = y1 + 1;
+  p.rbz0 = z0;
+  p.rbz1 = z1 + 1;
+}
+
+int ensure_force_scratch(lbm_session *s) {
+  const StepParams &p = s->sp;
+  if (!p.force_on) return LBM_OK;
+  const int need = (p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0);
+  if (need <= s->force_nparts) return LBM_OK;
+  if (s->force_partials) {
+    cudaFree(s->force_partials);
+    s->bytes -= (int64_t)s->force_nparts * kForceSlots * 8;
+  }
+  s->force_partials = nullptr;
+  CK(s, cudaMalloc(&s->force_partials, (size_t)need * kForceSlots * sizeof(double)));
+  s->force_nparts = need;
+  s->bytes += (int64_t)need * kForceSlots * 8;
+  return LBM_OK;
+}
+
+void fill_params(lbm_session *s) {
+  const lbm_config &c = s->cfg;
+  StepParams &p = s->sp;
+  p.nx = c.nx; p.ny = c.ny; p.nz = c.nz; p.n = s->n;
+  p.omega = 1.0f / c.tau;
+  p.fx = c.force[0]; p.fy = c.force[1]; p.fz = c.q == 9 ? 0.f : c.force[2];
+  p.wall_x = c.q == 9 ? 0 : c.wall[0];
+  p.wall_y = c.wall[1];
+  p.wall_z = c.q == 9 ? 0 : c.wall[2];
+  p.wall_u0 = c.wall_u[0]; p.wall_u1 = c.wall_u[1];
+  p.has_body = c.has_body; p.bb = c.use_bounceback; p.solid_eq = c.solid_eq;
+  p.rho_w_local = c.rho_w_local;
+  p.chi_eps = c.chi_eps;
+  p.sponge_w = c.sponge_w;
+  p.sax = c.sponge_axis[0]; p.say = c.sponge_axis[1]; p.saz = c.sponge_axis[2];
+  const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.q == 9 ? 0.f : c.sponge_u[2];
+  const float ufar = c.q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);
+  for (int i = 0; i < 27; ++i) p.ftarget[i] = 0.f;
+  for (int i = 0; i < c.q; ++i) {
+    int ex, ey, ez;
+    dir_of(c.q, i, ex, ey, ez);
+    const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
+    p.ftarget[i] = weight_of(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * ufar);
+  }
+  p.body = c.body;
+  p.write_mac = 0;
+  p.partials = s->force_partials;
+  p.counter = s->force_counter;
+  p.force_out = s->force_out;
+  set_force_region(s);
+}
+
+void release(lbm_session *s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  cudaFree(s->f[0]);
+  cudaFree(s->f[1]);
+  cudaFree(s->mac);
+  cudaFree(s->force_partials);
+  cudaFree(s->force_counter);
+  cudaFree(s->force_out);
+  cudaFree(s->tot_partials);
+  cudaFree(s->tot_counter);
+  cudaFree(s->tot_out);
+  if (s->host_out) cudaFreeHost(s->host_out);
+  if (s->own) cudaStreamDestroy(s->own);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lbm_version(void) { return "getting-air-b200 dense 0.1 (sm_100a)"; }
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+int lbm_config_default(lbm_config *cfg, int q, int nx, int ny, int nz) {
+  if (!cfg) return LBM_EINVAL;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->q = q;
+  cfg->nx = nx; cfg->ny = ny; cfg->nz = nz;
+  cfg->tau = 0.8f;  // OMEGA 1.25 (common_d3_step.wgsl:151)
+  cfg->solid_eq = 1;
+  cfg->rho_w_local = 1;
+  cfg->swept_force = 1;
+  cfg->chi_eps = 1.5f;
+  cfg->sponge_w = q == 9 ? 4.0f : 0.0f;  // lbm_step.wgsl SPONGE_W = 4; 3D default 0
+  cfg->sponge_axis[0] = cfg->sponge_axis[1] = cfg->sponge_axis[2] = 1;
+  cfg->body.qw = 1.0f;
+  cfg->body.shape = q == 9 ? LBM_SHAPE_ELLIPSE : LBM_SHAPE_SPHERE;
+  cfg->storage = LBM_STORE_FP32;
+  return LBM_OK;
+}
+
+int lbm_create(const lbm_config *cfg, lbm_session **out) {
+  if (!out) return fail(nullptr, LBM_EINVAL, "out is NULL");
+  *out = nullptr;
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(nullptr, rc, why);
+  lbm_session *s = new lbm_session();
+  s->cfg = *cfg;
+  s->q = cfg->q;
+  s->storage = cfg->storage;
+  s->elem = cfg->storage == LBM_STORE_FP32 ? 4 : 2;
+  s->n = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+  auto bail = [&](cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    release(s);
+    delete s;
+    return fail(nullptr, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA, m);
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking))) return bail(e, "stream");
+  s->stream = s->own;
+  const size_t fbytes = (size_t)s->q * s->n * s->elem;
+  if ((e = cudaMalloc(&s->f[0], fbytes))) return bail(e, "cudaMalloc f[0]");
+  if ((e = cudaMalloc(&s->f[1], fbytes))) return bail(e, "cudaMalloc f[1]");
+  if ((e = cudaMalloc(&s->mac, (size_t)s->n * 16))) return bail(e, "cudaMalloc mac");
+  if ((e = cudaMalloc(&s->force_counter, sizeof(unsigned int)))) return bail(e, "cudaMalloc counter");
+  if ((e = cudaMalloc(&s->force_out, kForceSlots * sizeof(double)))) return bail(e, "cudaMalloc force");
+  if ((e = cudaMalloc(&s->tot_partials, (size_t)totals_blocks() * kTotalsSlots * sizeof(double))))
+    return bail(e, "cudaMalloc totals");
+  if ((e = cudaMalloc(&s->tot_counter, sizeof(unsigned int)))) return bail(e, "cudaMalloc counter");
+  if ((e = cudaMalloc(&s->tot_out, kTotalsSlots * sizeof(double)))) return bail(e, "cudaMalloc totals");
+  if ((e = cudaMallocHost(&s->host_out, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
+  cudaMemsetAsync(s->force_counter, 0, sizeof(unsigned int), s->stream);
+  cudaMemsetAsync(s->tot_counter, 0, sizeof(unsigned int), s->stream);
+  cudaMemsetAsync(s->force_out, 0, kForceSlots * sizeof(double), s->stream);
+  cudaMemsetAsync(s->mac, 0, (size_t)s->n * 16, s->stream);
+  cudaMemsetAsync(s->f[0], 0, fbytes, s->stream);
+  s->bytes = 2 * (int64_t)fbytes + s->n * 16 + totals_blocks() * kTotalsSlots * 8 + 200;
+  fill_params(s);
+  if (ensure_force_scratch(s)) {
+    std::string m = s->err;
+    release(s);
+    delete s;
+    return fail(nullptr, LBM_ENOMEM, m);
+  }
+  s->sp.partials = s->force_partials;
+  if ((e = cudaStreamSynchronize(s->stream))) return bail(e, "initialise");
+  *out = s;
+  return LBM_OK;
+}
+
+void lbm_destroy(lbm_session *s) {
+  release(s);
+  delete s;
+}
+
+const char *lbm_last_error(const lbm_session *s) {
+  return s ? s->err.c_str() : g_create_error.c_str();
+}
+
+int lbm_set_stream(lbm_session *s, void *stream) {
+  if (!s) return LBM_EINVAL;
+  CK(s, cudaStreamSynchronize(s->stream));
+  s->stream = stream ? (cudaStream_t)stream : s->own;
+  return LBM_OK;
+}
+
+int lbm_init_macro(lbm_session *s, const float *mac) {
+  if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
+  CK(s, cudaMemcpyAsync(s->mac, mac, (size_t)s->n * 16, cudaMemcpyHostToDevice, s->stream));
+  CK(s, launch_init_eq(s->q, s->storage, s->mac, s->f[s->cur], s->n, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int lbm_write_f(lbm_session *s, const float *f) {
+  if (!s || !f) return s ? fail(s, LBM_EINVAL, "f is NULL") : LBM_EINVAL;
+  const size_t bytes = (size_t)s->q * s->n * 4;
+  if (s->storage == LBM_STORE_FP32) {
+    CK(s, cudaMemcpyAsync(s->f[s->cur], f, bytes, cudaMemcpyHostToDevice, s->stream));
+  } else {
+    float *tmp = nullptr;
+    CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
+    cudaError_t e = cudaMemcpyAsync(tmp, f, bytes, cudaMemcpyHostToDevice, s->stream);
+    if (!e) e = launch_pack(s->q, s->storage, tmp, s->f[s->cur], s->n, s->stream);
+    cudaFreeAsync(tmp, s->stream);
+    if (e) return cuda_fail(s, e, "pack f");
+  }
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int lbm_read_f(lbm_session *s, float *f) {
+  if (!s || !f) return s ? fail(s, LBM_EINVAL, "f is NULL") : LBM_EINVAL;
+  const size_t bytes = (size_t)s->q * s->n * 4;
+  if (s->storage == LBM_STORE_FP32) {
+    CK(s, cudaMemcpyAsync(f, s->f[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+  } else {
+    float *tmp = nullptr;
+    CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
+    cudaError_t e = launch_unpack(s->q, s->storage, s->f[s->cur], tmp, s->n, s->stream);
+    if (!e) e = cudaMemcpyAsync(f, tmp, bytes, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(tmp, s->stream);
+    if (e) return cuda_fail(s, e, "unpack f");
+  }
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int lbm_read_mac(lbm_session *s, float *mac) {
+  if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
+  CK(s, cudaMemcpyAsync(mac, s->mac, (size_t)s->n * 16, cudaMemcpyDeviceToHost, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int lbm_step(lbm_session *s, int n) {
+  if (!s) return LBM_EINVAL;
+  if (n < 0) return fail(s, LBM_EINVAL, "step count must be >= 0");
+  for (int k = 0; k < n; ++k) {
+    s->sp.write_mac = (k == n - 1);
+    CK(s, launch_step(s->q, s->storage, s->f[s->cur], s->f[1 - s->cur], s->mac, s->sp, s->stream));
+    s->cur = 1 - s->cur;
+  }
+  return LBM_OK;
+}
+
+int lbm_set_body(lbm_session *s, const lbm_body *body) {
+  if (!s || !body) return s ? fail(s, LBM_EINVAL, "body is NULL") : LBM_EINVAL;
+  lbm_config c = s->cfg;
+  c.body = *body;
+  std::string why;
+  if (validate(&c, why)) return fail(s, LBM_EINVAL, why);
+  s->cfg = c;
+  fill_params(s);
+  int rc = ensure_force_scratch(s);
+  if (rc) return rc;
+  s->sp.partials = s->force_partials;
+  return LBM_OK;
+}
+
+int lbm_forces(lbm_session *s, double out[6]) {
+  if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  if (!s->sp.force_on) {
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    return LBM_OK;
+  }
+  CK(s, cudaMemcpyAsync(s->host_out, s->force_out, 6 * sizeof(double), cudaMemcpyDeviceToHost,
+                        s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 6; ++k) out[k] = s->host_out[k];
+  return LBM_OK;
+}
+
+int lbm_totals(lbm_session *s, double out[8]) {
+  if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  CK(s, launch_totals(s->q, s->storage, s->f[s->cur], s->n, s->tot_partials, s->tot_counter,
+                      s->tot_out, s->stream));
+  CK(s, cudaMemcpyAsync(s->host_out, s->tot_out, 8 * sizeof(double), cudaMemcpyDeviceToHost,
+                        s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 8; ++k) out[k] = s->host_out[k];
+  return LBM_OK;
+}
+
+int lbm_sync(lbm_session *s) {
+  if (!s) return LBM_EINVAL;
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int64_t lbm_device_bytes(const lbm_session *s) { return s ? s->bytes : 0; }
+
+int lbm_lattice_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez, float *w, int32_t *opp) {
+  switch (q) {
+    case 9: tables<9>(ex, ey, ez, w, opp); return LBM_OK;
+    case 19: tables<19>(ex, ey, ez, w, opp); return LBM_OK;
+    case 27: tables<27>(ex, ey, ez, w, opp); return LBM_OK;
+    default: return LBM_EINVAL;
+  }
+}
+
+// Round-to-nearest-even f32 -> binary16 through the f32 bit pattern, the
+// semantics of f-pack.mjs:44-77 (which is what the GPU's pack2x16float does).
+uint16_t lbm_f32_to_f16_bits(float v) {
+  uint32_t x;
+  std::memcpy(&x, &v, 4);
+  const uint32_t sign = (x >> 16) & 0x8000u;
+  const int exp = (int)((x >> 23) & 0xffu);
+  uint32_t man = x & 0x7fffffu;
+  if (exp == 0xff) return (uint16_t)(sign | 0x7c00u | (man ? 0x200u : 0u));
+  const int e = exp - 112;
+  if (e >= 0x1f) return (uint16_t)(sign | 0x7c00u);
+  if (e <= 0) {
+    if (e < -10) return (uint16_t)sign;
+    man |= 0x800000u;
+    const int shift = 14 - e;
+    uint32_t h = man >> shift;
+    const uint32_t rem = man & ((1u << shift) - 1u);
+    const uint32_t half = 1u << (shift - 1);
+    if (rem > half || (rem == half && (h & 1u))) h += 1;
+    return (uint16_t)(sign | h);
+  }
+  uint32_t h = ((uint32_t)e << 10) | (man >> 13);
+  const uint32_t rem = man & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) h += 1;
+  return (uint16_t)(sign | h);
+}
+
+float lbm_f16_bits_to_f32(uint16_t h) {
+  const float s = (h & 0x8000u) ? -1.0f : 1.0f;
+  const int e = (h >> 10) & 0x1f;
+  const int m = h & 0x3ff;
+  if (e == 0) return s * (float)m * 5.9604644775390625e-8f;
+  if (e == 31) return m ? NAN : s * INFINITY;
+  return s * (1.0f + (float)m / 1024.0f) * std::ldexp(1.0f, e - 15);
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+"""Synthetic inputs: the reference's scenario seeds, restated.
+
+* :func:`sphere` -- d3-scenarios.mjs:350-389 (`SCENARIOS.sphere`): domain
+  12D x 8D x 8D unless dims are given, centre (3D, NY/2, NZ/2), tau from Re,
+  sponge width max(6, round(D/2)) toward (u0, 0, 0), uniform seed
+  rho = 1 - |u|^2 / (2 cs^2) (seedMacro3, d3-scenarios.mjs:245-261).
+* :func:`tgv2d_field` -- main-tgv.js:69-89 analyticField: the exact decaying
+  Taylor-Green field with its O(Ma^2) density term; :func:`tgv2d_f` seeds f
+  at equilibrium in f64 and rounds to f32 (main-tgv.js:136 initF).
+* :func:`cylinder2d` -- the pinned-cylinder crossflow of the 2D cylinder
+  pages: circle of radius r, sponge toward (u0, 0).
+* :func:`mulberry32` -- the seeded generator the reference uses for
+  perturbations (d3-scenarios.mjs:207-215).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+CS2 = 1.0 / 3.0
+
+
+def nu_from_tau(tau: float) -> float:
+    return CS2 * (tau - 0.5)
+
+
+def tau_from_nu(nu: float) -> float:
+    return nu / CS2 + 0.5
+
+
+def mulberry32(seed: int):
+    s = seed & 0xFFFFFFFF
+
+    def imul(a, b):
+        return (a * b) & 0xFFFFFFFF
+
+    def nxt():
+        nonlocal s
+        s = (s + 0x6D2B79F5) & 0xFFFFFFFF
+        t = imul(s ^ (s >> 15), 1 | s)
+        t = ((t + imul(t ^ (t >> 7), 61 | t)) & 0xFFFFFFFF) ^ t
+        return ((t ^ (t >> 14)) & 0xFFFFFFFF) / 4294967296.0
+
+    return nxt
+
+
+def uniform_macro(ncells: int, u=(0.0, 0.0, 0.0)) -> np.ndarray:
+    ux, uy, uz = u
+    mac = np.empty((ncells, 4), np.float32)
+    mac[:, 0] = np.float32(1 - (ux * ux + uy * uy + uz * uz) / (2 * CS2))
+    mac[:, 1], mac[:, 2], mac[:, 3] = ux, uy, uz
+    return mac
+
+
+def sphere(n: int = 16, u0: float = 0.05, re: float = 100.0, tau: float | None = None,
+           dims=None, q: int = 19, bounceback: bool = True, force=(0.0, 0.0, 0.0),
+           storage: str = "fp32") -> dict:
+    """Flow past a pinned sphere of diameter n (cells). Returns solver kwargs + seed."""
+    if tau is None:
+        nu = u0 * n / re
+        tau = tau_from_nu(nu)
+    d = list(dims) if dims is not None else [round(12 * n), round(8 * n), round(8 * n)]
+    R = n / 2
+    body = dict(shape="sphere", centre=(3 * n, d[1] / 2, d[2] / 2), a=R)
+    kw = dict(tau=float(tau), has_body=1, use_bounceback=int(bounceback), body=body,
+              sponge_w=float(max(6, round(n / 2))), sponge_u=(u0, 0.0, 0.0), force=tuple(force),
+              storage=storage)
+    return {"q": q, "dims": tuple(d), "kw": kw, "mac": uniform_macro(d[0] * d[1] * d[2], (u0, 0, 0)),
+            "area": math.pi * R * R, "u0": u0}
+
+
+def tgv2d_field(N: int, u0: float, tau: float, t: float = 0.0):
+    """Analytic TGV (ux, uy, rho) on an N x N periodic box at time t, f64."""
+    k = 2 * math.pi / N
+    nu = nu_from_tau(tau)
+    td = 1.0 / (nu * (k * k + k * k))
+    x = np.arange(N)[None, :].astype(np.float64)
+    y = np.arange(N)[:, None].astype(np.float64)
+    dec, dec2 = math.exp(-t / td), math.exp(-2 * t / td)
+    ux = -u0 * np.cos(k * x) * np.sin(k * y) * dec
+    uy = u0 * np.sin(k * x) * np.cos(k * y) * dec
+    p = -(u0 * u0 / 4) * (np.cos(2 * k * x) + np.cos(2 * k * y)) * dec2
+    rho = 1 + p / CS2
+    return ux.ravel(), uy.ravel(), rho.ravel(), td
+
+
+def tgv2d_f(N: int, u0: float, tau: float, w) -> np.ndarray:
+    """Equilibrium seed (9 x N^2, f32) from the analytic t=0 field."""
+    ux, uy, rho, _ = tgv2d_field(N, u0, tau)
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1], np.float64)
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1], np.float64)
+    f = np.empty((9, N * N), np.float32)
+    usq = ux * ux + uy * uy
+    for i in range(9):
+        eu = ex[i] * ux + ey[i] * uy
+        f[i] = (float(w[i]) * rho * (1 + eu * 3 + eu * eu * 4.5 - usq * 1.5)).astype(np.float32)
+    return f
+
+
+def cylinder2d(W: int = 256, H: int = 128, r: float = 10.0, u0: float = 0.05, tau: float = 0.6,
+               centre=None, bounceback: bool = True, sponge_w: float = 8.0) -> dict:
+    cx, cy = centre if centre is not None else (W / 4, H / 2)
+    body = dict(shape="ellipse", centre=(cx, cy, 0.0), a=r, b=r)
+    kw = dict(tau=float(tau), has_body=1, use_bounceback=int(bounceback), body=body,
+              sponge_w=float(sponge_w), sponge_u=(u0, 0.0, 0.0))
+    return {"q": 9, "dims": (W, H, 1), "kw": kw, "mac": uniform_macro(W * H, (u0, 0, 0))}

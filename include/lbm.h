@@ -1,0 +1,200 @@
+/*
+ * lbm.h -- C ABI of the B200 lattice-Boltzmann hot path.
+ *
+ * The reference (c7t/getting-air) drives its solver from JavaScript page
+ * objects that own WebGPU buffers: `init` seeds f from a macroscopic field,
+ * `step` encodes fused stream-collide dispatches, the force kernels feed
+ * drag/lift, and host code sums conserved totals over a readback. This
+ * header is the same behaviour as plain C entry points over an opaque
+ * session that owns its device memory, so a Node N-API shim, a ctypes
+ * stub or a C++ host can bind it without any torch or CUDA types.
+ *
+ * Conventions (mirroring the reference's error handling):
+ *   - every call returns 0 (LBM_OK) or a negative lbm_status;
+ *   - configuration errors the reference throws as `Error` (bad Q, bad
+ *     tau, a non-dividing block size, ...) return LBM_EINVAL and leave a
+ *     message for lbm_last_error();
+ *   - device faults the reference counts rather than throws (non-finite
+ *     force partials) are counted, see lbm_totals() out[7];
+ *   - host buffers are caller-owned; device memory is library-owned;
+ *   - one CUDA stream per session; a session is not thread-safe, distinct
+ *     sessions are.
+ *
+ * Field wire format is the reference's: f as Q planes of f32, plane-major
+ * (`f[i * ncells + cell]`, cell = (z*NY + y)*NX + x), whatever the on-device
+ * storage (f-pack.mjs:6-17 keeps f32 plane-major on the wire for the same
+ * reason). The macroscopic field is [rho, ux, uy, uz] per cell, interleaved
+ * (common_d3_step.wgsl:57-61 `mac : array<vec4<f32>>`).
+ */
+#ifndef LBM_H
+#define LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; everything declared here is
+ * exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define LBM_ABI_VERSION 1
+
+typedef enum {
+  LBM_OK = 0,
+  LBM_EINVAL = -1,    /* bad argument or configuration (reference: throws) */
+  LBM_ENOMEM = -2,    /* device allocation failed */
+  LBM_ECUDA = -3,     /* a CUDA call failed; message has the CUDA error */
+  LBM_ETIMEDOUT = -4, /* a bounded device wait gave up */
+  LBM_ENOTSUP = -5,   /* option not built into this library */
+  LBM_ESTATE = -6,    /* call not valid in the session's current state */
+  LBM_ENOSPC = -7     /* pool or budget exhausted (reference: refusal) */
+} lbm_status;
+
+/* On-device storage of f. The wire format is always f32 planes. */
+typedef enum {
+  LBM_STORE_FP32 = 0, /* plain f32 planes                                   */
+  LBM_STORE_FP16 = 1, /* binary16 planes holding f_i - w_i (f-pack mode 2)  */
+  LBM_STORE_BF16 = 2  /* bfloat16 planes holding f_i - w_i                  */
+} lbm_storage;
+
+/* Body shapes. 3D: common_d3_geometry.wgsl:40-42. D2Q9 uses ELLIPSE
+ * (common_geometry.wgsl get_phi; a circle when a == b). */
+typedef enum {
+  LBM_SHAPE_SPHERE = 0,
+  LBM_SHAPE_SPHEROID = 1,
+  LBM_SHAPE_ROUNDBOX = 2,
+  LBM_SHAPE_ELLIPSE = 3
+} lbm_shape;
+
+/* Rigid body pose and kinematics. The subset of BodyState3D
+ * (common_d3_geometry.wgsl:25-58, d3-body.mjs:318 BODY_FIELDS) and CardState
+ * (common_geometry.wgsl:8-35) that the step and force kernels read.
+ * Quaternion order is [w, x, y, z] as in the reference. */
+typedef struct {
+  int32_t shape;
+  float cx, cy, cz;       /* centre, lattice units (cell centres at integers) */
+  float qw, qx, qy, qz;   /* 3D orientation, body -> world                    */
+  float theta;            /* D2Q9 orientation angle                           */
+  float vx, vy, vz;       /* linear velocity                                  */
+  float wx, wy, wz;       /* angular velocity (D2Q9 uses wz as omega)         */
+  float a, b, c, r;       /* semi-axes / half-extents; r = roundbox rounding  */
+} lbm_body;
+
+/* Dense-domain configuration: the override constants of
+ * common_d3_step.wgsl:125-213 and lbm_step.wgsl:36-135, as a plain struct. */
+typedef struct {
+  int32_t q;              /* 9 (D2Q9), 19 (D3Q19) or 27 (D3Q27)              */
+  int32_t nx, ny, nz;     /* nz must be 1 when q == 9                        */
+  float tau;              /* BGK relaxation time; omega = 1/tau              */
+  float force[3];         /* uniform Guo body-force density FORCE_X/Y/Z      */
+  int32_t wall[3];        /* stationary no-slip walls normal to x, y, z      */
+  float wall_u[2];        /* D2Q9: x-velocity of the y=0 / y=H-1 walls       */
+  int32_t has_body;       /* HAS_BODY                                        */
+  int32_t use_bounceback; /* USE_BOUNCEBACK: 1 = sharp Ladd, 0 = chi penalty */
+  int32_t solid_eq;       /* SOLID_EQ                                        */
+  int32_t rho_w_local;    /* RHO_W_LOCAL (3D)                                */
+  int32_t swept_force;    /* SWEPT_FORCE (3D)                                */
+  float chi_eps;          /* CHI_EPS / K_EPS band width, cells               */
+  float sponge_w;         /* SPONGE_W; <= 0 disables the sponge              */
+  int32_t sponge_axis[3]; /* SPONGE_AX/AY/AZ                                 */
+  float sponge_u[3];      /* SPONGE_UX/UY/UZ far-field velocity              */
+  lbm_body body;
+  int32_t storage;        /* lbm_storage                                     */
+  int32_t reserved[7];    /* zero                                            */
+} lbm_config;
+
+typedef struct lbm_session lbm_session;
+
+/* Library version string and ABI version. */
+const char *lbm_version(void);
+int lbm_abi_version(void);
+
+/* Fills `cfg` with the reference's defaults (common_d3_step.wgsl overrides:
+ * OMEGA 1.25, CHI_EPS 1.5, SOLID_EQ 1, RHO_W_LOCAL 1, SWEPT_FORCE 1, sponge
+ * axes on, no walls, no body, FP32 storage) for a q-lattice of the given
+ * size. Pure host function. */
+int lbm_config_default(lbm_config *cfg, int q, int nx, int ny, int nz);
+
+/* Creates a dense session on the current CUDA device and allocates its
+ * device state (two f buffers, the mac field, reduction scratch).
+ * Replaces the page-side pipeline/buffer set-up of main-3d.js:980-1010 and
+ * main-cylinder.js:400-430. Returns LBM_EINVAL for an invalid config. */
+int lbm_create(const lbm_config *cfg, lbm_session **out);
+void lbm_destroy(lbm_session *s);
+
+/* Message for the last failed call on `s` (or, with s == NULL, the last
+ * failed lbm_create on this thread). Never NULL. */
+const char *lbm_last_error(const lbm_session *s);
+
+/* Sets the CUDA stream (a cudaStream_t passed as void*) the session
+ * launches on; NULL restores the session's own stream. */
+int lbm_set_stream(lbm_session *s, void *cuda_stream);
+
+/* Seeds f at equilibrium from a host macroscopic field, [rho,ux,uy,uz] per
+ * cell -- common_d3_step.wgsl:206-222 initEq (and main-tgv.js:136 initF in
+ * 2D). Also sets the session's mac field. Synchronous. */
+int lbm_init_macro(lbm_session *s, const float *mac);
+
+/* Writes / reads f in the f32 plane-major wire format (Q * ncells floats).
+ * Packed storages convert on the device. Synchronous. */
+int lbm_write_f(lbm_session *s, const float *f);
+int lbm_read_f(lbm_session *s, float *f);
+
+/* Reads the macroscopic field of the last step (4 floats per cell). */
+int lbm_read_mac(lbm_session *s, float *mac);
+
+/* Advances n fused stream-collide steps (common_d3_step.wgsl:224 `step`,
+ * lbm_step.wgsl:137 `main`), each fused with the body force/torque sum of
+ * common_d3_force.wgsl / lbm_force.wgsl over the pre-streaming f. mac is
+ * written on the last of the n steps only. Asynchronous on the session
+ * stream. */
+int lbm_step(lbm_session *s, int n);
+
+/* Replaces the body pose/kinematics used by subsequent steps. */
+int lbm_set_body(lbm_session *s, const lbm_body *body);
+
+/* Force and torque on the body from the most recent step, FP64:
+ * out = {fx, fy, fz, tx, ty, tz}. Synchronous (one 48-byte readback).
+ * Replaces the i32 fixed-point atomics of common_d3_force.wgsl:265-282. */
+int lbm_forces(lbm_session *s, double out[6]);
+
+/* Conserved totals over the current f, FP64 on the device:
+ * out = {sum(rho-1), sum(rho ux), sum(rho uy), sum(rho uz), rho_min, rho_max,
+ *        max|u|, non-finite cell count}.
+ * Replaces readConservedTotals (amr2d-gpu.mjs:698-736) and readStats
+ * (main-3d.js:3610-3643). Synchronous. */
+int lbm_totals(lbm_session *s, double out[8]);
+
+/* Blocks until the session's queued work is done. */
+int lbm_sync(lbm_session *s);
+
+/* Bytes of device memory the session holds. */
+int64_t lbm_device_bytes(const lbm_session *s);
+
+/* ---- pure host functions (the reference's JS modules) ------------------- */
+
+/* Lattice tables, lattice-2d.mjs:106-162 and lattice-3d.mjs:50-210:
+ * velocity set, f32 weights (exact bits), opposite index. Arrays hold q
+ * entries; ez is all zero for q == 9. Any pointer may be NULL. */
+int lbm_lattice_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez,
+                       float *w, int32_t *opp);
+
+/* f32 -> IEEE binary16 bits with round-to-nearest-even, subnormals and
+ * overflow to Inf, and its inverse (f-pack.mjs:44-88). */
+uint16_t lbm_f32_to_f16_bits(float v);
+float lbm_f16_bits_to_f32(uint16_t h);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_H */

@@ -1,0 +1,635 @@
+// ORACLE -- test infrastructure only. CPU restatement of the reference's
+// dense lattice-Boltzmann arithmetic, used by tests/, by
+// __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.
+// It is never linked into or called by the product library.
+//
+// Two precisions from one template:
+//   R = double  the FP64 oracle the GPU path is scored against (the
+//               reference's "JS FP64" semantics: f32 table constants, f64
+//               arithmetic);
+//   R = float   the reference's own f32 operation order, built with
+//               -ffp-contract=off so every operation rounds once, for
+//               tight short-horizon comparisons.
+//
+// Followed line by line (reference paths):
+//   lattice-2d.mjs:106-162        D2Q9 set, weights, OPP (derived here)
+//   lattice-3d.mjs:50-210         D3Q19/27 derived ordering, ulp-tweaked weights
+//   lbm_step.wgsl:137-270         2D fused step
+//   lbm_force.wgsl                2D force (separate pass on f_in, as the reference)
+//   common_geometry.wgsl:84-160   2D ellipse SDF
+//   common_d3_step.wgsl:206-400   3D initEq + fused step
+//   common_d3_force.wgsl:171-283  3D force (momentum exchange / swept / penalty)
+//   common_d3_geometry.wgsl       3D SDFs, quaternions, body velocity
+//   common_d3_sponge.wgsl, common_sponge.wgsl, common_walls.wgsl
+//   amr2d-gpu.mjs:698-736         conserved totals
+// Forces are summed in double in a fixed order (one partial per grid row,
+// rows summed in index order), independent of the thread count.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../include/lbm.h"
+
+namespace {
+
+struct Tables {
+  int q = 0;
+  int ex[27], ey[27], ez[27], opp[27];
+  float w[27];
+};
+
+float f32ulp(float x) {
+  int e = (int)std::floor(std::log2(std::fabs((double)x)));
+  return (float)std::ldexp(1.0, e - 23);
+}
+
+// Derives the velocity set and weights the way lattice-3d.mjs /
+// lattice-2d.mjs do (enumeration order, fraction -> f32 -> ulp tweak).
+Tables derive(int q) {
+  Tables t;
+  t.q = q;
+  if (q == 9) {
+    const int E[9][2] = {{0, 0}, {1, 0}, {0, 1}, {-1, 0}, {0, -1}, {1, 1}, {-1, 1}, {-1, -1}, {1, -1}};
+    const int num[3] = {4, 1, 1}, den[3] = {9, 9, 36};
+    for (int i = 0; i < 9; ++i) {
+      t.ex[i] = E[i][0]; t.ey[i] = E[i][1]; t.ez[i] = 0;
+      const int sh = E[i][0] * E[i][0] + E[i][1] * E[i][1];
+      t.w[i] = (float)((double)num[sh] / den[sh]);  // WEIGHT_ULP_TWEAK = [0,0,0]
+    }
+    for (int i = 0; i < 9; ++i)
+      for (int j = 0; j < 9; ++j)
+        if (t.ex[j] == -t.ex[i] && t.ey[j] == -t.ey[i]) t.opp[i] = j;
+    return t;
+  }
+  const int order[3] = {1, -1, 0};
+  int all[27][3], k = 0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c) { all[k][0] = order[a]; all[k][1] = order[b]; all[k][2] = order[c]; ++k; }
+  const int max_shell = q == 19 ? 2 : 3;
+  bool seen[27] = {};
+  int n = 0;
+  for (int shell = 0; shell <= max_shell; ++shell)
+    for (int j = 0; j < 27; ++j) {
+      const int *e = all[j];
+      if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] != shell || seen[j]) continue;
+      seen[j] = true;
+      t.ex[n] = e[0]; t.ey[n] = e[1]; t.ez[n] = e[2]; ++n;
+      if (shell) {
+        for (int m = 0; m < 27; ++m)
+          if (all[m][0] == -e[0] && all[m][1] == -e[1] && all[m][2] == -e[2]) seen[m] = true;
+        t.ex[n] = -e[0]; t.ey[n] = -e[1]; t.ez[n] = -e[2]; ++n;
+      }
+    }
+  const int num19[3] = {1, 1, 1}, den19[3] = {3, 18, 36}, tw19[3] = {1, -4, 2};
+  const int num27[4] = {8, 2, 1, 1}, den27[4] = {27, 27, 54, 216}, tw27[4] = {-1, 1, -1, 0};
+  for (int i = 0; i < q; ++i) {
+    const int sh = t.ex[i] * t.ex[i] + t.ey[i] * t.ey[i] + t.ez[i] * t.ez[i];
+    const int nu = q == 19 ? num19[sh] : num27[sh], de = q == 19 ? den19[sh] : den27[sh];
+    const int tw = q == 19 ? tw19[sh] : tw27[sh];
+    const float base = (float)((double)nu / de);
+    t.w[i] = (float)((double)base + tw * (double)f32ulp(base));
+  }
+  for (int i = 0; i < q; ++i)
+    for (int j = 0; j < q; ++j)
+      if (t.ex[j] == -t.ex[i] && t.ey[j] == -t.ey[i] && t.ez[j] == -t.ez[i]) t.opp[i] = j;
+  return t;
+}
+
+const Tables &tables(int q) {
+  static const Tables t9 = derive(9), t19 = derive(19), t27 = derive(27);
+  return q == 9 ? t9 : (q == 19 ? t19 : t27);
+}
+
+// ---- geometry (R precision) ------------------------------------------------
+
+template <class R> struct V3 { R x, y, z; };
+template <class R> struct Q4 { R w, x, y, z; };
+
+template <class R> Q4<R> qmul(Q4<R> p, Q4<R> q) {
+  return {p.w * q.w - p.x * q.x - p.y * q.y - p.z * q.z,
+          p.w * q.x + p.x * q.w + p.y * q.z - p.z * q.y,
+          p.w * q.y - p.x * q.z + p.y * q.w + p.z * q.x,
+          p.w * q.z + p.x * q.y - p.y * q.x + p.z * q.w};
+}
+template <class R> V3<R> qrotinv(Q4<R> q, V3<R> v) {
+  Q4<R> c{q.w, -q.x, -q.y, -q.z};
+  Q4<R> r = qmul(qmul(c, Q4<R>{R(0), v.x, v.y, v.z}), q);
+  return {r.x, r.y, r.z};
+}
+template <class R> R len3(V3<R> v) { return std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); }
+
+template <class R> R spheroid(V3<R> p, R a, R c) {
+  R r0 = std::sqrt(p.x * p.x + p.y * p.y);
+  if (std::fabs(a - c) <= R(1e-6) * std::fmax(a, c)) return std::sqrt(r0 * r0 + p.z * p.z) - a;
+  R x = std::fabs(r0), y = std::fabs(p.z);
+  R rr = std::sqrt((x * x) / (a * a) + (y * y) / (c * c));
+  bool inside = rr < R(1);
+  R t = std::atan2(y * a, x * c);
+  for (int i = 0; i < 3; ++i) {
+    R ct = std::cos(t), st = std::sin(t);
+    R ex = x - a * ct, ey = y - c * st;
+    R F = ex * (-a * st) + ey * (c * ct);
+    R Fp = -(a * a * st * st + c * c * ct * ct) + ex * (-a * ct) + ey * (-c * st);
+    t = t - F / (std::fabs(Fp) < R(1e-9) ? R(-1e-9) : Fp);
+    t = std::fmin(std::fmax(t, R(0)), R(1.5707963));
+  }
+  R dx = x - a * std::cos(t), dy = y - c * std::sin(t);
+  R d = std::sqrt(dx * dx + dy * dy);
+  return inside ? -d : d;
+}
+
+template <class R> R sdf_local(V3<R> lp, const lbm_body &b) {
+  if (b.shape == LBM_SHAPE_SPHERE) return len3(lp) - R(b.a);
+  if (b.shape == LBM_SHAPE_SPHEROID) return spheroid<R>(lp, R(b.a), R(b.c));
+  V3<R> q{std::fabs(lp.x) - (R(b.a) - R(b.r)), std::fabs(lp.y) - (R(b.b) - R(b.r)),
+          std::fabs(lp.z) - (R(b.c) - R(b.r))};
+  V3<R> m{std::fmax(q.x, R(0)), std::fmax(q.y, R(0)), std::fmax(q.z, R(0))};
+  return len3(m) + std::fmin(std::fmax(q.x, std::fmax(q.y, q.z)), R(0)) - R(b.r);
+}
+
+template <class R> Q4<R> bquat(const lbm_body &b) { return {R(b.qw), R(b.qx), R(b.qy), R(b.qz)}; }
+
+template <class R> R phi3(V3<R> p, const lbm_body &b) {
+  V3<R> d{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
+  return sdf_local<R>(qrotinv(bquat<R>(b), d), b);
+}
+
+template <class R> R phi3_ahead(V3<R> p, const lbm_body &b, R dt) {
+  V3<R> w{R(b.wx), R(b.wy), R(b.wz)};
+  R m = len3(w);
+  Q4<R> e{R(1), R(0), R(0), R(0)};
+  if (!(m <= R(1e-12))) {
+    R half = R(0.5) * m * dt;
+    R s = std::sin(half);
+    e = {std::cos(half), s * w.x / m, s * w.y / m, s * w.z / m};
+  }
+  V3<R> c{R(b.cx) + R(b.vx) * dt, R(b.cy) + R(b.vy) * dt, R(b.cz) + R(b.vz) * dt};
+  Q4<R> q = qmul(e, bquat<R>(b));
+  return sdf_local<R>(qrotinv(q, V3<R>{p.x - c.x, p.y - c.y, p.z - c.z}), b);
+}
+
+template <class R> V3<R> body_vel3(V3<R> p, const lbm_body &b) {
+  V3<R> r{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
+  return {R(b.vx) + (R(b.wy) * r.z - R(b.wz) * r.y), R(b.vy) + (R(b.wz) * r.x - R(b.wx) * r.z),
+          R(b.vz) + (R(b.wx) * r.y - R(b.wy) * r.x)};
+}
+
+template <class R> R chi_of(R phi, R eps) {
+  R a = phi / eps;
+  a = std::fmin(std::fmax(a, R(-20)), R(20));
+  return R(0.5) * (R(1) - std::tanh(a));
+}
+
+template <class R> R wrapd(R d, R n) { return d - n * std::nearbyint(d / n); }
+
+template <class R> R phi2(R px, R py, const lbm_body &b, R W, R H) {
+  R ca = std::cos(R(b.theta)), sa = std::sin(R(b.theta));
+  R dx = wrapd(px - R(b.cx), W), dy = wrapd(py - R(b.cy), H);
+  R lx = dx * ca + dy * sa, ly = -dx * sa + dy * ca;
+  R a = R(b.a), bb = R(b.b);
+  if (std::fabs(a - bb) <= R(1e-6) * std::fmax(a, bb)) return std::sqrt(lx * lx + ly * ly) - a;
+  R x = std::fabs(lx), y = std::fabs(ly);
+  R r = std::sqrt((x * x) / (a * a) + (y * y) / (bb * bb));
+  R alg = (r - R(1)) * bb;
+  if (alg > R(64)) return alg;
+  bool inside = r < R(1);
+  R t = std::atan2(y * a, x * bb);
+  for (int i = 0; i < 3; ++i) {
+    R ct = std::cos(t), st = std::sin(t);
+    R ex = x - a * ct, ey = y - bb * st;
+    R F = ex * (-a * st) + ey * (bb * ct);
+    R Fp = -(a * a * st * st + bb * bb * ct * ct) + ex * (-a * ct) + ey * (-bb * st);
+    t = t - F / (std::fabs(Fp) < R(1e-9) ? R(-1e-9) : Fp);
+    t = std::fmin(std::fmax(t, R(0)), R(1.5707963));
+  }
+  R ddx = x - a * std::cos(t), ddy = y - bb * std::sin(t);
+  R d = std::sqrt(ddx * ddx + ddy * ddy);
+  return inside ? -d : d;
+}
+
+template <class R> R sponge(R d, R sw) {
+  if (sw <= R(0)) return R(0);
+  R w = std::fmin(std::fmax(R(1) - d / sw, R(0)), R(1));
+  return w * w * (R(3) - R(2) * w);
+}
+
+// ---- 3D --------------------------------------------------------------------
+
+template <class R>
+void force3(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
+  const Tables &T = tables(c.q);
+  const int NX = c.nx, NY = c.ny, NZ = c.nz, Q = c.q;
+  const int64_t N = (int64_t)NX * NY * NZ;
+  const lbm_body &b = c.body;
+  const R CS2 = R(1) / R(3);
+  std::vector<double> rows((size_t)NY * NZ * 7, 0.0);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int z = 0; z < NZ; ++z)
+    for (int y = 0; y < NY; ++y) {
+      double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int x = 0; x < NX; ++x) {
+        const int64_t cell = ((int64_t)z * NY + y) * NX + x;
+        V3<R> p{R(x), R(y), R(z)};
+        R phi = phi3(p, b);
+        V3<R> r{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
+        V3<R> us = body_vel3(p, b);
+        V3<R> fb{0, 0, 0}, tb{0, 0, 0};
+        if (c.use_bounceback) {
+          if (phi >= R(0)) {
+            R rhoW = R(1);
+            if (c.rho_w_local && phi < R(2)) {
+              R s = 0;
+              for (int i = 0; i < Q; ++i) s += fin[i * N + cell];
+              rhoW = s;
+            }
+            for (int i = 0; i < Q; ++i) {
+              V3<R> sp{p.x - R(T.ex[i]), p.y - R(T.ey[i]), p.z - R(T.ez[i])};
+              if (phi3(sp, b) < R(0)) {
+                R fo = fin[T.opp[i] * N + cell];
+                R corr = R(2) * R(T.w[i]) * rhoW *
+                         (R(T.ex[i]) * us.x + R(T.ey[i]) * us.y + R(T.ez[i]) * us.z) / CS2;
+                R m = R(2) * fo + corr;
+                fb.x += -R(T.ex[i]) * m;
+                fb.y += -R(T.ey[i]) * m;
+                fb.z += -R(T.ez[i]) * m;
+              }
+            }
+          }
+          if (c.swept_force) {
+            bool now = phi < R(0);
+            if (now != (phi3_ahead(p, b, R(1)) < R(0))) {
+              V3<R> mc{0, 0, 0};
+              for (int i = 0; i < Q; ++i) {
+                R v = fin[i * N + cell];
+                mc.x += v * R(T.ex[i]); mc.y += v * R(T.ey[i]); mc.z += v * R(T.ez[i]);
+              }
+              if (!now) { fb.x += mc.x; fb.y += mc.y; fb.z += mc.z; }
+              else { fb.x += -mc.x; fb.y += -mc.y; fb.z += -mc.z; }
+            }
+          }
+          tb = {r.y * fb.z - r.z * fb.y, r.z * fb.x - r.x * fb.z, r.x * fb.y - r.y * fb.x};
+        } else {
+          R chi = chi_of(phi, R(c.chi_eps));
+          if (chi >= R(1e-6)) {
+            R rho = 0, mx = 0, my = 0, mz = 0;
+            for (int i = 0; i < Q; ++i) {
+              int sx = (x - T.ex[i] + NX) % NX, sy = (y - T.ey[i] + NY) % NY, sz = (z - T.ez[i] + NZ) % NZ;
+              R v = fin[i * N + ((int64_t)sz * NY + sy) * NX + sx];
+              rho += v; mx += v * R(T.ex[i]); my += v * R(T.ey[i]); mz += v * R(T.ez[i]);
+            }
+            R den = std::fmax(rho, R(1e-6));
+            V3<R> ust{mx / den, my / den, mz / den};
+            R rc = rho * chi;
+            fb = {-(rc * (us.x - ust.x)), -(rc * (us.y - ust.y)), -(rc * (us.z - ust.z))};
+            tb = {r.y * fb.z - r.z * fb.y, r.z * fb.x - r.x * fb.z, r.x * fb.y - r.y * fb.x};
+          }
+        }
+        R v6[6] = {fb.x, fb.y, fb.z, tb.x, tb.y, tb.z};
+        for (int k = 0; k < 6; ++k) {
+          if (std::isfinite((double)v6[k])) acc[k] += (double)v6[k];
+          else acc[6] += 1.0;
+        }
+      }
+      for (int k = 0; k < 7; ++k) rows[((size_t)z * NY + y) * 7 + k] = acc[k];
+    }
+  for (int k = 0; k < 8; ++k) out[k] = 0.0;
+  for (size_t j = 0; j < (size_t)NY * NZ; ++j)
+    for (int k = 0; k < 7; ++k) out[k] += rows[j * 7 + k];
+}
+
+template <class R>
+void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout, double *mac) {
+  const Tables &T = tables(c.q);
+  const int NX = c.nx, NY = c.ny, NZ = c.nz, Q = c.q;
+  const int64_t N = (int64_t)NX * NY * NZ;
+  const lbm_body &b = c.body;
+  const R CS2 = R(1) / R(3);
+  const R OMEGA = R(1) / R(c.tau);
+  const R FX = R(c.force[0]), FY = R(c.force[1]), FZ = R(c.force[2]);
+  const R SUX = R(c.sponge_u[0]), SUY = R(c.sponge_u[1]), SUZ = R(c.sponge_u[2]);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int z = 0; z < NZ; ++z)
+    for (int y = 0; y < NY; ++y)
+      for (int x = 0; x < NX; ++x) {
+        const int64_t cell = ((int64_t)z * NY + y) * NX + x;
+        V3<R> p{R(x), R(y), R(z)};
+        R phi = c.has_body ? phi3(p, b) : R(1e30f);
+        V3<R> us = c.has_body ? body_vel3(p, b) : V3<R>{0, 0, 0};
+        const bool bb = c.has_body && c.use_bounceback;
+        R rhoW = R(1);
+        if (bb && c.rho_w_local && phi < R(2)) {
+          R s = 0;
+          for (int i = 0; i < Q; ++i) s += fin[i * N + cell];
+          rhoW = s;
+        }
+        R f[27];
+        for (int i = 0; i < Q; ++i) {
+          int sxi = x - T.ex[i], syi = y - T.ey[i], szi = z - T.ez[i];
+          if (bb && phi3(V3<R>{R(sxi), R(syi), R(szi)}, b) < R(0)) {
+            R corr = R(2) * R(T.w[i]) * rhoW *
+                     (R(T.ex[i]) * us.x + R(T.ey[i]) * us.y + R(T.ez[i]) * us.z) / CS2;
+            f[i] = fin[T.opp[i] * N + cell] + corr;
+          } else if ((c.wall[0] && (sxi < 0 || sxi >= NX)) || (c.wall[1] && (syi < 0 || syi >= NY)) ||
+                     (c.wall[2] && (szi < 0 || szi >= NZ))) {
+            f[i] = fin[T.opp[i] * N + cell];
+          } else {
+            int sx = (sxi + NX) % NX, sy = (syi + NY) % NY, sz = (szi + NZ) % NZ;
+            f[i] = fin[i * N + ((int64_t)sz * NY + sy) * NX + sx];
+          }
+        }
+        R rho = 0, mx = 0, my = 0, mz = 0;
+        for (int i = 0; i < Q; ++i) {
+          rho += f[i];
+          mx += f[i] * R(T.ex[i]); my += f[i] * R(T.ey[i]); mz += f[i] * R(T.ez[i]);
+        }
+        R den = std::fmax(rho, R(1e-6));
+        R uxs = mx / den, uys = my / den, uzs = mz / den;
+        R chi = (c.has_body && !c.use_bounceback) ? chi_of(phi, R(c.chi_eps)) : R(0);
+        R Fx = rho * chi * (us.x - uxs) + FX;
+        R Fy = rho * chi * (us.y - uys) + FY;
+        R Fz = rho * chi * (us.z - uzs) + FZ;
+        R ux = uxs + Fx / (R(2) * den), uy = uys + Fy / (R(2) * den), uz = uzs + Fz / (R(2) * den);
+        R usq = ux * ux + uy * uy + uz * uz;
+        R sw = R(0);
+        if (c.sponge_w > 0) {
+          R dx = c.sponge_axis[0] ? std::fmin(p.x, R(NX - 1) - p.x) : R(1e30f);
+          R dy = c.sponge_axis[1] ? std::fmin(p.y, R(NY - 1) - p.y) : R(1e30f);
+          R dz = c.sponge_axis[2] ? std::fmin(p.z, R(NZ - 1) - p.z) : R(1e30f);
+          sw = sponge(std::fmin(dx, std::fmin(dy, dz)), R(c.sponge_w));
+        }
+        const bool solid = c.solid_eq && bb && phi < R(0);
+        R ussq = us.x * us.x + us.y * us.y + us.z * us.z;
+        R ufar = SUX * SUX + SUY * SUY + SUZ * SUZ;
+        for (int i = 0; i < Q; ++i) {
+          R exf = R(T.ex[i]), eyf = R(T.ey[i]), ezf = R(T.ez[i]), w = R(T.w[i]);
+          R o;
+          if (solid) {
+            R eu = exf * us.x + eyf * us.y + ezf * us.z;
+            o = w * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * ussq);
+          } else {
+            R eu = exf * ux + eyf * uy + ezf * uz;
+            R feq = w * rho * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * usq);
+            R t2 = eu * R(9);
+            R dot = ((exf - ux) * R(3) + t2 * exf) * Fx + ((eyf - uy) * R(3) + t2 * eyf) * Fy +
+                    ((ezf - uz) * R(3) + t2 * ezf) * Fz;
+            R Si = (R(1) - R(0.5) * OMEGA) * w * dot;
+            R fc = f[i] - OMEGA * (f[i] - feq) + Si;
+            R euf = exf * SUX + eyf * SUY + ezf * SUZ;
+            R ft = w * (R(1) + R(3) * euf + R(4.5) * euf * euf - R(1.5) * ufar);
+            o = fc * (R(1) - sw) + ft * sw;
+          }
+          fout[i * N + cell] = o;
+        }
+        if (mac) {
+          double *m = mac + 4 * cell;
+          if (solid) { m[0] = 1; m[1] = (double)us.x; m[2] = (double)us.y; m[3] = (double)us.z; }
+          else { m[0] = (double)rho; m[1] = (double)ux; m[2] = (double)uy; m[3] = (double)uz; }
+        }
+      }
+}
+
+// ---- 2D --------------------------------------------------------------------
+
+template <class R>
+void force2(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
+  const Tables &T = tables(9);
+  const int W = c.nx, H = c.ny;
+  const int64_t N = (int64_t)W * H;
+  const lbm_body &b = c.body;
+  const R CS2 = R(1) / R(3), fW = R(W), fH = R(H);
+  std::vector<double> rows((size_t)H * 4, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < H; ++y) {
+    double acc[4] = {0, 0, 0, 0};
+    for (int x = 0; x < W; ++x) {
+      const int64_t cell = (int64_t)y * W + x;
+      R px = R(x), py = R(y);
+      R phi = phi2(px, py, b, fW, fH);
+      R chi = chi_of(phi, R(c.chi_eps));
+      R rx = wrapd(px - R(b.cx), fW), ry = wrapd(py - R(b.cy), fH);
+      R usx = R(b.vx) - R(b.wz) * ry, usy = R(b.vy) + R(b.wz) * rx;
+      R fx = 0, fy = 0, tz = 0;
+      if (c.use_bounceback) {
+        if (phi >= R(0)) {
+          for (int i = 0; i < 9; ++i) {
+            int nx_ = (x - T.ex[i] + W) % W, ny_ = (y - T.ey[i] + H) % H;
+            if (phi2(R(nx_), R(ny_), b, fW, fH) < R(0)) {
+              R fo = fin[T.opp[i] * N + cell];
+              R corr = R(2) * R(T.w[i]) * (R(T.ex[i]) * usx + R(T.ey[i]) * usy) / CS2;
+              fx += -R(T.ex[i]) * (R(2) * fo + corr);
+              fy += -R(T.ey[i]) * (R(2) * fo + corr);
+            }
+          }
+          tz = rx * fy - ry * fx;
+        }
+      } else if (chi >= R(1e-6)) {
+        R rho = 0, uxs = 0, uys = 0;
+        for (int i = 0; i < 9; ++i) {
+          int sx = (x - T.ex[i] + W) % W, sy = (y - T.ey[i] + H) % H;
+          R v = fin[i * N + (int64_t)sy * W + sx];
+          rho += v; uxs += v * R(T.ex[i]); uys += v * R(T.ey[i]);
+        }
+        uxs /= std::fmax(rho, R(1e-6)); uys /= std::fmax(rho, R(1e-6));
+        R Fx = rho * chi * (usx - uxs), Fy = rho * chi * (usy - uys);
+        fx = -Fx; fy = -Fy;
+        tz = rx * fy - ry * fx;
+      }
+      R v3[3] = {fx, fy, tz};
+      for (int k = 0; k < 3; ++k) {
+        if (std::isfinite((double)v3[k])) acc[k] += (double)v3[k];
+        else acc[3] += 1.0;
+      }
+    }
+    for (int k = 0; k < 4; ++k) rows[(size_t)y * 4 + k] = acc[k];
+  }
+  for (int k = 0; k < 8; ++k) out[k] = 0.0;
+  for (int y = 0; y < H; ++y) {
+    out[0] += rows[y * 4 + 0];
+    out[1] += rows[y * 4 + 1];
+    out[5] += rows[y * 4 + 2];
+    out[6] += rows[y * 4 + 3];
+  }
+}
+
+template <class R>
+void step2(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout, double *mac) {
+  const Tables &T = tables(9);
+  const int W = c.nx, H = c.ny;
+  const int64_t N = (int64_t)W * H;
+  const lbm_body &b = c.body;
+  const R CS2 = R(1) / R(3), fW = R(W), fH = R(H);
+  const R omg = R(1) / R(c.tau);
+  const R SUX = R(c.sponge_u[0]), SUY = R(c.sponge_u[1]);
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const int64_t cell = (int64_t)y * W + x;
+      R px = R(x), py = R(y);
+      R rx = 0, ry = 0, usx = 0, usy = 0, phi = R(1e30f);
+      if (c.has_body) {
+        rx = wrapd(px - R(b.cx), fW); ry = wrapd(py - R(b.cy), fH);
+        usx = R(b.vx) - R(b.wz) * ry; usy = R(b.vy) + R(b.wz) * rx;
+        phi = phi2(px, py, b, fW, fH);
+      }
+      R f[9];
+      for (int i = 0; i < 9; ++i) {
+        int sx = (x + W - T.ex[i]) % W, sy = (y + H - T.ey[i]) % H;
+        int ysrc = y - T.ey[i];
+        if (c.use_bounceback && c.has_body && phi2(R(sx), R(sy), b, fW, fH) < R(0)) {
+          R corr = R(2) * R(T.w[i]) * (R(T.ex[i]) * usx + R(T.ey[i]) * usy) / CS2;
+          f[i] = fin[T.opp[i] * N + cell] + corr;
+        } else if (c.wall[1] && (ysrc < 0 || ysrc >= H)) {
+          R wu = ysrc < 0 ? R(c.wall_u[0]) : R(c.wall_u[1]);
+          R corr = R(2) * R(T.w[i]) * R(T.ex[i]) * wu / CS2;
+          f[i] = fin[T.opp[i] * N + cell] + corr;
+        } else {
+          f[i] = fin[i * N + (int64_t)sy * W + sx];
+        }
+      }
+      R rho = 0, uxs = 0, uys = 0;
+      for (int i = 0; i < 9; ++i) { rho += f[i]; uxs += f[i] * R(T.ex[i]); uys += f[i] * R(T.ey[i]); }
+      R den = std::fmax(rho, R(1e-6));
+      uxs /= den; uys /= den;
+      R chi = (c.use_bounceback || !c.has_body) ? R(0) : chi_of(phi, R(c.chi_eps));
+      R Fx = rho * chi * (usx - uxs) + R(c.force[0]);
+      R Fy = rho * chi * (usy - uys) + R(c.force[1]);
+      R ux = uxs + Fx / (R(2) * den), uy = uys + Fy / (R(2) * den);
+      R usq = ux * ux + uy * uy;
+      R dx = std::fmin(px, R(W - 1 - x)), dy = std::fmin(py, R(H - 1 - y));
+      R sw = sponge(std::fmin(dx, dy), R(c.sponge_w));
+      const bool solid = c.solid_eq && c.use_bounceback && c.has_body && phi < R(0);
+      for (int i = 0; i < 9; ++i) {
+        R exf = R(T.ex[i]), eyf = R(T.ey[i]), w = R(T.w[i]);
+        R o;
+        if (solid) {
+          R eu = exf * usx + eyf * usy;
+          o = w * R(1) * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * (usx * usx + usy * usy));
+        } else {
+          R eu = exf * ux + eyf * uy;
+          R feq = w * rho * (R(1) + R(3) * eu + R(4.5) * eu * eu - R(1.5) * usq);
+          R t2 = (exf * ux + eyf * uy) * R(9);
+          R Si = (R(1) - R(0.5) * omg) * w *
+                 (((exf - ux) * R(3) + t2 * exf) * Fx + ((eyf - uy) * R(3) + t2 * eyf) * Fy);
+          R fc = f[i] - omg * (f[i] - feq) + Si;
+          R euf = exf * SUX + eyf * SUY;
+          R ft = w * (R(1) + R(3) * euf + R(4.5) * euf * euf - R(1.5) * (SUX * SUX + SUY * SUY));
+          o = fc * (R(1) - sw) + ft * sw;
+        }
+        fout[i * N + cell] = o;
+      }
+      if (mac) {
+        double *m = mac + 4 * cell;
+        m[0] = (double)rho; m[1] = (double)ux; m[2] = (double)uy; m[3] = 0;
+      }
+    }
+}
+
+template <class R>
+void run(const lbm_config &c, double *f, int nsteps, double *mac, double *forces) {
+  const int64_t N = (int64_t)c.nx * c.ny * c.nz;
+  const int64_t tot = N * c.q;
+  std::vector<R> a(tot), b(tot);
+  for (int64_t i = 0; i < tot; ++i) a[i] = R(f[i]);
+  for (int s = 0; s < nsteps; ++s) {
+    double fo[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (c.has_body) {
+      if (c.q == 9) force2<R>(c, a, fo); else force3<R>(c, a, fo);
+    }
+    if (forces) std::memcpy(forces + 8 * s, fo, sizeof(fo));
+    double *m = (s == nsteps - 1) ? mac : nullptr;
+    if (c.q == 9) step2<R>(c, a, b, m); else step3<R>(c, a, b, m);
+    a.swap(b);
+  }
+  for (int64_t i = 0; i < tot; ++i) f[i] = (double)a[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Derived lattice tables (weights as exact f32 values).
+int oracle_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez, float *w, int32_t *opp) {
+  if (q != 9 && q != 19 && q != 27) return -1;
+  const Tables &t = tables(q);
+  for (int i = 0; i < q; ++i) {
+    ex[i] = t.ex[i]; ey[i] = t.ey[i]; ez[i] = t.ez[i]; w[i] = t.w[i]; opp[i] = t.opp[i];
+  }
+  return 0;
+}
+
+// Equilibrium seeding (initEq): f_i = feq(rho, u) per cell, in R precision.
+int oracle_init_eq(int q, int64_t n, int fp32, const double *mac, double *f) {
+  const Tables &t = tables(q);
+  for (int64_t c = 0; c < n; ++c) {
+    const double *m = mac + 4 * c;
+    for (int i = 0; i < q; ++i) {
+      if (fp32) {
+        float rho = (float)m[0], ux = (float)m[1], uy = (float)m[2], uz = q == 9 ? 0.f : (float)m[3];
+        float eu = (float)t.ex[i] * ux + (float)t.ey[i] * uy + (float)t.ez[i] * uz;
+        float usq = q == 9 ? ux * ux + uy * uy : ux * ux + uy * uy + uz * uz;
+        f[i * n + c] = t.w[i] * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
+      } else {
+        double rho = m[0], ux = m[1], uy = m[2], uz = q == 9 ? 0.0 : m[3];
+        double eu = t.ex[i] * ux + t.ey[i] * uy + t.ez[i] * uz;
+        double usq = ux * ux + uy * uy + uz * uz;
+        f[i * n + c] = (double)t.w[i] * rho * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * usq);
+      }
+    }
+  }
+  return 0;
+}
+
+// Runs `nsteps` of force pass + fused step in place on f (Q*n doubles).
+// mac (4*n) receives the last step's macroscopic field, forces (8*nsteps)
+// the per-step force/torque sums; either may be NULL.
+int oracle_run(const lbm_config *c, int fp32, double *f, int nsteps, double *mac, double *forces) {
+  if (!c || !f || nsteps < 0) return -1;
+  if (fp32) run<float>(*c, f, nsteps, mac, forces);
+  else run<double>(*c, f, nsteps, mac, forces);
+  return 0;
+}
+
+// Conserved totals in f64, readConservedTotals semantics (amr2d-gpu.mjs:698).
+int oracle_totals(int q, int64_t n, const double *f, double out[8]) {
+  const Tables &t = tables(q);
+  double mass = 0, px = 0, py = 0, pz = 0, rmin = 1e300, rmax = -1e300, u2 = 0, bad = 0;
+  for (int64_t c = 0; c < n; ++c) {
+    double rho = 0, mx = 0, my = 0, mz = 0;
+    for (int i = 0; i < q; ++i) {
+      double v = f[i * n + c];
+      rho += v; mx += v * t.ex[i]; my += v * t.ey[i]; mz += v * t.ez[i];
+    }
+    if (!std::isfinite(rho + mx + my + mz)) { bad += 1; continue; }
+    mass += rho - 1.0; px += mx; py += my; pz += mz;
+    rmin = std::fmin(rmin, rho); rmax = std::fmax(rmax, rho);
+    u2 = std::fmax(u2, (mx * mx + my * my + mz * mz) / (rho * rho));
+  }
+  out[0] = mass; out[1] = px; out[2] = py; out[3] = pz;
+  out[4] = rmin; out[5] = rmax; out[6] = std::sqrt(u2); out[7] = bad;
+  return 0;
+}
+
+// binary16 encode by exact arithmetic on the value (not bit surgery): scale
+// into the 11-bit significand grid, round half to even with nearbyint.
+uint16_t oracle_f16_bits(float v) {
+  if (std::isnan(v)) return 0x7e00;
+  const uint16_t sign = std::signbit(v) ? 0x8000 : 0;
+  double a = std::fabs((double)v);
+  if (a == 0.0) return sign;
+  if (std::isinf(a)) return sign | 0x7c00;
+  int e;
+  std::frexp(a, &e);           // a = m * 2^e, m in [0.5, 1)
+  int E = e - 1;               // a in [2^E, 2^(E+1))
+  if (E < -14) E = -14;        // subnormal grid
+  const double q = std::ldexp(1.0, E - 10);
+  double k = std::nearbyint(a / q);  // ties to even under the default mode
+  if (k >= 2048.0) { k /= 2; E += 1; }
+  if (E > 15) return sign | 0x7c00;
+  if (k < 1024.0) return (uint16_t)(sign | (uint16_t)k);  // subnormal (E == -14)
+  return (uint16_t)(sign | (uint16_t)((E + 15) << 10) | (uint16_t)((int)k - 1024));
+}
+
+}  // extern "C"
