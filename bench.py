@@ -242,6 +242,63 @@ def time_e2e(lbm, wl, steps, warmup, world):
     return ms, h2d, d2h
 
 
+def time_batched(lbm, steps, warmup, world, plain_steps=20):
+    """Batched form (512 D2Q9 domains, log-uniform 64^2..512^2, seeded) in one
+    persistent graph-captured launch per step after autotuning the tile
+    shape, against the plain form: the same domains as 512 dense sessions
+    stepped one launch each."""
+    import torch
+    from getting_air_b200 import scenarios as sc
+    doms = sc.batched_domains(count=512, seed=12345)
+    w = lbm.lattice_tables(9)["w"]
+    cfgs = [lbm.config_from(9, d["dims"], **d["kw"]) for d in doms]
+    seeds = [sc.seed_domain(d, w) for d in doms]
+    cells = sum(int(np.prod(d["dims"])) for d in doms)
+    b = lbm.Batch(cfgs)
+    for k, f0 in enumerate(seeds):
+        b.write_f(k, f0)
+    tune_ms = b.autotune(3)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    b.step(warmup)
+    b.sync()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    a.record(stream)
+    b.step(steps)
+    z.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(z), world)
+    tiling = b.tiling()
+    b.close()
+    batched = {"mlups": cells * steps * world / (ms * 1e-3) / 1e6, "ms_per_step": ms / steps,
+               "domains": len(doms), "cells": cells, "tiling": {"threads": tiling[0], "cells_per_thread": tiling[1],
+                                                              "ctas_per_sm": tiling[2]},
+               "autotune_best_ms": tune_ms, "gbs": 72 * cells / (ms / steps * 1e-3) / 1e9,
+               "launches_per_step": 1, "graph_steps": 16}
+    sols = []
+    for cfg, f0 in zip(cfgs, seeds):
+        s = lbm.Solver(cfg)
+        s.write_f(f0)
+        sols.append(s)
+    for s in sols:
+        s.step(warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(plain_steps):
+        for s in sols:
+            s.step(1)
+    torch.cuda.synchronize()
+    pms = max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+    for s in sols:
+        s.close()
+    plain = {"mlups": cells * plain_steps * world / (pms * 1e-3) / 1e6, "ms_per_step": pms / plain_steps,
+             "launches_per_step": len(doms), "timing": "host wall clock around device-synchronised loop"}
+    return batched, plain
+
+
 def cpu_baseline(seconds=10.0):
     """The oracle's f32 path (a restatement of the reference's shader math) on
     this host's cores, on a half-scale copy of the workload (same scenario,
@@ -295,6 +352,7 @@ def run_ours(args):
                          "ms_per_step": tm / args.steps,
                          "gbs": BYTES_PER_LU[("d3q19", st)] * cells / (statistics.mean(lm) * 1e-3) / 1e9,
                          "fx_last": fo[0]}
+        forms["batched"], forms["batched_plain"] = time_batched(lbm, args.steps, args.warmup, world)
     peak, peak_kind = hbm_peak()
     achieved = BYTES_PER_LU[("d3q19", "fp32")] * cells / (kern_ms * 1e-3) / 1e9
     traffic = profiled_traffic("d3q19_sphere_step")

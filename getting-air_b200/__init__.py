@@ -85,6 +85,22 @@ def _load() -> C.CDLL:
         "lbm_totals": ([P, D], I),
         "lbm_sync": ([P], I),
         "lbm_device_bytes": ([P], C.c_int64),
+        "lbm_batch_create": ([C.POINTER(Config), I, C.POINTER(P)], I),
+        "lbm_batch_destroy": ([P], None),
+        "lbm_batch_last_error": ([P], C.c_char_p),
+        "lbm_batch_set_stream": ([P, P], I),
+        "lbm_batch_domains": ([P], I),
+        "lbm_batch_cells": ([P], C.c_int64),
+        "lbm_batch_init_macro": ([P, I, F], I),
+        "lbm_batch_write_f": ([P, I, F], I),
+        "lbm_batch_read_f": ([P, I, F], I),
+        "lbm_batch_read_mac": ([P, I, F], I),
+        "lbm_batch_step": ([P, I], I),
+        "lbm_batch_set_tiling": ([P, I, I, I], I),
+        "lbm_batch_get_tiling": ([P, C.POINTER(I), C.POINTER(I), C.POINTER(I)], I),
+        "lbm_batch_autotune": ([P, I, F], I),
+        "lbm_batch_forces": ([P, D], I),
+        "lbm_batch_sync": ([P], I),
         "lbm_lattice_tables": ([I, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), F, C.POINTER(C.c_int32)], I),
         "lbm_f32_to_f16_bits": ([C.c_float], C.c_uint16),
@@ -185,19 +201,7 @@ class Solver:
 
     @classmethod
     def create(cls, q: int, dims, **kw) -> "Solver":
-        cfg = default_config(q, dims)
-        for k, v in kw.items():
-            if k == "storage" and isinstance(v, str):
-                v = STORAGE[v]
-            if k == "body" and isinstance(v, dict):
-                v = make_body(**v)
-            if isinstance(getattr(cfg, k), C.Array):
-                arr = getattr(cfg, k)
-                for j, x in enumerate(v):
-                    arr[j] = x
-            else:
-                setattr(cfg, k, v)
-        return cls(cfg)
+        return cls(config_from(q, dims, **kw))
 
     def _check(self, rc: int):
         if rc:
@@ -267,3 +271,103 @@ class Solver:
 
     def device_bytes(self) -> int:
         return int(lib.lbm_device_bytes(self._h))
+
+
+def config_from(q: int, dims, **kw) -> Config:
+    """An lbm_config for q/dims with fields overridden by keyword (the same
+    keywords Solver.create takes)."""
+    cfg = default_config(q, dims)
+    for k, v in kw.items():
+        if k == "storage" and isinstance(v, str):
+            v = STORAGE[v]
+        if k == "body" and isinstance(v, dict):
+            v = make_body(**v)
+        if isinstance(getattr(cfg, k), C.Array):
+            arr = getattr(cfg, k)
+            for j, x in enumerate(v):
+                arr[j] = x
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class Batch:
+    """Many independent domains advanced by one persistent launch per step.
+
+    ``cfgs`` is a list of :class:`Config` (same q and storage). Per-domain
+    calls take the domain index; ``forces()`` returns an (n, 6) array."""
+
+    def __init__(self, cfgs):
+        arr = (Config * len(cfgs))(*cfgs)
+        self.cfgs = list(cfgs)
+        self.q = cfgs[0].q
+        self.ncells = [c.nx * c.ny * c.nz for c in cfgs]
+        h = C.c_void_p()
+        rc = lib.lbm_batch_create(arr, len(cfgs), C.byref(h))
+        if rc:
+            raise LbmError(rc, lib.lbm_batch_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc:
+            raise LbmError(rc, lib.lbm_batch_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def cells(self) -> int:
+        return int(lib.lbm_batch_cells(self._h))
+
+    def set_stream(self, stream_ptr):
+        self._check(lib.lbm_batch_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def init_macro(self, d: int, mac):
+        mac = np.ascontiguousarray(mac, dtype=np.float32).reshape(self.ncells[d], 4)
+        self._check(lib.lbm_batch_init_macro(self._h, d, _ptr(mac, C.c_float)))
+
+    def write_f(self, d: int, f):
+        f = np.ascontiguousarray(f, dtype=np.float32).reshape(self.q, self.ncells[d])
+        self._check(lib.lbm_batch_write_f(self._h, d, _ptr(f, C.c_float)))
+
+    def read_f(self, d: int) -> np.ndarray:
+        out = np.empty((self.q, self.ncells[d]), np.float32)
+        self._check(lib.lbm_batch_read_f(self._h, d, _ptr(out, C.c_float)))
+        return out
+
+    def read_mac(self, d: int) -> np.ndarray:
+        out = np.empty((self.ncells[d], 4), np.float32)
+        self._check(lib.lbm_batch_read_mac(self._h, d, _ptr(out, C.c_float)))
+        return out
+
+    def step(self, n: int = 1):
+        self._check(lib.lbm_batch_step(self._h, int(n)))
+
+    def set_tiling(self, threads: int, cells_per_thread: int, ctas_per_sm: int):
+        self._check(lib.lbm_batch_set_tiling(self._h, threads, cells_per_thread, ctas_per_sm))
+
+    def tiling(self):
+        t, c, k = C.c_int(), C.c_int(), C.c_int()
+        self._check(lib.lbm_batch_get_tiling(self._h, C.byref(t), C.byref(c), C.byref(k)))
+        return t.value, c.value, k.value
+
+    def autotune(self, trials: int = 3) -> float:
+        ms = C.c_float()
+        self._check(lib.lbm_batch_autotune(self._h, trials, C.byref(ms)))
+        return ms.value
+
+    def forces(self) -> np.ndarray:
+        out = np.zeros((len(self.cfgs), 6), np.float64)
+        self._check(lib.lbm_batch_forces(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def sync(self):
+        self._check(lib.lbm_batch_sync(self._h))

@@ -17,7 +17,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "liblbm.so"
 NVCC_FLAGS = [
-    "-std=c++20",
+    "-std=c++17",
     "-O3",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",

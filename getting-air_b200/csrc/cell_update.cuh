@@ -1,0 +1,472 @@
+// Per-cell LBM update shared by the dense, batched and served kernels, plus
+// the storage codecs and the deterministic FP64 block reduction.
+//
+// A "domain" is a box of cells stored in an arena of Q planes with plane
+// stride p.n; its cells start at arena index p.base and run
+// (z*NY + y)*NX + x. The dense solver is one domain at base 0; the batched
+// and served forms place many domains in one arena. Whatever the launch
+// shape, every cell goes through cell3()/cell2() below, so the arithmetic of
+// all forms is the same instruction stream.
+//
+// Reference arithmetic:
+//   cell3   common_d3_step.wgsl:224-400 (step) + common_d3_force.wgsl:171-283
+//   cell2   lbm_step.wgsl:137-270 (step) + lbm_force.wgsl main
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "dense.cuh"
+#include "geometry.cuh"
+#include "lattice.cuh"
+
+namespace lbm {
+
+constexpr float kCS2 = 1.0f / 3.0f;
+
+// ---- storage codecs --------------------------------------------------------
+// The 16-bit forms hold f_i - w_i (the f-pack mode-2 offset,
+// common_fpack.wgsl:91-121), rounded to nearest even; arithmetic stays f32.
+template <typename S> struct Codec;
+#ifndef LBM_STREAMING_STORES
+#define LBM_STREAMING_STORES 0
+#endif
+template <> struct Codec<float> {
+  static __device__ __forceinline__ float ld(const float *p, float) { return __ldg(p); }
+  static __device__ __forceinline__ void st(float *p, float v, float) {
+    if (LBM_STREAMING_STORES) __stcs(p, v); else *p = v;
+  }
+};
+template <> struct Codec<__half> {
+  static __device__ __forceinline__ float ld(const __half *p, float w) {
+    return __half2float(__ldg(p)) + w;
+  }
+  static __device__ __forceinline__ void st(__half *p, float v, float w) {
+    *p = __float2half_rn(v - w);
+  }
+};
+template <> struct Codec<__nv_bfloat16> {
+  static __device__ __forceinline__ float ld(const __nv_bfloat16 *p, float w) {
+    return __bfloat162float(__ldg(p)) + w;
+  }
+  static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, float w) {
+    *p = __float2bfloat16_rn(v - w);
+  }
+};
+
+// ---- deterministic block reduction + last-block finish -------------------
+
+template <int NV, int THREADS>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sm) {
+  constexpr int NW = THREADS / 32;
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sm[k * NW + warp] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = lane < NW ? sm[k * NW + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      v[k] = t;
+    }
+  }
+}
+
+// Writes this block's partial (thread 0 holds it), and if this block is the
+// last of `nparts` to do so, sums all partials in index order into `out` and
+// re-arms the ticket counter for the next step.
+template <int NV, int THREADS>
+__device__ void finish_sum(const double (&v)[NV], double *partials, unsigned int *counter,
+                           int nparts, int part, double *out, double *sm) {
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[(int64_t)part * NV + k] = v[k];
+    __threadfence();
+    unsigned int ticket = atomicAdd(counter, 1u);
+    s_last = (ticket == (unsigned int)(nparts - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (int j = threadIdx.x; j < nparts; j += THREADS)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(int64_t)j * NV + k]);
+  block_sum<NV, THREADS>(acc, sm);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = acc[k];
+    *counter = 0u;
+  }
+}
+
+__device__ __forceinline__ float sponge_weight(float d, float sw) {
+  if (sw <= 0.0f) return 0.0f;
+  float w = fminf(fmaxf(1.0f - d / sw, 0.0f), 1.0f);
+  return w * w * (3.0f - 2.0f * w);
+}
+
+__device__ __forceinline__ double finite_or_zero(float v, double &bad) {
+  if (isfinite(v)) return (double)v;
+  bad += 1.0;
+  return 0.0;
+}
+
+// Force/torque contribution of one cell to the body (f32, as the reference
+// forms it per cell); summed in FP64 by the caller.
+struct CellForce {
+  float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+  __device__ __forceinline__ void add(const CellForce &o) {
+    fx += o.fx; fy += o.fy; fz += o.fz; tx += o.tx; ty += o.ty; tz += o.tz;
+  }
+};
+
+template <int THREADS>
+__device__ __forceinline__ void reduce_force(const CellForce &c, double *partials, unsigned int *counter,
+                                             int nparts, int part, double *out) {
+  __shared__ double sm[kForceSlots * (THREADS / 32)];
+  double bad = 0.0;
+  double v[kForceSlots];
+  v[0] = finite_or_zero(c.fx, bad);
+  v[1] = finite_or_zero(c.fy, bad);
+  v[2] = finite_or_zero(c.fz, bad);
+  v[3] = finite_or_zero(c.tx, bad);
+  v[4] = finite_or_zero(c.ty, bad);
+  v[5] = finite_or_zero(c.tz, bad);
+  v[6] = bad;
+  v[7] = 0.0;
+  block_sum<kForceSlots, THREADS>(v, sm);
+  finish_sum<kForceSlots, THREADS>(v, partials, counter, nparts, part, out, sm);
+}
+
+// ---- 3D cell update ---------------------------------------------------------
+// Pull-stream (periodic sources, then bounce-back patches: body first with
+// Ladd's correction at local rho_w, then walls), moments, Guo forcing with
+// the chi penalty, BGK collide, sponge blend, SOLID_EQ; returns this cell's
+// force/torque contribution when p.force_on.
+
+template <int Q, typename S>
+__device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
+                                      float *__restrict__ mac, const StepParams &p, int x, int y,
+                                      int z, CellForce &cf) {
+  using L = Lattice<Q>;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int64_t n = p.n;
+  const S *fi = fin + p.base;
+  S *fo_ = fout + p.base;
+  const int cell = (z * ny + y) * nx + x;
+  const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
+  const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+  const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+
+  // 1. Pull-stream from the periodic sources.
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
+    const int sx = ex == 1 ? xm : (ex == -1 ? xp : x);
+    const int sy = ey == 1 ? ym : (ey == -1 ? yp : y);
+    const int sz = ez == 1 ? zm : (ez == -1 ? zp : z);
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + ((sz * ny + sy) * nx + sx), L::w(i));
+  }
+
+  const V3 pos = {(float)x, (float)y, (float)z};
+  float phi = 1e30f;
+  V3 us = {0.f, 0.f, 0.f};
+  if (p.has_body) {
+    phi = phi3(pos, p.body);
+    us = body_velocity3(pos, p.body);
+  }
+  const bool bbody = p.has_body && p.bb;
+  const bool at_wall = (p.wall_x && (x == 0 || x == nx - 1)) || (p.wall_y && (y == 0 || y == ny - 1)) ||
+                       (p.wall_z && (z == 0 || z == nz - 1));
+  // A link reaches a solid source only from within |e| <= sqrt(3) of the
+  // surface, and a signed distance is 1-Lipschitz.
+  const bool near = bbody && phi < 2.5f;
+  float fbx = 0.f, fby = 0.f, fbz = 0.f;
+
+  // 1b. Bounce-back links.
+  if (near || at_wall) {
+    float rhoW = 1.f;
+    if (bbody && p.rho_w_local && phi < 2.f) {
+      float s = 0.f;
+#pragma unroll
+      for (int i = 0; i < Q; ++i) s += Codec<S>::ld(fi + (int64_t)i * n + cell, L::w(i));
+      rhoW = s;
+    }
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
+      const int o = L::opp(i);
+      bool solid = false;
+      if (near) solid = phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body) < 0.f;
+      if (solid) {
+        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+        const float corr =
+            2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) / kCS2;
+        f[i] = fopp + corr;
+        if (phi >= 0.f) {
+          const float m = 2.f * fopp + corr;
+          fbx += -(float)ex * m;
+          fby += -(float)ey * m;
+          fbz += -(float)ez * m;
+        }
+      } else if (at_wall) {
+        const int sx = x - ex, sy = y - ey, sz = z - ez;
+        const bool out = (p.wall_x && (sx < 0 || sx >= nx)) || (p.wall_y && (sy < 0 || sy >= ny)) ||
+                         (p.wall_z && (sz < 0 || sz >= nz));
+        if (out) f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+      }
+    }
+  }
+
+  // 2. Moments.
+  float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    rho += f[i];
+    mx += f[i] * (float)L::ex(i);
+    my += f[i] * (float)L::ey(i);
+    mz += f[i] * (float)L::ez(i);
+  }
+  const float rhoDen = fmaxf(rho, 1e-6f);
+  const float inv = 1.0f / rhoDen;
+  const float uxs = mx * inv, uys = my * inv, uzs = mz * inv;
+
+  // 3. Solid coupling and Guo forcing: u = u* + F / (2 rho).
+  const float chi = (p.has_body && !p.bb) ? chi_from_phi(phi, p.chi_eps) : 0.f;
+  const float rc = rho * chi;
+  const float Fx = rc * (us.x - uxs) + p.fx;
+  const float Fy = rc * (us.y - uys) + p.fy;
+  const float Fz = rc * (us.z - uzs) + p.fz;
+  const float hinv = 0.5f * inv;
+  const float ux = fmaf(Fx, hinv, uxs);
+  const float uy = fmaf(Fy, hinv, uys);
+  const float uz = fmaf(Fz, hinv, uzs);
+  const float usq = ux * ux + uy * uy + uz * uz;
+
+  float spw = 0.f;
+  if (p.sponge_w > 0.f) {
+    const float dx = p.sax ? fminf(pos.x, (float)(nx - 1 - x)) : 1e30f;
+    const float dy = p.say ? fminf(pos.y, (float)(ny - 1 - y)) : 1e30f;
+    const float dz = p.saz ? fminf(pos.z, (float)(nz - 1 - z)) : 1e30f;
+    spw = sponge_weight(fminf(dx, fminf(dy, dz)), p.sponge_w);
+  }
+
+  // 4. Collide + sponge blend, 5. solid interior held at feq(1, u_body).
+  // feq_i  = w_i rho (1 - 1.5 u.u + e.u (3 + 4.5 e.u))
+  // S_i    = (1 - omega/2) w_i ((e_i - u).F * 3 + 9 (e.u)(e.F))
+  //        = (1 - omega/2) w_i (e.F (3 + 9 e.u) - 3 u.F)
+  // f_out  = f + omega (feq - f) + S_i, then f_out + s (f_far - f_out).
+  const float omg = p.omega;
+  const float sfac = 1.0f - 0.5f * omg;
+  const bool in_solid = p.solid_eq && bbody && phi < 0.f;
+  if (!in_solid) {
+    const float base = 1.0f - 1.5f * usq;
+    const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
+      const float w = L::w(i);
+      const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
+      const float eF = (float)ex * Fx + (float)ey * Fy + (float)ez * Fz;
+      const float feq = (w * rho) * fmaf(eu, fmaf(4.5f, eu, 3.0f), base);
+      const float Si = (sfac * w) * fmaf(eF, fmaf(9.0f, eu, 3.0f), -uF3);
+      const float fc = fmaf(omg, feq - f[i], f[i]) + Si;
+      const float out = spw > 0.f ? fmaf(spw, p.ftarget[i] - fc, fc) : fc;
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, out, w);
+    }
+  } else {
+    const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const float w = L::w(i);
+      const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), w);
+    }
+  }
+  if (p.write_mac) {
+    float4 m = in_solid ? make_float4(1.f, us.x, us.y, us.z) : make_float4(rho, ux, uy, uz);
+    reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = m;
+  }
+
+  // Force on the body from this cell (bounce-back links were summed above).
+  if (p.force_on) {
+    if (bbody) {
+      if (p.swept && fabsf(phi) < p.swept_band) {
+        const bool solid_now = phi < 0.f;
+        const bool solid_next = phi3_ahead(pos, p.body, 1.f) < 0.f;
+        if (solid_now != solid_next) {
+          float cx = 0.f, cy = 0.f, cz = 0.f;
+#pragma unroll
+          for (int i = 0; i < Q; ++i) {
+            const float v = Codec<S>::ld(fi + (int64_t)i * n + cell, L::w(i));
+            cx += v * (float)L::ex(i);
+            cy += v * (float)L::ey(i);
+            cz += v * (float)L::ez(i);
+          }
+          if (!solid_now) { fbx += cx; fby += cy; fbz += cz; }
+          else { fbx += -cx; fby += -cy; fbz += -cz; }
+        }
+      }
+    } else if (p.has_body) {
+      const float c2 = chi_from_phi(phi, p.chi_eps);
+      if (c2 >= 1e-6f) {
+        const float rc2 = rho * c2;
+        fbx = -(rc2 * (us.x - uxs));
+        fby = -(rc2 * (us.y - uys));
+        fbz = -(rc2 * (us.z - uzs));
+      }
+    }
+    const float rx = pos.x - p.body.cx, ry = pos.y - p.body.cy, rz = pos.z - p.body.cz;
+    cf.fx = fbx; cf.fy = fby; cf.fz = fbz;
+    cf.tx = ry * fbz - rz * fby;
+    cf.ty = rz * fbx - rx * fbz;
+    cf.tz = rx * fby - ry * fbx;
+  }
+}
+
+// ---- 2D cell update (D2Q9) ---------------------------------------------------
+
+template <typename S>
+__device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__ fout,
+                                      float *__restrict__ mac, const StepParams &p, int x, int y,
+                                      CellForce &cf) {
+  using L = Lattice<9>;
+  const int W = p.nx, H = p.ny;
+  const int64_t n = p.n;
+  const S *fi = fin + p.base;
+  S *fo_ = fout + p.base;
+  const int cell = y * W + x;
+  const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
+  const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+  float f[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int ex = L::ex(i), ey = L::ey(i);
+    const int sx = ex == 1 ? xm : (ex == -1 ? xp : x);
+    const int sy = ey == 1 ? ym : (ey == -1 ? yp : y);
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (sy * W + sx), L::w(i));
+  }
+  const float fW = (float)W, fH = (float)H;
+  const float px = (float)x, py = (float)y;
+  float rx = 0.f, ry = 0.f, usx = 0.f, usy = 0.f, phi = 1e30f;
+  if (p.has_body) {
+    rx = wrap_delta(px - p.body.cx, fW);
+    ry = wrap_delta(py - p.body.cy, fH);
+    usx = p.body.vx - p.body.wz * ry;
+    usy = p.body.vy + p.body.wz * rx;
+    phi = phi2(px, py, p.body, fW, fH);
+  }
+  const bool bbody = p.has_body && p.bb;
+  const bool near = bbody && phi < 2.5f;
+  const bool at_wall = p.wall_y && (y == 0 || y == H - 1);
+  float fbx = 0.f, fby = 0.f;
+  if (near || at_wall) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const int ex = L::ex(i), ey = L::ey(i), o = L::opp(i);
+      bool solid = false;
+      if (near) {
+        const int sx = ex == 1 ? xm : (ex == -1 ? xp : x);
+        const int sy = ey == 1 ? ym : (ey == -1 ? yp : y);
+        solid = phi2((float)sx, (float)sy, p.body, fW, fH) < 0.f;
+      }
+      if (solid) {
+        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+        const float corr = 2.f * L::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+        f[i] = fopp + corr;
+        if (phi >= 0.f) {
+          const float m = 2.f * fopp + corr;
+          fbx += -(float)ex * m;
+          fby += -(float)ey * m;
+        }
+      } else if (at_wall) {
+        const int ysrc = y - ey;
+        if (ysrc < 0 || ysrc >= H) {
+          const float wu = ysrc < 0 ? p.wall_u0 : p.wall_u1;
+          const float corr = 2.f * L::w(i) * (float)ex * wu / kCS2;
+          f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o)) + corr;
+        }
+      }
+    }
+  }
+  float rho = 0.f, mxs = 0.f, mys = 0.f;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    rho += f[i];
+    mxs += f[i] * (float)L::ex(i);
+    mys += f[i] * (float)L::ey(i);
+  }
+  const float rhoDen = fmaxf(rho, 1e-6f);
+  const float inv = 1.0f / rhoDen;
+  const float uxs = mxs * inv, uys = mys * inv;
+  const float chi = (p.has_body && !p.bb) ? chi_from_phi(phi, p.chi_eps) : 0.f;
+  const float Fx = rho * chi * (usx - uxs) + p.fx;
+  const float Fy = rho * chi * (usy - uys) + p.fy;
+  const float hinv = 0.5f * inv;
+  const float ux = fmaf(Fx, hinv, uxs);
+  const float uy = fmaf(Fy, hinv, uys);
+  const float usq = ux * ux + uy * uy;
+
+  float spw = 0.f;
+  if (p.sponge_w > 0.f) {
+    const float dx = fminf(px, (float)(W - 1 - x));
+    const float dy = fminf(py, (float)(H - 1 - y));
+    spw = sponge_weight(fminf(dx, dy), p.sponge_w);
+  }
+  const float omg = p.omega;
+  const float sfac = 1.0f - 0.5f * omg;
+  const bool in_solid = p.solid_eq && bbody && phi < 0.f;
+  if (!in_solid) {
+    const float base = 1.0f - 1.5f * usq;
+    const float uF3 = 3.0f * (ux * Fx + uy * Fy);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const int ex = L::ex(i), ey = L::ey(i);
+      const float w = L::w(i);
+      const float eu = (float)ex * ux + (float)ey * uy;
+      const float eF = (float)ex * Fx + (float)ey * Fy;
+      const float feq = (w * rho) * fmaf(eu, fmaf(4.5f, eu, 3.0f), base);
+      const float Si = (sfac * w) * fmaf(eF, fmaf(9.0f, eu, 3.0f), -uF3);
+      const float fc = fmaf(omg, feq - f[i], f[i]) + Si;
+      const float out = spw > 0.f ? fmaf(spw, p.ftarget[i] - fc, fc) : fc;
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, out, w);
+    }
+  } else {
+    const float ussq = usx * usx + usy * usy;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const float w = L::w(i);
+      const float eu = (float)L::ex(i) * usx + (float)L::ey(i) * usy;
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * 1.0f * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), w);
+    }
+  }
+  if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, 0.f);
+
+  if (p.force_on) {
+    if (!bbody && p.has_body) {
+      const float c2 = chi_from_phi(phi, p.chi_eps);
+      if (c2 >= 1e-6f) {
+        fbx = -(rho * c2 * (usx - uxs));
+        fby = -(rho * c2 * (usy - uys));
+      }
+    }
+    cf.fx = fbx;
+    cf.fy = fby;
+    cf.tz = rx * fby - ry * fbx;
+  }
+}
+
+}  // namespace lbm

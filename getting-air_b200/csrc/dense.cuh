@@ -11,7 +11,8 @@ namespace lbm {
 // override constants of common_d3_step.wgsl:125-213 / lbm_step.wgsl:36-135.
 struct StepParams {
   int nx, ny, nz;
-  int64_t n;            // cells per plane
+  int64_t n;            // plane stride of the arena the domain lives in (cells)
+  int64_t base;         // arena index of the domain's cell 0
   float omega;          // 1 / tau
   float fx, fy, fz;     // uniform Guo body force
   int wall_x, wall_y, wall_z;
@@ -30,10 +31,22 @@ struct StepParams {
   double *partials;        // 8 doubles per region block
   unsigned int *counter;   // last-block ticket, returns to 0 after each step
   double *force_out;       // 8 doubles: fx fy fz tx ty tz nonfinite 0
+  // Multi-domain launches: the domain's first tile, and the tile range
+  // [ft0, ft1) (relative to tile0) whose cells can see the body.
+  int tile0, ft0, ft1;
 };
 
-// Reduction constants.
-constexpr int kStepThreads = 128;
+// Launch shape of the dense step (threads per CTA along x, and the CTAs per
+// SM the register budget is sized for). Compile-time so the tuning sweep can
+// build variants; the defaults are the measured best.
+#ifndef LBM_STEP_THREADS
+#define LBM_STEP_THREADS 128
+#endif
+#ifndef LBM_STEP_MIN_BLOCKS
+#define LBM_STEP_MIN_BLOCKS 8
+#endif
+constexpr int kStepThreads = LBM_STEP_THREADS;
+constexpr int kStepMinBlocks = LBM_STEP_MIN_BLOCKS;
 constexpr int kReduceThreads = 256;
 constexpr int kForceSlots = 8;
 constexpr int kTotalsSlots = 8;
@@ -52,5 +65,10 @@ cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, i
 int totals_blocks();
 cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, double *partials,
                           unsigned int *counter, double *out, cudaStream_t st);
+
+// One step of every domain of a batch (batch.cu).
+cudaError_t launch_batch_step(int q, int storage, int threads, int ctas, cudaStream_t st, const void *fin,
+                              void *fout, float *mac, const StepParams *doms, const int2 *tiles, int ntiles,
+                              int cells_per_tile, int write_mac);
 
 }  // namespace lbm

@@ -36,7 +36,12 @@ __device__ __forceinline__ V3 q_rot_inv(Q4 q, V3 v) {
   return {r.x, r.y, r.z};
 }
 
-__device__ __forceinline__ float len3(V3 v) { return sqrtf(v.x * v.x + v.y * v.y + v.z * v.z); }
+// Explicitly rounded (no contraction) so every call site, inlined or not,
+// produces the same bits -- which link bounces back must not depend on how
+// the compiler fused a sum of squares.
+__device__ __forceinline__ float len3(V3 v) {
+  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)), __fmul_rn(v.z, v.z)));
+}
 
 __device__ __forceinline__ float sd_round_box(V3 p, V3 h, float r) {
   V3 q = {fabsf(p.x) - (h.x - r), fabsf(p.y) - (h.y - r), fabsf(p.z) - (h.z - r)};
@@ -71,9 +76,24 @@ __device__ __forceinline__ float sdf_local3(V3 lp, const lbm_body &b) {
   return sd_round_box(lp, {b.a, b.b, b.c}, b.r);
 }
 
-__device__ __forceinline__ float phi3(V3 p, const lbm_body &b) {
+__device__ __forceinline__ float phi3_inline(V3 p, const lbm_body &b) {
   V3 d = {p.x - b.cx, p.y - b.cy, p.z - b.cz};
   return sdf_local3(q_rot_inv({b.qw, b.qx, b.qy, b.qz}, d), b);
+}
+
+// Out of line: called per bounce-back link candidate, which only the thin
+// shell of cells next to the body evaluates; inlining it at 19-27 sites
+// bloats the step kernel past the instruction cache.
+static __device__ __noinline__ float phi3_call(float x, float y, float z, const lbm_body *b) {
+  return phi3_inline({x, y, z}, *b);
+}
+
+// A sphere's distance does not depend on its orientation, so the per-cell
+// evaluation skips the rotation (bit-identical to the rotated form for the
+// identity quaternion, the only orientation a pinned sphere has).
+__device__ __forceinline__ float phi3(V3 p, const lbm_body &b) {
+  if (b.shape == LBM_SHAPE_SPHERE) return len3({p.x - b.cx, p.y - b.cy, p.z - b.cz}) - b.a;
+  return phi3_call(p.x, p.y, p.z, &b);
 }
 
 // exp map of an angular velocity over dt, common_d3_geometry.wgsl:86-91.
@@ -109,7 +129,7 @@ __device__ __forceinline__ float chi_from_phi(float phi, float eps) {
 // WGSL round() ties to even; rintf does the same in the default mode.
 __device__ __forceinline__ float wrap_delta(float d, float n) { return d - n * rintf(d / n); }
 
-__device__ __forceinline__ float phi2(float px, float py, const lbm_body &b, float W, float H) {
+__device__ __forceinline__ float phi2_inline(float px, float py, const lbm_body &b, float W, float H) {
   float ca = cosf(b.theta), sa = sinf(b.theta);
   float dx = px - b.cx, dy = py - b.cy;
   dx = wrap_delta(dx, W);
@@ -117,7 +137,8 @@ __device__ __forceinline__ float phi2(float px, float py, const lbm_body &b, flo
   float lx = dx * ca + dy * sa;
   float ly = -dx * sa + dy * ca;
   float a = b.a, bb = b.b;
-  if (fabsf(a - bb) <= 1e-6f * fmaxf(a, bb)) return sqrtf(lx * lx + ly * ly) - a;
+  if (fabsf(a - bb) <= 1e-6f * fmaxf(a, bb))
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(lx, lx), __fmul_rn(ly, ly))) - a;
   float x = fabsf(lx), y = fabsf(ly);
   float r = sqrtf((x * x) / (a * a) + (y * y) / (bb * bb));
   float algebraic = (r - 1.0f) * bb;
@@ -136,6 +157,21 @@ __device__ __forceinline__ float phi2(float px, float py, const lbm_body &b, flo
   float ddx = x - a * cosf(t), ddy = y - bb * sinf(t);
   float d = sqrtf(ddx * ddx + ddy * ddy);
   return inside ? -d : d;
+}
+
+static __device__ __noinline__ float phi2_call(float px, float py, const lbm_body *b, float W, float H) {
+  return phi2_inline(px, py, *b, W, H);
+}
+
+// An unrotated circle (every pinned cylinder) takes the closed form inline:
+// cos(0) = 1 and sin(0) = 0 make the rotation exact, so this is the same
+// value the general path returns.
+__device__ __forceinline__ float phi2(float px, float py, const lbm_body &b, float W, float H) {
+  if (b.theta == 0.0f && fabsf(b.a - b.b) <= 1e-6f * fmaxf(b.a, b.b)) {
+    const float lx = wrap_delta(px - b.cx, W), ly = wrap_delta(py - b.cy, H);
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(lx, lx), __fmul_rn(ly, ly))) - b.a;
+  }
+  return phi2_call(px, py, &b, W, H);
 }
 
 }  // namespace lbm

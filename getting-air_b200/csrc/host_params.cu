@@ -1,0 +1,105 @@
+// Host-side parameter translation shared by every form of the solver.
+#include <cmath>
+
+#include "host_params.cuh"
+#include "lattice.cuh"
+
+namespace lbm {
+
+namespace {
+template <int Q> float weight(int i) { return Lattice<Q>::w(i); }
+void dir_of(int q, int i, int &ex, int &ey, int &ez) {
+  if (q == 9) { ex = Lattice<9>::ex(i); ey = Lattice<9>::ey(i); ez = 0; }
+  else { ex = Lattice<27>::ex(i); ey = Lattice<27>::ey(i); ez = Lattice<27>::ez(i); }
+}
+float circumradius(const lbm_body &b) {
+  switch (b.shape) {
+    case LBM_SHAPE_SPHERE: return b.a;
+    case LBM_SHAPE_SPHEROID: return std::fmax(b.a, b.c);
+    case LBM_SHAPE_ELLIPSE: return std::fmax(b.a, b.b);
+    default: return std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c);
+  }
+}
+}  // namespace
+
+float lattice_weight(int q, int i) {
+  return q == 9 ? weight<9>(i) : (q == 19 ? weight<19>(i) : weight<27>(i));
+}
+
+int validate_config(const lbm_config *c, std::string &why) {
+  if (!c) { why = "config is NULL"; return LBM_EINVAL; }
+  if (c->q != 9 && c->q != 19 && c->q != 27) { why = "q must be 9, 19 or 27"; return LBM_EINVAL; }
+  if (c->nx < 3 || c->ny < 3 || c->nz < 1) { why = "grid must be at least 3 cells per axis"; return LBM_EINVAL; }
+  if (c->q == 9 && c->nz != 1) { why = "D2Q9 requires nz == 1"; return LBM_EINVAL; }
+  if (c->q != 9 && c->nz < 3) { why = "3D lattices need nz >= 3"; return LBM_EINVAL; }
+  if (c->ny > 65535 || c->nz > 65535) { why = "ny and nz are limited to 65535"; return LBM_EINVAL; }
+  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
+  if (n > 0x7fffffffLL) { why = "grid exceeds 2^31-1 cells"; return LBM_EINVAL; }
+  if (!(c->tau > 0.5f) || !std::isfinite(c->tau)) { why = "tau must be finite and > 0.5"; return LBM_EINVAL; }
+  if (c->storage < 0 || c->storage > 2) { why = "unknown storage"; return LBM_EINVAL; }
+  if (c->has_body) {
+    const int sh = c->body.shape;
+    if (c->q == 9 && sh != LBM_SHAPE_ELLIPSE) { why = "D2Q9 bodies are ellipses"; return LBM_EINVAL; }
+    if (c->q != 9 && (sh < 0 || sh > 2)) { why = "3D body shape must be sphere, spheroid or roundbox"; return LBM_EINVAL; }
+    if (!(c->body.a > 0.f)) { why = "body size must be positive"; return LBM_EINVAL; }
+    if (!c->use_bounceback && !(c->chi_eps > 0.f)) { why = "chi_eps must be positive"; return LBM_EINVAL; }
+  }
+  return LBM_OK;
+}
+
+void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &p) {
+  p.nx = c.nx; p.ny = c.ny; p.nz = c.nz; p.n = n; p.base = base;
+  p.omega = 1.0f / c.tau;
+  p.fx = c.force[0]; p.fy = c.force[1]; p.fz = c.q == 9 ? 0.f : c.force[2];
+  p.wall_x = c.q == 9 ? 0 : c.wall[0];
+  p.wall_y = c.wall[1];
+  p.wall_z = c.q == 9 ? 0 : c.wall[2];
+  p.wall_u0 = c.wall_u[0]; p.wall_u1 = c.wall_u[1];
+  p.has_body = c.has_body; p.bb = c.use_bounceback; p.solid_eq = c.solid_eq;
+  p.rho_w_local = c.rho_w_local;
+  p.chi_eps = c.chi_eps;
+  p.sponge_w = c.sponge_w;
+  p.sax = c.sponge_axis[0]; p.say = c.sponge_axis[1]; p.saz = c.sponge_axis[2];
+  const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.q == 9 ? 0.f : c.sponge_u[2];
+  const float ufar = c.q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);
+  for (int i = 0; i < 27; ++i) p.ftarget[i] = 0.f;
+  for (int i = 0; i < c.q; ++i) {
+    int ex, ey, ez;
+    dir_of(c.q, i, ex, ey, ez);
+    const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
+    p.ftarget[i] = lattice_weight(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * ufar);
+  }
+  p.body = c.body;
+  p.write_mac = 0;
+  p.force_on = 0;
+  p.swept = 0;
+  p.swept_band = 0.f;
+}
+
+bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]) {
+  if (!c.has_body) return false;
+  const lbm_body &b = c.body;
+  const float rc = circumradius(b);
+  const float speed = std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
+                      std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc;
+  p.swept = (c.q != 9 && c.use_bounceback && c.swept_force && speed > 0.f) ? 1 : 0;
+  p.swept_band = 2.0f + speed;
+  // |e| <= sqrt(3) for a bounce-back link, the one-step sweep for the
+  // swept-cell term, and chi < 1e-6 beyond ~6.9 band widths for the penalty.
+  const float margin = c.use_bounceback ? (3.0f + speed) : (8.0f * c.chi_eps + 2.0f);
+  const float reach = rc + margin;
+  auto range = [&](float centre, int len, bool periodic_image, int &lo, int &hi) {
+    int a = (int)std::floor(centre - reach), e = (int)std::ceil(centre + reach);
+    if (periodic_image && (a < 0 || e > len - 1)) { lo = 0; hi = len - 1; return; }
+    lo = a < 0 ? 0 : a;
+    hi = e > len - 1 ? len - 1 : e;
+  };
+  const bool wrap2d = (c.q == 9);  // the 2D SDF takes the nearest periodic image
+  range(b.cx, c.nx, wrap2d, box[0], box[1]);
+  range(b.cy, c.ny, wrap2d, box[2], box[3]);
+  box[4] = box[5] = 0;
+  if (c.q != 9) range(b.cz, c.nz, false, box[4], box[5]);
+  return box[0] <= box[1] && box[2] <= box[3] && box[4] <= box[5];
+}
+
+}  // namespace lbm

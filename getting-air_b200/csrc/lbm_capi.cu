@@ -14,6 +14,7 @@
 
 #include "../../include/lbm.h"
 #include "dense.cuh"
+#include "host_params.cuh"
 #include "lattice.cuh"
 
 using namespace lbm;
@@ -69,83 +70,19 @@ template <int Q> void tables(int32_t *ex, int32_t *ey, int32_t *ez, float *w, in
   }
 }
 
-template <int Q> float weight(int i) { return Lattice<Q>::w(i); }
-float weight_of(int q, int i) {
-  return q == 9 ? weight<9>(i) : (q == 19 ? weight<19>(i) : weight<27>(i));
-}
-void dir_of(int q, int i, int &ex, int &ey, int &ez) {
-  if (q == 9) { ex = Lattice<9>::ex(i); ey = Lattice<9>::ey(i); ez = 0; }
-  else { ex = Lattice<27>::ex(i); ey = Lattice<27>::ey(i); ez = Lattice<27>::ez(i); }
-}
-
-float circumradius(const lbm_body &b) {
-  switch (b.shape) {
-    case LBM_SHAPE_SPHERE: return b.a;
-    case LBM_SHAPE_SPHEROID: return std::fmax(b.a, b.c);
-    case LBM_SHAPE_ELLIPSE: return std::fmax(b.a, b.b);
-    default: return std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c);
-  }
-}
-
-int validate(const lbm_config *c, std::string &why) {
-  if (!c) { why = "config is NULL"; return LBM_EINVAL; }
-  if (c->q != 9 && c->q != 19 && c->q != 27) { why = "q must be 9, 19 or 27"; return LBM_EINVAL; }
-  if (c->nx < 3 || c->ny < 3 || c->nz < 1) { why = "grid must be at least 3 cells per axis"; return LBM_EINVAL; }
-  if (c->q == 9 && c->nz != 1) { why = "D2Q9 requires nz == 1"; return LBM_EINVAL; }
-  if (c->q != 9 && c->nz < 3) { why = "3D lattices need nz >= 3"; return LBM_EINVAL; }
-  if (c->ny > 65535 || c->nz > 65535) { why = "ny and nz are limited to 65535"; return LBM_EINVAL; }
-  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
-  if (n > 0x7fffffffLL) { why = "grid exceeds 2^31-1 cells"; return LBM_EINVAL; }
-  if (!(c->tau > 0.5f) || !std::isfinite(c->tau)) { why = "tau must be finite and > 0.5"; return LBM_EINVAL; }
-  if (c->storage < 0 || c->storage > 2) { why = "unknown storage"; return LBM_EINVAL; }
-  if (c->has_body) {
-    const int sh = c->body.shape;
-    if (c->q == 9 && sh != LBM_SHAPE_ELLIPSE) { why = "D2Q9 bodies are ellipses"; return LBM_EINVAL; }
-    if (c->q != 9 && (sh < 0 || sh > 2)) { why = "3D body shape must be sphere, spheroid or roundbox"; return LBM_EINVAL; }
-    if (!(c->body.a > 0.f)) { why = "body size must be positive"; return LBM_EINVAL; }
-    if (!c->use_bounceback && !(c->chi_eps > 0.f)) { why = "chi_eps must be positive"; return LBM_EINVAL; }
-  }
-  return LBM_OK;
-}
-
-// Which launch blocks can receive a force contribution: cells within the
-// body's circumradius plus the widest band any contribution comes from
-// (|e| for a bounce-back link, the one-step sweep for the swept-cell term,
-// the point where chi drops below 1e-6 for the penalty).
+// Which launch blocks can receive a force contribution: the blocks covering
+// the cell box of force_cell_box().
 void set_force_region(lbm_session *s) {
   StepParams &p = s->sp;
-  const lbm_config &c = s->cfg;
-  p.force_on = c.has_body ? 1 : 0;
-  if (!c.has_body) return;
-  const lbm_body &b = c.body;
-  const float rc = circumradius(b);
-  const float speed = std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
-                      std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc;
-  p.swept = (c.q != 9 && c.use_bounceback && c.swept_force && speed > 0.f) ? 1 : 0;
-  p.swept_band = 2.0f + speed;
-  const float margin = c.use_bounceback ? (3.0f + speed) : (8.0f * c.chi_eps + 2.0f);
-  const float reach = rc + margin;
-  auto range = [&](float centre, int len, bool periodic_image, int &lo, int &hi) {
-    int a = (int)std::floor(centre - reach), e = (int)std::ceil(centre + reach);
-    if (periodic_image && (a < 0 || e > len - 1)) { lo = 0; hi = len - 1; return; }
-    lo = a < 0 ? 0 : a;
-    hi = e > len - 1 ? len - 1 : e;
-  };
-  const bool wrap2d = (c.q == 9);
-  int x0, x1, y0, y1, z0 = 0, z1 = 0;
-  range(b.cx, c.nx, wrap2d, x0, x1);
-  range(b.cy, c.ny, wrap2d, y0, y1);
-  if (c.q != 9) range(b.cz, c.nz, false, z0, z1);
-  if (x0 > x1 || y0 > y1 || z0 > z1) {
-    p.force_on = 0;
-    return;
-  }
-  p.rbx0 = x0 / kStepThreads;
-  p.rbx1 = x1 / kStepThreads + 1;
-  p.rby0 = y0;
-  p.rby1 = y1 + 1;
-  p.rbz0 = z0;
-  p.rbz1 = z1 + 1;
+  int box[6];
+  p.force_on = force_cell_box(s->cfg, p, box) ? 1 : 0;
+  if (!p.force_on) return;
+  p.rbx0 = box[0] / kStepThreads;
+  p.rbx1 = box[1] / kStepThreads + 1;
+  p.rby0 = box[2];
+  p.rby1 = box[3] + 1;
+  p.rbz0 = box[4];
+  p.rbz1 = box[5] + 1;
 }
 
 int ensure_force_scratch(lbm_session *s) {
@@ -165,31 +102,8 @@ int ensure_force_scratch(lbm_session *s) {
 }
 
 void fill_params(lbm_session *s) {
-  const lbm_config &c = s->cfg;
   StepParams &p = s->sp;
-  p.nx = c.nx; p.ny = c.ny; p.nz = c.nz; p.n = s->n;
-  p.omega = 1.0f / c.tau;
-  p.fx = c.force[0]; p.fy = c.force[1]; p.fz = c.q == 9 ? 0.f : c.force[2];
-  p.wall_x = c.q == 9 ? 0 : c.wall[0];
-  p.wall_y = c.wall[1];
-  p.wall_z = c.q == 9 ? 0 : c.wall[2];
-  p.wall_u0 = c.wall_u[0]; p.wall_u1 = c.wall_u[1];
-  p.has_body = c.has_body; p.bb = c.use_bounceback; p.solid_eq = c.solid_eq;
-  p.rho_w_local = c.rho_w_local;
-  p.chi_eps = c.chi_eps;
-  p.sponge_w = c.sponge_w;
-  p.sax = c.sponge_axis[0]; p.say = c.sponge_axis[1]; p.saz = c.sponge_axis[2];
-  const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.q == 9 ? 0.f : c.sponge_u[2];
-  const float ufar = c.q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);
-  for (int i = 0; i < 27; ++i) p.ftarget[i] = 0.f;
-  for (int i = 0; i < c.q; ++i) {
-    int ex, ey, ez;
-    dir_of(c.q, i, ex, ey, ez);
-    const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
-    p.ftarget[i] = weight_of(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * ufar);
-  }
-  p.body = c.body;
-  p.write_mac = 0;
+  fill_step_params(s->cfg, s->n, 0, p);
   p.partials = s->force_partials;
   p.counter = s->force_counter;
   p.force_out = s->force_out;
@@ -241,7 +155,7 @@ int lbm_create(const lbm_config *cfg, lbm_session **out) {
   if (!out) return fail(nullptr, LBM_EINVAL, "out is NULL");
   *out = nullptr;
   std::string why;
-  int rc = validate(cfg, why);
+  int rc = validate_config(cfg, why);
   if (rc) return fail(nullptr, rc, why);
   lbm_session *s = new lbm_session();
   s->cfg = *cfg;
@@ -369,7 +283,7 @@ int lbm_set_body(lbm_session *s, const lbm_body *body) {
   lbm_config c = s->cfg;
   c.body = *body;
   std::string why;
-  if (validate(&c, why)) return fail(s, LBM_EINVAL, why);
+  if (validate_config(&c, why)) return fail(s, LBM_EINVAL, why);
   s->cfg = c;
   fill_params(s);
   int rc = ensure_force_scratch(s);

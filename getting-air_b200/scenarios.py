@@ -105,3 +105,38 @@ def cylinder2d(W: int = 256, H: int = 128, r: float = 10.0, u0: float = 0.05, ta
     kw = dict(tau=float(tau), has_body=1, use_bounceback=int(bounceback), body=body,
               sponge_w=float(sponge_w), sponge_u=(u0, 0.0, 0.0))
     return {"q": 9, "dims": (W, H, 1), "kw": kw, "mac": uniform_macro(W * H, (u0, 0, 0))}
+
+
+def batched_domains(count: int = 512, seed: int = 12345, nmin: int = 64, nmax: int = 512,
+                    tau_range=(0.55, 0.9), u0: float = 0.04):
+    """The batched D2Q9 workload: `count` square domains with N = round(nmin *
+    (nmax/nmin)^U), U uniform on [0, 1) from mulberry32(seed), tau uniform in
+    tau_range, alternating a periodic Taylor-Green vortex (amplitude u0) and
+    a plane Poiseuille channel (walls on y, body force for a peak of u0).
+    Returns a list of dicts: q, dims, kw (Solver keywords), kind, and a seed
+    ('f' for TGV, 'mac' for the channel)."""
+    rng = mulberry32(seed)
+    out = []
+    ratio = nmax / nmin
+    for k in range(count):
+        n = int(round(nmin * ratio ** rng()))
+        tau = tau_range[0] + (tau_range[1] - tau_range[0]) * rng()
+        tau = float(np.float32(tau))
+        if k % 2 == 0:
+            out.append({"q": 9, "dims": (n, n, 1), "kind": "tgv", "u0": u0,
+                        "kw": dict(tau=tau, sponge_w=0.0)})
+        else:
+            nu = nu_from_tau(tau)
+            g = 8.0 * nu * u0 / (n * n)      # plane Poiseuille: u_max = g H^2 / (8 nu)
+            out.append({"q": 9, "dims": (n, n, 1), "kind": "channel", "u0": u0,
+                        "kw": dict(tau=tau, sponge_w=0.0, wall=(0, 1, 0), force=(g, 0.0, 0.0))})
+    return out
+
+
+def seed_domain(dom, w) -> np.ndarray:
+    """Initial f (9 x N^2, f32) for a batched_domains entry."""
+    n = dom["dims"][0]
+    if dom["kind"] == "tgv":
+        return tgv2d_f(n, dom["u0"], dom["kw"]["tau"], w)
+    # channel: fluid at rest, rho = 1 (f_i = w_i), driven by the body force
+    return np.repeat(np.asarray(w, np.float32)[:, None], n * n, axis=1)

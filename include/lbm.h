@@ -176,6 +176,39 @@ int lbm_sync(lbm_session *s);
 /* Bytes of device memory the session holds. */
 int64_t lbm_device_bytes(const lbm_session *s);
 
+/* ---- batched form ----------------------------------------------------------
+ * Many independent domains of uneven sizes (same q and storage) in one
+ * arena, advanced by one persistent launch per step replayed from a CUDA
+ * graph. Each domain is a full lbm_config and is stepped with exactly the
+ * arithmetic of a dense session. The reference has no batched form (one page
+ * per domain, main-3d.js encodeSteps); these calls are its N-page loop. */
+typedef struct lbm_batch lbm_batch;
+
+int lbm_batch_create(const lbm_config *domains, int ndomains, lbm_batch **out);
+void lbm_batch_destroy(lbm_batch *b);
+/* Last error of `b`, or with b == NULL of the last failed create. */
+const char *lbm_batch_last_error(const lbm_batch *b);
+int lbm_batch_set_stream(lbm_batch *b, void *cuda_stream);
+int lbm_batch_domains(const lbm_batch *b);
+int64_t lbm_batch_cells(const lbm_batch *b);
+/* Per-domain state transfer, same formats as the dense calls. */
+int lbm_batch_init_macro(lbm_batch *b, int domain, const float *mac);
+int lbm_batch_write_f(lbm_batch *b, int domain, const float *f);
+int lbm_batch_read_f(lbm_batch *b, int domain, float *f);
+int lbm_batch_read_mac(lbm_batch *b, int domain, float *mac);
+/* n steps of every domain; mac is written on the last one. */
+int lbm_batch_step(lbm_batch *b, int n);
+/* Tile shape of the persistent launch: threads per CTA (128 or 256), cells
+ * per thread per tile, resident CTAs per SM. */
+int lbm_batch_set_tiling(lbm_batch *b, int threads, int cells_per_thread, int ctas_per_sm);
+int lbm_batch_get_tiling(const lbm_batch *b, int *threads, int *cells_per_thread, int *ctas_per_sm);
+/* Times every candidate tiling on this batch (stepping into the spare
+ * buffer, so the state is unchanged) and keeps the fastest. */
+int lbm_batch_autotune(lbm_batch *b, int trials, float *best_ms);
+/* Force/torque of every domain from the last step: 6 doubles per domain. */
+int lbm_batch_forces(lbm_batch *b, double *out);
+int lbm_batch_sync(lbm_batch *b);
+
 /* ---- pure host functions (the reference's JS modules) ------------------- */
 
 /* Lattice tables, lattice-2d.mjs:106-162 and lattice-3d.mjs:50-210:

@@ -74,3 +74,10 @@ def test_default_config_matches_reference_overrides(lbm):
     assert c.chi_eps == 1.5 and c.solid_eq == 1 and c.rho_w_local == 1 and c.swept_force == 1
     assert c.sponge_w == 0.0
     assert lbm.default_config(9, (8, 8, 1)).sponge_w == 4.0   # lbm_step.wgsl SPONGE_W
+
+
+def test_batch_rejects_mixed_lattices_before_device_work(lbm):
+    with pytest.raises(lbm.LbmError, match="share q"):
+        lbm.Batch([lbm.config_from(19, (8, 8, 8)), lbm.config_from(27, (8, 8, 8))])
+    with pytest.raises(lbm.LbmError, match="domain 1"):
+        lbm.Batch([lbm.config_from(19, (8, 8, 8)), lbm.config_from(19, (8, 8, 8), tau=0.4)])

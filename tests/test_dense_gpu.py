@@ -111,13 +111,20 @@ def test_rotated_bodies(lbm, oracle, shape):
 
 
 def test_duct_walls(lbm, oracle):
+    # Seeded with a uniform stream so the walls shear a flow of O(0.02):
+    # started from rest, |u| after 30 steps is O(1e-4) and a relative norm
+    # would measure f32 rounding of f (~1e-8) against a vanishing velocity.
+    from getting_air_b200 import scenarios as sc
     dims = (16, 20, 18)
     kw = dict(tau=0.8, wall=(0, 1, 1), force=(1e-5, 0, 0))
-    mac = np.zeros((np.prod(dims), 4))
-    mac[:, 0] = 1
+    mac = sc.uniform_macro(int(np.prod(dims)), (0.02, 0.0, 0.0))
     g, o = both(lbm, oracle, 19, dims, kw, 30, mac=mac)
     check(g, o, forces=False)
-    assert g[1][:, 1].max() > 1e-5
+    g32, o32 = both(lbm, oracle, 19, dims, kw, 30, mac=mac, fp32_oracle=True)
+    check(g32, o32, forces=False)
+    # the walls slow the flow next to them
+    u = g[1][:, 1].reshape(dims[2], dims[1], dims[0])
+    assert u[:, 0, :].mean() < u[:, dims[1] // 2, :].mean()
 
 
 @pytest.mark.parametrize("bb", [1, 0], ids=["bounceback", "penalty"])
@@ -133,8 +140,8 @@ def test_d2q9_ellipse_and_couette(lbm, oracle):
     kw = dict(tau=0.7, has_body=1, use_bounceback=1, body=body, wall=(0, 1, 0), wall_u=(0.0, 0.04),
               sponge_w=0.0)
     dims = (64, 40, 1)
-    mac = np.zeros((64 * 40, 4))
-    mac[:, 0] = 1
+    from getting_air_b200 import scenarios as sc
+    mac = sc.uniform_macro(64 * 40, (0.02, 0.0, 0.0))
     g, o = both(lbm, oracle, 9, dims, kw, 30, mac=mac)
     check(g, o)
 
@@ -225,7 +232,8 @@ def test_init_macro_matches_oracle_init(lbm, oracle):
     s.init_macro(mac)
     f = s.read_f().astype(np.float64)
     o = oracle.init_eq(27, mac.astype(np.float64), fp32=True)
-    assert np.abs(f - o).max() <= 2e-8
+    # the device contracts multiply-adds, the f32 oracle rounds each: 1 ulp
+    assert np.abs(f - o).max() <= 2 ** -24 * np.abs(o).max() * 2
     s.close()
 
 
