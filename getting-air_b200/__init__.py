@@ -49,6 +49,15 @@ class Body(C.Structure):
                 ("a", C.c_float), ("b", C.c_float), ("c", C.c_float), ("r", C.c_float)]
 
 
+class Amr2DConfig(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("levels", C.c_int32), ("rb", C.c_int32),
+                ("tau", C.c_float), ("max_slots", C.c_int32), ("use_bounceback", C.c_int32),
+                ("solid_eq", C.c_int32), ("k_eps", C.c_float), ("sponge_w", C.c_float),
+                ("sponge_u", C.c_float * 2), ("force", C.c_float * 2), ("body", Body),
+                ("refine_every", C.c_int32), ("refine_thresh", C.c_float), ("refine_margin", C.c_float),
+                ("refine_lookahead", C.c_float), ("auto_refine", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
 class Config(C.Structure):
     _fields_ = [("q", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("tau", C.c_float), ("force", C.c_float * 3), ("wall", C.c_int32 * 3),
@@ -101,6 +110,29 @@ def _load() -> C.CDLL:
         "lbm_batch_autotune": ([P, I, F], I),
         "lbm_batch_forces": ([P, D], I),
         "lbm_batch_sync": ([P], I),
+        "lbm_amr2d_config_default": ([C.POINTER(Amr2DConfig), I, I], I),
+        "lbm_amr2d_create": ([C.POINTER(Amr2DConfig), C.POINTER(P)], I),
+        "lbm_amr2d_destroy": ([P], None),
+        "lbm_amr2d_last_error": ([P], C.c_char_p),
+        "lbm_amr2d_set_stream": ([P, P], I),
+        "lbm_amr2d_write_root": ([P, F, F], I),
+        "lbm_amr2d_read_root": ([P, F, F], I),
+        "lbm_amr2d_read_pool": ([P, F, F], I),
+        "lbm_amr2d_step": ([P, I], I),
+        "lbm_amr2d_forces": ([P, D], I),
+        "lbm_amr2d_read_topology": ([P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32), F, C.POINTER(C.c_uint32)], I),
+        "lbm_amr2d_cell_updates": ([P], C.c_int64),
+        "lbm_amr2d_sync": ([P], I),
+        "lbm_tau_at_level": ([C.c_double, I], C.c_double),
+        "lbm_dc_rescale_c2f": ([C.c_double, C.c_double], C.c_double),
+        "lbm_dc_rescale_f2c": ([C.c_double, C.c_double], C.c_double),
+        "lbm_tau_chain_singularity": ([C.c_double, I, C.c_double], I),
+        "lbm_grant_assignment": ([C.POINTER(C.c_int32), I, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32)], I),
+        "lbm_release_assignment": ([C.POINTER(C.c_int32), I, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], I),
+        "lbm_active_slot_list": ([C.POINTER(C.c_int32), I, C.POINTER(C.c_int32)], I),
+        "lbm_cascade21": ([C.POINTER(C.POINTER(C.c_uint8)), I, I, I], I),
         "lbm_lattice_tables": ([I, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), F, C.POINTER(C.c_int32)], I),
         "lbm_f32_to_f16_bits": ([C.c_float], C.c_uint16),
@@ -371,3 +403,156 @@ class Batch:
 
     def sync(self):
         self._check(lib.lbm_batch_sync(self._h))
+
+
+# ---- AMR host rules (amr2d.mjs) ------------------------------------------------
+
+def tau_at_level(tau0: float, m: int) -> float:
+    return float(lib.lbm_tau_at_level(tau0, m))
+
+
+def dc_rescale_c2f(tc: float, tf: float) -> float:
+    return float(lib.lbm_dc_rescale_c2f(tc, tf))
+
+
+def dc_rescale_f2c(tc: float, tf: float) -> float:
+    return float(lib.lbm_dc_rescale_f2c(tc, tf))
+
+
+def tau_chain_singularity(tau0: float, levels: int, band: float = 0.01):
+    m = int(lib.lbm_tau_chain_singularity(tau0, levels, band))
+    return None if m < 0 else m
+
+
+def grant_assignment(candidates, free_count: int):
+    """grantAssignment: ({granted: [(id, free_index)], refused: [ids], free_count})."""
+    c = np.ascontiguousarray(candidates, np.int32)
+    ids = np.zeros(max(len(c), 1), np.int32)
+    idx = np.zeros(max(len(c), 1), np.int32)
+    ng = C.c_int32()
+    fc = lib.lbm_grant_assignment(_ptr(c, C.c_int32), len(c), free_count, _ptr(ids, C.c_int32),
+                                  _ptr(idx, C.c_int32), C.byref(ng))
+    granted = [(int(i), int(j)) for i, j in zip(ids[:len(c)], idx[:len(c)]) if j >= 0]
+    refused = [int(i) for i, j in zip(ids[:len(c)], idx[:len(c)]) if j < 0]
+    return {"granted": granted, "refused": refused, "free_count": int(fc)}
+
+
+def release_assignment(releases, free_count: int):
+    r = np.ascontiguousarray(releases, np.int32)
+    ids = np.zeros(max(len(r), 1), np.int32)
+    idx = np.zeros(max(len(r), 1), np.int32)
+    fc = lib.lbm_release_assignment(_ptr(r, C.c_int32), len(r), free_count, _ptr(ids, C.c_int32),
+                                    _ptr(idx, C.c_int32))
+    return {"writes": [(int(i), int(j)) for i, j in zip(ids[:len(r)], idx[:len(r)])], "free_count": int(fc)}
+
+
+def active_slot_list(slot_to_block):
+    s = np.ascontiguousarray(slot_to_block, np.int32)
+    out = np.zeros(max(len(s), 1), np.int32)
+    n = lib.lbm_active_slot_list(_ptr(s, C.c_int32), len(s), _ptr(out, C.c_int32))
+    return out[:n].tolist()
+
+
+def cascade21(want_levels, levels: int, nbx1: int, nby1: int):
+    """Closes per-level block masks in place (list indexed by level; entry 0
+    unused). Returns (masks, number added)."""
+    masks = [None] + [np.ascontiguousarray(want_levels[m], np.uint8).ravel().copy() for m in range(1, levels)]
+    ptrs = (C.POINTER(C.c_uint8) * levels)()
+    for m in range(1, levels):
+        ptrs[m] = masks[m].ctypes.data_as(C.POINTER(C.c_uint8))
+    n = lib.lbm_cascade21(ptrs, levels, nbx1, nby1)
+    if n < 0:
+        raise LbmError(n, "cascade21")
+    return masks, int(n)
+
+
+def amr2d_config(nx: int, ny: int, **kw) -> Amr2DConfig:
+    cfg = Amr2DConfig()
+    lib.lbm_amr2d_config_default(C.byref(cfg), nx, ny)
+    for k, v in kw.items():
+        if k == "body" and isinstance(v, dict):
+            v = make_body(**v)
+        if isinstance(getattr(cfg, k), C.Array):
+            arr = getattr(cfg, k)
+            for j, x in enumerate(v):
+                arr[j] = x
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class Amr2D:
+    """Two-level D2Q9 block-structured AMR session (root + one pool level)."""
+
+    def __init__(self, cfg: Amr2DConfig):
+        self.cfg = cfg
+        self.W, self.H, self.rb = cfg.nx, cfg.ny, cfg.rb
+        self.fb = 2 * cfg.rb + 4
+        self.nbx, self.nby = cfg.nx // cfg.rb, cfg.ny // cfg.rb
+        self.slots = cfg.max_slots
+        h = C.c_void_p()
+        rc = lib.lbm_amr2d_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise LbmError(rc, lib.lbm_amr2d_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc:
+            raise LbmError(rc, lib.lbm_amr2d_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.lbm_amr2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, ptr):
+        self._check(lib.lbm_amr2d_set_stream(self._h, C.c_void_p(ptr or 0)))
+
+    def write_root(self, f, vel):
+        f = np.ascontiguousarray(f, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        self._check(lib.lbm_amr2d_write_root(self._h, _ptr(f, C.c_float), _ptr(vel, C.c_float)))
+
+    def read_root(self):
+        f = np.empty((9, self.W * self.H), np.float32)
+        v = np.empty((self.W * self.H, 2), np.float32)
+        self._check(lib.lbm_amr2d_read_root(self._h, _ptr(f, C.c_float), _ptr(v, C.c_float)))
+        return f, v
+
+    def read_pool(self):
+        n = self.slots * self.fb * self.fb
+        f = np.empty((9, n), np.float32)
+        v = np.empty((n, 2), np.float32)
+        self._check(lib.lbm_amr2d_read_pool(self._h, _ptr(f, C.c_float), _ptr(v, C.c_float)))
+        return f, v
+
+    def step(self, n: int = 1):
+        self._check(lib.lbm_amr2d_step(self._h, int(n)))
+
+    def forces(self):
+        out = np.zeros(4, np.float64)
+        self._check(lib.lbm_amr2d_forces(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def topology(self) -> dict:
+        nb = self.nbx * self.nby
+        bs, sb = np.zeros(nb, np.int32), np.zeros(self.slots, np.int32)
+        fl, cnt = np.zeros(self.slots // 4, np.int32), np.zeros(2, np.int32)
+        al, cr, wa = np.zeros(self.slots, np.int32), np.zeros(nb, np.float32), np.zeros(nb, np.uint32)
+        self._check(lib.lbm_amr2d_read_topology(self._h, _ptr(bs, C.c_int32), _ptr(sb, C.c_int32),
+                                                 _ptr(fl, C.c_int32), _ptr(cnt, C.c_int32), _ptr(al, C.c_int32),
+                                                 _ptr(cr, C.c_float), _ptr(wa, C.c_uint32)))
+        return {"block_slot": bs, "slot_to_block": sb, "free_list": fl, "free_count": int(cnt[0]),
+                "active": al[:cnt[1]].copy(), "criterion": cr, "want": wa}
+
+    def cell_updates(self) -> int:
+        return int(lib.lbm_amr2d_cell_updates(self._h))
+
+    def sync(self):
+        self._check(lib.lbm_amr2d_sync(self._h))

@@ -1,0 +1,834 @@
+// 2D block-structured AMR (D2Q9, root + one pool level) on the device.
+//
+// Layout in HBM:
+//   root      dense W x H, 9 planes, two buffers; mac float4 per cell (the
+//             root velocity the criterion reads).
+//   pool      S tiles of FB x FB cells (FB = 2 RB + 4: one block of RB x RB
+//             root cells refined 2:1, plus a 2-cell ring), 9 planes of S*FB^2,
+//             two buffers (a/b), slot-major `slot*FB^2 + fy*FB + fx` (the
+//             reference's pool layout, amr2d.mjs:220 makePool).
+//   topology  blockSlot[NBX*NBY], slotToBlock[S], parentSlot[S],
+//             freeList[S/4] (quads), counts {free quads, active slots},
+//             activeList[S], want/criterion[NBX*NBY], newly[S].
+//
+// One macro-step (main-cylinder-amr.js:1831 dispatchMacroStep, `interp`
+// interface of amr2d-gpu.mjs:1120 S_Advance):
+//   [every refine_every: criterion -> decide -> coarsen/refine (serial,
+//    deterministic) -> active list -> whole-tile fill of new tiles]
+//   force on the pool (FP64, deterministic)   amr_force1.wgsl
+//   ring fill from neighbour or root          common_interp_kernel.wgsl GHOST_ONLY
+//   root step (dense d2 kernel, writes mac)   amr_step1.wgsl NO_PARENT
+//   pool substep a->b, b->a at tau_f          amr_step1.wgsl stepCell
+//   restriction of the pool into the root     common_average.wgsl
+// Every pool kernel runs one CTA per slot of the active list (count read on
+// the device), so the non-refine macro-step is topology-independent and is
+// replayed from a CUDA graph.
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm.h"
+#include "cell_update.cuh"
+#include "dense.cuh"
+#include "host_params.cuh"
+
+namespace lbm {
+namespace {
+
+constexpr int kPoolThreads = 256;
+
+struct AmrParams {
+  int W, H, RB, G, FB, RB2, NBX, NBY, PNX, PNY, S;
+  int64_t N0, N1;
+  float tau_c, tau_f, omega_f, eps_f, sponge_w, sux, suy, fx, fy, margin, lookahead;
+  float resc_c2f, resc_f2c;
+  double thr;
+  int vort_on, bb, solid_eq;
+  float ftarget[9];
+  lbm_body body;
+  int *blockSlot, *slotToBlock, *parentSlot, *freeList, *counts, *activeList;
+  unsigned *want, *newly;
+  float *crit;
+  double *partials;
+  unsigned *counter;
+  double *force_out;
+};
+
+using L9 = Lattice<9>;
+
+__device__ __forceinline__ float feq9(float rho, float ux, float uy, int i) {
+  const float eu = (float)L9::ex(i) * ux + (float)L9::ey(i) * uy;
+  return L9::w(i) * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * (ux * ux + uy * uy));
+}
+
+__device__ __forceinline__ float pool_pos(const AmrParams &p, int b, int f) {
+  return (float)(b * p.RB) - 0.25f + 0.5f * (float)(f - p.G);
+}
+
+__device__ __forceinline__ int64_t pcell(const AmrParams &p, int slot, int fx, int fy) {
+  return (int64_t)slot * p.FB * p.FB + (int64_t)fy * p.FB + fx;
+}
+
+// ---- refine round ------------------------------------------------------------
+
+// Max |discrete curl| of the root velocity over each level-1 block's RB x RB
+// root cells (amr_criterion_pool.wgsl, GHOST == 0 branch). Every operation is
+// rounded on its own so the value is reproducible bit for bit.
+__global__ void amr_criterion(const float4 *__restrict__ mac, const __grid_constant__ AmrParams p) {
+  const int b = blockIdx.x;
+  const int bx = b % p.NBX, by = b / p.NBX;
+  float m = 0.f;
+  for (int k = threadIdx.x; k < p.RB * p.RB; k += blockDim.x) {
+    const int x = bx * p.RB + k % p.RB, y = by * p.RB + k / p.RB;
+    const int xp = x + 1 == p.W ? 0 : x + 1, xm = x == 0 ? p.W - 1 : x - 1;
+    const int yp = y + 1 == p.H ? 0 : y + 1, ym = y == 0 ? p.H - 1 : y - 1;
+    const float a = mac[(int64_t)y * p.W + xp].z, bb = mac[(int64_t)y * p.W + xm].z;
+    const float c = mac[(int64_t)yp * p.W + x].y, d = mac[(int64_t)ym * p.W + x].y;
+    const float om = __fsub_rn(__fmul_rn(__fsub_rn(a, bb), 0.5f), __fmul_rn(__fsub_rn(c, d), 0.5f));
+    m = fmaxf(m, fabsf(om));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  __shared__ float sm[32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float r = 0.f;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) r = fmaxf(r, sm[w]);
+    p.crit[b] = r;
+  }
+}
+
+// nearBodyBox (common_geometry.wgsl:230-290): branch and bound on a
+// 1-Lipschitz distance, conservative at every depth.
+__device__ bool near_body_box(const AmrParams &p, float cx, float cy, float half) {
+  const float SQRT2_UP = 1.4142136f;
+  lbm_body fut = p.body;
+  fut.theta = __fadd_rn(p.body.theta, __fmul_rn(p.body.wz, p.lookahead));
+  float sx[16], sy[16], sh[16];
+  int sd[16];
+  int sp = 0;
+  sx[0] = cx; sy[0] = cy; sh[0] = half; sd[0] = 3; sp = 1;
+  const float Wf = (float)p.W, Hf = (float)p.H;
+  while (sp > 0) {
+    --sp;
+    const float x = sx[sp], y = sy[sp], h = sh[sp];
+    const int d = sd[sp];
+    const float now = phi2(x, y, p.body, Wf, Hf);
+    const float fu = phi2(__fsub_rn(x, __fmul_rn(p.body.vx, p.lookahead)),
+                          __fsub_rn(y, __fmul_rn(p.body.vy, p.lookahead)), fut, Wf, Hf);
+    const float phi = fminf(now, fu);
+    if (__fsub_rn(phi, __fmul_rn(h, SQRT2_UP)) > p.margin) continue;
+    if (phi <= p.margin) return true;
+    if (d == 0) return true;
+    const float hh = __fmul_rn(h, 0.5f);
+    for (int i = 0; i < 4; ++i) {
+      sx[sp] = __fadd_rn(x, (i & 1) ? hh : -hh);
+      sy[sp] = __fadd_rn(y, (i & 2) ? hh : -hh);
+      sh[sp] = hh;
+      sd[sp] = d - 1;
+      ++sp;
+    }
+  }
+  return false;
+}
+
+// decide (amr_manage_pool.wgsl): per root block, want all four children if
+// the body is within the margin of the block (now or lookahead steps on) or
+// the block's vorticity reaches the refine threshold.
+__global__ void amr_decide(const __grid_constant__ AmrParams p) {
+  const int pb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pb >= p.PNX * p.PNY) return;
+  const int bxP = pb % p.PNX, byP = pb / p.PNX;
+  float mc = 0.f;
+  for (int q = 0; q < 4; ++q) mc = fmaxf(mc, p.crit[(byP * 2 + (q >> 1)) * p.NBX + bxP * 2 + (q & 1)]);
+  const bool vort = p.vort_on && fmax((double)mc, 1e-6) >= p.thr;
+  const float half = (float)p.RB;
+  const float cx = (float)(bxP * p.RB2) + half - 0.5f, cy = (float)(byP * p.RB2) + half - 0.5f;
+  const bool w = vort || near_body_box(p, cx, cy, half);
+  for (int q = 0; q < 4; ++q) p.want[(byP * 2 + (q >> 1)) * p.NBX + bxP * 2 + (q & 1)] = w ? 1u : 0u;
+}
+
+// Coarsen then refine in the deterministic serial order of DET_SLOTS
+// (amr_manage_pool.wgsl coarsen/refine), then compact the active list
+// (amr_active_list.wgsl). One thread: a few thousand integer steps once per
+// refine round.
+__global__ void amr_coarsen_refine(const __grid_constant__ AmrParams p) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int count = p.counts[0];
+  for (int s = 0; s < p.S; s += 4) {
+    const int b = p.slotToBlock[s];
+    if (b < 0 || p.want[b]) continue;
+    p.freeList[count++] = s / 4;
+    for (int q = 0; q < 4; ++q) {
+      const int bb = p.slotToBlock[s + q];
+      if (bb >= 0) p.blockSlot[bb] = -1;
+      p.slotToBlock[s + q] = -1;
+    }
+  }
+  for (int ps = 0; ps < p.PNX * p.PNY; ++ps) {
+    const int bxP = ps % p.PNX, byP = ps / p.PNX;
+    const int b0 = (byP * 2) * p.NBX + bxP * 2;
+    if (p.blockSlot[b0] >= 0 || !p.want[b0]) continue;
+    if (count <= 0) continue;
+    count -= 1;
+    const int quad = p.freeList[count];
+    for (int qy = 0; qy < 2; ++qy)
+      for (int qx = 0; qx < 2; ++qx) {
+        const int slot = quad * 4 + qx + 2 * qy;
+        const int bid = (byP * 2 + qy) * p.NBX + bxP * 2 + qx;
+        p.blockSlot[bid] = slot;
+        p.slotToBlock[slot] = bid;
+        p.parentSlot[slot] = ps;
+        p.newly[slot] = 1u;
+      }
+  }
+  p.counts[0] = count;
+  int n = 0;
+  for (int s = 0; s < p.S; ++s)
+    if (p.slotToBlock[s] >= 0) p.activeList[n++] = s;
+  p.counts[1] = n;
+}
+
+// ---- transfers ------------------------------------------------------------------
+
+struct Sample {
+  float rho, ux, uy, fneq[9];
+};
+
+__device__ __forceinline__ void sample_root(const AmrParams &p, const float *__restrict__ f0, int gx, int gy,
+                                            Sample &s) {
+  gx = ((gx % p.W) + p.W) % p.W;
+  gy = ((gy % p.H) + p.H) % p.H;
+  const int64_t cell = (int64_t)gy * p.W + gx;
+  float f[9], rho = 0.f, ux = 0.f, uy = 0.f;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    f[i] = __ldg(f0 + i * p.N0 + cell);
+    rho += f[i];
+    ux += f[i] * (float)L9::ex(i);
+    uy += f[i] * (float)L9::ey(i);
+  }
+  ux /= fmaxf(rho, 1e-6f);
+  uy /= fmaxf(rho, 1e-6f);
+  s.rho = rho; s.ux = ux; s.uy = uy;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) s.fneq[i] = f[i] - feq9(rho, ux, uy, i);
+}
+
+// Bilinear rho, u, fneq from the four root cells around the pool cell,
+// f = feq + 0.5 (tf-1)/(tc-1) fneq (common_interp.wgsl interpCoarseToFine).
+__device__ void interp_cell(const AmrParams &p, const float *__restrict__ f0, float *__restrict__ f1, int slot,
+                            int bx, int by, int fx, int fy) {
+  const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
+  const int x0 = (int)floorf(px), y0 = (int)floorf(py);
+  const float tx = px - (float)x0, ty = py - (float)y0;
+  Sample s00, s10, s01, s11;
+  sample_root(p, f0, x0, y0, s00);
+  sample_root(p, f0, x0 + 1, y0, s10);
+  sample_root(p, f0, x0, y0 + 1, s01);
+  sample_root(p, f0, x0 + 1, y0 + 1, s11);
+  const float w00 = (1.f - tx) * (1.f - ty), w10 = tx * (1.f - ty), w01 = (1.f - tx) * ty, w11 = tx * ty;
+  const float rho = w00 * s00.rho + w10 * s10.rho + w01 * s01.rho + w11 * s11.rho;
+  const float ux = w00 * s00.ux + w10 * s10.ux + w01 * s01.ux + w11 * s11.ux;
+  const float uy = w00 * s00.uy + w10 * s10.uy + w01 * s01.uy + w11 * s11.uy;
+  const int64_t cell = pcell(p, slot, fx, fy);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const float fneq = w00 * s00.fneq[i] + w10 * s10.fneq[i] + w01 * s01.fneq[i] + w11 * s11.fneq[i];
+    f1[i * p.N1 + cell] = feq9(rho, ux, uy, i) + p.resc_c2f * fneq;
+  }
+}
+
+// mode 0: ring of every active tile (same-level neighbour copy, else root
+// interpolation); mode 1: every cell of the tiles activated this round.
+__global__ void __launch_bounds__(kPoolThreads)
+    amr_fill(const float *__restrict__ f0, float *__restrict__ f1, int mode, const __grid_constant__ AmrParams p) {
+  const int n = p.counts[1];
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s = p.activeList[k];
+    if (mode == 1 && !p.newly[s]) continue;
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
+    const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
+    const int G = p.G, RB2 = p.RB2, FB = p.FB;
+    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+      const int fx = c % FB, fy = c / FB;
+      const bool inX = fx >= G && fx < G + RB2, inY = fy >= G && fy < G + RB2;
+      if (mode == 1) {
+        interp_cell(p, f0, f1, s, bx, by, fx, fy);
+        continue;
+      }
+      if (inX && inY) continue;
+      int ns, nfx = fx, nfy = fy;
+      if (inY && fx < G) { ns = p.blockSlot[by * p.NBX + bxm]; nfx = fx + RB2; }
+      else if (inY && fx >= G + RB2) { ns = p.blockSlot[by * p.NBX + bxp]; nfx = fx - RB2; }
+      else if (inX && fy < G) { ns = p.blockSlot[bym * p.NBX + bx]; nfy = fy + RB2; }
+      else if (inX && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bx]; nfy = fy - RB2; }
+      else if (fx < G && fy < G) { ns = p.blockSlot[bym * p.NBX + bxm]; nfx = fx + RB2; nfy = fy + RB2; }
+      else if (fx >= G + RB2 && fy < G) { ns = p.blockSlot[bym * p.NBX + bxp]; nfx = fx - RB2; nfy = fy + RB2; }
+      else if (fx < G && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bxm]; nfx = fx + RB2; nfy = fy - RB2; }
+      else { ns = p.blockSlot[byp * p.NBX + bxp]; nfx = fx - RB2; nfy = fy - RB2; }
+      if (ns >= 0) {
+        const int64_t dst = pcell(p, s, fx, fy), src = pcell(p, ns, nfx, nfy);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f1[i * p.N1 + dst] = f1[i * p.N1 + src];
+      } else {
+        interp_cell(p, f0, f1, s, bx, by, fx, fy);
+      }
+    }
+  }
+}
+
+// One pool substep (amr_step1.wgsl stepCell): DIRECT_GHOST pull (a source
+// past the tile interior comes from the same-level neighbour's interior when
+// that neighbour is refined, else from this tile's ring), BGK + Guo at
+// tau_f with the chi penalty on this level's band, sponge, SOLID_EQ. Every
+// cell of the tile, ring included, collides (COLLIDE_RING = 1).
+__global__ void __launch_bounds__(kPoolThreads)
+    amr_substep(const float *__restrict__ fin, float *__restrict__ fout, float2 *__restrict__ vel1,
+                const __grid_constant__ AmrParams p) {
+  const int n = p.counts[1];
+  const float Wf = (float)p.W, Hf = (float)p.H;
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
+    const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
+    const int G = p.G, RB2 = p.RB2, FB = p.FB;
+    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+      const int fx = c % FB, fy = c / FB;
+      const int offX = fx <= G ? -1 : (fx + 1 >= G + RB2 ? 1 : 0);
+      const int offY = fy <= G ? -1 : (fy + 1 >= G + RB2 ? 1 : 0);
+      const int cxb = offX > 0 ? bxp : (offX < 0 ? bxm : bx);
+      const int cyb = offY > 0 ? byp : (offY < 0 ? bym : by);
+      const int nbrX = offX ? p.blockSlot[by * p.NBX + cxb] : -1;
+      const int nbrY = offY ? p.blockSlot[cyb * p.NBX + bx] : -1;
+      const int nbrXY = (offX && offY) ? p.blockSlot[cyb * p.NBX + cxb] : -1;
+      const int64_t cell = pcell(p, s, fx, fy);
+      const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
+      float wx = fmodf(px, Wf); if (wx < 0.f) wx += Wf;
+      float wy = fmodf(py, Hf); if (wy < 0.f) wy += Hf;
+      const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
+      const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
+      const float phi = phi2(px, py, p.body, Wf, Hf);
+      const bool near = p.bb && phi < 2.0f;  // a link is at most sqrt(2)/2 root cells long here
+      float f[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const int ex = L9::ex(i), ey = L9::ey(i);
+        if (near && phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
+          const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+          f[i] = __ldg(fin + L9::opp(i) * p.N1 + cell) + corr;
+          continue;
+        }
+        int sx = fx - ex, sy = fy - ey, src = s;
+        const int ox = (sx < G || sx >= G + RB2) ? offX : 0;
+        const int oy = (sy < G || sy >= G + RB2) ? offY : 0;
+        const int ns = (ox && oy) ? nbrXY : (ox ? nbrX : (oy ? nbrY : -1));
+        if (ns >= 0) { src = ns; sx -= ox * RB2; sy -= oy * RB2; }
+        sx = min(max(sx, 0), FB - 1);
+        sy = min(max(sy, 0), FB - 1);
+        f[i] = __ldg(fin + i * p.N1 + pcell(p, src, sx, sy));
+      }
+      float rho = 0.f, uxs = 0.f, uys = 0.f;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        rho += f[i];
+        uxs += f[i] * (float)L9::ex(i);
+        uys += f[i] * (float)L9::ey(i);
+      }
+      const float den = fmaxf(rho, 1e-6f);
+      uxs /= den;
+      uys /= den;
+      const float chi = p.bb ? 0.f : chi_from_phi(phi, p.eps_f);
+      const float Fx = rho * chi * (usx - uxs) + p.fx;
+      const float Fy = rho * chi * (usy - uys) + p.fy;
+      const float ux = uxs + Fx / (2.0f * den), uy = uys + Fy / (2.0f * den);
+      const float usq = ux * ux + uy * uy;
+      vel1[cell] = make_float2(ux, uy);
+      const float dx = fminf(wx, Wf - 1.0f - wx), dy = fminf(wy, Hf - 1.0f - wy);
+      const float sw = sponge_weight(fminf(dx, dy), p.sponge_w);
+      const bool solid = p.solid_eq && p.bb && phi < 0.f;
+      const float omg = p.omega_f, sfac = 1.0f - 0.5f * omg;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const float exf = (float)L9::ex(i), eyf = (float)L9::ey(i), w = L9::w(i);
+        float o;
+        if (solid) {
+          o = feq9(1.0f, usx, usy, i);
+        } else {
+          const float eu = exf * ux + eyf * uy;
+          const float fe = w * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
+          const float t2 = (exf * ux + eyf * uy) * 9.0f;
+          const float Si = sfac * w * (((exf - ux) * 3.0f + t2 * exf) * Fx + ((eyf - uy) * 3.0f + t2 * eyf) * Fy);
+          const float fc = f[i] - omg * (f[i] - fe) + Si;
+          o = fc * (1.0f - sw) + p.ftarget[i] * sw;
+        }
+        fout[i * p.N1 + cell] = o;
+      }
+    }
+  }
+}
+
+// 4-child restriction into the root (common_average.wgsl averageCell).
+__global__ void __launch_bounds__(64)
+    amr_average(const float *__restrict__ f1, float *__restrict__ f0, const __grid_constant__ AmrParams p) {
+  const int n = p.counts[1];
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    for (int c = threadIdx.x; c < p.RB * p.RB; c += 64) {
+      const int lx = c % p.RB, ly = c / p.RB;
+      const int fx0 = p.G + 2 * lx, fy0 = p.G + 2 * ly;
+      const int64_t ch[4] = {pcell(p, s, fx0, fy0), pcell(p, s, fx0 + 1, fy0), pcell(p, s, fx0, fy0 + 1),
+                             pcell(p, s, fx0 + 1, fy0 + 1)};
+      float fneq_sum[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) fneq_sum[i] = 0.f;
+      float rs = 0.f, rxs = 0.f, rys = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float f[9], rho = 0.f, ux = 0.f, uy = 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          f[i] = __ldg(f1 + i * p.N1 + ch[q]);
+          rho += f[i];
+          ux += f[i] * (float)L9::ex(i);
+          uy += f[i] * (float)L9::ey(i);
+        }
+        ux /= fmaxf(rho, 1e-6f);
+        uy /= fmaxf(rho, 1e-6f);
+        rs += rho;
+        rxs += rho * ux;
+        rys += rho * uy;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) fneq_sum[i] += f[i] - feq9(rho, ux, uy, i);
+      }
+      const float ra = rs * 0.25f, den = fmaxf(rs, 1e-6f);
+      const float uxa = rxs / den, uya = rys / den;
+      const int64_t pc = (int64_t)(by * p.RB + ly) * p.W + (bx * p.RB + lx);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) f0[i * p.N0 + pc] = feq9(ra, uxa, uya, i) + p.resc_f2c * (fneq_sum[i] * 0.25f);
+    }
+  }
+}
+
+// Finest-level force (amr_force1.wgsl forceCell): interior cells of every
+// active tile, momentum exchange or penalty weighted by dx = 1/2, one FP64
+// partial per tile and a deterministic last-block sum.
+__global__ void __launch_bounds__(kPoolThreads)
+    amr_force(const float *__restrict__ f1, const __grid_constant__ AmrParams p) {
+  const int n = p.counts[1];
+  const float Wf = (float)p.W, Hf = (float)p.H;
+  if (n == 0) {
+    if (blockIdx.x == 0 && threadIdx.x < 4) p.force_out[threadIdx.x] = 0.0;
+    return;
+  }
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    ForceAcc acc;
+    for (int c = threadIdx.x; c < p.RB2 * p.RB2; c += kPoolThreads) {
+      const int fx = p.G + c % p.RB2, fy = p.G + c / p.RB2;
+      const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
+      const float phi = phi2(px, py, p.body, Wf, Hf);
+      const int64_t cell = pcell(p, s, fx, fy);
+      const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
+      const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
+      float fxb = 0.f, fyb = 0.f, tz = 0.f;
+      if (p.bb) {
+        if (phi >= 0.f && phi < 2.0f) {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) {
+            const int ex = L9::ex(i), ey = L9::ey(i);
+            if (phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
+              const float fo = __ldg(f1 + L9::opp(i) * p.N1 + cell);
+              const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+              fxb += -(float)ex * (2.f * fo + corr) * 0.5f;
+              fyb += -(float)ey * (2.f * fo + corr) * 0.5f;
+            }
+          }
+          tz = rx * fyb - ry * fxb;
+        }
+      } else {
+        const float chi = chi_from_phi(phi, p.eps_f);
+        if (chi >= 1e-6f) {
+          float rho = 0.f, ux = 0.f, uy = 0.f;
+#pragma unroll
+          for (int i = 0; i < 9; ++i) {
+            const int sx = min(max(fx - L9::ex(i), 0), p.FB - 1), sy = min(max(fy - L9::ey(i), 0), p.FB - 1);
+            const float v = __ldg(f1 + i * p.N1 + pcell(p, s, sx, sy));
+            rho += v;
+            ux += v * (float)L9::ex(i);
+            uy += v * (float)L9::ey(i);
+          }
+          ux /= fmaxf(rho, 1e-6f);
+          uy /= fmaxf(rho, 1e-6f);
+          const float Fx = rho * chi * (usx - ux), Fy = rho * chi * (usy - uy);
+          fxb = -Fx * 0.5f;
+          fyb = -Fy * 0.5f;
+          tz = rx * fyb - ry * fxb;
+        }
+      }
+      CellForce cf;
+      cf.fx = fxb;
+      cf.fy = fyb;
+      cf.tz = tz;
+      acc.add(cf);
+    }
+    reduce_force<kPoolThreads>(acc, p.partials, p.counter, n, k, p.force_out);
+    __syncthreads();
+  }
+}
+
+}  // namespace
+}  // namespace lbm
+
+// ---- session ---------------------------------------------------------------------
+
+using namespace lbm;
+
+struct lbm_amr2d {
+  lbm_amr2d_config cfg{};
+  AmrParams p{};
+  StepParams root{};
+  float *f0[2] = {nullptr, nullptr};
+  float4 *mac = nullptr;
+  float *f1[2] = {nullptr, nullptr};
+  float2 *vel1 = nullptr;
+  int cur = 0;
+  int64_t step = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double *host = nullptr;
+  int *host_counts = nullptr;
+  int grid_slots = 0;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_amr_error;
+
+int afail(lbm_amr2d *a, int code, const std::string &m) {
+  if (a) a->err = m; else g_amr_error = m;
+  return code;
+}
+
+#define ACK(a, call)                                                                   \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return afail(a, e_ == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA,        \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+void release_amr(lbm_amr2d *a) {
+  if (!a) return;
+  if (a->stream) cudaStreamSynchronize(a->stream);
+  for (auto &g : a->graph)
+    if (g) cudaGraphExecDestroy(g);
+  cudaFree(a->f0[0]); cudaFree(a->f0[1]); cudaFree(a->mac);
+  cudaFree(a->f1[0]); cudaFree(a->f1[1]); cudaFree(a->vel1);
+  AmrParams &p = a->p;
+  cudaFree(p.blockSlot); cudaFree(p.slotToBlock); cudaFree(p.parentSlot); cudaFree(p.freeList);
+  cudaFree(p.counts); cudaFree(p.activeList); cudaFree(p.want); cudaFree(p.newly); cudaFree(p.crit);
+  cudaFree(p.partials); cudaFree(p.counter); cudaFree(p.force_out);
+  if (a->host) cudaFreeHost(a->host);
+  if (a->host_counts) cudaFreeHost(a->host_counts);
+  if (a->own) cudaStreamDestroy(a->own);
+}
+
+int validate_amr(const lbm_amr2d_config *c, std::string &why) {
+  if (!c) { why = "config is NULL"; return LBM_EINVAL; }
+  if (c->levels != 2) { why = "levels must be 2 (root + one pool level)"; return LBM_EINVAL; }
+  if (c->rb < 2 || c->rb > 32) { why = "rb must be in [2, 32]"; return LBM_EINVAL; }
+  if (c->nx <= 0 || c->ny <= 0 || c->nx % (2 * c->rb) || c->ny % (2 * c->rb)) {
+    why = "nx and ny must be positive multiples of 2*rb (one root block is 2*rb cells)";
+    return LBM_EINVAL;
+  }
+  if (c->max_slots <= 0 || c->max_slots % 4) { why = "max_slots must be a positive multiple of 4 (quad allocation)"; return LBM_EINVAL; }
+  if (!(c->tau > 0.5f)) { why = "tau must be > 0.5"; return LBM_EINVAL; }
+  if (lbm_tau_chain_singularity(c->tau, c->levels, 0.01) >= 0) {
+    why = "a level's tau is within 0.01 of 1, where the post-collision coarse<->fine transfer is 0/0 "
+          "(amr2d.mjs:189 tauChainSingularity)";
+    return LBM_EINVAL;
+  }
+  if (c->body.shape != LBM_SHAPE_ELLIPSE || !(c->body.a > 0.f) || !(c->body.b > 0.f)) {
+    why = "the body must be an ellipse (a, b > 0)";
+    return LBM_EINVAL;
+  }
+  if (c->refine_every < 1) { why = "refine_every must be >= 1"; return LBM_EINVAL; }
+  return LBM_OK;
+}
+
+int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
+  AmrParams &p = a->p;
+  const int g = a->grid_slots;
+  amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
+  amr_fill<<<g, kPoolThreads, 0, st>>>(a->f0[from], a->f1[0], 0, p);
+  StepParams rp = a->root;
+  rp.write_mac = 1;
+  cudaError_t e = launch_step(9, 0, a->f0[from], a->f0[1 - from], (float *)a->mac, rp, st);
+  if (e) return afail(a, LBM_ECUDA, std::string("root step: ") + cudaGetErrorString(e));
+  amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
+  amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
+  amr_average<<<g, 64, 0, st>>>(a->f1[0], a->f0[1 - from], p);
+  ACK(a, cudaGetLastError());
+  return LBM_OK;
+}
+
+int refine_round(lbm_amr2d *a) {
+  AmrParams &p = a->p;
+  cudaStream_t st = a->stream;
+  ACK(a, cudaMemsetAsync(p.newly, 0, p.S * sizeof(unsigned), st));
+  amr_criterion<<<p.NBX * p.NBY, 64, 0, st>>>(a->mac, p);
+  ACK(a, cudaMemsetAsync(p.want, 0, (size_t)p.NBX * p.NBY * sizeof(unsigned), st));
+  amr_decide<<<(p.PNX * p.PNY + 127) / 128, 128, 0, st>>>(p);
+  amr_coarsen_refine<<<1, 1, 0, st>>>(p);
+  amr_fill<<<a->grid_slots, kPoolThreads, 0, st>>>(a->f0[a->cur], a->f1[0], 1, p);
+  ACK(a, cudaGetLastError());
+  return LBM_OK;
+}
+
+int build_graph(lbm_amr2d *a, int from) {
+  cudaStream_t cs;
+  ACK(a, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  int rc = LBM_OK;
+  if (e == cudaSuccess) rc = macro_launches(a, cs, from);
+  cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess && rc == LBM_OK) e = cudaGraphInstantiate(&a->graph[from], g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  if (rc) return rc;
+  if (e != cudaSuccess) return afail(a, LBM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_amr2d_config_default(lbm_amr2d_config *c, int nx, int ny) {
+  if (!c) return LBM_EINVAL;
+  std::memset(c, 0, sizeof(*c));
+  c->nx = nx; c->ny = ny;
+  c->levels = 2;
+  c->rb = 8;
+  c->tau = 0.6f;
+  c->max_slots = 4 * ((nx / 16) * (ny / 16));
+  c->solid_eq = 1;
+  c->k_eps = 1.5f;
+  c->sponge_w = 4.0f;
+  c->body.shape = LBM_SHAPE_ELLIPSE;
+  c->body.qw = 1.f;
+  c->body.a = c->body.b = 1.f;
+  c->refine_every = 16;
+  c->refine_thresh = -8.0f;
+  c->refine_margin = 8.0f;
+  c->refine_lookahead = 16.0f;
+  c->auto_refine = 1;
+  return LBM_OK;
+}
+
+int lbm_amr2d_create(const lbm_amr2d_config *cfg, lbm_amr2d **out) {
+  if (!out) return afail(nullptr, LBM_EINVAL, "out is NULL");
+  *out = nullptr;
+  std::string why;
+  if (validate_amr(cfg, why)) return afail(nullptr, LBM_EINVAL, why);
+  lbm_amr2d *a = new lbm_amr2d();
+  a->cfg = *cfg;
+  AmrParams &p = a->p;
+  const lbm_amr2d_config &c = *cfg;
+  p.W = c.nx; p.H = c.ny; p.RB = c.rb; p.G = 2; p.RB2 = 2 * c.rb; p.FB = p.RB2 + 2 * p.G;
+  p.NBX = c.nx / c.rb; p.NBY = c.ny / c.rb; p.PNX = c.nx / p.RB2; p.PNY = c.ny / p.RB2; p.S = c.max_slots;
+  p.N0 = (int64_t)c.nx * c.ny; p.N1 = (int64_t)p.S * p.FB * p.FB;
+  p.tau_c = c.tau;
+  p.tau_f = 2.0f * c.tau - 0.5f;
+  p.omega_f = 1.0f / p.tau_f;
+  p.eps_f = c.k_eps * 0.5f;
+  p.sponge_w = c.sponge_w; p.sux = c.sponge_u[0]; p.suy = c.sponge_u[1];
+  p.fx = c.force[0]; p.fy = c.force[1];
+  p.margin = c.refine_margin; p.lookahead = c.refine_lookahead;
+  p.resc_c2f = 0.5f * (p.tau_f - 1.0f) / (p.tau_c - 1.0f);
+  p.resc_f2c = 2.0f * (p.tau_c - 1.0f) / (p.tau_f - 1.0f);
+  p.vort_on = c.refine_thresh <= 1.0f;
+  p.thr = std::exp2((double)c.refine_thresh);
+  p.bb = c.use_bounceback; p.solid_eq = c.solid_eq;
+  p.body = c.body;
+  for (int i = 0; i < 9; ++i) {
+    const int ex = Lattice<9>::ex(i), ey = Lattice<9>::ey(i);
+    const float eu = (float)ex * p.sux + (float)ey * p.suy;
+    p.ftarget[i] = Lattice<9>::w(i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * (p.sux * p.sux + p.suy * p.suy));
+  }
+  // The root level is a dense D2Q9 domain stepped by the dense kernel.
+  lbm_config rc;
+  lbm_config_default(&rc, 9, c.nx, c.ny, 1);
+  rc.tau = c.tau; rc.force[0] = c.force[0]; rc.force[1] = c.force[1];
+  rc.has_body = 1; rc.use_bounceback = c.use_bounceback; rc.solid_eq = c.solid_eq; rc.chi_eps = c.k_eps;
+  rc.sponge_w = c.sponge_w; rc.sponge_u[0] = c.sponge_u[0]; rc.sponge_u[1] = c.sponge_u[1];
+  rc.body = c.body;
+  fill_step_params(rc, p.N0, 0, a->root);
+  a->root.force_on = 0;  // the body force is measured on the finest level
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  a->grid_slots = std::min(p.S, 8 * sms);
+  auto bail = [&](cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    release_amr(a);
+    delete a;
+    return afail(nullptr, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA, m);
+  };
+  cudaError_t e;
+#define AM(ptr, bytes) if ((e = cudaMalloc(&(ptr), (bytes)))) return bail(e, "cudaMalloc " #ptr)
+  if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
+  a->stream = a->own;
+  AM(a->f0[0], 9 * p.N0 * 4); AM(a->f0[1], 9 * p.N0 * 4); AM(a->mac, p.N0 * 16);
+  AM(a->f1[0], 9 * p.N1 * 4); AM(a->f1[1], 9 * p.N1 * 4); AM(a->vel1, p.N1 * 8);
+  AM(p.blockSlot, p.NBX * p.NBY * 4); AM(p.slotToBlock, p.S * 4); AM(p.parentSlot, p.S * 4);
+  AM(p.freeList, (p.S / 4) * 4); AM(p.counts, 2 * 4); AM(p.activeList, p.S * 4);
+  AM(p.want, p.NBX * p.NBY * 4); AM(p.newly, p.S * 4); AM(p.crit, p.NBX * p.NBY * 4);
+  AM(p.partials, (size_t)p.S * kForceSlots * 8); AM(p.counter, 4); AM(p.force_out, kForceSlots * 8);
+#undef AM
+  if ((e = cudaMallocHost(&a->host, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
+  if ((e = cudaMallocHost(&a->host_counts, 4 * sizeof(int)))) return bail(e, "cudaMallocHost");
+  std::vector<int> neg(std::max<int64_t>(p.NBX * p.NBY, p.S), -1), fl(p.S / 4);
+  for (int i = 0; i < p.S / 4; ++i) fl[i] = i;  // writePoolInitialState: free list 0..n-1
+  int counts[2] = {p.S / 4, 0};
+  cudaMemcpy(p.blockSlot, neg.data(), p.NBX * p.NBY * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(p.slotToBlock, neg.data(), p.S * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(p.freeList, fl.data(), (p.S / 4) * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(p.counts, counts, 8, cudaMemcpyHostToDevice);
+  cudaMemset(p.parentSlot, 0, p.S * 4);
+  cudaMemset(p.activeList, 0xff, p.S * 4);
+  cudaMemset(p.want, 0, p.NBX * p.NBY * 4);
+  cudaMemset(p.newly, 0, p.S * 4);
+  cudaMemset(p.crit, 0, p.NBX * p.NBY * 4);
+  cudaMemset(p.counter, 0, 4);
+  cudaMemset(p.force_out, 0, kForceSlots * 8);
+  cudaMemset(a->f1[0], 0, 9 * p.N1 * 4);
+  cudaMemset(a->f1[1], 0, 9 * p.N1 * 4);
+  cudaMemset(a->mac, 0, p.N0 * 16);
+  if ((e = cudaDeviceSynchronize())) return bail(e, "initialise");
+  *out = a;
+  return LBM_OK;
+}
+
+void lbm_amr2d_destroy(lbm_amr2d *a) {
+  release_amr(a);
+  delete a;
+}
+
+const char *lbm_amr2d_last_error(const lbm_amr2d *a) { return a ? a->err.c_str() : g_amr_error.c_str(); }
+
+int lbm_amr2d_set_stream(lbm_amr2d *a, void *stream) {
+  if (!a) return LBM_EINVAL;
+  ACK(a, cudaStreamSynchronize(a->stream));
+  a->stream = stream ? (cudaStream_t)stream : a->own;
+  return LBM_OK;
+}
+
+int lbm_amr2d_write_root(lbm_amr2d *a, const float *f, const float *vel) {
+  if (!a || !f || !vel) return a ? afail(a, LBM_EINVAL, "NULL argument") : LBM_EINVAL;
+  const AmrParams &p = a->p;
+  ACK(a, cudaMemcpyAsync(a->f0[a->cur], f, 9 * p.N0 * 4, cudaMemcpyHostToDevice, a->stream));
+  std::vector<float4> m(p.N0);
+  for (int64_t k = 0; k < p.N0; ++k) m[k] = make_float4(1.f, vel[2 * k], vel[2 * k + 1], 0.f);
+  ACK(a, cudaMemcpyAsync(a->mac, m.data(), p.N0 * 16, cudaMemcpyHostToDevice, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr2d_read_root(lbm_amr2d *a, float *f, float *vel) {
+  if (!a) return LBM_EINVAL;
+  const AmrParams &p = a->p;
+  if (f) ACK(a, cudaMemcpyAsync(f, a->f0[a->cur], 9 * p.N0 * 4, cudaMemcpyDeviceToHost, a->stream));
+  std::vector<float4> m;
+  if (vel) {
+    m.resize(p.N0);
+    ACK(a, cudaMemcpyAsync(m.data(), a->mac, p.N0 * 16, cudaMemcpyDeviceToHost, a->stream));
+  }
+  ACK(a, cudaStreamSynchronize(a->stream));
+  if (vel)
+    for (int64_t k = 0; k < p.N0; ++k) { vel[2 * k] = m[k].y; vel[2 * k + 1] = m[k].z; }
+  return LBM_OK;
+}
+
+int lbm_amr2d_read_pool(lbm_amr2d *a, float *f, float *vel) {
+  if (!a) return LBM_EINVAL;
+  const AmrParams &p = a->p;
+  if (f) ACK(a, cudaMemcpyAsync(f, a->f1[0], 9 * p.N1 * 4, cudaMemcpyDeviceToHost, a->stream));
+  if (vel) ACK(a, cudaMemcpyAsync(vel, a->vel1, p.N1 * 8, cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr2d_step(lbm_amr2d *a, int n) {
+  if (!a) return LBM_EINVAL;
+  if (n < 0) return afail(a, LBM_EINVAL, "step count must be >= 0");
+  for (int k = 0; k < n; ++k) {
+    if (a->cfg.auto_refine && a->step % a->cfg.refine_every == 0) {
+      int rc = refine_round(a);
+      if (rc) return rc;
+    }
+    ++a->step;
+    if (!a->graph[a->cur]) {
+      int rc = build_graph(a, a->cur);
+      if (rc) return rc;
+    }
+    ACK(a, cudaGraphLaunch(a->graph[a->cur], a->stream));
+    a->cur = 1 - a->cur;
+  }
+  return LBM_OK;
+}
+
+int lbm_amr2d_forces(lbm_amr2d *a, double out[4]) {
+  if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  ACK(a, cudaMemcpyAsync(a->host, a->p.force_out, kForceSlots * 8, cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  out[0] = a->host[0]; out[1] = a->host[1]; out[2] = a->host[5]; out[3] = a->host[6];
+  return LBM_OK;
+}
+
+int lbm_amr2d_read_topology(lbm_amr2d *a, int32_t *block_slot, int32_t *slot_to_block, int32_t *free_list,
+                            int32_t counts[2], int32_t *active_list, float *criterion, uint32_t *want) {
+  if (!a) return LBM_EINVAL;
+  const AmrParams &p = a->p;
+  cudaStream_t st = a->stream;
+  const size_t nb = (size_t)p.NBX * p.NBY;
+  if (block_slot) ACK(a, cudaMemcpyAsync(block_slot, p.blockSlot, nb * 4, cudaMemcpyDeviceToHost, st));
+  if (slot_to_block) ACK(a, cudaMemcpyAsync(slot_to_block, p.slotToBlock, p.S * 4, cudaMemcpyDeviceToHost, st));
+  if (free_list) ACK(a, cudaMemcpyAsync(free_list, p.freeList, (p.S / 4) * 4, cudaMemcpyDeviceToHost, st));
+  if (counts) ACK(a, cudaMemcpyAsync(counts, p.counts, 8, cudaMemcpyDeviceToHost, st));
+  if (active_list) ACK(a, cudaMemcpyAsync(active_list, p.activeList, p.S * 4, cudaMemcpyDeviceToHost, st));
+  if (criterion) ACK(a, cudaMemcpyAsync(criterion, p.crit, nb * 4, cudaMemcpyDeviceToHost, st));
+  if (want) ACK(a, cudaMemcpyAsync(want, p.want, nb * 4, cudaMemcpyDeviceToHost, st));
+  ACK(a, cudaStreamSynchronize(st));
+  return LBM_OK;
+}
+
+int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a) {
+  if (!a) return 0;
+  lbm_amr2d *m = const_cast<lbm_amr2d *>(a);
+  if (cudaMemcpyAsync(m->host_counts, a->p.counts, 8, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(a->stream) != cudaSuccess) return -1;
+  const int64_t active = m->host_counts[1];
+  return a->p.N0 + active * (int64_t)a->p.RB2 * a->p.RB2 * 2;
+}
+
+int lbm_amr2d_sync(lbm_amr2d *a) {
+  if (!a) return LBM_EINVAL;
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+}  // extern "C"

@@ -52,22 +52,21 @@ __global__ void __launch_bounds__(THREADS)
     const int nx = sp.nx, ny = sp.ny;
     const int ncell = nx * ny * sp.nz;
     const int end = min(td.y + cells_per_tile, ncell);
-    CellForce acc;
+    const int lt = t - sp.tile0;
+    const bool region = sp.force_on && lt >= sp.ft0 && lt < sp.ft1;
+    ForceAcc acc;
     for (int c = td.y + threadIdx.x; c < end; c += THREADS) {
       const int x = c % nx, r = c / nx;
       CellForce cf;
       if constexpr (Q == 9) {
-        cell2<S>(fin, fout, mac, sp, x, r, cf);
+        cell2<S>(fin, fout, mac, sp, x, r, region, cf);
       } else {
-        cell3<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, cf);
+        cell3<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, region, cf);
       }
-      acc.add(cf);
+      if (region) acc.add(cf);
     }
-    if (sp.force_on) {
-      const int lt = t - sp.tile0;
-      if (lt >= sp.ft0 && lt < sp.ft1)
-        reduce_force<THREADS>(acc, sp.partials, sp.counter, sp.ft1 - sp.ft0, lt - sp.ft0, sp.force_out);
-    }
+    if (region)
+      reduce_force<THREADS>(acc, sp.partials, sp.counter, sp.ft1 - sp.ft0, lt - sp.ft0, sp.force_out);
     __syncthreads();
   }
 }

@@ -124,61 +124,137 @@ __device__ __forceinline__ double finite_or_zero(float v, double &bad) {
 }
 
 // Force/torque contribution of one cell to the body (f32, as the reference
-// forms it per cell); summed in FP64 by the caller.
+// forms it per cell).
 struct CellForce {
   float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
-  __device__ __forceinline__ void add(const CellForce &o) {
-    fx += o.fx; fy += o.fy; fz += o.fz; tx += o.tx; ty += o.ty; tz += o.tz;
+};
+
+// A thread's FP64 running sum of cell contributions; a non-finite cell
+// component is counted and contributes 0 (the reference's safeFixed).
+struct ForceAcc {
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  double bad = 0.0;
+  __device__ __forceinline__ void add(const CellForce &c) {
+    v[0] += finite_or_zero(c.fx, bad);
+    v[1] += finite_or_zero(c.fy, bad);
+    v[2] += finite_or_zero(c.fz, bad);
+    v[3] += finite_or_zero(c.tx, bad);
+    v[4] += finite_or_zero(c.ty, bad);
+    v[5] += finite_or_zero(c.tz, bad);
   }
 };
 
 template <int THREADS>
-__device__ __forceinline__ void reduce_force(const CellForce &c, double *partials, unsigned int *counter,
+__device__ __forceinline__ void reduce_force(const ForceAcc &a, double *partials, unsigned int *counter,
                                              int nparts, int part, double *out) {
   __shared__ double sm[kForceSlots * (THREADS / 32)];
-  double bad = 0.0;
   double v[kForceSlots];
-  v[0] = finite_or_zero(c.fx, bad);
-  v[1] = finite_or_zero(c.fy, bad);
-  v[2] = finite_or_zero(c.fz, bad);
-  v[3] = finite_or_zero(c.tx, bad);
-  v[4] = finite_or_zero(c.ty, bad);
-  v[5] = finite_or_zero(c.tz, bad);
-  v[6] = bad;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = a.v[k];
+  v[6] = a.bad;
   v[7] = 0.0;
   block_sum<kForceSlots, THREADS>(v, sm);
   finish_sum<kForceSlots, THREADS>(v, partials, counter, nparts, part, out, sm);
 }
 
+// The BGK collision with Guo forcing, written over opposite pairs (e, -e):
+//   feq(+-e)  = w rho (1 - 1.5 u.u + 4.5 (e.u)^2)  +-  3 w rho (e.u)
+//   S(+-e)    = (1 - omega/2) w (9 (e.F)(e.u) - 3 u.F)  +-  3 (1 - omega/2) w (e.F)
+// so one pair costs one symmetric and one antisymmetric term. f_out =
+// (1 - omega) f + omega feq + S, then the sponge blend f_out + s (f_far - f_out).
+// Same algebra as the reference's per-direction form
+// (common_d3_step.wgsl:331-357), reassociated.
+template <class L, int Q, typename S>
+__device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, float ux, float uy, float uz, float Fx,
+                                              float Fy, float Fz, float omg, float spw, const float *ftarget,
+                                              S *fo_, int64_t n, int cell) {
+  const float usq = ux * ux + uy * uy + uz * uz;
+  const float base = 1.0f - 1.5f * usq;
+  const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
+  const float sfac = 1.0f - 0.5f * omg;
+  const float keep = 1.0f - omg;
+  {
+    const float w = L::w(0);
+    const float fc = fmaf(keep, f[0], fmaf(omg, (w * rho) * base, -(sfac * w) * uF3));
+    const float out = spw > 0.f ? fmaf(spw, ftarget[0] - fc, fc) : fc;
+    Codec<S>::st(fo_ + cell, out, w);
+  }
+#pragma unroll
+  for (int i = 1; i < Q; ++i) {
+    const int j = L::opp(i);
+    if (j < i) continue;
+    const float ex = (float)L::ex(i), ey = (float)L::ey(i), ez = (float)L::ez(i);
+    const float w = L::w(i);
+    const float eu = ex * ux + ey * uy + ez * uz;
+    const float eF = ex * Fx + ey * Fy + ez * Fz;
+    const float wr = w * rho, ws = sfac * w;
+    const float sym = wr * fmaf(4.5f * eu, eu, base);
+    const float anti = (3.0f * wr) * eu;
+    const float symS = ws * fmaf(9.0f * eF, eu, -uF3);
+    const float antiS = (3.0f * ws) * eF;
+    const float A = fmaf(omg, sym, symS), B = fmaf(omg, anti, antiS);
+    const float fci = fmaf(keep, f[i], A + B);
+    const float fcj = fmaf(keep, f[j], A - B);
+    const float oi = spw > 0.f ? fmaf(spw, ftarget[i] - fci, fci) : fci;
+    const float oj = spw > 0.f ? fmaf(spw, ftarget[j] - fcj, fcj) : fcj;
+    Codec<S>::st(fo_ + (int64_t)i * n + cell, oi, w);
+    Codec<S>::st(fo_ + (int64_t)j * n + cell, oj, w);
+  }
+}
+
+// rho and rho u* from the gathered populations, summed over opposite pairs.
+template <class L, int Q>
+__device__ __forceinline__ void moments(const float (&f)[Q], float &rho, float &mx, float &my, float &mz) {
+  rho = f[0];
+  mx = my = mz = 0.f;
+#pragma unroll
+  for (int i = 1; i < Q; ++i) {
+    const int j = L::opp(i);
+    if (j < i) continue;
+    const float s = f[i] + f[j], d = f[i] - f[j];
+    rho += s;
+    if (L::ex(i) == 1) mx += d; else if (L::ex(i) == -1) mx -= d;
+    if (L::ey(i) == 1) my += d; else if (L::ey(i) == -1) my -= d;
+    if (L::ez(i) == 1) mz += d; else if (L::ez(i) == -1) mz -= d;
+  }
+}
+
+__device__ __forceinline__ float sponge_weight_inv(float d, float inv_sw) {
+  float w = fminf(fmaxf(1.0f - d * inv_sw, 0.0f), 1.0f);
+  return w * w * (3.0f - 2.0f * w);
+}
+
 // ---- 3D cell update ---------------------------------------------------------
 // Pull-stream (periodic sources, then bounce-back patches: body first with
 // Ladd's correction at local rho_w, then walls), moments, Guo forcing with
-// the chi penalty, BGK collide, sponge blend, SOLID_EQ; returns this cell's
-// force/torque contribution when p.force_on.
+// the chi penalty, BGK collide, sponge blend, SOLID_EQ. When `force` is set
+// (the caller's block can see the body) the cell's force/torque contribution
+// is returned in cf.
 
 template <int Q, typename S>
 __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
                                       float *__restrict__ mac, const StepParams &p, int x, int y,
-                                      int z, CellForce &cf) {
+                                      int z, bool force, CellForce &cf) {
   using L = Lattice<Q>;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int64_t n = p.n;
   const S *fi = fin + p.base;
   S *fo_ = fout + p.base;
-  const int cell = (z * ny + y) * nx + x;
-  const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
-  const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
-  const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
+  const int nxny = nx * ny;
+  const int cell = z * nxny + y * nx + x;
+  // Offset of the pull source for e = +1 / -1 on each axis, periodic.
+  const int xo_p = x == 0 ? nx - 1 : -1, xo_m = x == nx - 1 ? 1 - nx : 1;
+  const int yo_p = y == 0 ? (ny - 1) * nx : -nx, yo_m = y == ny - 1 ? (1 - ny) * nx : nx;
+  const int zo_p = z == 0 ? (nz - 1) * nxny : -nxny, zo_m = z == nz - 1 ? (1 - nz) * nxny : nxny;
 
   // 1. Pull-stream from the periodic sources.
   float f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
-    const int sx = ex == 1 ? xm : (ex == -1 ? xp : x);
-    const int sy = ey == 1 ? ym : (ey == -1 ? yp : y);
-    const int sz = ez == 1 ? zm : (ez == -1 ? zp : z);
-    f[i] = Codec<S>::ld(fi + (int64_t)i * n + ((sz * ny + sy) * nx + sx), L::w(i));
+    const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0)) +
+                    (ez == 1 ? zo_p : (ez == -1 ? zo_m : 0));
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), L::w(i));
   }
 
   const V3 pos = {(float)x, (float)y, (float)z};
@@ -232,14 +308,8 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   }
 
   // 2. Moments.
-  float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    rho += f[i];
-    mx += f[i] * (float)L::ex(i);
-    my += f[i] * (float)L::ey(i);
-    mz += f[i] * (float)L::ez(i);
-  }
+  float rho, mx, my, mz;
+  moments<L, Q>(f, rho, mx, my, mz);
   const float rhoDen = fmaxf(rho, 1e-6f);
   const float inv = 1.0f / rhoDen;
   const float uxs = mx * inv, uys = my * inv, uzs = mz * inv;
@@ -254,39 +324,19 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   const float ux = fmaf(Fx, hinv, uxs);
   const float uy = fmaf(Fy, hinv, uys);
   const float uz = fmaf(Fz, hinv, uzs);
-  const float usq = ux * ux + uy * uy + uz * uz;
 
   float spw = 0.f;
   if (p.sponge_w > 0.f) {
     const float dx = p.sax ? fminf(pos.x, (float)(nx - 1 - x)) : 1e30f;
     const float dy = p.say ? fminf(pos.y, (float)(ny - 1 - y)) : 1e30f;
     const float dz = p.saz ? fminf(pos.z, (float)(nz - 1 - z)) : 1e30f;
-    spw = sponge_weight(fminf(dx, fminf(dy, dz)), p.sponge_w);
+    spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), p.sponge_inv);
   }
 
   // 4. Collide + sponge blend, 5. solid interior held at feq(1, u_body).
-  // feq_i  = w_i rho (1 - 1.5 u.u + e.u (3 + 4.5 e.u))
-  // S_i    = (1 - omega/2) w_i ((e_i - u).F * 3 + 9 (e.u)(e.F))
-  //        = (1 - omega/2) w_i (e.F (3 + 9 e.u) - 3 u.F)
-  // f_out  = f + omega (feq - f) + S_i, then f_out + s (f_far - f_out).
-  const float omg = p.omega;
-  const float sfac = 1.0f - 0.5f * omg;
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    const float base = 1.0f - 1.5f * usq;
-    const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
-      const float w = L::w(i);
-      const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
-      const float eF = (float)ex * Fx + (float)ey * Fy + (float)ez * Fz;
-      const float feq = (w * rho) * fmaf(eu, fmaf(4.5f, eu, 3.0f), base);
-      const float Si = (sfac * w) * fmaf(eF, fmaf(9.0f, eu, 3.0f), -uF3);
-      const float fc = fmaf(omg, feq - f[i], f[i]) + Si;
-      const float out = spw > 0.f ? fmaf(spw, p.ftarget[i] - fc, fc) : fc;
-      Codec<S>::st(fo_ + (int64_t)i * n + cell, out, w);
-    }
+    collide_store<L, Q, S>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, fo_, n, cell);
   } else {
     const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
 #pragma unroll
@@ -302,7 +352,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   }
 
   // Force on the body from this cell (bounce-back links were summed above).
-  if (p.force_on) {
+  if (force) {
     if (bbody) {
       if (p.swept && fabsf(phi) < p.swept_band) {
         const bool solid_now = phi < 0.f;
@@ -342,22 +392,21 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
 template <typename S>
 __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__ fout,
                                       float *__restrict__ mac, const StepParams &p, int x, int y,
-                                      CellForce &cf) {
+                                      bool force, CellForce &cf) {
   using L = Lattice<9>;
   const int W = p.nx, H = p.ny;
   const int64_t n = p.n;
   const S *fi = fin + p.base;
   S *fo_ = fout + p.base;
   const int cell = y * W + x;
-  const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
-  const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+  const int xo_p = x == 0 ? W - 1 : -1, xo_m = x == W - 1 ? 1 - W : 1;
+  const int yo_p = y == 0 ? (H - 1) * W : -W, yo_m = y == H - 1 ? (1 - H) * W : W;
   float f[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const int ex = L::ex(i), ey = L::ey(i);
-    const int sx = ex == 1 ? xm : (ex == -1 ? xp : x);
-    const int sy = ey == 1 ? ym : (ey == -1 ? yp : y);
-    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (sy * W + sx), L::w(i));
+    const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0));
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), L::w(i));
   }
   const float fW = (float)W, fH = (float)H;
   const float px = (float)x, py = (float)y;
@@ -374,6 +423,8 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   const bool at_wall = p.wall_y && (y == 0 || y == H - 1);
   float fbx = 0.f, fby = 0.f;
   if (near || at_wall) {
+    const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       const int ex = L::ex(i), ey = L::ey(i), o = L::opp(i);
@@ -402,13 +453,8 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
       }
     }
   }
-  float rho = 0.f, mxs = 0.f, mys = 0.f;
-#pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    rho += f[i];
-    mxs += f[i] * (float)L::ex(i);
-    mys += f[i] * (float)L::ey(i);
-  }
+  float rho, mxs, mys, mzs;
+  moments<L, 9>(f, rho, mxs, mys, mzs);
   const float rhoDen = fmaxf(rho, 1e-6f);
   const float inv = 1.0f / rhoDen;
   const float uxs = mxs * inv, uys = mys * inv;
@@ -418,32 +464,16 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   const float hinv = 0.5f * inv;
   const float ux = fmaf(Fx, hinv, uxs);
   const float uy = fmaf(Fy, hinv, uys);
-  const float usq = ux * ux + uy * uy;
 
   float spw = 0.f;
   if (p.sponge_w > 0.f) {
     const float dx = fminf(px, (float)(W - 1 - x));
     const float dy = fminf(py, (float)(H - 1 - y));
-    spw = sponge_weight(fminf(dx, dy), p.sponge_w);
+    spw = sponge_weight_inv(fminf(dx, dy), p.sponge_inv);
   }
-  const float omg = p.omega;
-  const float sfac = 1.0f - 0.5f * omg;
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    const float base = 1.0f - 1.5f * usq;
-    const float uF3 = 3.0f * (ux * Fx + uy * Fy);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      const int ex = L::ex(i), ey = L::ey(i);
-      const float w = L::w(i);
-      const float eu = (float)ex * ux + (float)ey * uy;
-      const float eF = (float)ex * Fx + (float)ey * Fy;
-      const float feq = (w * rho) * fmaf(eu, fmaf(4.5f, eu, 3.0f), base);
-      const float Si = (sfac * w) * fmaf(eF, fmaf(9.0f, eu, 3.0f), -uF3);
-      const float fc = fmaf(omg, feq - f[i], f[i]) + Si;
-      const float out = spw > 0.f ? fmaf(spw, p.ftarget[i] - fc, fc) : fc;
-      Codec<S>::st(fo_ + (int64_t)i * n + cell, out, w);
-    }
+    collide_store<L, 9, S>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, fo_, n, cell);
   } else {
     const float ussq = usx * usx + usy * usy;
 #pragma unroll
@@ -455,7 +485,7 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   }
   if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, 0.f);
 
-  if (p.force_on) {
+  if (force) {
     if (!bbody && p.has_body) {
       const float c2 = chi_from_phi(phi, p.chi_eps);
       if (c2 >= 1e-6f) {

@@ -20,7 +20,7 @@ struct StepParams {
   int has_body, bb, solid_eq, rho_w_local, swept;
   float swept_band;     // |phi| below which a cell can change hands in one step
   float chi_eps;
-  float sponge_w;
+  float sponge_w, sponge_inv;  // band width and its reciprocal
   int sax, say, saz;
   float ftarget[27];    // sponge far-field equilibrium per direction (rho = 1)
   lbm_body body;
@@ -40,10 +40,10 @@ struct StepParams {
 // SM the register budget is sized for). Compile-time so the tuning sweep can
 // build variants; the defaults are the measured best.
 #ifndef LBM_STEP_THREADS
-#define LBM_STEP_THREADS 128
+#define LBM_STEP_THREADS 64
 #endif
 #ifndef LBM_STEP_MIN_BLOCKS
-#define LBM_STEP_MIN_BLOCKS 8
+#define LBM_STEP_MIN_BLOCKS 16
 #endif
 constexpr int kStepThreads = LBM_STEP_THREADS;
 constexpr int kStepMinBlocks = LBM_STEP_MIN_BLOCKS;

@@ -42,15 +42,17 @@ __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) /
     d3_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
             const __grid_constant__ StepParams p) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x;
+  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+  const bool region = p.force_on && bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1 &&
+                      bz >= p.rbz0 && bz < p.rbz1;
   CellForce cf;
-  if (x < p.nx) cell3<Q, S>(fin, fout, mac, p, x, blockIdx.y, blockIdx.z, cf);
-  if (p.force_on) {
-    const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-    if (bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1 && bz >= p.rbz0 && bz < p.rbz1) {
-      const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
-      const int part = ((bz - p.rbz0) * ry + (by - p.rby0)) * rx + (bx - p.rbx0);
-      reduce_force<kStepThreads>(cf, p.partials, p.counter, rx * ry * rz, part, p.force_out);
-    }
+  if (x < p.nx) cell3<Q, S>(fin, fout, mac, p, x, by, bz, region, cf);
+  if (region) {
+    const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
+    const int part = ((bz - p.rbz0) * ry + (by - p.rby0)) * rx + (bx - p.rbx0);
+    ForceAcc acc;
+    acc.add(cf);
+    reduce_force<kStepThreads>(acc, p.partials, p.counter, rx * ry * rz, part, p.force_out);
   }
 }
 
@@ -59,15 +61,16 @@ __global__ void __launch_bounds__(kStepThreads)
     d2_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
             const __grid_constant__ StepParams p) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const bool region = p.force_on && bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1;
   CellForce cf;
-  if (x < p.nx) cell2<S>(fin, fout, mac, p, x, blockIdx.y, cf);
-  if (p.force_on) {
-    const int bx = blockIdx.x, by = blockIdx.y;
-    if (bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1) {
-      const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0;
-      reduce_force<kStepThreads>(cf, p.partials, p.counter, rx * ry, (by - p.rby0) * rx + (bx - p.rbx0),
-                                 p.force_out);
-    }
+  if (x < p.nx) cell2<S>(fin, fout, mac, p, x, by, region, cf);
+  if (region) {
+    const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0;
+    ForceAcc acc;
+    acc.add(cf);
+    reduce_force<kStepThreads>(acc, p.partials, p.counter, rx * ry, (by - p.rby0) * rx + (bx - p.rbx0),
+                               p.force_out);
   }
 }
 

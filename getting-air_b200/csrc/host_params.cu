@@ -59,6 +59,7 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
   p.rho_w_local = c.rho_w_local;
   p.chi_eps = c.chi_eps;
   p.sponge_w = c.sponge_w;
+  p.sponge_inv = c.sponge_w > 0.f ? 1.0f / c.sponge_w : 0.f;
   p.sax = c.sponge_axis[0]; p.say = c.sponge_axis[1]; p.saz = c.sponge_axis[2];
   const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.q == 9 ? 0.f : c.sponge_u[2];
   const float ufar = c.q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);

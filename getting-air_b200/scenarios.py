@@ -140,3 +140,34 @@ def seed_domain(dom, w) -> np.ndarray:
         return tgv2d_f(n, dom["u0"], dom["kw"]["tau"], w)
     # channel: fluid at rest, rho = 1 (f_i = w_i), driven by the body force
     return np.repeat(np.asarray(w, np.float32)[:, None], n * n, axis=1)
+
+
+def cylinder_amr(W: int = 1024, H: int = 256, r: float = 20.0, centre=(256.0, 128.0), u0: float = 0.08,
+                 re: float = 100.0, perturb: float = 0.02, seed: int = 12345, bounceback: bool = False,
+                 max_slots=None) -> dict:
+    """The 2D AMR cylinder: root W x H, circle of radius r, tau from Re on the
+    diameter, sponge (width 4) toward (u0, 0), diffuse (chi) coupling unless
+    bounceback, and the reference's seed (main-cylinder-amr.js:803-830):
+    every root cell at feq(1, u0, uy) with uy = (rng*2-1) * perturb * u0 from
+    mulberry32(seed), the same (u0, uy) as the initial root velocity."""
+    nu = u0 * 2 * r / re
+    tau = float(np.float32(tau_from_nu(nu)))
+    rng = mulberry32(seed)
+    n = W * H
+    uy = np.array([(rng() * 2 - 1) * perturb * u0 for _ in range(n)], np.float64)
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1], np.float64)
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1], np.float64)
+    w = np.array([0.44444444775581360, 0.11111111193895340, 0.11111111193895340, 0.11111111193895340,
+                  0.11111111193895340, 0.027777777984738350, 0.027777777984738350, 0.027777777984738350,
+                  0.027777777984738350])
+    f = np.empty((9, n), np.float32)
+    usq = u0 * u0 + uy * uy
+    for i in range(9):
+        eu = ex[i] * u0 + ey[i] * uy
+        f[i] = (w[i] * (1 + eu * 3 + eu * eu * 4.5 - usq * 1.5)).astype(np.float32)
+    vel = np.stack([np.full(n, u0), uy], 1).astype(np.float32)
+    kw = dict(tau=tau, use_bounceback=int(bounceback), sponge_w=4.0, sponge_u=(u0, 0.0),
+              body=dict(shape="ellipse", centre=(centre[0], centre[1], 0.0), a=r, b=r))
+    if max_slots is not None:
+        kw["max_slots"] = max_slots
+    return {"dims": (W, H), "kw": kw, "f": f, "vel": vel, "u0": u0, "r": r}

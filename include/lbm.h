@@ -209,6 +209,68 @@ int lbm_batch_autotune(lbm_batch *b, int trials, float *best_ms);
 int lbm_batch_forces(lbm_batch *b, double *out);
 int lbm_batch_sync(lbm_batch *b);
 
+/* ---- 2D block-structured AMR (D2Q9) --------------------------------------
+ * Root level L0 is the dense W x H grid; level m >= 1 is a pool of tiles,
+ * each one block of RB x RB cells of level m-1 refined 2:1 into
+ * (2 RB + 2 G)^2 cells with a G = 2 ring (amr2d.mjs:220 makePool, FB = 20 at
+ * RB = 8). Tiles are granted and released in quads (the four children of one
+ * parent block, amr_manage_pool.wgsl grantQuad) from a deterministic free
+ * list (the DET_SLOTS serial order, amr2d.mjs:1078 grantAssignment). One
+ * macro-step follows main-cylinder-amr.js:1831 dispatchMacroStep with the
+ * default `interp` interface (amr2d-gpu.mjs:1060 S_Advance): refine round
+ * every refine_every steps, finest-level force, ring fill from the parent,
+ * root step, two fine substeps at tau_f = 2 tau_c - 1/2, restriction back to
+ * the root. */
+typedef struct {
+  int32_t nx, ny;            /* root grid; multiples of 2*rb                     */
+  int32_t levels;            /* 2 (root + one pool level)                        */
+  int32_t rb;                /* block size in parent cells (8)                   */
+  float tau;                 /* root relaxation time                             */
+  int32_t max_slots;         /* pool capacity in tiles, multiple of 4            */
+  int32_t use_bounceback;    /* 0: chi penalty (default), 1: Ladd bounce-back    */
+  int32_t solid_eq;
+  float k_eps;               /* chi band in cells of each level (1.5)            */
+  float sponge_w;            /* 4                                                */
+  float sponge_u[2];         /* far-field velocity                               */
+  float force[2];            /* uniform body force                               */
+  lbm_body body;             /* LBM_SHAPE_ELLIPSE (circle when a == b)           */
+  int32_t refine_every;      /* 16                                               */
+  float refine_thresh;       /* -8: refine where log2 max|curl| >= this          */
+  float refine_margin;       /* 8: refine blocks within this distance of body    */
+  float refine_lookahead;    /* 16 macro-steps                                   */
+  int32_t auto_refine;       /* 1                                                */
+  int32_t reserved[8];
+} lbm_amr2d_config;
+
+typedef struct lbm_amr2d lbm_amr2d;
+
+/* Defaults of main-cylinder-amr.js (REFINE_EVERY 16, REFINE_THRESH -8,
+ * FORCE_REFINE_MARGIN 8, LOOKAHEAD 16, K_EPS 1.5, SPONGE_W 4, RB 8). */
+int lbm_amr2d_config_default(lbm_amr2d_config *cfg, int nx, int ny);
+int lbm_amr2d_create(const lbm_amr2d_config *cfg, lbm_amr2d **out);
+void lbm_amr2d_destroy(lbm_amr2d *a);
+const char *lbm_amr2d_last_error(const lbm_amr2d *a);
+int lbm_amr2d_set_stream(lbm_amr2d *a, void *cuda_stream);
+/* Root populations (9 planes of nx*ny) and root velocity (2 per cell, the
+ * field the first refine round's criterion reads). */
+int lbm_amr2d_write_root(lbm_amr2d *a, const float *f, const float *vel);
+int lbm_amr2d_read_root(lbm_amr2d *a, float *f, float *vel);
+/* Pool populations of level 1 (9 planes of max_slots * FB^2, FB = 2rb+4). */
+int lbm_amr2d_read_pool(lbm_amr2d *a, float *f, float *vel);
+/* n macro-steps. */
+int lbm_amr2d_step(lbm_amr2d *a, int n);
+/* Drag/lift/torque of the last macro-step, FP64: {fx, fy, tz, nonfinite}. */
+int lbm_amr2d_forces(lbm_amr2d *a, double out[4]);
+/* Level-1 topology: block_slot[nbx*nby], slot_to_block[max_slots],
+ * free_list[max_slots/4], counts = {free quads, active slots}, active list
+ * (ascending slots), criterion[nbx*nby], want[nbx*nby]. Any may be NULL. */
+int lbm_amr2d_read_topology(lbm_amr2d *a, int32_t *block_slot, int32_t *slot_to_block, int32_t *free_list,
+                            int32_t counts[2], int32_t *active_list, float *criterion, uint32_t *want);
+/* Lattice updates per macro-step at the current topology:
+ * root cells + sum over levels of active * (2 rb)^2 * 2^m (amr2d.mjs:558). */
+int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a);
+int lbm_amr2d_sync(lbm_amr2d *a);
+
 /* ---- pure host functions (the reference's JS modules) ------------------- */
 
 /* Lattice tables, lattice-2d.mjs:106-162 and lattice-3d.mjs:50-210:
@@ -221,6 +283,33 @@ int lbm_lattice_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez,
  * overflow to Inf, and its inverse (f-pack.mjs:44-88). */
 uint16_t lbm_f32_to_f16_bits(float v);
 float lbm_f16_bits_to_f32(uint16_t h);
+
+/* AMR host rules of amr2d.mjs, as pure functions. */
+/* tauAtLevel (card-params.mjs:188): tau_m = 2 tau_{m-1} - 1/2. */
+double lbm_tau_at_level(double tau0, int m);
+/* Post-collision coarse->fine and fine->coarse non-equilibrium factors,
+ * 0.5 (tf-1)/(tc-1) and 2 (tc-1)/(tf-1) (amr2d.mjs:136-141). */
+double lbm_dc_rescale_c2f(double tau_coarse, double tau_fine);
+double lbm_dc_rescale_f2c(double tau_coarse, double tau_fine);
+/* First level within `band` of tau = 1 (the transfer's 0/0), or -1
+ * (amr2d.mjs:189 tauChainSingularity). */
+int lbm_tau_chain_singularity(double tau0, int levels, double band);
+/* grantAssignment (amr2d.mjs:1078): candidates served in id order, each
+ * popping free_list[--free_count]; granted_free_index[k] = -1 for refusals.
+ * Returns the new free count. */
+int lbm_grant_assignment(const int32_t *candidates, int n, int free_count, int32_t *granted_ids,
+                         int32_t *granted_free_index, int32_t *n_granted);
+/* releaseAssignment (amr2d.mjs:1094): releases pushed in id order at
+ * free_count, free_count+1, ... Returns the new free count. */
+int lbm_release_assignment(const int32_t *releases, int n, int free_count, int32_t *ids, int32_t *free_index);
+/* activeSlotList (amr2d.mjs:578): ascending slots with slot_to_block >= 0. */
+int lbm_active_slot_list(const int32_t *slot_to_block, int nslots, int32_t *out);
+/* cascade21 (amr2d.mjs:988) on per-level block masks: want[m] is a
+ * nbx(m)*nby(m) byte mask for m = 1..levels-1 (want[0] unused), nbx(m) =
+ * nbx1 * 2^(m-1). Closes it in place deepest-first: quad completion at
+ * m >= 2 and the parents of all 9 periodic neighbours. Returns the number of
+ * blocks added. */
+int lbm_cascade21(uint8_t **want, int levels, int nbx1, int nby1);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

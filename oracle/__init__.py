@@ -30,6 +30,15 @@ def lib() -> C.CDLL:
         L.oracle_init_eq.argtypes = [I, C.c_int64, I, D, D]
         L.oracle_run.argtypes = [P, I, D, I, D, D]
         L.oracle_totals.argtypes = [I, C.c_int64, D, D]
+        L.oracle_amr2d_create.argtypes = [P, I]
+        L.oracle_amr2d_create.restype = P
+        L.oracle_amr2d_destroy.argtypes = [P]
+        L.oracle_amr2d_write_root.argtypes = [P, D, D]
+        L.oracle_amr2d_step.argtypes = [P, I]
+        L.oracle_amr2d_refine_from_vel.argtypes = [P, C.POINTER(C.c_float)]
+        L.oracle_amr2d_set_topology.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                                C.POINTER(C.c_int32), C.c_int32]
+        L.oracle_amr2d_read.argtypes = [P, D, D, D, D, C.POINTER(C.c_int32), C.POINTER(C.c_float), D]
         L.oracle_f16_bits.argtypes = [C.c_float]
         L.oracle_f16_bits.restype = C.c_uint16
         _LIB = L
@@ -79,3 +88,64 @@ def totals(q: int, f: np.ndarray) -> np.ndarray:
 
 def f16_bits(v: float) -> int:
     return int(lib().oracle_f16_bits(float(v)))
+
+
+class Amr2D:
+    """The AMR macro-step restated on the CPU (FP64, or the f32 operation
+    order with fp32=True). cfg is the product's Amr2DConfig structure."""
+
+    def __init__(self, cfg, fp32: bool = False):
+        self.cfg = cfg
+        self.W, self.H, self.rb, self.S = cfg.nx, cfg.ny, cfg.rb, cfg.max_slots
+        self.fb = 2 * cfg.rb + 4
+        self.nb = (cfg.nx // cfg.rb) * (cfg.ny // cfg.rb)
+        self._h = lib().oracle_amr2d_create(C.cast(C.byref(cfg), C.c_void_p), int(fp32))
+
+    def close(self):
+        if self._h:
+            lib().oracle_amr2d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def write_root(self, f, vel):
+        f = np.ascontiguousarray(f, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        lib().oracle_amr2d_write_root(self._h, _d(f), _d(vel))
+
+    def step(self, n=1):
+        lib().oracle_amr2d_step(self._h, int(n))
+
+    def refine_from_vel(self, vel):
+        v = np.ascontiguousarray(vel, np.float32)
+        lib().oracle_amr2d_refine_from_vel(self._h, v.ctypes.data_as(C.POINTER(C.c_float)))
+
+    def set_topology(self, block_slot, slot_to_block, free_list, free_count: int):
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        bs, sb, fl = i32(block_slot), i32(slot_to_block), i32(free_list)
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        lib().oracle_amr2d_set_topology(self._h, p(bs), p(sb), p(fl), int(free_count))
+
+    def read(self) -> dict:
+        n0, n1 = self.W * self.H, self.S * self.fb * self.fb
+        f0, v0 = np.zeros((9, n0)), np.zeros((n0, 2))
+        f1, v1 = np.zeros((9, n1)), np.zeros((n1, 2))
+        topo = np.zeros(self.nb + self.S + self.S // 4 + 2 + self.S + self.nb, np.int32)
+        crit = np.zeros(self.nb, np.float32)
+        force = np.zeros(4)
+        lib().oracle_amr2d_read(self._h, _d(f0), _d(v0), _d(f1), _d(v1),
+                                topo.ctypes.data_as(C.POINTER(C.c_int32)),
+                                crit.ctypes.data_as(C.POINTER(C.c_float)), _d(force))
+        o = 0
+        out = {"f0": f0, "vel0": v0, "f1": f1, "vel1": v1, "criterion": crit, "force": force}
+        out["block_slot"] = topo[o:o + self.nb]; o += self.nb
+        out["slot_to_block"] = topo[o:o + self.S]; o += self.S
+        out["free_list"] = topo[o:o + self.S // 4]; o += self.S // 4
+        out["free_count"] = int(topo[o]); n_act = int(topo[o + 1]); o += 2
+        out["active"] = topo[o:o + n_act].copy(); o += self.S
+        out["want"] = topo[o:o + self.nb].astype(np.uint32)
+        return out

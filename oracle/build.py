@@ -12,7 +12,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_build" / "liboracle.so"
-SOURCES = ["dense_oracle.cpp"]
+SOURCES = ["dense_oracle.cpp", "amr2d_oracle.cpp"]
 FLAGS = ["-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared"]
 
 
@@ -26,7 +26,7 @@ def _cxx() -> str:
 
 def build() -> Path:
     srcs = [HERE / s for s in SOURCES]
-    deps = srcs + [HERE.parent / "include" / "lbm.h"]
+    deps = srcs + [HERE / "common.h", HERE.parent / "include" / "lbm.h"]
     if OUT.exists() and all(p.stat().st_mtime <= OUT.stat().st_mtime for p in deps):
         return OUT
     OUT.parent.mkdir(exist_ok=True)

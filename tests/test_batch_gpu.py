@@ -49,7 +49,8 @@ def test_batch_equals_dense_sessions_3d(lbm, oracle, tiling):
     for (f, m), (wf_, wm) in zip(got, want):
         assert np.array_equal(f, wf_)
         assert np.array_equal(m, wm)
-    assert np.allclose(gf, wf, rtol=1e-12, atol=1e-14)
+    # same per-cell f32 contributions, FP64 sums over different partitions
+    assert np.allclose(gf, wf, rtol=1e-10, atol=1e-12 * np.abs(wf).max())
     assert abs(gf[0, 0]) > 0 and abs(gf[1, 0]) > 0
 
 
