@@ -124,6 +124,8 @@ def _load() -> C.CDLL:
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), F, C.POINTER(C.c_uint32)], I),
         "lbm_amr2d_cell_updates": ([P], C.c_int64),
         "lbm_amr2d_sync": ([P], I),
+        "lbm_step_noalloc": ([C.POINTER(Config), P, P, P, P, P], I),
+        "lbm_noalloc_last_error": ([], C.c_char_p),
         "lbm_tau_at_level": ([C.c_double, I], C.c_double),
         "lbm_dc_rescale_c2f": ([C.c_double, C.c_double], C.c_double),
         "lbm_dc_rescale_f2c": ([C.c_double, C.c_double], C.c_double),
@@ -556,3 +558,13 @@ class Amr2D:
 
     def sync(self):
         self._check(lib.lbm_amr2d_sync(self._h))
+
+
+def step_noalloc(cfg: Config, f_in_ptr: int, f_out_ptr: int, mac_ptr: int | None = None,
+                 force_ptr: int | None = None, stream_ptr: int | None = None):
+    """One dense step between caller-owned device buffers, with no device
+    allocation inside the library (lbm_step_noalloc)."""
+    rc = lib.lbm_step_noalloc(C.byref(cfg), C.c_void_p(f_in_ptr), C.c_void_p(f_out_ptr),
+                              C.c_void_p(mac_ptr or 0), C.c_void_p(force_ptr or 0), C.c_void_p(stream_ptr or 0))
+    if rc:
+        raise LbmError(rc, lib.lbm_noalloc_last_error().decode())

@@ -1,0 +1,118 @@
+// A dense step that allocates nothing: lbm_step_noalloc().
+//
+// Who needs it. Some callers cannot call cudaMalloc: a host that owns every
+// byte of device memory through its own arena (an engine binding its own
+// buffers through the FFI), a time-stepping loop that must not hit the
+// implicit device-wide synchronisation of cudaMalloc/cudaFree while other
+// streams are busy, or code that runs under a fixed memory budget decided
+// up front. They already hold the populations; what the step additionally
+// needs is scratch for the deterministic FP64 body-force reduction (one
+// partial per launch block near the body plus a ticket counter). Here that
+// scratch is a file-scope device array, so the entry point only launches.
+//
+// Limits and rules of use:
+//  * the scratch holds kNoAllocMaxParts block partials (512 KiB); a body
+//    whose force region needs more launch blocks is refused with
+//    LBM_ENOSPC;
+//  * every GPU that loads this library holds the array until the process
+//    exits;
+//  * the first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress) with that device current and caches it; make
+//    that first call before any stream capture;
+//  * all calls on a device share the one array, which keeps the last call's
+//    contents: the ticket counter is cleared on the caller's stream before
+//    every launch, and two calls whose kernels overlap on the GPU race.
+//
+// The step itself is the dense kernel of dense_kernels.cu, unchanged.
+
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm.h"
+#include "dense.cuh"
+#include "host_params.cuh"
+
+namespace {
+
+constexpr int kNoAllocMaxParts = 8192;
+// Partials (kForceSlots doubles per block), then one slot whose first four
+// bytes are the ticket counter.
+constexpr int kScratchDoubles = kNoAllocMaxParts * lbm::kForceSlots + 32;
+
+static __device__ __align__(256) double g_step_scratch[kScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+double *g_scratch_addr[kMaxDevices] = {};
+thread_local std::string g_noalloc_error;
+
+int nfail(int code, const std::string &m) {
+  g_noalloc_error = m;
+  return code;
+}
+
+// Device address of the scratch array on the current device, looked up once.
+int scratch_for_current_device(double **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return nfail(LBM_ENOTSUP, "device index beyond the scratch cache");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_scratch_addr[dev]) {
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_step_scratch);
+    if (e != cudaSuccess || !ptr)
+      return nfail(LBM_ECUDA, std::string("cudaGetSymbolAddress(step scratch): ") + cudaGetErrorString(e));
+    g_scratch_addr[dev] = (double *)ptr;
+  }
+  *out = g_scratch_addr[dev];
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lbm_noalloc_last_error(void) { return g_noalloc_error.c_str(); }
+
+int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float *mac, double *force_out,
+                     void *cuda_stream) {
+  std::string why;
+  if (lbm::validate_config(cfg, why)) return nfail(LBM_EINVAL, why);
+  const int64_t n = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+  lbm::StepParams p{};
+  lbm::fill_step_params(*cfg, n, 0, p);
+  int box[6];
+  p.force_on = (force_out && lbm::force_cell_box(*cfg, p, box)) ? 1 : 0;
+  if (p.force_on) {
+    p.rbx0 = box[0] / lbm::kStepThreads;
+    p.rbx1 = box[1] / lbm::kStepThreads + 1;
+    p.rby0 = box[2];
+    p.rby1 = box[3] + 1;
+    p.rbz0 = box[4];
+    p.rbz1 = box[5] + 1;
+    const int64_t parts = (int64_t)(p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0);
+    if (parts > kNoAllocMaxParts)
+      return nfail(LBM_ENOSPC, "the body's force region spans " + std::to_string(parts) +
+                                   " launch blocks; the fixed scratch holds " + std::to_string(kNoAllocMaxParts));
+  }
+  if (!f_in || !f_out || f_in == f_out) return nfail(LBM_EINVAL, "f_in and f_out must be distinct device buffers");
+  double *scratch = nullptr;
+  int rc = scratch_for_current_device(&scratch);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(scratch + kNoAllocMaxParts * lbm::kForceSlots);
+  p.partials = scratch;
+  p.counter = ticket;
+  p.force_out = force_out;
+  p.write_mac = mac ? 1 : 0;
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned int), st);
+  if (e == cudaSuccess) e = lbm::launch_step(cfg->q, cfg->storage, f_in, f_out, mac, p, st);
+  if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("step: ") + cudaGetErrorString(e));
+  return LBM_OK;
+}
+
+}  // extern "C"

@@ -176,6 +176,24 @@ int lbm_sync(lbm_session *s);
 /* Bytes of device memory the session holds. */
 int64_t lbm_device_bytes(const lbm_session *s);
 
+/* ---- allocation-free stepping --------------------------------------------
+ * No counterpart in the reference: added for callers that cannot call
+ * cudaMalloc -- hosts that own all device memory through their own arena,
+ * and loops that must not take the implicit device-wide synchronisation of
+ * cudaMalloc/cudaFree. Advances one dense step of `cfg` from the caller's
+ * device buffer f_in into the caller's f_out (Q planes in cfg->storage),
+ * optionally writing mac (4 floats per cell, device) and the body's
+ * force/torque (8 doubles, device: fx fy fz tx ty tz nonfinite 0), launched
+ * on cuda_stream. Allocates nothing: the force reduction's scratch is a fixed
+ * 512 KiB device array inside the library (8192 launch blocks of partials);
+ * a force region needing more returns LBM_ENOSPC. The first call on a device
+ * looks up that array's address and must come before any stream capture.
+ * All calls share the array: calls whose kernels overlap on the GPU race.
+ * Errors are reported by lbm_noalloc_last_error(). */
+int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float *mac, double *force_out,
+                     void *cuda_stream);
+const char *lbm_noalloc_last_error(void);
+
 /* ---- batched form ----------------------------------------------------------
  * Many independent domains of uneven sizes (same q and storage) in one
  * arena, advanced by one persistent launch per step replayed from a CUDA
