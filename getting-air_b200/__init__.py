@@ -58,6 +58,11 @@ class Amr2DConfig(C.Structure):
                 ("refine_lookahead", C.c_float), ("auto_refine", C.c_int32), ("reserved", C.c_int32 * 8)]
 
 
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("steps", C.c_int32), ("forces", C.c_double * 6),
+                ("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double)]
+
+
 class Config(C.Structure):
     _fields_ = [("q", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("tau", C.c_float), ("force", C.c_float * 3), ("wall", C.c_int32 * 3),
@@ -92,6 +97,7 @@ def _load() -> C.CDLL:
         "lbm_set_body": ([P, C.POINTER(Body)], I),
         "lbm_forces": ([P, D], I),
         "lbm_totals": ([P, D], I),
+        "lbm_forces_async": ([P, C.c_void_p], I),
         "lbm_sync": ([P], I),
         "lbm_device_bytes": ([P], C.c_int64),
         "lbm_batch_create": ([C.POINTER(Config), I, C.POINTER(P)], I),
@@ -124,6 +130,14 @@ def _load() -> C.CDLL:
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), F, C.POINTER(C.c_uint32)], I),
         "lbm_amr2d_cell_updates": ([P], C.c_int64),
         "lbm_amr2d_sync": ([P], I),
+        "lbm_server_create": ([C.c_int64, C.POINTER(P)], I),
+        "lbm_server_destroy": ([P], None),
+        "lbm_server_last_error": ([P], C.c_char_p),
+        "lbm_server_submit": ([P, C.c_int64, C.POINTER(Config), F, I], I),
+        "lbm_server_poll": ([P, I, C.POINTER(Result), I, C.POINTER(I)], I),
+        "lbm_server_read": ([P, C.c_int64, F, F], I),
+        "lbm_server_release": ([P, C.c_int64], I),
+        "lbm_server_stats": ([P, C.POINTER(C.c_int64)], I),
         "lbm_step_noalloc": ([C.POINTER(Config), P, P, P, P, P], I),
         "lbm_noalloc_last_error": ([], C.c_char_p),
         "lbm_tau_at_level": ([C.c_double, I], C.c_double),
@@ -293,6 +307,11 @@ class Solver:
         out = np.zeros(6, np.float64)
         self._check(lib.lbm_forces(self._h, _ptr(out, C.c_double)))
         return out
+
+    def forces_async(self, out_ptr: int):
+        """Queue the last step's force/torque (6 doubles) into host memory at
+        out_ptr (pinned) without waiting; valid after sync()."""
+        self._check(lib.lbm_forces_async(self._h, C.c_void_p(out_ptr)))
 
     def totals(self) -> dict:
         out = np.zeros(8, np.float64)
@@ -568,3 +587,63 @@ def step_noalloc(cfg: Config, f_in_ptr: int, f_out_ptr: int, mac_ptr: int | None
                               C.c_void_p(mac_ptr or 0), C.c_void_p(force_ptr or 0), C.c_void_p(stream_ptr or 0))
     if rc:
         raise LbmError(rc, lib.lbm_noalloc_last_error().decode())
+
+
+class Server:
+    """Continuous-batching request loop over one device arena (lbm_server)."""
+
+    def __init__(self, budget_bytes: int):
+        h = C.c_void_p()
+        rc = lib.lbm_server_create(int(budget_bytes), C.byref(h))
+        if rc:
+            raise LbmError(rc, lib.lbm_server_last_error(None).decode())
+        self._h = h
+        self._results = (Result * 256)()
+
+    def _check(self, rc):
+        if rc:
+            raise LbmError(rc, lib.lbm_server_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.lbm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, rid: int, cfg: Config, steps: int, mac=None):
+        ptr = None
+        if mac is not None:
+            mac = np.ascontiguousarray(mac, np.float32)
+            ptr = _ptr(mac, C.c_float)
+        self._check(lib.lbm_server_submit(self._h, int(rid), C.byref(cfg), ptr, int(steps)))
+
+    def poll(self, max_steps: int = 64):
+        n = C.c_int()
+        self._check(lib.lbm_server_poll(self._h, int(max_steps), self._results, len(self._results), C.byref(n)))
+        out = []
+        for k in range(n.value):
+            r = self._results[k]
+            out.append({"id": r.id, "steps": r.steps, "forces": list(r.forces), "submit_s": r.submit_s,
+                        "admit_s": r.admit_s, "done_s": r.done_s})
+        return out
+
+    def read(self, rid: int, cfg: Config, f: bool = True):
+        n = cfg.nx * cfg.ny * cfg.nz
+        mac = np.empty((n, 4), np.float32)
+        ff = np.empty((cfg.q, n), np.float32) if f else None
+        self._check(lib.lbm_server_read(self._h, int(rid), _ptr(ff, C.c_float) if f else None, _ptr(mac, C.c_float)))
+        return ff, mac
+
+    def release(self, rid: int):
+        self._check(lib.lbm_server_release(self._h, int(rid)))
+
+    def stats(self) -> dict:
+        out = np.zeros(6, np.int64)
+        self._check(lib.lbm_server_stats(self._h, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return dict(zip(("queued", "resident", "finished", "bytes_used", "budget", "lattice_updates"),
+                        out.tolist()))

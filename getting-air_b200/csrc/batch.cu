@@ -364,7 +364,7 @@ int lbm_batch_init_macro(lbm_batch *b, int d, const float *mac) {
   const size_t fb = (size_t)b->q * b->ncell[d] * b->elem;
   void *tmp = nullptr;
   BCK(b, cudaMallocAsync(&tmp, fb, b->stream));
-  cudaError_t e = launch_init_eq(b->q, b->storage, m, tmp, b->ncell[d], b->stream);
+  cudaError_t e = launch_init_eq(b->q, b->storage, m, tmp, b->ncell[d], b->h_doms[d].pk, b->stream);
   for (int i = 0; e == cudaSuccess && i < b->q; ++i)
     e = cudaMemcpyAsync((char *)b->f[b->cur] + ((size_t)i * b->total + b->base[d]) * b->elem,
                         (char *)tmp + (size_t)i * b->ncell[d] * b->elem, (size_t)b->ncell[d] * b->elem,
@@ -383,7 +383,7 @@ int lbm_batch_write_f(lbm_batch *b, int d, const float *f) {
   BCK(b, cudaMallocAsync(&t32, (size_t)b->q * n * 4, b->stream));
   BCK(b, cudaMallocAsync(&tmp, (size_t)b->q * n * b->elem, b->stream));
   cudaError_t e = cudaMemcpyAsync(t32, f, (size_t)b->q * n * 4, cudaMemcpyHostToDevice, b->stream);
-  if (!e) e = launch_pack(b->q, b->storage, t32, tmp, n, b->stream);
+  if (!e) e = launch_pack(b->q, b->storage, t32, tmp, n, b->h_doms[d].pk, b->stream);
   for (int i = 0; e == cudaSuccess && i < b->q; ++i)
     e = cudaMemcpyAsync((char *)b->f[b->cur] + ((size_t)i * b->total + b->base[d]) * b->elem,
                         (char *)tmp + (size_t)i * n * b->elem, (size_t)n * b->elem, cudaMemcpyDeviceToDevice,
@@ -407,7 +407,7 @@ int lbm_batch_read_f(lbm_batch *b, int d, float *f) {
     e = cudaMemcpyAsync((char *)tmp + (size_t)i * n * b->elem,
                         (char *)b->f[b->cur] + ((size_t)i * b->total + b->base[d]) * b->elem, (size_t)n * b->elem,
                         cudaMemcpyDeviceToDevice, b->stream);
-  if (!e) e = launch_unpack(b->q, b->storage, tmp, t32, n, b->stream);
+  if (!e) e = launch_unpack(b->q, b->storage, tmp, t32, n, b->h_doms[d].pk, b->stream);
   if (!e) e = cudaMemcpyAsync(f, t32, (size_t)b->q * n * 4, cudaMemcpyDeviceToHost, b->stream);
   cudaFreeAsync(t32, b->stream);
   cudaFreeAsync(tmp, b->stream);

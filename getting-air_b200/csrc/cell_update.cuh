@@ -25,32 +25,32 @@ namespace lbm {
 constexpr float kCS2 = 1.0f / 3.0f;
 
 // ---- storage codecs --------------------------------------------------------
-// The 16-bit forms hold f_i - w_i (the f-pack mode-2 offset,
-// common_fpack.wgsl:91-121), rounded to nearest even; arithmetic stays f32.
-template <typename S> struct Codec;
+// FP32 planes hold f itself; the 16-bit planes hold (f - off_i) * scale (see
+// Pack), rounded to nearest even. Arithmetic is f32 throughout.
 #ifndef LBM_STREAMING_STORES
 #define LBM_STREAMING_STORES 0
 #endif
+template <typename S> struct Codec;
 template <> struct Codec<float> {
-  static __device__ __forceinline__ float ld(const float *p, float) { return __ldg(p); }
-  static __device__ __forceinline__ void st(float *p, float v, float) {
+  static __device__ __forceinline__ float ld(const float *p, int, const Pack &) { return __ldg(p); }
+  static __device__ __forceinline__ void st(float *p, float v, int, const Pack &) {
     if (LBM_STREAMING_STORES) __stcs(p, v); else *p = v;
   }
 };
 template <> struct Codec<__half> {
-  static __device__ __forceinline__ float ld(const __half *p, float w) {
-    return __half2float(__ldg(p)) + w;
+  static __device__ __forceinline__ float ld(const __half *p, int i, const Pack &k) {
+    return fmaf(__half2float(__ldg(p)), k.inv, k.off[i]);
   }
-  static __device__ __forceinline__ void st(__half *p, float v, float w) {
-    *p = __float2half_rn(v - w);
+  static __device__ __forceinline__ void st(__half *p, float v, int i, const Pack &k) {
+    *p = __float2half_rn((v - k.off[i]) * k.scale);
   }
 };
 template <> struct Codec<__nv_bfloat16> {
-  static __device__ __forceinline__ float ld(const __nv_bfloat16 *p, float w) {
-    return __bfloat162float(__ldg(p)) + w;
+  static __device__ __forceinline__ float ld(const __nv_bfloat16 *p, int i, const Pack &k) {
+    return fmaf(__bfloat162float(__ldg(p)), k.inv, k.off[i]);
   }
-  static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, float w) {
-    *p = __float2bfloat16_rn(v - w);
+  static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, int i, const Pack &k) {
+    *p = __float2bfloat16_rn((v - k.off[i]) * k.scale);
   }
 };
 
@@ -167,7 +167,7 @@ __device__ __forceinline__ void reduce_force(const ForceAcc &a, double *partials
 template <class L, int Q, typename S>
 __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, float ux, float uy, float uz, float Fx,
                                               float Fy, float Fz, float omg, float spw, const float *ftarget,
-                                              S *fo_, int64_t n, int cell) {
+                                              const Pack &pk, S *fo_, int64_t n, int cell) {
   const float usq = ux * ux + uy * uy + uz * uz;
   const float base = 1.0f - 1.5f * usq;
   const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
@@ -177,7 +177,7 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
     const float w = L::w(0);
     const float fc = fmaf(keep, f[0], fmaf(omg, (w * rho) * base, -(sfac * w) * uF3));
     const float out = spw > 0.f ? fmaf(spw, ftarget[0] - fc, fc) : fc;
-    Codec<S>::st(fo_ + cell, out, w);
+    Codec<S>::st(fo_ + cell, out, 0, pk);
   }
 #pragma unroll
   for (int i = 1; i < Q; ++i) {
@@ -197,8 +197,8 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
     const float fcj = fmaf(keep, f[j], A - B);
     const float oi = spw > 0.f ? fmaf(spw, ftarget[i] - fci, fci) : fci;
     const float oj = spw > 0.f ? fmaf(spw, ftarget[j] - fcj, fcj) : fcj;
-    Codec<S>::st(fo_ + (int64_t)i * n + cell, oi, w);
-    Codec<S>::st(fo_ + (int64_t)j * n + cell, oj, w);
+    Codec<S>::st(fo_ + (int64_t)i * n + cell, oi, i, pk);
+    Codec<S>::st(fo_ + (int64_t)j * n + cell, oj, j, pk);
   }
 }
 
@@ -254,7 +254,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
     const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
     const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0)) +
                     (ez == 1 ? zo_p : (ez == -1 ? zo_m : 0));
-    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), L::w(i));
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
   }
 
   const V3 pos = {(float)x, (float)y, (float)z};
@@ -278,7 +278,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
     if (bbody && p.rho_w_local && phi < 2.f) {
       float s = 0.f;
 #pragma unroll
-      for (int i = 0; i < Q; ++i) s += Codec<S>::ld(fi + (int64_t)i * n + cell, L::w(i));
+      for (int i = 0; i < Q; ++i) s += Codec<S>::ld(fi + (int64_t)i * n + cell, i, p.pk);
       rhoW = s;
     }
 #pragma unroll
@@ -288,7 +288,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
       bool solid = false;
       if (near) solid = phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body) < 0.f;
       if (solid) {
-        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
         const float corr =
             2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) / kCS2;
         f[i] = fopp + corr;
@@ -302,7 +302,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
         const int sx = x - ex, sy = y - ey, sz = z - ez;
         const bool out = (p.wall_x && (sx < 0 || sx >= nx)) || (p.wall_y && (sy < 0 || sy >= ny)) ||
                          (p.wall_z && (sz < 0 || sz >= nz));
-        if (out) f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+        if (out) f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
       }
     }
   }
@@ -336,14 +336,14 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   // 4. Collide + sponge blend, 5. solid interior held at feq(1, u_body).
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    collide_store<L, Q, S>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, fo_, n, cell);
+    collide_store<L, Q, S>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, p.pk, fo_, n, cell);
   } else {
     const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const float w = L::w(i);
       const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
-      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), w);
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), i, p.pk);
     }
   }
   if (p.write_mac) {
@@ -361,7 +361,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
           float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
           for (int i = 0; i < Q; ++i) {
-            const float v = Codec<S>::ld(fi + (int64_t)i * n + cell, L::w(i));
+            const float v = Codec<S>::ld(fi + (int64_t)i * n + cell, i, p.pk);
             cx += v * (float)L::ex(i);
             cy += v * (float)L::ey(i);
             cz += v * (float)L::ez(i);
@@ -406,7 +406,7 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   for (int i = 0; i < 9; ++i) {
     const int ex = L::ex(i), ey = L::ey(i);
     const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0));
-    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), L::w(i));
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
   }
   const float fW = (float)W, fH = (float)H;
   const float px = (float)x, py = (float)y;
@@ -435,7 +435,7 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
         solid = phi2((float)sx, (float)sy, p.body, fW, fH) < 0.f;
       }
       if (solid) {
-        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o));
+        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
         const float corr = 2.f * L::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
         f[i] = fopp + corr;
         if (phi >= 0.f) {
@@ -448,7 +448,7 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
         if (ysrc < 0 || ysrc >= H) {
           const float wu = ysrc < 0 ? p.wall_u0 : p.wall_u1;
           const float corr = 2.f * L::w(i) * (float)ex * wu / kCS2;
-          f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, L::w(o)) + corr;
+          f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk) + corr;
         }
       }
     }
@@ -473,14 +473,14 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   }
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    collide_store<L, 9, S>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, fo_, n, cell);
+    collide_store<L, 9, S>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, p.pk, fo_, n, cell);
   } else {
     const float ussq = usx * usx + usy * usy;
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
       const float w = L::w(i);
       const float eu = (float)L::ex(i) * usx + (float)L::ey(i) * usy;
-      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * 1.0f * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), w);
+      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * 1.0f * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), i, p.pk);
     }
   }
   if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, 0.f);

@@ -7,6 +7,17 @@
 
 namespace lbm {
 
+// How 16-bit storage encodes a population: s = (f - off[i]) * scale, stored
+// rounded to nearest even; f = s * inv + off[i]. off[i] is the equilibrium of
+// the domain's far field, feq_i(rho = 1, u = U_far) (f-pack mode 2 with the
+// rest state replaced by the free stream: the stored value is the flow's
+// deviation from it), and scale = 2^10 for FP16 keeps small deviations out
+// of the subnormal range. Unused by FP32 storage.
+struct Pack {
+  float off[27];
+  float scale, inv;
+};
+
 // Per-step constants of the fused stream-collide kernels. Mirrors the
 // override constants of common_d3_step.wgsl:125-213 / lbm_step.wgsl:36-135.
 struct StepParams {
@@ -31,6 +42,7 @@ struct StepParams {
   double *partials;        // 8 doubles per region block
   unsigned int *counter;   // last-block ticket, returns to 0 after each step
   double *force_out;       // 8 doubles: fx fy fz tx ty tz nonfinite 0
+  Pack pk;                 // 16-bit storage encoding
   // Multi-domain launches: the domain's first tile, and the tile range
   // [ft0, ft1) (relative to tile0) whose cells can see the body.
   int tile0, ft0, ft1;
@@ -54,16 +66,16 @@ constexpr int kTotalsSlots = 8;
 // storage: 0 fp32, 1 fp16 offset, 2 bf16 offset
 cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float *mac,
                         const StepParams &p, cudaStream_t st);
-cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n,
+cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n, const Pack &pk,
                            cudaStream_t st);
-cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n,
+cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n, const Pack &pk,
                         cudaStream_t st);
-cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n,
+cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n, const Pack &pk,
                           cudaStream_t st);
 // Totals over the current f, FP64; `partials` holds totals_partials() * 8
 // doubles, `counter` one zeroed unsigned int.
 int totals_blocks();
-cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, double *partials,
+cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, const Pack &pk, double *partials,
                           unsigned int *counter, double *out, cudaStream_t st);
 
 // One step of every domain of a batch (batch.cu).

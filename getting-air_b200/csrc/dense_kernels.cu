@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kStepThreads)
 // ---- seeding and storage conversion ----------------------------------------
 
 template <int Q, typename S>
-__global__ void init_eq(const float4 *__restrict__ mac, S *__restrict__ f, int64_t n) {
+__global__ void init_eq(const float4 *__restrict__ mac, S *__restrict__ f, int64_t n, const Pack pk) {
   using L = Lattice<Q>;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
@@ -88,27 +88,27 @@ __global__ void init_eq(const float4 *__restrict__ mac, S *__restrict__ f, int64
     for (int i = 0; i < Q; ++i) {
       const float eu = (float)L::ex(i) * ux + (float)L::ey(i) * uy + (float)L::ez(i) * uz;
       const float v = L::w(i) * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
-      Codec<S>::st(f + (int64_t)i * n + c, v, L::w(i));
+      Codec<S>::st(f + (int64_t)i * n + c, v, i, pk);
     }
   }
 }
 
 template <int Q, typename S>
-__global__ void pack_planes(const float *__restrict__ src, S *__restrict__ dst, int64_t n) {
+__global__ void pack_planes(const float *__restrict__ src, S *__restrict__ dst, int64_t n, const Pack pk) {
   using L = Lattice<Q>;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x)
 #pragma unroll
-    for (int i = 0; i < Q; ++i) Codec<S>::st(dst + (int64_t)i * n + c, src[(int64_t)i * n + c], L::w(i));
+    for (int i = 0; i < Q; ++i) Codec<S>::st(dst + (int64_t)i * n + c, src[(int64_t)i * n + c], i, pk);
 }
 
 template <int Q, typename S>
-__global__ void unpack_planes(const S *__restrict__ src, float *__restrict__ dst, int64_t n) {
+__global__ void unpack_planes(const S *__restrict__ src, float *__restrict__ dst, int64_t n, const Pack pk) {
   using L = Lattice<Q>;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x)
 #pragma unroll
-    for (int i = 0; i < Q; ++i) dst[(int64_t)i * n + c] = Codec<S>::ld(src + (int64_t)i * n + c, L::w(i));
+    for (int i = 0; i < Q; ++i) dst[(int64_t)i * n + c] = Codec<S>::ld(src + (int64_t)i * n + c, i, pk);
 }
 
 // ---- conserved totals ------------------------------------------------------
@@ -120,7 +120,7 @@ constexpr int kTotalsBlocks = 148 * 4;
 
 template <int Q, typename S>
 __global__ void __launch_bounds__(kReduceThreads)
-    totals_kernel(const S *__restrict__ f, int64_t n, double *partials, unsigned int *counter,
+    totals_kernel(const S *__restrict__ f, int64_t n, const Pack pk, double *partials, unsigned int *counter,
                   double *out) {
   using L = Lattice<Q>;
   double mass = 0.0, px = 0.0, py = 0.0, pz = 0.0, bad = 0.0;
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kReduceThreads)
     double rho = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const double v = (double)Codec<S>::ld(f + (int64_t)i * n + c, L::w(i));
+      const double v = (double)Codec<S>::ld(f + (int64_t)i * n + c, i, pk);
       rho += v;
       mx += v * L::ex(i);
       my += v * L::ey(i);
@@ -230,26 +230,26 @@ cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float
   });
 }
 
-cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n,
+cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n, const Pack &pk,
                            cudaStream_t st) {
-  LBM_DISPATCH(q, storage, init_eq<Q, S><<<grid_for(n, 256), 256, 0, st>>>((const float4 *)mac_in, (S *)f_out, n));
+  LBM_DISPATCH(q, storage, init_eq<Q, S><<<grid_for(n, 256), 256, 0, st>>>((const float4 *)mac_in, (S *)f_out, n, pk));
 }
 
-cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n,
+cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n, const Pack &pk,
                         cudaStream_t st) {
-  LBM_DISPATCH(q, storage, pack_planes<Q, S><<<grid_for(n, 256), 256, 0, st>>>(f32, (S *)f_store, n));
+  LBM_DISPATCH(q, storage, pack_planes<Q, S><<<grid_for(n, 256), 256, 0, st>>>(f32, (S *)f_store, n, pk));
 }
 
-cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n,
+cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n, const Pack &pk,
                           cudaStream_t st) {
-  LBM_DISPATCH(q, storage, unpack_planes<Q, S><<<grid_for(n, 256), 256, 0, st>>>((const S *)f_store, f32, n));
+  LBM_DISPATCH(q, storage, unpack_planes<Q, S><<<grid_for(n, 256), 256, 0, st>>>((const S *)f_store, f32, n, pk));
 }
 
 int totals_blocks() { return kTotalsBlocks; }
 
-cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, double *partials,
+cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, const Pack &pk, double *partials,
                           unsigned int *counter, double *out, cudaStream_t st) {
-  LBM_DISPATCH(q, storage, (totals_kernel<Q, S><<<kTotalsBlocks, kReduceThreads, 0, st>>>((const S *)f, n, partials, counter, out)));
+  LBM_DISPATCH(q, storage, (totals_kernel<Q, S><<<kTotalsBlocks, kReduceThreads, 0, st>>>((const S *)f, n, pk, partials, counter, out)));
 }
 
 }  // namespace lbm

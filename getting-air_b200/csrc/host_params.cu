@@ -47,6 +47,21 @@ int validate_config(const lbm_config *c, std::string &why) {
   return LBM_OK;
 }
 
+Pack make_pack(const lbm_config &c) {
+  Pack k{};
+  const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.q == 9 ? 0.f : c.sponge_u[2];
+  const float usq = c.q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);
+  for (int i = 0; i < c.q; ++i) {
+    int ex, ey, ez;
+    dir_of(c.q, i, ex, ey, ez);
+    const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
+    k.off[i] = lattice_weight(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
+  }
+  k.scale = c.storage == LBM_STORE_FP16 ? 1024.0f : 1.0f;
+  k.inv = 1.0f / k.scale;
+  return k;
+}
+
 void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &p) {
   p.nx = c.nx; p.ny = c.ny; p.nz = c.nz; p.n = n; p.base = base;
   p.omega = 1.0f / c.tau;
@@ -70,6 +85,7 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
     const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
     p.ftarget[i] = lattice_weight(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * ufar);
   }
+  p.pk = make_pack(c);
   p.body = c.body;
   p.write_mac = 0;
   p.force_on = 0;

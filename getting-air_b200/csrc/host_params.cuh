@@ -27,4 +27,7 @@ bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]);
 
 float lattice_weight(int q, int i);
 
+// 16-bit storage encoding of a domain (far-field equilibrium offsets).
+Pack make_pack(const lbm_config &c);
+
 }  // namespace lbm

@@ -221,7 +221,7 @@ int lbm_set_stream(lbm_session *s, void *stream) {
 int lbm_init_macro(lbm_session *s, const float *mac) {
   if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
   CK(s, cudaMemcpyAsync(s->mac, mac, (size_t)s->n * 16, cudaMemcpyHostToDevice, s->stream));
-  CK(s, launch_init_eq(s->q, s->storage, s->mac, s->f[s->cur], s->n, s->stream));
+  CK(s, launch_init_eq(s->q, s->storage, s->mac, s->f[s->cur], s->n, s->sp.pk, s->stream));
   CK(s, cudaStreamSynchronize(s->stream));
   return LBM_OK;
 }
@@ -235,7 +235,7 @@ int lbm_write_f(lbm_session *s, const float *f) {
     float *tmp = nullptr;
     CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
     cudaError_t e = cudaMemcpyAsync(tmp, f, bytes, cudaMemcpyHostToDevice, s->stream);
-    if (!e) e = launch_pack(s->q, s->storage, tmp, s->f[s->cur], s->n, s->stream);
+    if (!e) e = launch_pack(s->q, s->storage, tmp, s->f[s->cur], s->n, s->sp.pk, s->stream);
     cudaFreeAsync(tmp, s->stream);
     if (e) return cuda_fail(s, e, "pack f");
   }
@@ -251,7 +251,7 @@ int lbm_read_f(lbm_session *s, float *f) {
   } else {
     float *tmp = nullptr;
     CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
-    cudaError_t e = launch_unpack(s->q, s->storage, s->f[s->cur], tmp, s->n, s->stream);
+    cudaError_t e = launch_unpack(s->q, s->storage, s->f[s->cur], tmp, s->n, s->sp.pk, s->stream);
     if (!e) e = cudaMemcpyAsync(f, tmp, bytes, cudaMemcpyDeviceToHost, s->stream);
     cudaFreeAsync(tmp, s->stream);
     if (e) return cuda_fail(s, e, "unpack f");
@@ -305,9 +305,19 @@ int lbm_forces(lbm_session *s, double out[6]) {
   return LBM_OK;
 }
 
+int lbm_forces_async(lbm_session *s, double out[6]) {
+  if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  if (!s->sp.force_on) {
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    return LBM_OK;
+  }
+  CK(s, cudaMemcpyAsync(out, s->force_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  return LBM_OK;
+}
+
 int lbm_totals(lbm_session *s, double out[8]) {
   if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
-  CK(s, launch_totals(s->q, s->storage, s->f[s->cur], s->n, s->tot_partials, s->tot_counter,
+  CK(s, launch_totals(s->q, s->storage, s->f[s->cur], s->n, s->sp.pk, s->tot_partials, s->tot_counter,
                       s->tot_out, s->stream));
   CK(s, cudaMemcpyAsync(s->host_out, s->tot_out, 8 * sizeof(double), cudaMemcpyDeviceToHost,
                         s->stream));

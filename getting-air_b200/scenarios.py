@@ -171,3 +171,31 @@ def cylinder_amr(W: int = 1024, H: int = 256, r: float = 20.0, centre=(256.0, 12
     if max_slots is not None:
         kw["max_slots"] = max_slots
     return {"dims": (W, H), "kw": kw, "f": f, "vel": vel, "u0": u0, "r": r}
+
+
+def serving_stream(count: int = 48, seed: int = 2024, rate: float = 200.0, nmin: int = 32, nmax: int = 192,
+                   steps=(500, 2000)):
+    """Seeded Poisson stream of 3D obstacle solves: arrival times with mean
+    rate `rate`/s, cubic domains N^3 with N log-uniform in [nmin, nmax],
+    D3Q19 or D3Q27, a pinned sphere (radius N/8) or rounded box (half-extent
+    N/8), bounce-back, sponge (width max(6, N/16)) toward u0 = 0.05 along x,
+    tau uniform in [0.55, 0.7], steps uniform in the given range. Returns a
+    list of dicts: t (arrival, s), q, dims, kw (Solver keywords), steps."""
+    rng = mulberry32(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += -math.log(1.0 - rng()) / rate
+        n = int(round(nmin * (nmax / nmin) ** rng()))
+        q = 19 if rng() < 0.5 else 27
+        box = rng() < 0.5
+        tau = float(np.float32(0.55 + 0.15 * rng()))
+        nsteps = int(steps[0] + (steps[1] - steps[0]) * rng())
+        a = n / 8.0
+        centre = (round(n / 3), n / 2, n / 2)
+        body = (dict(shape="roundbox", centre=centre, a=a, b=a, c=a, r=a / 4) if box else
+                dict(shape="sphere", centre=centre, a=a))
+        kw = dict(tau=tau, has_body=1, use_bounceback=1, body=body, sponge_w=float(max(6, n // 16)),
+                  sponge_u=(0.05, 0.0, 0.0))
+        out.append({"t": t, "q": q, "dims": (n, n, n), "kw": kw, "steps": nsteps, "id": k})
+    return out

@@ -163,6 +163,13 @@ int lbm_set_body(lbm_session *s, const lbm_body *body);
  * Replaces the i32 fixed-point atomics of common_d3_force.wgsl:265-282. */
 int lbm_forces(lbm_session *s, double out[6]);
 
+/* Queues a copy of the most recent step's {fx, fy, fz, tx, ty, tz} into
+ * host memory `out` (pinned for a true asynchronous copy) on the session
+ * stream and returns without waiting: a caller can record every step's force
+ * while the device keeps stepping, then lbm_sync() once. The buffer must
+ * stay valid until that sync. */
+int lbm_forces_async(lbm_session *s, double out[6]);
+
 /* Conserved totals over the current f, FP64 on the device:
  * out = {sum(rho-1), sum(rho ux), sum(rho uy), sum(rho uz), rho_min, rho_max,
  *        max|u|, non-finite cell count}.
@@ -288,6 +295,42 @@ int lbm_amr2d_read_topology(lbm_amr2d *a, int32_t *block_slot, int32_t *slot_to_
  * root cells + sum over levels of active * (2 rb)^2 * 2^m (amr2d.mjs:558). */
 int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a);
 int lbm_amr2d_sync(lbm_amr2d *a);
+
+/* ---- serving form -------------------------------------------------------------
+ * A request loop over one device arena of `budget_bytes` allocated at
+ * creation: submitted solves (a dense lbm_config + a step count) are admitted
+ * first-fit in FIFO order as memory frees up, stay resident on the device,
+ * and every poll advances all resident solves together (one persistent launch
+ * per lattice per step) up to the soonest completion, then retires the
+ * finished ones. A result is bit-identical to the same solve in a dense
+ * session. No counterpart in the reference (one page, one domain). */
+typedef struct lbm_server lbm_server;
+
+typedef struct {
+  int64_t id;          /* the caller's request id                          */
+  int32_t status;      /* 0                                                 */
+  int32_t steps;       /* steps run                                         */
+  double forces[6];    /* body force/torque of the last step, FP64         */
+  double submit_s;     /* server clock (seconds since create) at submit    */
+  double admit_s;      /*   ... when admitted into device memory           */
+  double done_s;       /*   ... when retired                                */
+} lbm_result;
+
+int lbm_server_create(int64_t budget_bytes, lbm_server **out);
+void lbm_server_destroy(lbm_server *s);
+const char *lbm_server_last_error(const lbm_server *s);
+/* Queues a solve; `mac` (host, 4 floats per cell) seeds it, or NULL for the
+ * uniform freestream at cfg->sponge_u. LBM_ENOSPC when it can never fit. */
+int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const float *mac, int steps);
+/* Admits what fits, runs one tick of at most max_steps steps, and returns up
+ * to max_done finished solves. Finished solves keep their device state until
+ * lbm_server_release. */
+int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done, int *n_done);
+/* Final f (FP32 storage only) and mac of a finished solve. */
+int lbm_server_read(lbm_server *s, int64_t id, float *f, float *mac);
+int lbm_server_release(lbm_server *s, int64_t id);
+/* {queued, resident, finished-not-released, bytes in use, budget, lattice updates run}. */
+int lbm_server_stats(lbm_server *s, int64_t out[6]);
 
 /* ---- pure host functions (the reference's JS modules) ------------------- */
 

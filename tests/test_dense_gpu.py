@@ -66,14 +66,16 @@ def check(g, o, u_tol=U_TOL, rho_tol=RHO_TOL, f_tol=F_TOL, forces=True):
 
 @pytest.mark.parametrize("q", [19, 27])
 def test_periodic_random_field(lbm, oracle, q):
+    # White noise (rho +-1 %, u +-0.03 per cell) is the worst case for f32
+    # cancellation in the moments; its stated bound is 5e-5.
     dims = (20, 12, 10)
     rng = np.random.default_rng(q)
     mac = seed_random(q, np.prod(dims), rng)
     g, o = both(lbm, oracle, q, dims, dict(tau=0.7), 12, mac=mac)
-    check(g, o, forces=False)
-    # the f32 oracle too (same operation order, no FMA on the CPU side)
+    check(g, o, u_tol=5e-5, forces=False)
+    # the f32 oracle too (the reference's operation order, no FMA on the CPU side)
     g2, o2 = both(lbm, oracle, q, dims, dict(tau=0.7), 12, mac=mac, fp32_oracle=True)
-    check(g2, o2, forces=False)
+    check(g2, o2, u_tol=5e-5, forces=False)
 
 
 @pytest.mark.parametrize("q", [19, 27])
@@ -178,6 +180,22 @@ def test_totals_match_oracle(lbm, oracle, q):
     assert np.array_equal(got[4:6], o[4:6])  # min/max of the same per-cell f64 sums
     assert abs(got[6] - o[6]) <= 1e-14 and got[7] == o[7] == 0
     s.close()
+
+
+def test_forces_async_matches_sync(lbm, oracle):
+    import torch
+    from getting_air_b200 import scenarios as sc
+    s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40)
+    sol = lbm.Solver.create(19, s["dims"], **s["kw"])
+    sol.init_macro(s["mac"])
+    hist = torch.zeros((5, 6), dtype=torch.float64).pin_memory()
+    for k in range(5):
+        sol.step(1)
+        sol.forces_async(hist[k].data_ptr())
+    sol.sync()
+    assert np.array_equal(hist[4].numpy(), sol.forces())
+    assert not np.array_equal(hist[0].numpy(), hist[4].numpy())
+    sol.close()
 
 
 def test_totals_count_nonfinite_cells(lbm, oracle):

@@ -1,0 +1,90 @@
+"""GPU tests of the serving form: a solve's result is the same alone and in
+a mix (bit-identical to a dense session), admission respects the HBM budget,
+and oversized requests are refused."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def mix(lbm):
+    from getting_air_b200 import scenarios as sc
+    reqs = sc.serving_stream(count=6, seed=5, nmin=16, nmax=40, steps=(20, 60))
+    out = []
+    for r in reqs:
+        out.append((r["id"], lbm.config_from(r["q"], r["dims"], **r["kw"]), r["steps"]))
+    # a diffuse-coupling D2Q9 cylinder in the same server
+    from getting_air_b200 import scenarios as sc2
+    c = sc2.cylinder2d(W=64, H=32, r=5.0, bounceback=False)
+    out.append((99, lbm.config_from(9, c["dims"], **c["kw"]), 33))
+    return out
+
+
+def drain(srv, ids):
+    got = {}
+    for _ in range(10000):
+        for r in srv.poll(16):
+            got[r["id"]] = r
+        if set(got) >= set(ids):
+            return got
+    raise AssertionError("server did not finish")
+
+
+def test_results_same_alone_and_in_mix(lbm):
+    reqs = mix(lbm)
+    srv = lbm.Server(2 << 30)
+    for rid, cfg, steps in reqs:
+        srv.submit(rid, cfg, steps)
+    got = drain(srv, [r[0] for r in reqs])
+    for rid, cfg, steps in reqs:
+        f, mac = srv.read(rid, cfg)
+        alone = lbm.Solver(cfg)
+        # the server's default seed, in the same f32 arithmetic
+        ux, uy = np.float32(cfg.sponge_u[0]), np.float32(cfg.sponge_u[1])
+        uz = np.float32(0) if cfg.q == 9 else np.float32(cfg.sponge_u[2])
+        rho = np.float32(1) - (ux * ux + uy * uy + uz * uz) * np.float32(1.5)
+        seed = np.tile(np.array([rho, ux, uy, uz], np.float32), (cfg.nx * cfg.ny * cfg.nz, 1))
+        alone.init_macro(seed)
+        alone.step(steps)
+        assert got[rid]["steps"] == steps
+        assert np.array_equal(f, alone.read_f()), rid
+        assert np.array_equal(mac, alone.read_mac()), rid
+        want = alone.forces()
+        assert np.allclose(got[rid]["forces"], want, rtol=1e-10, atol=1e-12 * max(np.abs(want).max(), 1e-30))
+        alone.close()
+        srv.release(rid)
+    assert srv.stats()["bytes_used"] == 0
+    srv.close()
+
+
+def test_budget_admission_queues_and_completes(lbm):
+    reqs = mix(lbm)
+    # room for the largest solve and a little more, so the others queue
+    need = [2 * c.q * c.nx * c.ny * c.nz * 4 + 16 * c.nx * c.ny * c.nz for _, c, _ in reqs]
+    srv = lbm.Server(int(max(need) * 1.3) + (1 << 20))
+    for rid, cfg, steps in reqs:
+        srv.submit(rid, cfg, steps)
+    saw_queue = False
+    done = {}
+    for _ in range(10000):
+        st = srv.stats()
+        saw_queue |= st["queued"] > 0 and st["resident"] > 0
+        assert st["bytes_used"] <= st["budget"]
+        for r in srv.poll(8):
+            done[r["id"]] = r
+            srv.release(r["id"])
+        if len(done) == len(reqs):
+            break
+    assert len(done) == len(reqs) and saw_queue
+    # FIFO admission: admits happen in submission order
+    admits = [done[rid]["admit_s"] for rid, _, _ in reqs]
+    assert admits == sorted(admits)
+    srv.close()
+
+
+def test_oversized_request_is_refused(lbm):
+    srv = lbm.Server(8 << 20)
+    cfg = lbm.config_from(19, (64, 64, 64))
+    with pytest.raises(lbm.LbmError, match="budget"):
+        srv.submit(1, cfg, 10)
+    srv.close()
