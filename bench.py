@@ -407,6 +407,29 @@ def time_served(lbm, world, count=48, budget_gb=48):
     return served, plain
 
 
+def packed_accuracy(lbm, steps=1000):
+    """Error of each storage form against the FP64 oracle on a reduced copy of
+    the workload (the same sphere scenario at 48 x 32 x 32, r = 4), from the
+    same f32 start state: velocity and density relative L2 and drag."""
+    import oracle
+    s32 = workload("fp32", dims=(48, 32, 32), n=8)
+    cfg = lbm.config_from(19, s32["dims"], **s32["kw"])
+    f0 = oracle.init_eq(19, s32["mac"], fp32=True).astype(np.float32)
+    _, om, of = oracle.run(cfg, f0.astype(np.float64), steps)
+    out = {"case": f"sphere 48x32x32 r=4, {steps} steps from the same f32 start; FP64 oracle on the host"}
+    for st in ("fp32", "fp16", "bf16"):
+        sol = lbm.Solver(lbm.config_from(19, s32["dims"], **(s32["kw"] | {"storage": st})))
+        sol.write_f(f0)
+        sol.step(steps)
+        m = sol.read_mac().astype(np.float64)
+        fx = sol.forces()[0]
+        sol.close()
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        out[st] = {"u_rel_l2": rel(m[:, 1:4], om[:, 1:4]), "rho_rel_l2": rel(m[:, 0], om[:, 0]),
+                   "drag_rel": abs(fx - of[-1, 0]) / abs(of[-1, 0])}
+    return out
+
+
 def cpu_baseline(seconds=10.0):
     """The oracle's f32 path (a restatement of the reference's shader math) on
     this host's cores, on a half-scale copy of the workload (same scenario,
@@ -463,6 +486,8 @@ def run_ours(args):
         forms["batched"], forms["batched_plain"] = time_batched(lbm, args.steps, args.warmup, world)
         forms["amr2d_cylinder"] = time_amr(lbm, args.steps, args.warmup, world)
         forms["served"], forms["served_plain"] = time_served(lbm, world)
+        if rank == 0:
+            forms["accuracy_vs_fp64"] = packed_accuracy(lbm)
     peak, peak_kind = hbm_peak()
     achieved = BYTES_PER_LU[("d3q19", "fp32")] * cells / (kern_ms * 1e-3) / 1e9
     traffic = profiled_traffic("d3q19_sphere_step")

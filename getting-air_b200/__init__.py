@@ -92,6 +92,8 @@ def _load() -> C.CDLL:
         "lbm_init_macro": ([P, F], I),
         "lbm_write_f": ([P, F], I),
         "lbm_read_f": ([P, F], I),
+        "lbm_write_f_raw": ([P, P], I),
+        "lbm_read_f_raw": ([P, P], I),
         "lbm_read_mac": ([P, F], I),
         "lbm_step": ([P, I], I),
         "lbm_set_body": ([P, C.POINTER(Body)], I),
@@ -290,6 +292,19 @@ class Solver:
     def read_f(self) -> np.ndarray:
         out = np.empty((self.q, self.ncells), np.float32)
         self._check(lib.lbm_read_f(self._h, _ptr(out, C.c_float)))
+        return out
+
+    def _raw_dtype(self):
+        return np.float32 if self.cfg.storage == STORAGE["fp32"] else np.uint16
+
+    def write_f_raw(self, planes: np.ndarray):
+        """Stored planes verbatim (uint16 bit patterns for the 16-bit storages)."""
+        planes = np.ascontiguousarray(planes, dtype=self._raw_dtype()).reshape(self.q, self.ncells)
+        self._check(lib.lbm_write_f_raw(self._h, planes.ctypes.data_as(C.c_void_p)))
+
+    def read_f_raw(self) -> np.ndarray:
+        out = np.empty((self.q, self.ncells), self._raw_dtype())
+        self._check(lib.lbm_read_f_raw(self._h, out.ctypes.data_as(C.c_void_p)))
         return out
 
     def read_mac(self) -> np.ndarray:

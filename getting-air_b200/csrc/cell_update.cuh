@@ -164,10 +164,24 @@ __device__ __forceinline__ void reduce_force(const ForceAcc &a, double *partials
 // (1 - omega) f + omega feq + S, then the sponge blend f_out + s (f_far - f_out).
 // Same algebra as the reference's per-direction form
 // (common_d3_step.wgsl:331-357), reassociated.
-template <class L, int Q, typename S>
+// Where a cell's post-collision populations go: MemSink stores them (the
+// step); NullSink drops them (a force-only pass, whose collision the
+// compiler then removes as dead code).
+template <typename S> struct MemSink {
+  S *fo;
+  int64_t n;
+  int cell;
+  const Pack &pk;
+  __device__ __forceinline__ void put(int i, float v) { Codec<S>::st(fo + (int64_t)i * n + cell, v, i, pk); }
+};
+struct NullSink {
+  __device__ __forceinline__ void put(int, float) {}
+};
+
+template <class L, int Q, class Sink>
 __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, float ux, float uy, float uz, float Fx,
                                               float Fy, float Fz, float omg, float spw, const float *ftarget,
-                                              const Pack &pk, S *fo_, int64_t n, int cell) {
+                                              Sink &sink) {
   const float usq = ux * ux + uy * uy + uz * uz;
   const float base = 1.0f - 1.5f * usq;
   const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
@@ -177,7 +191,7 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
     const float w = L::w(0);
     const float fc = fmaf(keep, f[0], fmaf(omg, (w * rho) * base, -(sfac * w) * uF3));
     const float out = spw > 0.f ? fmaf(spw, ftarget[0] - fc, fc) : fc;
-    Codec<S>::st(fo_ + cell, out, 0, pk);
+    sink.put(0, out);
   }
 #pragma unroll
   for (int i = 1; i < Q; ++i) {
@@ -195,10 +209,8 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
     const float A = fmaf(omg, sym, symS), B = fmaf(omg, anti, antiS);
     const float fci = fmaf(keep, f[i], A + B);
     const float fcj = fmaf(keep, f[j], A - B);
-    const float oi = spw > 0.f ? fmaf(spw, ftarget[i] - fci, fci) : fci;
-    const float oj = spw > 0.f ? fmaf(spw, ftarget[j] - fcj, fcj) : fcj;
-    Codec<S>::st(fo_ + (int64_t)i * n + cell, oi, i, pk);
-    Codec<S>::st(fo_ + (int64_t)j * n + cell, oj, j, pk);
+    sink.put(i, spw > 0.f ? fmaf(spw, ftarget[i] - fci, fci) : fci);
+    sink.put(j, spw > 0.f ? fmaf(spw, ftarget[j] - fcj, fcj) : fcj);
   }
 }
 
@@ -231,32 +243,17 @@ __device__ __forceinline__ float sponge_weight_inv(float d, float inv_sw) {
 // (the caller's block can see the body) the cell's force/torque contribution
 // is returned in cf.
 
-template <int Q, typename S>
-__device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
-                                      float *__restrict__ mac, const StepParams &p, int x, int y,
-                                      int z, bool force, CellForce &cf) {
+// Everything after the pull gather, for one cell: bounce-back patches,
+// moments, forcing, collision into `sink`, mac, force. `fi` is the domain's
+// base in the input arena (own-cell loads of the bounce-back patches).
+template <int Q, typename S, class Sink>
+__device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[Q], float *__restrict__ mac,
+                                           const StepParams &p, int x, int y, int z, bool force, CellForce &cf,
+                                           Sink &sink) {
   using L = Lattice<Q>;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int64_t n = p.n;
-  const S *fi = fin + p.base;
-  S *fo_ = fout + p.base;
-  const int nxny = nx * ny;
-  const int cell = z * nxny + y * nx + x;
-  // Offset of the pull source for e = +1 / -1 on each axis, periodic.
-  const int xo_p = x == 0 ? nx - 1 : -1, xo_m = x == nx - 1 ? 1 - nx : 1;
-  const int yo_p = y == 0 ? (ny - 1) * nx : -nx, yo_m = y == ny - 1 ? (1 - ny) * nx : nx;
-  const int zo_p = z == 0 ? (nz - 1) * nxny : -nxny, zo_m = z == nz - 1 ? (1 - nz) * nxny : nxny;
-
-  // 1. Pull-stream from the periodic sources.
-  float f[Q];
-#pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
-    const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0)) +
-                    (ez == 1 ? zo_p : (ez == -1 ? zo_m : 0));
-    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
-  }
-
+  const int cell = (z * ny + y) * nx + x;
   const V3 pos = {(float)x, (float)y, (float)z};
   float phi = 1e30f;
   V3 us = {0.f, 0.f, 0.f};
@@ -336,14 +333,14 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   // 4. Collide + sponge blend, 5. solid interior held at feq(1, u_body).
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    collide_store<L, Q, S>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, p.pk, fo_, n, cell);
+    collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, sink);
   } else {
     const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const float w = L::w(i);
       const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
-      Codec<S>::st(fo_ + (int64_t)i * n + cell, w * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq), i, p.pk);
+      sink.put(i, w * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq));
     }
   }
   if (p.write_mac) {
@@ -385,6 +382,37 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
     cf.ty = rz * fbx - rx * fbz;
     cf.tz = rx * fby - ry * fbx;
   }
+}
+
+
+template <int Q, typename S>
+__device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
+                                      float *__restrict__ mac, const StepParams &p, int x, int y,
+                                      int z, bool force, CellForce &cf) {
+  using L = Lattice<Q>;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int64_t n = p.n;
+  const S *fi = fin + p.base;
+  S *fo_ = fout + p.base;
+  const int nxny = nx * ny;
+  const int cell = z * nxny + y * nx + x;
+  // Offset of the pull source for e = +1 / -1 on each axis, periodic.
+  const int xo_p = x == 0 ? nx - 1 : -1, xo_m = x == nx - 1 ? 1 - nx : 1;
+  const int yo_p = y == 0 ? (ny - 1) * nx : -nx, yo_m = y == ny - 1 ? (1 - ny) * nx : nx;
+  const int zo_p = z == 0 ? (nz - 1) * nxny : -nxny, zo_m = z == nz - 1 ? (1 - nz) * nxny : nxny;
+
+  // 1. Pull-stream from the periodic sources.
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
+    const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0)) +
+                    (ez == 1 ? zo_p : (ez == -1 ? zo_m : 0));
+    f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
+  }
+
+  MemSink<S> sink{fo_, n, cell, p.pk};
+  cell3_core<Q, S>(fi, f, mac, p, x, y, z, force, cf, sink);
 }
 
 // ---- 2D cell update (D2Q9) ---------------------------------------------------
@@ -473,7 +501,8 @@ __device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__
   }
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    collide_store<L, 9, S>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, p.pk, fo_, n, cell);
+    MemSink<S> sink{fo_, n, cell, p.pk};
+    collide_store<L, 9>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, sink);
   } else {
     const float ussq = usx * usx + usy * usy;
 #pragma unroll

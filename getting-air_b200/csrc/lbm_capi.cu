@@ -260,6 +260,20 @@ int lbm_read_f(lbm_session *s, float *f) {
   return LBM_OK;
 }
 
+int lbm_write_f_raw(lbm_session *s, const void *planes) {
+  if (!s || !planes) return s ? fail(s, LBM_EINVAL, "planes is NULL") : LBM_EINVAL;
+  CK(s, cudaMemcpyAsync(s->f[s->cur], planes, (size_t)s->q * s->n * s->elem, cudaMemcpyHostToDevice, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+int lbm_read_f_raw(lbm_session *s, void *planes) {
+  if (!s || !planes) return s ? fail(s, LBM_EINVAL, "planes is NULL") : LBM_EINVAL;
+  CK(s, cudaMemcpyAsync(planes, s->f[s->cur], (size_t)s->q * s->n * s->elem, cudaMemcpyDeviceToHost, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
 int lbm_read_mac(lbm_session *s, float *mac) {
   if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
   CK(s, cudaMemcpyAsync(mac, s->mac, (size_t)s->n * 16, cudaMemcpyDeviceToHost, s->stream));

@@ -145,6 +145,15 @@ int lbm_init_macro(lbm_session *s, const float *mac);
 int lbm_write_f(lbm_session *s, const float *f);
 int lbm_read_f(lbm_session *s, float *f);
 
+/* Writes / reads the populations exactly as stored: Q planes of ncells
+ * elements of the session's storage type (4 bytes for FP32, 2 for the
+ * 16-bit storages, which hold (f - off_i) * scale). An exact checkpoint of a
+ * packed session, with no re-quantisation; for FP32 the same as
+ * lbm_write_f / lbm_read_f. Synchronous. No reference counterpart (the
+ * reference's snapshots carry f32 or f16 planes, f-pack.mjs:6-17). */
+int lbm_write_f_raw(lbm_session *s, const void *planes);
+int lbm_read_f_raw(lbm_session *s, void *planes);
+
 /* Reads the macroscopic field of the last step (4 floats per cell). */
 int lbm_read_mac(lbm_session *s, float *mac);
 

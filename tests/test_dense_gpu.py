@@ -257,20 +257,49 @@ def test_init_macro_matches_oracle_init(lbm, oracle):
 
 @pytest.mark.parametrize("storage", ["fp16", "bf16"])
 def test_packed_storage_error_is_bounded(lbm, oracle, storage):
-    """Equilibrium-offset 16-bit storage against the FP64 oracle: the error
-    is the storage quantum, so it is bounded loosely and reported."""
+    """16-bit storage holds (f - feq(1, U_far)) * scale: the round trip is
+    within the 16-bit quantum of that deviation, and the velocity after 200
+    steps stays within the stated bound of the FP64 oracle (1e-4 for FP16,
+    1e-3 for BF16; north_star asks for 1e-3)."""
     from getting_air_b200 import scenarios as sc
     s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40, storage=storage)
     f0 = oracle.init_eq(19, s["mac"], fp32=True).astype(np.float32)
     sol = lbm.Solver.create(19, s["dims"], **s["kw"])
     sol.write_f(f0)
     back = sol.read_f()
-    w = lbm.lattice_tables(19)["w"][:, None]
+    t = lbm.lattice_tables(19)
+    eu = t["ex"] * 0.05
+    off = (t["w"] * (1 + 3 * eu + 4.5 * eu * eu - 1.5 * 0.05 ** 2)).astype(np.float32)[:, None]
     quantum = 2.0 ** -11 if storage == "fp16" else 2.0 ** -8
-    assert np.abs(back - f0).max() <= quantum * np.abs(f0 - w).max() + 1e-12
-    sol.step(20)
+    assert (np.abs(back - f0) <= quantum * np.abs(f0 - off) * 1.0001 + 2.0 ** -34).all()
+    sol.step(200)
     m = sol.read_mac().astype(np.float64)
-    _, om, _ = oracle.run(sol.cfg, back.astype(np.float64), 20)
+    _, om, _ = oracle.run(sol.cfg, back.astype(np.float64), 200)
     err = rel_l2(m[:, 1:4], om[:, 1:4])
-    assert err <= (2e-3 if storage == "fp16" else 2e-2), err
+    assert err <= (1e-4 if storage == "fp16" else 1e-3), err
     sol.close()
+
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+def test_raw_planes_give_an_exact_restart(lbm, oracle, storage):
+    """lbm_read_f_raw / lbm_write_f_raw move the stored planes verbatim, so a
+    second session restarted from them continues bit for bit (a decode and
+    re-encode through the f32 wire format would re-quantise)."""
+    from getting_air_b200 import scenarios as sc
+    s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40, storage=storage, force=(1e-6, 0.0, 0.0))
+    a = lbm.Solver.create(19, s["dims"], **s["kw"])
+    a.init_macro(s["mac"])
+    a.step(7)
+    raw = a.read_f_raw()
+    assert raw.dtype == (np.float32 if storage == "fp32" else np.uint16)
+    b = lbm.Solver.create(19, s["dims"], **s["kw"])
+    b.write_f_raw(raw)
+    assert np.array_equal(b.read_f_raw(), raw)
+    a.step(5)
+    b.step(5)
+    assert np.array_equal(a.read_f_raw(), b.read_f_raw())
+    assert np.array_equal(a.read_mac(), b.read_mac())
+    assert np.array_equal(a.forces(), b.forces())
+    a.close()
+    b.close()
