@@ -49,6 +49,28 @@ class Body(C.Structure):
                 ("a", C.c_float), ("b", C.c_float), ("c", C.c_float), ("r", C.c_float)]
 
 
+class BodyState(C.Structure):
+    """lbm_body_state: FP64 state of a free rigid body (d3-body.mjs makeBodyState)."""
+    _fields_ = [("x", C.c_double * 3), ("q", C.c_double * 4), ("v", C.c_double * 3), ("L", C.c_double * 3),
+                ("omega", C.c_double * 3), ("d", C.c_double * 3), ("force", C.c_double * 3),
+                ("torque", C.c_double * 3), ("mass", C.c_double), ("ibody", C.c_double * 3),
+                ("steps", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        out = {k: np.array(getattr(self, k)[:]) for k in ("x", "q", "v", "L", "omega", "d", "force", "torque",
+                                                          "ibody")}
+        out["mass"] = float(self.mass)
+        out["steps"] = int(self.steps)
+        return out
+
+
+class BodyOpts(C.Structure):
+    """lbm_body_opts: the integrator's gravity, clamps, window wrap and switches."""
+    _fields_ = [("gravity", C.c_double * 3), ("v_max", C.c_double), ("o_max", C.c_double),
+                ("wrap", C.c_double * 3), ("planar", C.c_int32), ("no_fluid_force", C.c_int32),
+                ("pinned", C.c_int32), ("reserved", C.c_int32)]
+
+
 class Amr2DConfig(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("levels", C.c_int32), ("rb", C.c_int32),
                 ("tau", C.c_float), ("max_slots", C.c_int32), ("use_bounceback", C.c_int32),
@@ -153,6 +175,11 @@ def _load() -> C.CDLL:
         "lbm_cascade21": ([C.POINTER(C.POINTER(C.c_uint8)), I, I, I], I),
         "lbm_lattice_tables": ([I, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), F, C.POINTER(C.c_int32)], I),
+        "lbm_set_free_body": ([P, C.POINTER(BodyState), C.POINTER(BodyOpts)], I),
+        "lbm_read_body_state": ([P, C.POINTER(BodyState)], I),
+        "lbm_body_opts_default": ([C.POINTER(BodyOpts)], None),
+        "lbm_body_state_make": ([C.POINTER(Body), C.c_double, C.POINTER(BodyState)], I),
+        "lbm_body_advance": ([C.POINTER(BodyState), D, D, C.POINTER(BodyOpts), I], I),
         "lbm_f32_to_f16_bits": ([C.c_float], C.c_uint16),
         "lbm_f16_bits_to_f32": ([C.c_uint16], C.c_float),
     }
@@ -318,6 +345,17 @@ class Solver:
     def set_body(self, body: Body):
         self._check(lib.lbm_set_body(self._h, C.byref(body)))
 
+    def set_free_body(self, state: "BodyState | None", opts: "BodyOpts | None" = None):
+        """Integrate the body on the device from now on (force pass, 6-DOF
+        update, step); None returns it to the config's prescribed pose."""
+        self._check(lib.lbm_set_free_body(self._h, C.byref(state) if state is not None else None,
+                                          C.byref(opts) if opts is not None else None))
+
+    def body_state(self) -> BodyState:
+        out = BodyState()
+        self._check(lib.lbm_read_body_state(self._h, C.byref(out)))
+        return out
+
     def forces(self) -> np.ndarray:
         out = np.zeros(6, np.float64)
         self._check(lib.lbm_forces(self._h, _ptr(out, C.c_double)))
@@ -339,6 +377,41 @@ class Solver:
 
     def device_bytes(self) -> int:
         return int(lib.lbm_device_bytes(self._h))
+
+
+def body_opts(**kw) -> BodyOpts:
+    """lbm_body_opts_default (v_max 0.2, o_max 0.1) with fields overridden;
+    v_max / o_max of math.inf switch a clamp off."""
+    o = BodyOpts()
+    lib.lbm_body_opts_default(C.byref(o))
+    for k, v in kw.items():
+        if isinstance(getattr(o, k), C.Array):
+            arr = getattr(o, k)
+            for j, x in enumerate(v):
+                arr[j] = x
+        else:
+            setattr(o, k, v)
+    return o
+
+
+def body_state(body: Body, density: float = 1.0) -> BodyState:
+    """makeBodyState for a 3D body pose (make_body(...))."""
+    out = BodyState()
+    rc = lib.lbm_body_state_make(C.byref(body), float(density), C.byref(out))
+    if rc:
+        raise LbmError(rc, "invalid body for a body state")
+    return out
+
+
+def body_advance(state: BodyState, opts: BodyOpts, n: int = 1, force=(0.0, 0.0, 0.0),
+                 torque=(0.0, 0.0, 0.0)) -> BodyState:
+    """n host steps of stepFreeBody under a constant load (in place; returns state)."""
+    f = np.ascontiguousarray(force, np.float64)
+    t = np.ascontiguousarray(torque, np.float64)
+    rc = lib.lbm_body_advance(C.byref(state), _ptr(f, C.c_double), _ptr(t, C.c_double), C.byref(opts), int(n))
+    if rc:
+        raise LbmError(rc, "invalid body state or options")
+    return state
 
 
 def config_from(q: int, dims, **kw) -> Config:

@@ -42,7 +42,7 @@ template <> struct Codec<__half> {
     return fmaf(__half2float(__ldg(p)), k.inv, k.off[i]);
   }
   static __device__ __forceinline__ void st(__half *p, float v, int i, const Pack &k) {
-    *p = __float2half_rn((v - k.off[i]) * k.scale);
+    *p = __float2half_rn(fmaf(v, k.scale, k.noff[i]));
   }
 };
 template <> struct Codec<__nv_bfloat16> {
@@ -50,7 +50,7 @@ template <> struct Codec<__nv_bfloat16> {
     return fmaf(__bfloat162float(__ldg(p)), k.inv, k.off[i]);
   }
   static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, int i, const Pack &k) {
-    *p = __float2bfloat16_rn((v - k.off[i]) * k.scale);
+    *p = __float2bfloat16_rn(fmaf(v, k.scale, k.noff[i]));
   }
 };
 
@@ -84,7 +84,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm) {
 // last of `nparts` to do so, sums all partials in index order into `out` and
 // re-arms the ticket counter for the next step.
 template <int NV, int THREADS>
-__device__ void finish_sum(const double (&v)[NV], double *partials, unsigned int *counter,
+__device__ bool finish_sum(const double (&v)[NV], double *partials, unsigned int *counter,
                            int nparts, int part, double *out, double *sm) {
   __shared__ bool s_last;
   if (threadIdx.x == 0) {
@@ -95,7 +95,7 @@ __device__ void finish_sum(const double (&v)[NV], double *partials, unsigned int
     s_last = (ticket == (unsigned int)(nparts - 1));
   }
   __syncthreads();
-  if (!s_last) return;
+  if (!s_last) return false;
   __threadfence();
   double acc[NV];
 #pragma unroll
@@ -109,6 +109,7 @@ __device__ void finish_sum(const double (&v)[NV], double *partials, unsigned int
     for (int k = 0; k < NV; ++k) out[k] = acc[k];
     *counter = 0u;
   }
+  return true;
 }
 
 __device__ __forceinline__ float sponge_weight(float d, float sw) {
@@ -144,8 +145,9 @@ struct ForceAcc {
   }
 };
 
+// Returns true in the block that summed the partials (the last to finish).
 template <int THREADS>
-__device__ __forceinline__ void reduce_force(const ForceAcc &a, double *partials, unsigned int *counter,
+__device__ __forceinline__ bool reduce_force(const ForceAcc &a, double *partials, unsigned int *counter,
                                              int nparts, int part, double *out) {
   __shared__ double sm[kForceSlots * (THREADS / 32)];
   double v[kForceSlots];
@@ -154,16 +156,21 @@ __device__ __forceinline__ void reduce_force(const ForceAcc &a, double *partials
   v[6] = a.bad;
   v[7] = 0.0;
   block_sum<kForceSlots, THREADS>(v, sm);
-  finish_sum<kForceSlots, THREADS>(v, partials, counter, nparts, part, out, sm);
+  return finish_sum<kForceSlots, THREADS>(v, partials, counter, nparts, part, out, sm);
 }
 
-// The BGK collision with Guo forcing, written over opposite pairs (e, -e):
-//   feq(+-e)  = w rho (1 - 1.5 u.u + 4.5 (e.u)^2)  +-  3 w rho (e.u)
-//   S(+-e)    = (1 - omega/2) w (9 (e.F)(e.u) - 3 u.F)  +-  3 (1 - omega/2) w (e.F)
-// so one pair costs one symmetric and one antisymmetric term. f_out =
-// (1 - omega) f + omega feq + S, then the sponge blend f_out + s (f_far - f_out).
-// Same algebra as the reference's per-direction form
-// (common_d3_step.wgsl:331-357), reassociated.
+// The BGK collision with Guo forcing and the sponge blend, written over
+// opposite pairs (e, -e). With a = (1-s) omega rho, b = (1-s)(1 - omega/2)
+// (s the sponge weight) and per direction eu = e.u, eF = e.F:
+//   (1-s)[omega feq + S](+-e) = w (A +- B),
+//     A = c0 + eu (4.5 a eu + 9 b eF),   c0 = a (1 - 1.5 u.u) - 3 b u.F
+//     B = 3 a eu + 3 b eF
+//   f_out(+-e) = (1-s)(1-omega) f(+-e) + s f_far(+-e) + w (A +- B).
+// The products of w with a, b and c0 are formed once per weight class, so
+// a pair costs about a dozen FP32 instructions. Outside the sponge (s = 0)
+// this is the plain BGK + Guo update. The reference's per-direction form
+// (common_d3_step.wgsl:331-357) and mix() blend (common_sponge.wgsl:7-11),
+// reassociated.
 // Where a cell's post-collision populations go: MemSink stores them (the
 // step); NullSink drops them (a force-only pass, whose collision the
 // compiler then removes as dead code).
@@ -183,16 +190,13 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
                                               float Fy, float Fz, float omg, float spw, const float *ftarget,
                                               Sink &sink) {
   const float usq = ux * ux + uy * uy + uz * uz;
-  const float base = 1.0f - 1.5f * usq;
-  const float uF3 = 3.0f * (ux * Fx + uy * Fy + uz * Fz);
-  const float sfac = 1.0f - 0.5f * omg;
-  const float keep = 1.0f - omg;
-  {
-    const float w = L::w(0);
-    const float fc = fmaf(keep, f[0], fmaf(omg, (w * rho) * base, -(sfac * w) * uF3));
-    const float out = spw > 0.f ? fmaf(spw, ftarget[0] - fc, fc) : fc;
-    sink.put(0, out);
-  }
+  const float uF = ux * Fx + uy * Fy + uz * Fz;
+  const float ks = 1.0f - spw;
+  const float a = (omg * ks) * rho;
+  const float b = (1.0f - 0.5f * omg) * ks;
+  const float keep = (1.0f - omg) * ks;
+  const float c0 = fmaf(a, fmaf(-1.5f, usq, 1.0f), -3.0f * b * uF);
+  sink.put(0, fmaf(keep, f[0], fmaf(spw, ftarget[0], L::w(0) * c0)));
 #pragma unroll
   for (int i = 1; i < Q; ++i) {
     const int j = L::opp(i);
@@ -201,16 +205,11 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
     const float w = L::w(i);
     const float eu = ex * ux + ey * uy + ez * uz;
     const float eF = ex * Fx + ey * Fy + ez * Fz;
-    const float wr = w * rho, ws = sfac * w;
-    const float sym = wr * fmaf(4.5f * eu, eu, base);
-    const float anti = (3.0f * wr) * eu;
-    const float symS = ws * fmaf(9.0f * eF, eu, -uF3);
-    const float antiS = (3.0f * ws) * eF;
-    const float A = fmaf(omg, sym, symS), B = fmaf(omg, anti, antiS);
-    const float fci = fmaf(keep, f[i], A + B);
-    const float fcj = fmaf(keep, f[j], A - B);
-    sink.put(i, spw > 0.f ? fmaf(spw, ftarget[i] - fci, fci) : fci);
-    sink.put(j, spw > 0.f ? fmaf(spw, ftarget[j] - fcj, fcj) : fcj);
+    const float t = fmaf((9.0f * w) * b, eF, ((4.5f * w) * a) * eu);
+    const float A = fmaf(eu, t, w * c0);
+    const float B = fmaf((3.0f * w) * a, eu, ((3.0f * w) * b) * eF);
+    sink.put(i, fmaf(keep, f[i], fmaf(spw, ftarget[i], A + B)));
+    sink.put(j, fmaf(keep, f[j], fmaf(spw, ftarget[j], A - B)));
   }
 }
 
@@ -385,24 +384,19 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
 }
 
 
+// Pull gather of one cell from the periodic sources.
 template <int Q, typename S>
-__device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
-                                      float *__restrict__ mac, const StepParams &p, int x, int y,
-                                      int z, bool force, CellForce &cf) {
+__device__ __forceinline__ void gather3(const S *__restrict__ fi, const StepParams &p, int x, int y, int z,
+                                        float (&f)[Q]) {
   using L = Lattice<Q>;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int64_t n = p.n;
-  const S *fi = fin + p.base;
-  S *fo_ = fout + p.base;
   const int nxny = nx * ny;
   const int cell = z * nxny + y * nx + x;
   // Offset of the pull source for e = +1 / -1 on each axis, periodic.
   const int xo_p = x == 0 ? nx - 1 : -1, xo_m = x == nx - 1 ? 1 - nx : 1;
   const int yo_p = y == 0 ? (ny - 1) * nx : -nx, yo_m = y == ny - 1 ? (1 - ny) * nx : nx;
   const int zo_p = z == 0 ? (nz - 1) * nxny : -nxny, zo_m = z == nz - 1 ? (1 - nz) * nxny : nxny;
-
-  // 1. Pull-stream from the periodic sources.
-  float f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
@@ -410,9 +404,29 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
                     (ez == 1 ? zo_p : (ez == -1 ? zo_m : 0));
     f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
   }
+}
 
-  MemSink<S> sink{fo_, n, cell, p.pk};
+template <int Q, typename S>
+__device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
+                                      float *__restrict__ mac, const StepParams &p, int x, int y,
+                                      int z, bool force, CellForce &cf) {
+  const S *fi = fin + p.base;
+  float f[Q];
+  gather3<Q, S>(fi, p, x, y, z, f);
+  MemSink<S> sink{fout + p.base, p.n, (z * p.ny + y) * p.nx + x, p.pk};
   cell3_core<Q, S>(fi, f, mac, p, x, y, z, force, cf, sink);
+}
+
+// Force contribution of one cell without the collision (a free body's
+// force pass).
+template <int Q, typename S>
+__device__ __forceinline__ void cell3_force(const S *__restrict__ fin, const StepParams &p, int x, int y, int z,
+                                            CellForce &cf) {
+  const S *fi = fin + p.base;
+  float f[Q];
+  gather3<Q, S>(fi, p, x, y, z, f);
+  NullSink sink;
+  cell3_core<Q, S>(fi, f, nullptr, p, x, y, z, true, cf, sink);
 }
 
 // ---- 2D cell update (D2Q9) ---------------------------------------------------

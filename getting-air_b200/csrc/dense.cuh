@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../../include/lbm.h"
+#include "body.cuh"
 
 namespace lbm {
 
@@ -13,8 +14,12 @@ namespace lbm {
 // rest state replaced by the free stream: the stored value is the flow's
 // deviation from it), and scale = 2^10 for FP16 keeps small deviations out
 // of the subnormal range. Unused by FP32 storage.
+// noff[i] = -off[i] * scale (exact: scale is a power of two), so that the
+// encode is one fused multiply-add, fma(f, scale, noff[i]) = (f - off) *
+// scale to the bit.
 struct Pack {
   float off[27];
+  float noff[27];
   float scale, inv;
 };
 
@@ -46,6 +51,12 @@ struct StepParams {
   // Multi-domain launches: the domain's first tile, and the tile range
   // [ft0, ft1) (relative to tile0) whose cells can see the body.
   int tile0, ft0, ft1;
+  // Free body (dense 3D only; all NULL otherwise): the pose this launch
+  // reads (and for a force pass, the pose its last block writes) and the
+  // integrator state.
+  const BodyPose *pose_in;
+  BodyPose *pose_out;
+  BodyDyn *dyn;
 };
 
 // Launch shape of the dense step (threads per CTA along x, and the CTAs per
@@ -66,6 +77,11 @@ constexpr int kTotalsSlots = 8;
 // storage: 0 fp32, 1 fp16 offset, 2 bf16 offset
 cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float *mac,
                         const StepParams &p, cudaStream_t st);
+// Free-body force pass: the cells near the body (pose p.pose_in), FP64
+// force/torque into p.force_out, then the body integrated into p.pose_out.
+// `cap` is the launch grid (the largest box, in blocks).
+cudaError_t launch_force_pass(int q, int storage, const void *f_in, const StepParams &p, const int cap[3],
+                              cudaStream_t st);
 cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n, const Pack &pk,
                            cudaStream_t st);
 cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n, const Pack &pk,

@@ -38,9 +38,8 @@ namespace {
 // row and plane come straight from blockIdx, no division.
 
 template <int Q, typename S>
-__global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
-    d3_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
-            const __grid_constant__ StepParams p) {
+__device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__restrict__ fout,
+                                              float *__restrict__ mac, const StepParams &p) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x;
   const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
   const bool region = p.force_on && bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1 &&
@@ -54,6 +53,99 @@ __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) /
     acc.add(cf);
     reduce_force<kStepThreads>(acc, p.partials, p.counter, rx * ry * rz, part, p.force_out);
   }
+}
+
+// A copy of the launch's parameters in shared memory with the body pose,
+// swept-cell band and force region of this step taken from the device
+// (free-body launches, where the pose is produced on the device).
+__device__ __forceinline__ void stage_pose(const StepParams &p, StepParams &sp) {
+  const unsigned *src = reinterpret_cast<const unsigned *>(&p);
+  unsigned *dst = reinterpret_cast<unsigned *>(&sp);
+  for (int k = threadIdx.x; k < (int)(sizeof(StepParams) / 4); k += blockDim.x) dst[k] = src[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const BodyPose &bp = *p.pose_in;
+    sp.body = bp.body;
+    sp.swept = bp.swept;
+    sp.swept_band = bp.swept_band;
+    sp.rbx0 = bp.box[0] / kStepThreads;
+    sp.rbx1 = bp.box[1] / kStepThreads + 1;
+    sp.rby0 = bp.box[2];
+    sp.rby1 = bp.box[3] + 1;
+    sp.rbz0 = bp.box[4];
+    sp.rbz1 = bp.box[5] + 1;
+  }
+  __syncthreads();
+}
+
+template <int Q, typename S>
+__global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
+    d3_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
+            const __grid_constant__ StepParams p) {
+  d3_step_block<Q, S>(fin, fout, mac, p);
+}
+
+// The step of a free body: the pose comes from the device (written by the
+// force pass just before); no force reduction.
+template <int Q, typename S>
+__global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
+    d3_step_free(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
+                 const __grid_constant__ StepParams p) {
+  __shared__ StepParams sp;
+  stage_pose(p, sp);
+  d3_step_block<Q, S>(fin, fout, mac, sp);
+}
+
+// Integrates the free body under the force just summed and publishes the
+// next pose with its force box (clipped to the launch capacity; a body
+// outside the domain keeps one block so the integrator still runs).
+__device__ __noinline__ void integrate_and_publish(BodyDyn *dyn, const double *force, BodyPose *next) {
+  const double F[3] = {force[0], force[1], force[2]}, T[3] = {force[3], force[4], force[5]};
+  body_step(dyn->st, F, T, dyn->opt);
+  BodyPose np;
+  np.body = body_pose(dyn->shape, dyn->st);
+  int box[6];
+  if (!body_cell_box(np.body, dyn->q, dyn->nx, dyn->ny, dyn->nz, dyn->bounceback, dyn->swept_force, dyn->chi_eps,
+                     box, &np.swept, &np.swept_band)) {
+    const float c[3] = {np.body.cx, np.body.cy, np.body.cz};
+    const int len[3] = {dyn->nx, dyn->ny, dyn->nz};
+    for (int a = 0; a < 3; ++a) {
+      const int v = (int)fminf(fmaxf(c[a], 0.f), (float)(len[a] - 1));
+      box[2 * a] = box[2 * a + 1] = v;
+    }
+  }
+  const int unit[3] = {kStepThreads, 1, 1};
+  for (int a = 0; a < 3; ++a) {
+    const int b0 = box[2 * a] / unit[a], b1 = box[2 * a + 1] / unit[a];
+    if (b1 - b0 + 1 > dyn->cap[a]) {
+      box[2 * a + 1] = (b0 + dyn->cap[a]) * unit[a] - 1;
+      dyn->overflow += 1;
+    }
+  }
+  for (int k = 0; k < 6; ++k) np.box[k] = box[k];
+  *next = np;
+}
+
+// Free-body force pass over the blocks of the current force box (the
+// launch grid is the largest box; blocks past this step's box leave at
+// once and take no part in the reduction). The last block to finish sums
+// the partials and integrates the body.
+template <int Q, typename S>
+__global__ void __launch_bounds__(kStepThreads)
+    d3_force_pass(const S *__restrict__ fin, const __grid_constant__ StepParams p) {
+  __shared__ StepParams sp;
+  stage_pose(p, sp);
+  const int bx = sp.rbx0 + blockIdx.x, by = sp.rby0 + blockIdx.y, bz = sp.rbz0 + blockIdx.z;
+  if (bx >= sp.rbx1 || by >= sp.rby1 || bz >= sp.rbz1) return;
+  const int x = bx * kStepThreads + threadIdx.x;
+  CellForce cf;
+  if (x < sp.nx) cell3_force<Q, S>(fin, sp, x, by, bz, cf);
+  const int rx = sp.rbx1 - sp.rbx0, ry = sp.rby1 - sp.rby0, rz = sp.rbz1 - sp.rbz0;
+  const int part = ((int)blockIdx.z * ry + (int)blockIdx.y) * rx + (int)blockIdx.x;
+  ForceAcc acc;
+  acc.add(cf);
+  const bool last = reduce_force<kStepThreads>(acc, sp.partials, sp.counter, rx * ry * rz, part, sp.force_out);
+  if (last && threadIdx.x == 0) integrate_and_publish(sp.dyn, sp.force_out, sp.pose_out);
 }
 
 template <typename S>
@@ -225,8 +317,19 @@ cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float
   LBM_DISPATCH(q, storage, {
     if constexpr (Q == 9)
       d2_step<S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+    else if (p.pose_in)
+      d3_step_free<Q, S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
     else
       d3_step<Q, S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+  });
+}
+
+cudaError_t launch_force_pass(int q, int storage, const void *f_in, const StepParams &p, const int cap[3],
+                              cudaStream_t st) {
+  if (q == 9 || !p.pose_in || !p.pose_out || !p.dyn) return cudaErrorInvalidValue;
+  dim3 grid(cap[0], cap[1], cap[2]);
+  LBM_DISPATCH(q, storage, {
+    if constexpr (Q != 9) d3_force_pass<Q, S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, p);
   });
 }
 

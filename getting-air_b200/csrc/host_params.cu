@@ -12,14 +12,6 @@ void dir_of(int q, int i, int &ex, int &ey, int &ez) {
   if (q == 9) { ex = Lattice<9>::ex(i); ey = Lattice<9>::ey(i); ez = 0; }
   else { ex = Lattice<27>::ex(i); ey = Lattice<27>::ey(i); ez = Lattice<27>::ez(i); }
 }
-float circumradius(const lbm_body &b) {
-  switch (b.shape) {
-    case LBM_SHAPE_SPHERE: return b.a;
-    case LBM_SHAPE_SPHEROID: return std::fmax(b.a, b.c);
-    case LBM_SHAPE_ELLIPSE: return std::fmax(b.a, b.b);
-    default: return std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c);
-  }
-}
 }  // namespace
 
 float lattice_weight(int q, int i) {
@@ -59,6 +51,7 @@ Pack make_pack(const lbm_config &c) {
   }
   k.scale = c.storage == LBM_STORE_FP16 ? 1024.0f : 1.0f;
   k.inv = 1.0f / k.scale;
+  for (int i = 0; i < 27; ++i) k.noff[i] = -k.off[i] * k.scale;
   return k;
 }
 
@@ -95,28 +88,8 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
 
 bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]) {
   if (!c.has_body) return false;
-  const lbm_body &b = c.body;
-  const float rc = circumradius(b);
-  const float speed = std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
-                      std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc;
-  p.swept = (c.q != 9 && c.use_bounceback && c.swept_force && speed > 0.f) ? 1 : 0;
-  p.swept_band = 2.0f + speed;
-  // |e| <= sqrt(3) for a bounce-back link, the one-step sweep for the
-  // swept-cell term, and chi < 1e-6 beyond ~6.9 band widths for the penalty.
-  const float margin = c.use_bounceback ? (3.0f + speed) : (8.0f * c.chi_eps + 2.0f);
-  const float reach = rc + margin;
-  auto range = [&](float centre, int len, bool periodic_image, int &lo, int &hi) {
-    int a = (int)std::floor(centre - reach), e = (int)std::ceil(centre + reach);
-    if (periodic_image && (a < 0 || e > len - 1)) { lo = 0; hi = len - 1; return; }
-    lo = a < 0 ? 0 : a;
-    hi = e > len - 1 ? len - 1 : e;
-  };
-  const bool wrap2d = (c.q == 9);  // the 2D SDF takes the nearest periodic image
-  range(b.cx, c.nx, wrap2d, box[0], box[1]);
-  range(b.cy, c.ny, wrap2d, box[2], box[3]);
-  box[4] = box[5] = 0;
-  if (c.q != 9) range(b.cz, c.nz, false, box[4], box[5]);
-  return box[0] <= box[1] && box[2] <= box[3] && box[4] <= box[5];
+  return body_cell_box(c.body, c.q, c.nx, c.ny, c.nz, c.use_bounceback, c.swept_force, c.chi_eps, box, &p.swept,
+                       &p.swept_band);
 }
 
 }  // namespace lbm

@@ -5,6 +5,7 @@
 // buffers (ping-pong), the mac field and the reduction scratch, and launches
 // on one CUDA stream.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +39,12 @@ struct lbm_session {
   StepParams sp{};
   int64_t bytes = 0;
   std::string err;
+  // Free body: two poses (by step parity) and the integrator state.
+  bool free_body = false;
+  int body_par = 0;
+  int cap[3] = {0, 0, 0};
+  BodyPose *pose = nullptr;
+  BodyDyn *dyn = nullptr;
 };
 
 namespace {
@@ -122,6 +129,8 @@ void release(lbm_session *s) {
   cudaFree(s->tot_partials);
   cudaFree(s->tot_counter);
   cudaFree(s->tot_out);
+  cudaFree(s->pose);
+  cudaFree(s->dyn);
   if (s->host_out) cudaFreeHost(s->host_out);
   if (s->own) cudaStreamDestroy(s->own);
 }
@@ -284,6 +293,25 @@ int lbm_read_mac(lbm_session *s, float *mac) {
 int lbm_step(lbm_session *s, int n) {
   if (!s) return LBM_EINVAL;
   if (n < 0) return fail(s, LBM_EINVAL, "step count must be >= 0");
+  if (s->free_body) {
+    for (int k = 0; k < n; ++k) {
+      StepParams fp = s->sp;
+      fp.pose_in = s->pose + s->body_par;
+      fp.pose_out = s->pose + (1 - s->body_par);
+      fp.dyn = s->dyn;
+      fp.force_on = 1;
+      fp.write_mac = 0;
+      CK(s, launch_force_pass(s->q, s->storage, s->f[s->cur], fp, s->cap, s->stream));
+      StepParams sp = s->sp;
+      sp.pose_in = s->pose + (1 - s->body_par);
+      sp.force_on = 0;
+      sp.write_mac = (k == n - 1);
+      CK(s, launch_step(s->q, s->storage, s->f[s->cur], s->f[1 - s->cur], s->mac, sp, s->stream));
+      s->cur = 1 - s->cur;
+      s->body_par = 1 - s->body_par;
+    }
+    return LBM_OK;
+  }
   for (int k = 0; k < n; ++k) {
     s->sp.write_mac = (k == n - 1);
     CK(s, launch_step(s->q, s->storage, s->f[s->cur], s->f[1 - s->cur], s->mac, s->sp, s->stream));
@@ -299,6 +327,7 @@ int lbm_set_body(lbm_session *s, const lbm_body *body) {
   std::string why;
   if (validate_config(&c, why)) return fail(s, LBM_EINVAL, why);
   s->cfg = c;
+  s->free_body = false;
   fill_params(s);
   int rc = ensure_force_scratch(s);
   if (rc) return rc;
@@ -306,9 +335,99 @@ int lbm_set_body(lbm_session *s, const lbm_body *body) {
   return LBM_OK;
 }
 
+int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_body_opts *opts) {
+  if (!s) return LBM_EINVAL;
+  if (!state) {
+    s->free_body = false;
+    return LBM_OK;
+  }
+  const lbm_config &c = s->cfg;
+  if (c.q == 9) return fail(s, LBM_ENOTSUP, "free bodies are 3D only");
+  if (!c.has_body) return fail(s, LBM_EINVAL, "the session has no body");
+  const lbm_body_state &st = *state;
+  bool ok = st.mass > 0.0 && std::isfinite(st.mass);
+  for (int k = 0; k < 3; ++k)
+    ok = ok && st.ibody[k] > 0.0 && std::isfinite(st.ibody[k]) && std::isfinite(st.x[k]) &&
+         std::isfinite(st.v[k]) && std::isfinite(st.L[k]);
+  const double qn = st.q[0] * st.q[0] + st.q[1] * st.q[1] + st.q[2] * st.q[2] + st.q[3] * st.q[3];
+  if (!ok || !(qn > 0.5 && qn < 2.0)) return fail(s, LBM_EINVAL, "body state must be finite, massive and unit-quaternion");
+  lbm_body_opts o;
+  if (opts) o = *opts; else lbm_body_opts_default(&o);
+  BodyDyn d{};
+  d.st = st;
+  d.opt = o;
+  d.shape = c.body;
+  d.q = c.q; d.nx = c.nx; d.ny = c.ny; d.nz = c.nz;
+  d.bounceback = c.use_bounceback;
+  d.swept_force = c.swept_force;
+  d.chi_eps = c.chi_eps;
+  // Largest force box the body can need: its reach at the clamped speeds
+  // (the whole domain when a clamp is off).
+  const double rc = body_circumradius(c.body);
+  const double vmax = (o.v_max > 0.0 && std::isfinite(o.v_max)) ? o.v_max : INFINITY;
+  const double omax = (o.o_max > 0.0 && std::isfinite(o.o_max)) ? o.o_max : INFINITY;
+  const double speed = vmax + 1.5 * omax * rc + 0.5;
+  const double margin = c.use_bounceback ? 3.0 + speed : 8.0 * c.chi_eps + 2.0;
+  const double cells = 2.0 * std::ceil(rc + margin) + 3.0;
+  const int nbx = (c.nx + kStepThreads - 1) / kStepThreads;
+  d.cap[0] = std::isfinite(cells) ? (int)std::min<double>(nbx, std::ceil(cells / kStepThreads) + 1) : nbx;
+  d.cap[1] = std::isfinite(cells) ? (int)std::min<double>(c.ny, cells) : c.ny;
+  d.cap[2] = std::isfinite(cells) ? (int)std::min<double>(c.nz, cells) : c.nz;
+  BodyPose p0{};
+  p0.body = body_pose(c.body, st);
+  int box[6];
+  if (!body_cell_box(p0.body, c.q, c.nx, c.ny, c.nz, c.use_bounceback, c.swept_force, c.chi_eps, box, &p0.swept,
+                     &p0.swept_band)) {
+    const float ctr[3] = {p0.body.cx, p0.body.cy, p0.body.cz};
+    const int len[3] = {c.nx, c.ny, c.nz};
+    for (int a = 0; a < 3; ++a) {
+      const int v = (int)std::fmin(std::fmax(ctr[a], 0.f), (float)(len[a] - 1));
+      box[2 * a] = box[2 * a + 1] = v;
+    }
+  }
+  const int unit[3] = {kStepThreads, 1, 1};
+  for (int a = 0; a < 3; ++a) {
+    const int b0 = box[2 * a] / unit[a], b1 = box[2 * a + 1] / unit[a];
+    if (b1 - b0 + 1 > d.cap[a]) box[2 * a + 1] = (b0 + d.cap[a]) * unit[a] - 1;
+  }
+  for (int k = 0; k < 6; ++k) p0.box[k] = box[k];
+  const int need = d.cap[0] * d.cap[1] * d.cap[2];
+  if (need > s->force_nparts) {
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->force_partials);
+    s->bytes -= (int64_t)s->force_nparts * kForceSlots * 8;
+    s->force_partials = nullptr;
+    s->force_nparts = 0;
+    CK(s, cudaMalloc(&s->force_partials, (size_t)need * kForceSlots * sizeof(double)));
+    s->force_nparts = need;
+    s->bytes += (int64_t)need * kForceSlots * 8;
+    s->sp.partials = s->force_partials;
+  }
+  if (!s->pose) {
+    CK(s, cudaMalloc(&s->pose, 2 * sizeof(BodyPose)));
+    CK(s, cudaMalloc(&s->dyn, sizeof(BodyDyn)));
+    s->bytes += 2 * sizeof(BodyPose) + sizeof(BodyDyn);
+  }
+  CK(s, cudaMemcpyAsync(s->pose, &p0, sizeof(BodyPose), cudaMemcpyHostToDevice, s->stream));
+  CK(s, cudaMemcpyAsync(s->dyn, &d, sizeof(BodyDyn), cudaMemcpyHostToDevice, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 3; ++k) s->cap[k] = d.cap[k];
+  s->body_par = 0;
+  s->free_body = true;
+  return LBM_OK;
+}
+
+int lbm_read_body_state(lbm_session *s, lbm_body_state *out) {
+  if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  if (!s->free_body) return fail(s, LBM_EINVAL, "the body is not free (lbm_set_free_body)");
+  CK(s, cudaMemcpyAsync(out, &s->dyn->st, sizeof(lbm_body_state), cudaMemcpyDeviceToHost, s->stream));
+  CK(s, cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
 int lbm_forces(lbm_session *s, double out[6]) {
   if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
-  if (!s->sp.force_on) {
+  if (!s->sp.force_on && !s->free_body) {
     for (int k = 0; k < 6; ++k) out[k] = 0.0;
     return LBM_OK;
   }
@@ -321,7 +440,7 @@ int lbm_forces(lbm_session *s, double out[6]) {
 
 int lbm_forces_async(lbm_session *s, double out[6]) {
   if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
-  if (!s->sp.force_on) {
+  if (!s->sp.force_on && !s->free_body) {
     for (int k = 0; k < 6; ++k) out[k] = 0.0;
     return LBM_OK;
   }

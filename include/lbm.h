@@ -110,6 +110,36 @@ typedef struct {
 
 typedef struct lbm_session lbm_session;
 
+/* State of a free (integrated) 3D rigid body, FP64 -- d3-body.mjs
+ * makeBodyState (:300-307) and the BodyState3D fields d3_physics.wgsl
+ * advances. Quaternions are {w, x, y, z}, body -> world. */
+typedef struct {
+  double x[3];       /* centre, lattice units (wrapped on windowed axes)        */
+  double q[4];       /* orientation                                             */
+  double v[3];       /* linear velocity, cells per step                         */
+  double L[3];       /* angular momentum, world frame (the integrated state)    */
+  double omega[3];   /* angular velocity of the last step (its midpoint value)  */
+  double d[3];       /* displacement since the state was made, unwrapped        */
+  double force[3];   /* fluid force drained at the last step                    */
+  double torque[3];  /* fluid torque drained at the last step                   */
+  double mass;
+  double ibody[3];   /* principal moments of inertia (body axes)                */
+  int64_t steps;     /* steps integrated (pinned steps included)                */
+} lbm_body_state;
+
+/* Options of the integrator -- the override constants of d3_physics.wgsl
+ * (GX/GY/GZ, NO_FLUID_FORCE, PLANAR), the v_max / o_max limiters of
+ * BodyState3D and the moving window's wrap lengths (d3-window.mjs). */
+typedef struct {
+  double gravity[3];       /* uniform acceleration                             */
+  double v_max, o_max;     /* magnitude clamps; <= 0 (or inf) = none           */
+  double wrap[3];          /* per-axis wrap length of the position, 0 = none   */
+  int32_t planar;          /* no z translation, rotation about z only          */
+  int32_t no_fluid_force;  /* integrate without the fluid load (it is still recorded) */
+  int32_t pinned;          /* record the load, do not move                     */
+  int32_t reserved;        /* zero                                             */
+} lbm_body_opts;
+
 /* Library version string and ABI version. */
 const char *lbm_version(void);
 int lbm_abi_version(void);
@@ -166,6 +196,19 @@ int lbm_step(lbm_session *s, int n);
 
 /* Replaces the body pose/kinematics used by subsequent steps. */
 int lbm_set_body(lbm_session *s, const lbm_body *body);
+
+/* Makes the body free: from the next step on, every step is a force pass
+ * over the cells near the body (FP64 sum), the 6-DOF update of `state` under
+ * that load on the device, then the lattice step with the new pose -- the
+ * reference's force -> physics -> step order (main-3d.js:3122-3145,
+ * d3_physics.wgsl). The body's shape and size stay those of the session's
+ * config. 3D sessions with a body only. NULL state leaves the body free with
+ * its current device state replaced by nothing: it returns to the config's
+ * prescribed pose (as lbm_set_body does). */
+int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_body_opts *opts);
+
+/* Reads the free body's state after the queued steps (synchronous). */
+int lbm_read_body_state(lbm_session *s, lbm_body_state *out);
 
 /* Force and torque on the body from the most recent step, FP64:
  * out = {fx, fy, fz, tx, ty, tz}. Synchronous (one 48-byte readback).
@@ -342,6 +385,19 @@ int lbm_server_release(lbm_server *s, int64_t id);
 int lbm_server_stats(lbm_server *s, int64_t out[6]);
 
 /* ---- pure host functions (the reference's JS modules) ------------------- */
+
+/* Integrator defaults (packBodyState: v_max 0.2, o_max 0.1; no gravity,
+ * window, planar constraint or pinning). */
+void lbm_body_opts_default(lbm_body_opts *o);
+
+/* makeBodyState (d3-body.mjs:300): mass = density x volume, principal
+ * inertia, L from the pose's angular velocity. 3D shapes only. */
+int lbm_body_state_make(const lbm_body *pose, double density, lbm_body_state *out);
+
+/* `nsteps` of stepFreeBody (d3-body.mjs:244-290) under a constant load, on
+ * the host: the same code the device runs after each force pass. */
+int lbm_body_advance(lbm_body_state *s, const double force[3], const double torque[3], const lbm_body_opts *o,
+                     int nsteps);
 
 /* Lattice tables, lattice-2d.mjs:106-162 and lattice-3d.mjs:50-210:
  * velocity set, f32 weights (exact bits), opposite index. Arrays hold q

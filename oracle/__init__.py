@@ -39,6 +39,9 @@ def lib() -> C.CDLL:
         L.oracle_amr2d_set_topology.argtypes = [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                                 C.POINTER(C.c_int32), C.c_int32]
         L.oracle_amr2d_read.argtypes = [P, D, D, D, D, C.POINTER(C.c_int32), C.POINTER(C.c_float), D]
+        L.oracle_body_make.argtypes = [P, C.c_double, P]
+        L.oracle_body_step.argtypes = [P, D, D, P, I]
+        L.oracle_run_free.argtypes = [P, I, D, I, P, P, D, D, D]
         L.oracle_f16_bits.argtypes = [C.c_float]
         L.oracle_f16_bits.restype = C.c_uint16
         _LIB = L
@@ -149,3 +152,35 @@ class Amr2D:
         out["active"] = topo[o:o + n_act].copy(); o += self.S
         out["want"] = topo[o:o + self.nb].astype(np.uint32)
         return out
+
+
+def body_make(body, density: float = 1.0):
+    """makeBodyState (FP64) -> the product's BodyState structure type."""
+    from getting_air_b200 import BodyState  # the ctypes layout only
+    out = BodyState()
+    if lib().oracle_body_make(C.addressof(body), float(density), C.addressof(out)):
+        raise ValueError("bad body")
+    return out
+
+
+def body_step(state, opts, n: int = 1, force=(0.0, 0.0, 0.0), torque=(0.0, 0.0, 0.0)):
+    """n steps of stepFreeBody under a constant load, in place."""
+    f = np.ascontiguousarray(force, np.float64)
+    t = np.ascontiguousarray(torque, np.float64)
+    lib().oracle_body_step(C.addressof(state), _d(f), _d(t), C.addressof(opts), int(n))
+    return state
+
+
+def run_free(cfg, f0: np.ndarray, nsteps: int, state, opts, fp32: bool = False):
+    """Coupled free-body run: returns (f, mac, forces[nsteps, 8], traj[nsteps, 16]);
+    `state` is advanced in place. traj rows: x(3) v(3) L(3) omega(3) q(4)."""
+    f = np.ascontiguousarray(f0, np.float64).copy()
+    n = cfg.nx * cfg.ny * cfg.nz
+    mac = np.zeros((n, 4))
+    forces = np.zeros((nsteps, 8))
+    traj = np.zeros((nsteps, 16))
+    rc = lib().oracle_run_free(C.addressof(cfg), int(fp32), _d(f), int(nsteps), C.addressof(state),
+                               C.addressof(opts), _d(mac), _d(forces), _d(traj))
+    if rc:
+        raise ValueError("oracle_run_free failed")
+    return f, mac, forces, traj

@@ -32,6 +32,7 @@
 
 #include "../include/lbm.h"
 
+#include "body.h"
 #include "common.h"
 
 namespace {
@@ -294,9 +295,70 @@ void run(const lbm_config &c, double *f, int nsteps, double *mac, double *forces
   for (int64_t i = 0; i < tot; ++i) f[i] = (double)a[i];
 }
 
+// The free-body loop in the reference's order (main-3d.js encodeSteps):
+// force pass on f_t at pose P_t, the 6-DOF update to P_t+1, then the step
+// on f_t with P_t+1.
+template <class R>
+void run_free(const lbm_config &c0, double *f, int nsteps, RigidBody &body, const lbm_body_opts &o, double *mac,
+              double *forces, double *traj) {
+  lbm_config c = c0;
+  const int64_t N = (int64_t)c.nx * c.ny * c.nz;
+  const int64_t tot = N * c.q;
+  std::vector<R> a(tot), b(tot);
+  for (int64_t i = 0; i < tot; ++i) a[i] = R(f[i]);
+  for (int s = 0; s < nsteps; ++s) {
+    c.body = pose_of(c0.body, body);
+    double fo[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    force3<R>(c, a, fo);
+    if (forces) std::memcpy(forces + 8 * s, fo, sizeof(fo));
+    step_free_body(body, {fo[0], fo[1], fo[2]}, {fo[3], fo[4], fo[5]}, o);
+    if (traj) {
+      double *t = traj + 16 * s;
+      for (int k = 0; k < 3; ++k) { t[k] = body.x[k]; t[3 + k] = body.v[k]; t[6 + k] = body.L[k]; t[9 + k] = body.omega[k]; }
+      for (int k = 0; k < 4; ++k) t[12 + k] = body.q[k];
+    }
+    c.body = pose_of(c0.body, body);
+    double *m = (s == nsteps - 1) ? mac : nullptr;
+    step3<R>(c, a, b, m);
+    a.swap(b);
+  }
+  for (int64_t i = 0; i < tot; ++i) f[i] = (double)a[i];
+}
+
 }  // namespace
 
 extern "C" {
+
+// makeBodyState for a 3D pose.
+int oracle_body_make(const lbm_body *pose, double density, lbm_body_state *out) {
+  if (!pose || !out) return -1;
+  *out = lbm_body_state{};
+  to_state(make_body_state(*pose, density), *out);
+  return 0;
+}
+
+// `nsteps` of stepFreeBody under a constant load.
+int oracle_body_step(lbm_body_state *s, const double force[3], const double torque[3], const lbm_body_opts *o,
+                     int nsteps) {
+  if (!s || !o) return -1;
+  RigidBody r = from_state(*s);
+  for (int k = 0; k < nsteps; ++k) step_free_body(r, {force[0], force[1], force[2]}, {torque[0], torque[1], torque[2]}, *o);
+  to_state(r, *s);
+  return 0;
+}
+
+// The coupled free-body run (3D): f in place, the body state in place,
+// mac of the last step, per-step forces (8 each) and trajectory (16 each:
+// x, v, L, omega, q after the update), any of the three NULL.
+int oracle_run_free(const lbm_config *c, int fp32, double *f, int nsteps, lbm_body_state *state,
+                    const lbm_body_opts *o, double *mac, double *forces, double *traj) {
+  if (!c || !f || !state || !o || c->q == 9 || nsteps < 0) return -1;
+  RigidBody r = from_state(*state);
+  if (fp32) run_free<float>(*c, f, nsteps, r, *o, mac, forces, traj);
+  else run_free<double>(*c, f, nsteps, r, *o, mac, forces, traj);
+  to_state(r, *state);
+  return 0;
+}
 
 // Derived lattice tables (weights as exact f32 values).
 int oracle_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez, float *w, int32_t *opp) {
