@@ -26,7 +26,7 @@ def _cxx() -> str:
 
 def build() -> Path:
     srcs = [HERE / s for s in SOURCES]
-    deps = srcs + [HERE / "common.h", HERE / "body.h", HERE.parent / "include" / "lbm.h"]
+    deps = srcs + [HERE / "common.h", HERE / "body.h", HERE / "dense3.h", HERE.parent / "include" / "lbm.h"]
     if OUT.exists() and all(p.stat().st_mtime <= OUT.stat().st_mtime for p in deps):
         return OUT
     OUT.parent.mkdir(exist_ok=True)
