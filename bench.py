@@ -340,6 +340,39 @@ def time_amr(lbm, steps, warmup, world):
             "timing": "CUDA events around the macro-steps; topology readback between 16-step chunks"}
 
 
+def time_amr3d(lbm, steps, warmup, world):
+    """3D AMR sphere (sphere-amr-Re20-D16: D = 16 pinned sphere at (48, 64, 64)
+    in 192 x 128 x 128, u0 = 0.05, Re = 20, the blocks within 2 cells of it
+    refined, RB = 4). MLUPS counts L0 cells outside the refined blocks plus
+    two substeps of every refined interior cell per macro-step."""
+    import torch
+    from getting_air_b200 import scenarios as sc
+    s = sc.sphere(n=16, u0=0.05, re=20)
+    cfg = lbm.amr3d_config(19, s["dims"], refine="body", margin=2.0, **s["kw"])
+    a = lbm.Amr3D(cfg)
+    stream = torch.cuda.Stream()
+    a.set_stream(stream.cuda_stream)
+    a.init_macro(s["mac"])
+    a.step(max(warmup, 3))
+    a.sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    a.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    upd = a.cell_updates()
+    f = a.forces()
+    out = {"mlups": upd * steps * world / (ms * 1e-3) / 1e6, "ms_per_macro_step": ms / steps,
+           "cell_updates_per_macro_step": upd, "tiles": a.slots,
+           "cd_last_step": f[0] / (0.5 * 0.05 ** 2 * s["area"]),
+           "timing": "CUDA events around the macro-steps (graph-launched), pool force every macro-step"}
+    a.close()
+    return out
+
+
 def time_served(lbm, world, count=48, budget_gb=48):
     """Serving: a seeded Poisson stream (200 req/s) of D3Q19/D3Q27 sphere or
     rounded-box solves, N^3 with N log-uniform in [32, 192], 500-2000 steps,
@@ -485,6 +518,7 @@ def run_ours(args):
                          "fx_last": fo[0]}
         forms["batched"], forms["batched_plain"] = time_batched(lbm, args.steps, args.warmup, world)
         forms["amr2d_cylinder"] = time_amr(lbm, args.steps, args.warmup, world)
+        forms["amr3d_sphere"] = time_amr3d(lbm, args.steps, args.warmup, world)
         forms["served"], forms["served_plain"] = time_served(lbm, world)
         if rank == 0:
             forms["accuracy_vs_fp64"] = packed_accuracy(lbm)

@@ -96,6 +96,16 @@ class Config(C.Structure):
                 ("body", Body), ("storage", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
+class Amr3DConfig(C.Structure):
+    _fields_ = [("root", Config), ("levels", C.c_int32), ("rb", C.c_int32), ("refine", C.c_int32),
+                ("margin", C.c_float), ("boxfrac", C.c_float), ("explode_linear", C.c_int32),
+                ("dynamic", C.c_int32), ("manage_every", C.c_int32), ("manage_start", C.c_int32),
+                ("max_slots", C.c_int32), ("slot_headroom", C.c_float), ("reserved", C.c_int32 * 5)]
+
+
+REFINE = {"body": 0, "box": 1, "bar": 2, "slab": 3, "all": 4, "list": 5}
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is missing: build it with getting-air_b200/build.py "
@@ -180,6 +190,25 @@ def _load() -> C.CDLL:
         "lbm_body_opts_default": ([C.POINTER(BodyOpts)], None),
         "lbm_body_state_make": ([C.POINTER(Body), C.c_double, C.POINTER(BodyState)], I),
         "lbm_body_advance": ([C.POINTER(BodyState), D, D, C.POINTER(BodyOpts), I], I),
+        "lbm_amr3d_config_default": ([C.POINTER(Amr3DConfig), I, I, I, I], I),
+        "lbm_amr3d_create": ([C.POINTER(Amr3DConfig), C.POINTER(C.c_uint8), C.POINTER(P)], I),
+        "lbm_amr3d_destroy": ([P], None),
+        "lbm_amr3d_last_error": ([P], C.c_char_p),
+        "lbm_amr3d_set_stream": ([P, P], I),
+        "lbm_amr3d_init_macro": ([P, F], I),
+        "lbm_amr3d_step": ([P, I], I),
+        "lbm_amr3d_forces": ([P, D], I),
+        "lbm_amr3d_set_body": ([P, C.POINTER(Body)], I),
+        "lbm_amr3d_pool_stats": ([P, C.POINTER(C.c_int32)], I),
+        "lbm_amr3d_totals": ([P, D], I),
+        "lbm_amr3d_read_coarse": ([P, F, F], I),
+        "lbm_amr3d_read_pool": ([P, F, F], I),
+        "lbm_amr3d_topology": ([P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)], I),
+        "lbm_amr3d_cell_updates": ([P], C.c_int64),
+        "lbm_amr3d_sync": ([P], I),
+        "lbm_amr3d_refine_blocks": ([C.POINTER(Amr3DConfig), C.POINTER(C.c_uint8)], I),
+        "lbm_resolve_source": ([I, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32), C.POINTER(C.c_int32)], I),
         "lbm_f32_to_f16_bits": ([C.c_float], C.c_uint16),
         "lbm_f16_bits_to_f32": ([C.c_uint16], C.c_float),
     }
@@ -665,6 +694,140 @@ class Amr2D:
 
     def sync(self):
         self._check(lib.lbm_amr2d_sync(self._h))
+
+
+def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, boxfrac: float = 0.5,
+                 explode_linear: int = 1, dynamic: int = 0, manage_every: int = 16, manage_start: int = 0,
+                 max_slots: int = 0, slot_headroom: float = 1.5, **root_kw) -> Amr3DConfig:
+    """lbm_amr3d_config: the L0 grid/physics as config_from's keywords, plus the hierarchy."""
+    c = Amr3DConfig()
+    rc = lib.lbm_amr3d_config_default(C.byref(c), q, *dims)
+    if rc:
+        raise LbmError(rc, "bad dims")
+    c.root = config_from(q, dims, **root_kw)
+    c.rb = rb
+    c.refine = REFINE[refine] if isinstance(refine, str) else int(refine)
+    c.margin = margin
+    c.boxfrac = boxfrac
+    c.explode_linear = explode_linear
+    c.dynamic = dynamic
+    c.manage_every = manage_every
+    c.manage_start = manage_start
+    c.max_slots = max_slots
+    c.slot_headroom = slot_headroom
+    return c
+
+
+def amr3d_refine_blocks(cfg: Amr3DConfig) -> np.ndarray:
+    nb = (cfg.root.nx // cfg.rb) * (cfg.root.ny // cfg.rb) * (cfg.root.nz // cfg.rb)
+    out = np.zeros(nb, np.uint8)
+    rc = lib.lbm_amr3d_refine_blocks(C.byref(cfg), _ptr(out, C.c_uint8))
+    if rc:
+        raise LbmError(rc, "lbm_amr3d_refine_blocks")
+    return out
+
+
+def resolve_source(rb: int, nb, block_slot, block, src):
+    """d3-amr.mjs resolveSource: (slot, fx, fy, fz); slot -1 = own tile, -2 = no tile."""
+    nb = np.ascontiguousarray(nb, np.int32)
+    bs = np.ascontiguousarray(block_slot, np.int32)
+    b = np.ascontiguousarray(block, np.int32)
+    s = np.ascontiguousarray(src, np.int32)
+    out = np.zeros(4, np.int32)
+    i32 = lambda a: _ptr(a, C.c_int32)
+    rc = lib.lbm_resolve_source(int(rb), i32(nb), i32(bs), i32(b), i32(s), i32(out))
+    if rc:
+        raise LbmError(rc, "lbm_resolve_source")
+    return tuple(int(v) for v in out)
+
+
+class Amr3D:
+    """Two-level 3D AMR on the current GPU (the 3D page's AMR session)."""
+
+    def __init__(self, cfg: Amr3DConfig, block_want=None):
+        self.cfg = cfg
+        self.q = cfg.root.q
+        self.dims = (cfg.root.nx, cfg.root.ny, cfg.root.nz)
+        self.ncells = int(np.prod(self.dims))
+        h = C.c_void_p()
+        w = None
+        if block_want is not None:
+            self._want = np.ascontiguousarray(block_want, np.uint8)
+            w = _ptr(self._want, C.c_uint8)
+        rc = lib.lbm_amr3d_create(C.byref(cfg), w, C.byref(h))
+        if rc:
+            raise LbmError(rc, lib.lbm_amr3d_last_error(None).decode())
+        self._h = h
+        self.nb = tuple(d // cfg.rb for d in self.dims)
+        t = self.topology()
+        self.slots, self.fb = t["slots"], t["fb"]
+
+    def _check(self, rc: int):
+        if rc:
+            raise LbmError(rc, lib.lbm_amr3d_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.lbm_amr3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(lib.lbm_amr3d_set_stream(self._h, C.c_void_p(stream_ptr or 0)))
+
+    def init_macro(self, mac: np.ndarray):
+        mac = np.ascontiguousarray(mac, dtype=np.float32).reshape(self.ncells, 4)
+        self._check(lib.lbm_amr3d_init_macro(self._h, _ptr(mac, C.c_float)))
+
+    def step(self, n: int = 1):
+        self._check(lib.lbm_amr3d_step(self._h, int(n)))
+
+    def forces(self) -> np.ndarray:
+        out = np.zeros(6)
+        self._check(lib.lbm_amr3d_forces(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def totals(self) -> np.ndarray:
+        out = np.zeros(4)
+        self._check(lib.lbm_amr3d_totals(self._h, _ptr(out, C.c_double)))
+        return out
+
+    def read_coarse(self):
+        f = np.empty((self.q, self.ncells), np.float32)
+        mac = np.empty((self.ncells, 4), np.float32)
+        self._check(lib.lbm_amr3d_read_coarse(self._h, _ptr(f, C.c_float), _ptr(mac, C.c_float)))
+        return f, mac
+
+    def read_pool(self):
+        n = self.slots * self.fb ** 3
+        f = np.empty((self.q, n), np.float32)
+        mac = np.empty((n, 4), np.float32)
+        self._check(lib.lbm_amr3d_read_pool(self._h, _ptr(f, C.c_float), _ptr(mac, C.c_float)))
+        return f, mac
+
+    def topology(self) -> dict:
+        nb = int(np.prod([d // self.cfg.rb for d in self.dims]))
+        bs = np.zeros(nb, np.int32)
+        sb = np.zeros(nb, np.int32)
+        cnt = np.zeros(3, np.int32)
+        self._check(lib.lbm_amr3d_topology(self._h, _ptr(bs, C.c_int32), _ptr(sb, C.c_int32), _ptr(cnt, C.c_int32)))
+        return {"block_slot": bs, "slot_to_block": sb[:cnt[0]].copy(), "slots": int(cnt[0]), "fb": int(cnt[1])}
+
+    def set_body(self, body: Body):
+        self._check(lib.lbm_amr3d_set_body(self._h, C.byref(body)))
+
+    def pool_stats(self) -> dict:
+        out = np.zeros(4, np.int32)
+        self._check(lib.lbm_amr3d_pool_stats(self._h, _ptr(out, C.c_int32)))
+        return {"in_use": int(out[0]), "refusals": int(out[1]), "min_free": int(out[2]), "decisions": int(out[3])}
+
+    def cell_updates(self) -> int:
+        return int(lib.lbm_amr3d_cell_updates(self._h))
+
+    def sync(self):
+        self._check(lib.lbm_amr3d_sync(self._h))
 
 
 def step_noalloc(cfg: Config, f_in_ptr: int, f_out_ptr: int, mac_ptr: int | None = None,

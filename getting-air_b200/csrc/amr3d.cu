@@ -1,0 +1,1205 @@
+// 3D block-structured AMR, two levels, on the device: the kernels of one
+// macro-step and the session behind lbm_amr3d_*.
+//
+// One macro-step (main-3d.js:3219-3341, ?interface=explode):
+//   amr3_force     pool force on the tiles at time t (FP64, deterministic)
+//   amr3_explode   L0 (time t) -> every tile's ring, Chen et al. 2006: the
+//                  populations of an unrefined L0 cell V whose target V + e_i
+//                  is covered, moved unchanged into V's eight fine cells
+//                  (plus the linear term orthogonal to e_i), and the
+//                  in-orphans of a convex edge; common_d3_amr_explode.wgsl
+//   amr3_substep x2  the tiles, A then B: DIRECT_GHOST pull (a source past
+//                  the interior comes from the refined neighbour's interior,
+//                  else from the ring), BGK + Guo at tau_f = 2 tau - 1/2; the
+//                  ring advects without colliding; common_d3_amr_step1.wgsl
+//   amr3_coalesce  the tiles -> the covered L0 cells of the time-t buffer
+//                  (the mean of the eight fine cells that will be pulled),
+//                  the covered cells' mac, and the out/in orphan balance of
+//                  unrefined cells at a seam; common_d3_amr_coalesce.wgsl
+//   amr3_coarse    the dense step on L0, skipping covered blocks
+//                  (common_d3_step.wgsl:110 coveredByFiner)
+// All but the last macro-step of a call run from one CUDA graph per L0
+// parity; the last is launched directly with the mac writes switched on.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lbm.h"
+#include "amr3d.cuh"
+#include "cell_update.cuh"
+#include "host_params.cuh"
+
+namespace lbm {
+
+namespace {
+
+__device__ __forceinline__ int wrapi(int v, int n) { return ((v % n) + n) % n; }
+
+__device__ __forceinline__ bool covered(const Amr3Params &p, int x, int y, int z) {
+  x = wrapi(x, p.nx); y = wrapi(y, p.ny); z = wrapi(z, p.nz);
+  return p.block_slot[((z / p.rb) * p.nby + y / p.rb) * p.nbx + x / p.rb] >= 0;
+}
+
+__device__ __forceinline__ int64_t ccell(const Amr3Params &p, int x, int y, int z) {
+  return ((int64_t)wrapi(z, p.nz) * p.ny + wrapi(y, p.ny)) * p.nx + wrapi(x, p.nx);
+}
+
+__device__ __forceinline__ float f2c(int j, int origin) { return (float)origin - 0.25f + 0.5f * (float)(j - kAmrGhost); }
+
+__device__ __forceinline__ bool interior(const Amr3Params &p, int j) { return j >= kAmrGhost && j < kAmrGhost + p.RB2; }
+
+struct TileCell {
+  int slot, bx, by, bz, fx, fy, fz;
+  int64_t cell;
+};
+
+__device__ __forceinline__ bool tile_cell(const Amr3Params &p, TileCell &t) {
+  const int k = blockIdx.x * kTileThreads + threadIdx.x;
+  if (k >= p.T3) return false;
+  t.slot = blockIdx.y;
+  const int id = p.slot_to_block[t.slot];
+  if (id < 0) return false;
+  t.bx = id % p.nbx; t.by = (id / p.nbx) % p.nby; t.bz = id / (p.nbx * p.nby);
+  t.fx = k % p.FB; t.fy = (k / p.FB) % p.FB; t.fz = k / (p.FB * p.FB);
+  t.cell = (int64_t)t.slot * p.T3 + k;
+  return true;
+}
+
+template <int Q>
+__device__ __forceinline__ float feq3(int i, float rho, float ux, float uy, float uz) {
+  using L = Lattice<Q>;
+  const float eu = (float)L::ex(i) * ux + (float)L::ey(i) * uy + (float)L::ez(i) * uz;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  return L::w(i) * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
+}
+
+// ---- seed / fill: trilinear interpolation of L0 into a tile ----------------
+// interpCoarseToFine3: rho and u interpolated, f = feq(rho, u) + DC-rescaled
+// interpolated fneq (common_d3_pool.wgsl:192-220).
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_interp(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p,
+                int ring_only, const unsigned char *__restrict__ only_new) {
+  using L = Lattice<Q>;
+  TileCell t;
+  if (!tile_cell(p, t)) return;
+  if (only_new && !only_new[t.slot]) return;
+  if (ring_only && interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz)) return;
+  const float pos[3] = {f2c(t.fx, t.bx * p.rb), f2c(t.fy, t.by * p.rb), f2c(t.fz, t.bz * p.rb)};
+  int c0[3];
+  float tt[3];
+  for (int a = 0; a < 3; ++a) {
+    c0[a] = (int)floorf(pos[a]);
+    tt[a] = pos[a] - (float)c0[a];
+  }
+  float rho = 0.f, ux = 0.f, uy = 0.f, uz = 0.f, fneq[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fneq[i] = 0.f;
+  for (int k = 0; k < 8; ++k) {
+    const int di = k & 1, dj = (k >> 1) & 1, dk = (k >> 2) & 1;
+    const float w = (di ? tt[0] : 1.f - tt[0]) * (dj ? tt[1] : 1.f - tt[1]) * (dk ? tt[2] : 1.f - tt[2]);
+    const int64_t cc = ccell(p, c0[0] + di, c0[1] + dj, c0[2] + dk);
+    float f[Q], r, mx, my, mz;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = __ldg(fc + (int64_t)i * p.N + cc);
+    moments<L, Q>(f, r, mx, my, mz);
+    const float den = fmaxf(r, 1e-6f);
+    const float u0 = mx / den, u1 = my / den, u2 = mz / den;
+    rho += w * r;
+    ux += w * u0; uy += w * u1; uz += w * u2;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fneq[i] += w * (f[i] - feq3<Q>(i, r, u0, u1, u2));
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fp[(int64_t)i * p.P + t.cell] = feq3<Q>(i, rho, ux, uy, uz) + p.rescale_c2f * fneq[i];
+}
+
+// common_d3_moments.wgsl: the tiles' mac from their f.
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_moments(const float *__restrict__ fp, float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  TileCell t;
+  if (!tile_cell(p, t)) return;
+  float f[Q], rho, mx, my, mz;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = __ldg(fp + (int64_t)i * p.P + t.cell);
+  moments<L, Q>(f, rho, mx, my, mz);
+  const float den = fmaxf(rho, 1e-6f);
+  macp[t.cell] = make_float4(rho, mx / den, my / den, mz / den);
+}
+
+// ---- explode ------------------------------------------------------------
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  TileCell t;
+  if (!tile_cell(p, t)) return;
+  if (interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz)) return;
+  const int b[3] = {t.bx, t.by, t.bz};
+  const int fi[3] = {t.fx, t.fy, t.fz};
+  const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
+  int g[3], v[3];
+  for (int a = 0; a < 3; ++a) {
+    g[a] = wrapi(b[a] * p.RB2 + fi[a] - kAmrGhost, nf[a]);
+    v[a] = g[a] / 2;
+  }
+  // A ring cell inside a covered L0 cell is never read (DIRECT_GHOST).
+  if (covered(p, v[0], v[1], v[2])) return;
+  const int64_t vc = ccell(p, v[0], v[1], v[2]);
+  bool ok[3];
+  int64_t vm[3], vp[3];
+  for (int a = 0; a < 3; ++a) {
+    int m[3] = {v[0], v[1], v[2]}, q[3] = {v[0], v[1], v[2]};
+    m[a] -= 1;
+    q[a] += 1;
+    ok[a] = !covered(p, m[0], m[1], m[2]) && !covered(p, q[0], q[1], q[2]);
+    vm[a] = ccell(p, m[0], m[1], m[2]);
+    vp[a] = ccell(p, q[0], q[1], q[2]);
+  }
+  float d[3];
+  for (int a = 0; a < 3; ++a) d[a] = ((float)(g[a] - 2 * v[a]) - 0.5f) * 0.5f;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    float out;
+    if (!covered(p, v[0] + e[0], v[1] + e[1], v[2] + e[2])) {
+      // in-orphan: this child's own one-step destination is in this tile
+      int dg[3];
+      for (int a = 0; a < 3; ++a) dg[a] = wrapi(g[a] + e[a], nf[a]);
+      const bool into = covered(p, dg[0] / 2, dg[1] / 2, dg[2] / 2) && dg[0] / p.RB2 == b[0] &&
+                        dg[1] / p.RB2 == b[1] && dg[2] / p.RB2 == b[2];
+      out = into ? __ldg(fc + (int64_t)i * p.N + vc) : 0.f;
+    } else {
+      const float f = __ldg(fc + (int64_t)i * p.N + vc);
+      if (!p.linear) {
+        out = f;
+      } else {
+        float G[3];
+        for (int a = 0; a < 3; ++a)
+          G[a] = ok[a] ? 0.5f * (__ldg(fc + (int64_t)i * p.N + vp[a]) - __ldg(fc + (int64_t)i * p.N + vm[a])) : 0.f;
+        // projected orthogonal to e_i, so the two substeps see one state
+        const float ee = (float)(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        const float gd = (G[0] * (float)e[0] + G[1] * (float)e[1] + G[2] * (float)e[2]) / ee;
+        for (int a = 0; a < 3; ++a) G[a] -= (float)e[a] * gd;
+        out = f + (d[0] * G[0] + d[1] * G[1] + d[2] * G[2]);
+      }
+    }
+    fp[(int64_t)i * p.P + t.cell] = out;
+  }
+}
+
+// ---- one pool substep ----------------------------------------------------
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
+                 const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  TileCell t;
+  if (!tile_cell(p, t)) return;
+  const StepParams &c = p.c;
+  const int G = kAmrGhost, RB2 = p.RB2, FB = p.FB;
+  const int b[3] = {t.bx, t.by, t.bz};
+  const int fi[3] = {t.fx, t.fy, t.fz};
+  const int nb[3] = {p.nbx, p.nby, p.nbz};
+  int off[3], bn[3];
+  for (int a = 0; a < 3; ++a) {
+    off[a] = fi[a] <= G ? -1 : (fi[a] + 1 >= G + RB2 ? 1 : 0);
+    bn[a] = wrapi(b[a] + off[a], nb[a]);
+  }
+  // Same-level neighbour tiles, indexed by which axes step off the tile.
+  int nbr[8];
+  nbr[0] = t.slot;
+#pragma unroll
+  for (int m = 1; m < 8; ++m) {
+    const bool sx = m & 1, sy = m & 2, sz = m & 4;
+    const bool need = (!sx || off[0]) && (!sy || off[1]) && (!sz || off[2]);
+    nbr[m] = need ? p.block_slot[((sz ? bn[2] : b[2]) * p.nby + (sy ? bn[1] : b[1])) * p.nbx + (sx ? bn[0] : b[0])]
+                  : -1;
+  }
+  const V3 pos = {f2c(t.fx, b[0] * p.rb), f2c(t.fy, b[1] * p.rb), f2c(t.fz, b[2] * p.rb)};
+  float phi = 1e30f;
+  V3 us = {0.f, 0.f, 0.f};
+  if (c.has_body) {
+    phi = phi3(pos, c.body);
+    us = body_velocity3(pos, c.body);
+  }
+  const bool bb = c.has_body && c.bb;
+  // a fine link is sqrt(3)/2 L0 units long and phi is 1-Lipschitz
+  const bool near = bb && phi < 1.0f;
+  float rhoW = 1.f;
+  if (near && c.rho_w_local && phi < 2.f) {
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) s += __ldg(fin + (int64_t)i * p.P + t.cell);
+    rhoW = s;
+  }
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    int s[3] = {t.fx - e[0], t.fy - e[1], t.fz - e[2]};
+    if (near) {
+      const V3 sp = {f2c(s[0], b[0] * p.rb), f2c(s[1], b[1] * p.rb), f2c(s[2], b[2] * p.rb)};
+      if (phi3(sp, c.body) < 0.f) {
+        const float corr =
+            2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
+        f[i] = __ldg(fin + (int64_t)L::opp(i) * p.P + t.cell) + corr;
+        continue;
+      }
+    }
+    int m = 0, o[3];
+    for (int a = 0; a < 3; ++a) {
+      o[a] = (s[a] < G || s[a] >= G + RB2) ? off[a] : 0;
+      if (o[a]) m |= 1 << a;
+    }
+    int src = t.slot;
+    if (m) {
+      const int ns = nbr[m];
+      if (ns >= 0) {
+        src = ns;
+        for (int a = 0; a < 3; ++a) s[a] -= o[a] * RB2;
+      }
+    }
+    for (int a = 0; a < 3; ++a) s[a] = min(max(s[a], 0), FB - 1);
+    f[i] = __ldg(fin + (int64_t)i * p.P + (int64_t)src * p.T3 + (s[2] * FB + s[1]) * FB + s[0]);
+  }
+  float rho, mx, my, mz;
+  moments<L, Q>(f, rho, mx, my, mz);
+  const float den = fmaxf(rho, 1e-6f);
+  const float inv = 1.f / den;
+  const float uxs = mx * inv, uys = my * inv, uzs = mz * inv;
+  const float chi = (c.has_body && !c.bb) ? chi_from_phi(phi, p.chi_eps_f) : 0.f;
+  const float rc = rho * chi;
+  const float Fx = rc * (us.x - uxs) + c.fx, Fy = rc * (us.y - uys) + c.fy, Fz = rc * (us.z - uzs) + c.fz;
+  const float hinv = 0.5f * inv;
+  const float ux = fmaf(Fx, hinv, uxs), uy = fmaf(Fy, hinv, uys), uz = fmaf(Fz, hinv, uzs);
+  const bool in_tile = interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz);
+  MemSink<float> sink{fout, p.P, (int)t.cell, c.pk};
+  if (!in_tile) {
+    // the ring advects and does not collide (COLLIDE_RING = 0)
+    if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fout[(int64_t)i * p.P + t.cell] = f[i];
+    return;
+  }
+  float spw = 0.f;
+  if (c.sponge_w > 0.f) {
+    const float dx = c.sax ? fminf(pos.x, (float)(p.nx - 1) - pos.x) : 1e30f;
+    const float dy = c.say ? fminf(pos.y, (float)(p.ny - 1) - pos.y) : 1e30f;
+    const float dz = c.saz ? fminf(pos.z, (float)(p.nz - 1) - pos.z) : 1e30f;
+    spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), c.sponge_inv);
+  }
+  const bool solid = c.solid_eq && bb && phi < 0.f;
+  if (!solid) {
+    collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega_f, spw, c.ftarget, sink);
+    if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
+  } else {
+    const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
+      fout[(int64_t)i * p.P + t.cell] = L::w(i) * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq);
+    }
+    if (p.write_mac) macp[t.cell] = make_float4(1.f, us.x, us.y, us.z);
+  }
+}
+
+// ---- coalesce -------------------------------------------------------------
+// One thread per L0 cell of the interface blocks (covered blocks and the
+// blocks touching one). Each thread writes only its own L0 cell.
+__device__ __forceinline__ int local_in_tile(const Amr3Params &p, int g, int b, int nfine) {
+  int d = g - b * p.RB2;
+  if (d < -nfine / 2) d += nfine;
+  if (d > nfine / 2) d -= nfine;
+  return d + kAmrGhost;
+}
+
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_coalesce(const float *__restrict__ fp, float *__restrict__ fc, float4 *__restrict__ macc,
+                  const float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  const int rb3 = p.rb * p.rb * p.rb;
+  const int k = blockIdx.x * kTileThreads + threadIdx.x;
+  if (k >= p.n_iface * rb3) return;
+  const int id = p.iface ? p.iface[k / rb3] : k / rb3, l = k % rb3;
+  if (!p.iface && !p.iface_flag[id]) return;
+  const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
+  const int x = b[0] * p.rb + l % p.rb, y = b[1] * p.rb + (l / p.rb) % p.rb, z = b[2] * p.rb + l / (p.rb * p.rb);
+  const int cc[3] = {x, y, z};
+  const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
+  const int64_t cell = ccell(p, x, y, z);
+  const int slot = p.block_slot[id];
+  if (slot < 0) {
+    // out-orphans (half-step exits no coarse bucket absorbs) against
+    // in-orphans (what explode injected into this cell's own children)
+    bool nearc = false;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) nearc = nearc || covered(p, x + L::ex(i), y + L::ey(i), z + L::ez(i));
+    if (!nearc) return;
+#pragma unroll 1
+    for (int i = 1; i < Q; ++i) {
+      const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+      const int tc[3] = {x + e[0], y + e[1], z + e[2]};
+      if (covered(p, tc[0], tc[1], tc[2])) continue;
+      float sacc = 0.f, nin = 0.f;
+      for (int q = 0; q < 8; ++q) {
+        const int o[3] = {q & 1, (q >> 1) & 1, (q >> 2) & 1};
+        int pp[3], qq[3], qb[3];
+        for (int a = 0; a < 3; ++a) {
+          pp[a] = wrapi(wrapi(tc[a], a == 0 ? p.nx : (a == 1 ? p.ny : p.nz)) * 2 + o[a], nf[a]);
+          qq[a] = wrapi(pp[a] - e[a], nf[a]);
+          qb[a] = qq[a] / p.RB2;
+        }
+        const int qs = p.block_slot[(qb[2] * p.nby + qb[1]) * p.nbx + qb[0]];
+        if (qs >= 0) {
+          const int lx = local_in_tile(p, pp[0], qb[0], nf[0]), ly = local_in_tile(p, pp[1], qb[1], nf[1]),
+                    lz = local_in_tile(p, pp[2], qb[2], nf[2]);
+          sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)qs * p.T3 + (lz * p.FB + ly) * p.FB + lx);
+        }
+        int ch[3];
+        for (int a = 0; a < 3; ++a) ch[a] = wrapi(cc[a] * 2 + o[a] + e[a], nf[a]);
+        if (covered(p, ch[0] / 2, ch[1] / 2, ch[2] / 2)) nin += 1.f;
+      }
+      const float own = fc[(int64_t)i * p.N + cell];
+      const float net = sacc - nin * own;
+      if (net != 0.f) fc[(int64_t)i * p.N + cell] = own + net * 0.125f;
+    }
+    return;
+  }
+  const int lx0 = kAmrGhost + 2 * (x - b[0] * p.rb), ly0 = kAmrGhost + 2 * (y - b[1] * p.rb),
+            lz0 = kAmrGhost + 2 * (z - b[2] * p.rb);
+  if (p.write_mac) {
+    float rs = 0.f, m0 = 0.f, m1 = 0.f, m2 = 0.f;
+    for (int q = 0; q < 8; ++q) {
+      const float4 m = macp[(int64_t)slot * p.T3 + ((lz0 + ((q >> 2) & 1)) * p.FB + ly0 + ((q >> 1) & 1)) * p.FB +
+                            lx0 + (q & 1)];
+      rs += m.x;
+      m0 += m.x * m.y; m1 += m.x * m.z; m2 += m.x * m.w;
+    }
+    const float inv = 1.f / fmaxf(rs, 1e-6f);
+    macc[cell] = make_float4(rs * 0.125f, m0 * inv, m1 * inv, m2 * inv);
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    const int tc[3] = {x + e[0], y + e[1], z + e[2]};
+    if (covered(p, tc[0], tc[1], tc[2])) continue;
+    float sacc = 0.f;
+    for (int q = 0; q < 8; ++q) {
+      const int lx = local_in_tile(p, tc[0] * 2 + (q & 1), b[0], nf[0]);
+      const int ly = local_in_tile(p, tc[1] * 2 + ((q >> 1) & 1), b[1], nf[1]);
+      const int lz = local_in_tile(p, tc[2] * 2 + ((q >> 2) & 1), b[2], nf[2]);
+      sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)slot * p.T3 + (lz * p.FB + ly) * p.FB + lx);
+    }
+    fc[(int64_t)i * p.N + cell] = sacc * 0.125f;
+  }
+}
+
+// ---- L0 step, skipping covered blocks ------------------------------------
+template <int Q>
+__global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
+    amr3_coarse(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
+                const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby) {
+  const int x = blockIdx.x * kStepThreads + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= sp.nx) return;
+  if (block_slot[((z / rb) * nby + y / rb) * nbx + x / rb] >= 0) return;
+  CellForce cf;
+  cell3<Q, float>(fin, fout, mac, sp, x, y, z, false, cf);
+}
+
+// ---- pool force (common_d3_force_pool.wgsl) -------------------------------
+// Interior cells of every tile at time t: momentum exchange with local rho_w
+// weighted by dx^2 = 1/4, the swept-cell term by dx^3 = 1/8, or the chi
+// penalty with a tile-clamped gather; FP64 partial per CTA, last-CTA sum.
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_force(const float *__restrict__ fp, const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  const StepParams &c = p.c;
+  const int r3 = p.RB2 * p.RB2 * p.RB2;
+  const int k = blockIdx.x * kTileThreads + threadIdx.x;
+  CellForce cf;
+  const int slot = blockIdx.y;
+  const int id = p.slot_to_block[slot];
+  if (k < r3 && id >= 0) {
+    const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
+    const int fx = kAmrGhost + k % p.RB2, fy = kAmrGhost + (k / p.RB2) % p.RB2, fz = kAmrGhost + k / (p.RB2 * p.RB2);
+    const int64_t cell = (int64_t)slot * p.T3 + (fz * p.FB + fy) * p.FB + fx;
+    const V3 pos = {f2c(fx, b[0] * p.rb), f2c(fy, b[1] * p.rb), f2c(fz, b[2] * p.rb)};
+    const float phi = phi3(pos, c.body);
+    const V3 us = body_velocity3(pos, c.body);
+    float fbx = 0.f, fby = 0.f, fbz = 0.f, fsx = 0.f, fsy = 0.f, fsz = 0.f;
+    if (c.bb) {
+      if (phi >= 0.f && phi < 1.0f) {
+        float rhoW = 1.f;
+        if (c.rho_w_local && phi < 2.f) {
+          float s = 0.f;
+#pragma unroll
+          for (int i = 0; i < Q; ++i) s += __ldg(fp + (int64_t)i * p.P + cell);
+          rhoW = s;
+        }
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const V3 sp = {f2c(fx - L::ex(i), b[0] * p.rb), f2c(fy - L::ey(i), b[1] * p.rb),
+                         f2c(fz - L::ez(i), b[2] * p.rb)};
+          if (phi3(sp, c.body) < 0.f) {
+            const float fo = __ldg(fp + (int64_t)L::opp(i) * p.P + cell);
+            const float corr =
+                2.f * L::w(i) * rhoW * ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
+            const float m = 2.f * fo + corr;
+            fbx += -(float)L::ex(i) * m;
+            fby += -(float)L::ey(i) * m;
+            fbz += -(float)L::ez(i) * m;
+          }
+        }
+      }
+      if (c.swept && fabsf(phi) < c.swept_band) {
+        const bool now = phi < 0.f;
+        if (now != (phi3_ahead(pos, c.body, 1.f) < 0.f)) {
+          float mcx = 0.f, mcy = 0.f, mcz = 0.f;
+#pragma unroll
+          for (int i = 0; i < Q; ++i) {
+            const float v = __ldg(fp + (int64_t)i * p.P + cell);
+            mcx += v * (float)L::ex(i); mcy += v * (float)L::ey(i); mcz += v * (float)L::ez(i);
+          }
+          if (!now) { fsx = mcx; fsy = mcy; fsz = mcz; }
+          else { fsx = -mcx; fsy = -mcy; fsz = -mcz; }
+        }
+      }
+    } else {
+      const float chi = chi_from_phi(phi, p.chi_eps_f);
+      if (chi >= 1e-6f) {
+        float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const int sx = min(max(fx - L::ex(i), 0), p.FB - 1), sy = min(max(fy - L::ey(i), 0), p.FB - 1),
+                    sz = min(max(fz - L::ez(i), 0), p.FB - 1);
+          const float v = __ldg(fp + (int64_t)i * p.P + (int64_t)slot * p.T3 + (sz * p.FB + sy) * p.FB + sx);
+          rho += v;
+          mx += v * (float)L::ex(i); my += v * (float)L::ey(i); mz += v * (float)L::ez(i);
+        }
+        const float den = fmaxf(rho, 1e-6f);
+        fbx = -(rho * chi * (us.x - mx / den));
+        fby = -(rho * chi * (us.y - my / den));
+        fbz = -(rho * chi * (us.z - mz / den));
+      }
+    }
+    const float tx = fbx * 0.25f + fsx * 0.125f, ty = fby * 0.25f + fsy * 0.125f, tz = fbz * 0.25f + fsz * 0.125f;
+    const float rx = pos.x - c.body.cx, ry = pos.y - c.body.cy, rz = pos.z - c.body.cz;
+    cf.fx = tx; cf.fy = ty; cf.fz = tz;
+    cf.tx = ry * tz - rz * ty;
+    cf.ty = rz * tx - rx * tz;
+    cf.tz = rx * ty - ry * tx;
+  }
+  ForceAcc acc;
+  acc.add(cf);
+  reduce_force<kTileThreads>(acc, p.partials, p.counter, gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x,
+                             p.force_out);
+}
+
+// ---- the refinement manager (common_d3_manage.wgsl) ------------------------
+
+// blockWanted: does any point of the block come within margin + lead of the
+// body? One SDF evaluation brackets the minimum over a box of half-edge h as
+// phi(c) - h sqrt(3) <= min <= phi(c); undecided boxes split into octants,
+// three levels deep, accepting at the bottom. sqrt(3) rounded up.
+__device__ __noinline__ bool box_near_body(const lbm_body &b, float cx, float cy, float cz, float h0, float reach) {
+  const float S3 = 1.7320509f;
+  float R0 = h0 * S3;
+  const float p0 = phi3({cx, cy, cz}, b);
+  if (p0 - R0 > reach) return false;
+  if (p0 <= reach) return true;
+  const float h1 = h0 * 0.5f, R1 = R0 * 0.5f;
+  for (int i = 0; i < 8; ++i) {
+    const float c1x = cx + ((i & 1) ? h1 : -h1), c1y = cy + ((i & 2) ? h1 : -h1), c1z = cz + ((i & 4) ? h1 : -h1);
+    const float p1 = phi3({c1x, c1y, c1z}, b);
+    if (p1 - R1 > reach) continue;
+    if (p1 <= reach) return true;
+    const float h2 = h1 * 0.5f, R2 = R1 * 0.5f;
+    for (int j = 0; j < 8; ++j) {
+      const float c2x = c1x + ((j & 1) ? h2 : -h2), c2y = c1y + ((j & 2) ? h2 : -h2), c2z = c1z + ((j & 4) ? h2 : -h2);
+      const float p2 = phi3({c2x, c2y, c2z}, b);
+      if (p2 - R2 > reach) continue;
+      if (p2 <= reach) return true;
+      const float h3 = h2 * 0.5f, R3 = R2 * 0.5f;
+      for (int k = 0; k < 8; ++k) {
+        const float c3x = c2x + ((k & 1) ? h3 : -h3), c3y = c2y + ((k & 2) ? h3 : -h3),
+                    c3z = c2z + ((k & 4) ? h3 : -h3);
+        if (phi3({c3x, c3y, c3z}, b) - R3 <= reach) return true;
+      }
+    }
+  }
+  return false;
+}
+
+__global__ void amr3_decide(const __grid_constant__ Amr3Params p, unsigned char *__restrict__ want, float reach) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= p.nbx * p.nby * p.nbz) return;
+  const int bx = id % p.nbx, by = (id / p.nbx) % p.nby, bz = id / (p.nbx * p.nby);
+  const float half = 0.5f * (float)p.rb;
+  want[id] = box_near_body(p.c.body, (float)(bx * p.rb) + half, (float)(by * p.rb) + half,
+                           (float)(bz * p.rb) + half, half, reach) ? 1 : 0;
+}
+
+// drain (common_d3_amr_average.wgsl, DYING_ONLY): a tile about to be freed
+// restricts into its L0 cells at time t -- feq of the children's mean rho
+// and mass-weighted u plus the F2C-rescaled mean fneq, 2 (tau_c - 1)/(tau_f - 1).
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_drain(const float *__restrict__ fp, float *__restrict__ fc, float4 *__restrict__ macc,
+               const __grid_constant__ Amr3Params p, const unsigned char *__restrict__ want, float rescale_f2c) {
+  using L = Lattice<Q>;
+  const int rb3 = p.rb * p.rb * p.rb;
+  const int k = blockIdx.x * kTileThreads + threadIdx.x;
+  if (k >= rb3) return;
+  const int slot = blockIdx.y;
+  const int id = p.slot_to_block[slot];
+  if (id < 0 || want[id]) return;
+  const int lc[3] = {k % p.rb, (k / p.rb) % p.rb, k / (p.rb * p.rb)};
+  const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
+  float rs = 0.f, ms0 = 0.f, ms1 = 0.f, ms2 = 0.f, fneq[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fneq[i] = 0.f;
+  for (int c = 0; c < 8; ++c) {
+    const int64_t cell = (int64_t)slot * p.T3 +
+                         ((kAmrGhost + 2 * lc[2] + ((c >> 2) & 1)) * p.FB + kAmrGhost + 2 * lc[1] + ((c >> 1) & 1)) * p.FB +
+                         kAmrGhost + 2 * lc[0] + (c & 1);
+    float f[Q], r, mx, my, mz;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = __ldg(fp + (int64_t)i * p.P + cell);
+    moments<L, Q>(f, r, mx, my, mz);
+    const float den = fmaxf(r, 1e-6f);
+    const float u0 = mx / den, u1 = my / den, u2 = mz / den;
+    rs += r;
+    ms0 += r * u0; ms1 += r * u1; ms2 += r * u2;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fneq[i] += f[i] - feq3<Q>(i, r, u0, u1, u2);
+  }
+  const float ra = rs * 0.125f, inv = 1.f / fmaxf(rs, 1e-6f);
+  const float ua = ms0 * inv, va = ms1 * inv, wa = ms2 * inv;
+  const int64_t dst = ccell(p, b[0] * p.rb + lc[0], b[1] * p.rb + lc[1], b[2] * p.rb + lc[2]);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fc[(int64_t)i * p.N + dst] = feq3<Q>(i, ra, ua, va, wa) + rescale_f2c * (fneq[i] * 0.125f);
+  macc[dst] = make_float4(ra, ua, va, wa);
+}
+
+// Exclusive prefix sum of one flag per thread over a 1024-thread CTA.
+__device__ __forceinline__ int block_scan(int v, int *sm, int &total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    sm[32 + lane] = w;
+  }
+  __syncthreads();
+  total = sm[32 + (blockDim.x >> 5) - 1];
+  const int before = (warp ? sm[32 + warp - 1] : 0) + x - v;
+  __syncthreads();
+  return before;
+}
+
+constexpr int kManageThreads = 1024;
+
+// coarsen + refine in one CTA, deterministic: dying blocks push their slots
+// on the free stack in ascending block id, then newly wanted blocks pop
+// slots in ascending block id (the stack top first); a block the pool cannot
+// hold stays coarse and is counted. Then the coalesce's interface flags.
+// counts = {free, refusals, lowest free, decisions}.
+__global__ void __launch_bounds__(kManageThreads)
+    amr3_manage(int *block_slot, int *slot_to_block, int *free_list, int *counts, unsigned char *slot_new,
+                unsigned char *iface_flag, const unsigned char *__restrict__ want, int nbx, int nby, int nbz,
+                int capacity) {
+  __shared__ int sm[64];
+  const int nb = nbx * nby * nbz;
+  for (int s = threadIdx.x; s < capacity; s += kManageThreads) slot_new[s] = 0;
+  int fc = counts[0];
+  __syncthreads();
+  for (int base = 0; base < nb; base += kManageThreads) {
+    const int id = base + threadIdx.x;
+    const int slot = id < nb ? block_slot[id] : -1;
+    const int dying = (slot >= 0 && !want[id]) ? 1 : 0;
+    int total;
+    const int r = block_scan(dying, sm, total);
+    if (dying) {
+      free_list[fc + r] = slot;
+      block_slot[id] = -1;
+      slot_to_block[slot] = -1;
+    }
+    fc += total;
+    __syncthreads();
+  }
+  int refused = 0;
+  for (int base = 0; base < nb; base += kManageThreads) {
+    const int id = base + threadIdx.x;
+    const int born = (id < nb && block_slot[id] < 0 && want[id]) ? 1 : 0;
+    int total;
+    const int r = block_scan(born, sm, total);
+    if (born && r < fc) {
+      const int slot = free_list[fc - 1 - r];
+      block_slot[id] = slot;
+      slot_to_block[slot] = id;
+      slot_new[slot] = 1;
+    }
+    refused += total > fc ? total - fc : 0;
+    fc = total > fc ? 0 : fc - total;
+    __syncthreads();
+  }
+  for (int id = threadIdx.x; id < nb; id += kManageThreads) {
+    const int bx = id % nbx, by = (id / nbx) % nby, bz = id / (nbx * nby);
+    unsigned char f = 0;
+    for (int d = 0; d < 27 && !f; ++d) {
+      const int x = (bx + d % 3 - 1 + nbx) % nbx, y = (by + (d / 3) % 3 - 1 + nby) % nby, z = (bz + d / 9 - 1 + nbz) % nbz;
+      f = block_slot[(z * nby + y) * nbx + x] >= 0;
+    }
+    iface_flag[id] = f;
+  }
+  if (threadIdx.x == 0) {
+    counts[0] = fc;
+    counts[1] += refused;
+    counts[2] = min(counts[2], fc);
+    counts[3] += 1;
+  }
+}
+
+// ---- totals over the L0 mac ------------------------------------------------
+constexpr int kTotThreads = 256;
+__global__ void __launch_bounds__(kTotThreads)
+    amr3_totals(const float4 *__restrict__ mac, int64_t n, double *partials, unsigned int *counter, double *out) {
+  __shared__ double sm[4 * (kTotThreads / 32)];
+  double v[4] = {0, 0, 0, 0};
+  for (int64_t c = (int64_t)blockIdx.x * kTotThreads + threadIdx.x; c < n; c += (int64_t)gridDim.x * kTotThreads) {
+    const float4 m = mac[c];
+    v[0] += (double)m.x - 1.0;
+    v[1] += (double)m.x * m.y;
+    v[2] += (double)m.x * m.z;
+    v[3] += (double)m.x * m.w;
+  }
+  block_sum<4, kTotThreads>(v, sm);
+  finish_sum<4, kTotThreads>(v, partials, counter, gridDim.x, blockIdx.x, out, sm);
+}
+
+#define AMR3_DISPATCH(q, ...)                                    \
+  switch (q) {                                                   \
+    case 19: { constexpr int Q = 19; __VA_ARGS__; } break;       \
+    case 27: { constexpr int Q = 27; __VA_ARGS__; } break;       \
+    default: return cudaErrorInvalidValue;                       \
+  }                                                              \
+  return cudaGetLastError();
+
+}  // namespace
+
+}  // namespace lbm
+
+using namespace lbm;
+
+struct lbm_amr3d {
+  lbm_amr3d_config cfg{};
+  int q = 19;
+  Amr3Params p{};
+  StepParams sp{};  // L0 step
+  float *fc[2] = {nullptr, nullptr};
+  float *fp[2] = {nullptr, nullptr};
+  float *macc = nullptr;
+  float4 *macp = nullptr;
+  int *d_block_slot = nullptr, *d_slot_to_block = nullptr, *d_iface = nullptr;
+  std::vector<int> block_slot, slot_to_block, iface;
+  double *partials = nullptr, *force_out = nullptr, *tot_partials = nullptr, *tot_out = nullptr;
+  unsigned int *counter = nullptr, *tot_counter = nullptr;
+  double *host_out = nullptr;
+  int force_parts = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  int cp = 0;
+  bool seeded = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // dynamic refinement
+  bool dynamic = false;
+  int capacity = 0, initial = 0;
+  int64_t step_count = 0;
+  unsigned char *d_want = nullptr, *d_slot_new = nullptr, *d_iface_flag = nullptr;
+  int *d_free_list = nullptr, *d_counts = nullptr;
+  cudaGraphExec_t manage_graph[2] = {nullptr, nullptr};
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_amr3_error;
+
+int afail(lbm_amr3d *a, int code, const std::string &m) {
+  if (a) a->err = m; else g_amr3_error = m;
+  return code;
+}
+
+#define ACK(a, call)                                                                                       \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess)                                                                                 \
+      return afail(a, e_ == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA,                            \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
+  } while (0)
+
+dim3 tile_grid(const lbm_amr3d *a) { return dim3((a->p.T3 + kTileThreads - 1) / kTileThreads, a->p.slots); }
+
+cudaError_t launch_interp(lbm_amr3d *a, const float *fc, int ring_only, const unsigned char *only_new) {
+  if (!a->p.slots) return cudaSuccess;
+  const dim3 g = tile_grid(a);
+  AMR3_DISPATCH(a->q,
+                amr3_interp<Q><<<g, kTileThreads, 0, a->stream>>>(fc, a->fp[0], a->p, ring_only, only_new));
+}
+
+// One decision of the manager before the macro-step from L0 parity `cp`
+// (main-3d.js:3247-3317): decide, drain the dying tiles into the time-t L0
+// buffer, free and grant slots, fill the new tiles from that buffer.
+cudaError_t launch_manage(lbm_amr3d *a, int cp) {
+  const Amr3Params &p = a->p;
+  const lbm_body &b = p.c.body;
+  const float rc = body_circumradius(b);
+  const float lead = (float)a->cfg.manage_every *
+                     (sqrtf(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) + sqrtf(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc);
+  const int nb = p.nbx * p.nby * p.nbz;
+  cudaStream_t st = a->stream;
+  amr3_decide<<<(nb + 127) / 128, 128, 0, st>>>(p, a->d_want, a->cfg.margin + lead);
+  const float tc = a->cfg.root.tau, tf = 2.f * tc - 0.5f;
+  const float f2c_rescale = 2.f * (tc - 1.f) / (tf - 1.f);
+  const int rb3 = p.rb * p.rb * p.rb;
+  const dim3 gd((rb3 + kTileThreads - 1) / kTileThreads, p.slots);
+  cudaError_t e = cudaSuccess;
+  {
+    auto drain = [&]() -> cudaError_t {
+      AMR3_DISPATCH(a->q, amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, p,
+                                                                      a->d_want, f2c_rescale));
+    };
+    if ((e = drain()) != cudaSuccess) return e;
+  }
+  amr3_manage<<<1, kManageThreads, 0, st>>>(a->d_block_slot, a->d_slot_to_block, a->d_free_list, a->d_counts,
+                                           a->d_slot_new, a->d_iface_flag, a->d_want, p.nbx, p.nby, p.nbz,
+                                           a->capacity);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return launch_interp(a, a->fc[cp], 0, a->d_slot_new);
+}
+
+cudaError_t launch_moments(lbm_amr3d *a) {
+  if (!a->p.slots) return cudaSuccess;
+  const dim3 g = tile_grid(a);
+  AMR3_DISPATCH(a->q, amr3_moments<Q><<<g, kTileThreads, 0, a->stream>>>(a->fp[0], a->macp, a->p));
+}
+
+// One macro-step from L0 parity `cp`.
+cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
+  Amr3Params p = a->p;
+  p.write_mac = write_mac ? 1 : 0;
+  const int q = a->q;
+  cudaStream_t st = a->stream;
+  cudaError_t e = cudaSuccess;
+  if (p.slots) {
+    const dim3 g = tile_grid(a);
+    const int r3 = p.RB2 * p.RB2 * p.RB2;
+    const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
+    const int rb3 = p.rb * p.rb * p.rb;
+    const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
+    auto body = [&]() -> cudaError_t {
+      AMR3_DISPATCH(q, {
+        if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
+        amr3_explode<Q><<<g, kTileThreads, 0, st>>>(a->fc[cp], a->fp[0], p);
+        Amr3Params pa = p;
+        pa.write_mac = 0;
+        amr3_substep<Q><<<g, kTileThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
+        amr3_substep<Q><<<g, kTileThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
+        if (gc) amr3_coalesce<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
+      });
+    };
+    e = body();
+    if (e != cudaSuccess) return e;
+  }
+  StepParams sp = a->sp;
+  sp.write_mac = write_mac ? 1 : 0;
+  const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
+  AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
+                                                                 a->d_block_slot, p.rb, p.nbx, p.nby));
+}
+
+void destroy_graphs(lbm_amr3d *a) {
+  for (auto &g : a->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto &g : a->manage_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+template <class F> int capture(lbm_amr3d *a, cudaGraphExec_t *out, F &&launches) {
+  cudaGraph_t g = nullptr;
+  ACK(a, cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = launches();
+  cudaError_t e2 = cudaStreamEndCapture(a->stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return afail(a, LBM_ECUDA, std::string("capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  ACK(a, e);
+  return LBM_OK;
+}
+
+int build_graphs(lbm_amr3d *a) {
+  for (int cp = 0; cp < 2; ++cp) {
+    int rc = capture(a, &a->graph[cp], [&] { return launch_macro(a, cp, false); });
+    if (rc) return rc;
+    if (a->dynamic) {
+      rc = capture(a, &a->manage_graph[cp], [&] { return launch_manage(a, cp); });
+      if (rc) return rc;
+    }
+  }
+  return LBM_OK;
+}
+
+void release(lbm_amr3d *a) {
+  if (a->stream) cudaStreamSynchronize(a->stream);
+  destroy_graphs(a);
+  for (auto *ptr : {(void *)a->fc[0], (void *)a->fc[1], (void *)a->fp[0], (void *)a->fp[1], (void *)a->macc,
+                    (void *)a->macp, (void *)a->d_block_slot, (void *)a->d_slot_to_block, (void *)a->d_iface,
+                    (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
+                    (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
+                    (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts})
+    cudaFree(ptr);
+  if (a->host_out) cudaFreeHost(a->host_out);
+  if (a->own) cudaStreamDestroy(a->own);
+}
+
+constexpr int kTotBlocks = 296;
+
+}  // namespace
+
+extern "C" {
+
+int lbm_amr3d_config_default(lbm_amr3d_config *c, int q, int nx, int ny, int nz) {
+  if (!c) return LBM_EINVAL;
+  *c = lbm_amr3d_config{};
+  int rc = lbm_config_default(&c->root, q, nx, ny, nz);
+  if (rc) return rc;
+  c->levels = 2;
+  c->rb = 4;
+  c->refine = LBM_REFINE_BODY;
+  c->margin = 2.0f;
+  c->boxfrac = 0.5f;
+  c->explode_linear = 1;
+  return LBM_OK;
+}
+
+const char *lbm_amr3d_last_error(const lbm_amr3d *a) { return a ? a->err.c_str() : g_amr3_error.c_str(); }
+
+int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_amr3d **out) {
+  if (!out) return afail(nullptr, LBM_EINVAL, "out is NULL");
+  *out = nullptr;
+  std::string why;
+  int rc = amr3_validate(c, why);
+  if (rc) return afail(nullptr, rc, why);
+  if (validate_config(&c->root, why)) return afail(nullptr, LBM_EINVAL, why);
+  if (c->refine == LBM_REFINE_LIST && !block_want) return afail(nullptr, LBM_EINVAL, "refine = list needs block flags");
+  auto *a = new lbm_amr3d();
+  a->cfg = *c;
+  a->q = c->root.q;
+  Amr3Params &p = a->p;
+  const lbm_config &r = c->root;
+  p.nx = r.nx; p.ny = r.ny; p.nz = r.nz; p.rb = c->rb;
+  p.nbx = r.nx / c->rb; p.nby = r.ny / c->rb; p.nbz = r.nz / c->rb;
+  p.FB = 2 * c->rb + 2 * kAmrGhost;
+  p.RB2 = 2 * c->rb;
+  p.T3 = p.FB * p.FB * p.FB;
+  p.N = (int64_t)r.nx * r.ny * r.nz;
+  std::vector<uint8_t> want;
+  amr3_want(*c, block_want, want);
+  const int nb = p.nbx * p.nby * p.nbz;
+  a->block_slot.assign(nb, -1);
+  for (int id = 0; id < nb; ++id)
+    if (want[id]) {
+      a->block_slot[id] = (int)a->slot_to_block.size();
+      a->slot_to_block.push_back(id);
+    }
+  a->initial = (int)a->slot_to_block.size();
+  a->dynamic = c->dynamic != 0;
+  if (a->dynamic && c->refine != LBM_REFINE_BODY) {
+    delete a;
+    return afail(nullptr, LBM_ENOTSUP, "dynamic refinement decides by the body's geometry: refine must be body");
+  }
+  if (a->dynamic && c->manage_every < 1) {
+    delete a;
+    return afail(nullptr, LBM_EINVAL, "manage_every must be >= 1");
+  }
+  {
+    int cap = a->initial;
+    if (c->max_slots > 0) cap = std::max(c->max_slots, a->initial);
+    else if (a->dynamic) cap = (int)std::ceil(a->initial * (double)std::max(1.0f, c->slot_headroom));
+    a->capacity = std::max(1, std::min(cap, nb));
+  }
+  a->slot_to_block.resize(a->capacity, -1);
+  p.slots = a->capacity;
+  p.P = (int64_t)a->capacity * p.T3;
+  // interface blocks: covered, or a covered block among the 26 neighbours
+  for (int id = 0; id < nb; ++id) {
+    const int bx = id % p.nbx, by = (id / p.nbx) % p.nby, bz = id / (p.nbx * p.nby);
+    bool keep = false;
+    for (int d = 0; d < 27 && !keep; ++d) {
+      const int nx_ = ((bx + d % 3 - 1) % p.nbx + p.nbx) % p.nbx, ny_ = ((by + (d / 3) % 3 - 1) % p.nby + p.nby) % p.nby,
+                nz_ = ((bz + d / 9 - 1) % p.nbz + p.nbz) % p.nbz;
+      keep = a->block_slot[(nz_ * p.nby + ny_) * p.nbx + nx_] >= 0;
+    }
+    if (keep) a->iface.push_back(id);
+  }
+  p.n_iface = (int)a->iface.size();
+  if (a->dynamic) p.n_iface = nb;  // every block, filtered by the device's interface flags
+  const float tc = r.tau, tf = 2.f * tc - 0.5f;
+  p.omega_f = 1.f / tf;
+  p.rescale_c2f = 0.5f * (tf - 1.f) / (tc - 1.f);
+  p.chi_eps_f = r.chi_eps * 0.5f;
+  p.linear = c->explode_linear ? 1 : 0;
+  fill_step_params(r, p.N, 0, a->sp);
+  a->sp.force_on = 0;
+  {
+    StepParams tmp = a->sp;
+    int box[6];
+    force_cell_box(r, tmp, box);  // swept-cell switch and band for the pool force
+    a->sp.swept = tmp.swept;
+    a->sp.swept_band = tmp.swept_band;
+  }
+  p.c = a->sp;
+  auto bail = [&](cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    release(a);
+    delete a;
+    return afail(nullptr, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA, m);
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
+  a->stream = a->own;
+  const size_t fcb = (size_t)a->q * p.N * sizeof(float), fpb = (size_t)a->q * p.P * sizeof(float);
+  for (int k = 0; k < 2; ++k) {
+    if ((e = cudaMalloc(&a->fc[k], fcb))) return bail(e, "cudaMalloc L0 f");
+    if ((e = cudaMalloc(&a->fp[k], fpb))) return bail(e, "cudaMalloc pool f");
+    if ((e = cudaMemset(a->fp[k], 0, fpb))) return bail(e, "memset pool f");
+  }
+  if ((e = cudaMalloc(&a->macc, (size_t)p.N * 16))) return bail(e, "cudaMalloc L0 mac");
+  if ((e = cudaMalloc(&a->macp, (size_t)p.P * 16))) return bail(e, "cudaMalloc pool mac");
+  if ((e = cudaMemset(a->macp, 0, (size_t)p.P * 16))) return bail(e, "memset pool mac");
+  if ((e = cudaMalloc(&a->d_block_slot, nb * sizeof(int)))) return bail(e, "cudaMalloc block_slot");
+  if ((e = cudaMalloc(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "cudaMalloc slots");
+  if ((e = cudaMalloc(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "cudaMalloc iface");
+  cudaMemcpy(a->d_block_slot, a->block_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(a->d_slot_to_block, a->slot_to_block.data(), a->capacity * sizeof(int), cudaMemcpyHostToDevice);
+  if (a->dynamic) {
+    std::vector<unsigned char> flag(nb, 0);
+    for (int id : a->iface) flag[id] = 1;
+    const int nfree = a->capacity - a->initial;
+    std::vector<int> fl(std::max(1, a->capacity), 0);
+    for (int i = 0; i < nfree; ++i) fl[i] = a->initial + i;
+    const int counts[4] = {nfree, 0, nfree, 0};
+    if ((e = cudaMalloc(&a->d_want, nb))) return bail(e, "cudaMalloc want");
+    if ((e = cudaMalloc(&a->d_iface_flag, nb))) return bail(e, "cudaMalloc flags");
+    if ((e = cudaMalloc(&a->d_slot_new, a->capacity))) return bail(e, "cudaMalloc new");
+    if ((e = cudaMalloc(&a->d_free_list, fl.size() * sizeof(int)))) return bail(e, "cudaMalloc free list");
+    if ((e = cudaMalloc(&a->d_counts, 4 * sizeof(int)))) return bail(e, "cudaMalloc counts");
+    cudaMemset(a->d_want, 0, nb);
+    cudaMemset(a->d_slot_new, 0, a->capacity);
+    cudaMemcpy(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice);
+    cudaMemcpy(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice);
+  }
+  if (p.n_iface) cudaMemcpy(a->d_iface, a->iface.data(), p.n_iface * sizeof(int), cudaMemcpyHostToDevice);
+  const int r3 = p.RB2 * p.RB2 * p.RB2;
+  a->force_parts = std::max(1, ((r3 + kTileThreads - 1) / kTileThreads) * p.slots);
+  if ((e = cudaMalloc(&a->partials, (size_t)a->force_parts * kForceSlots * sizeof(double)))) return bail(e, "partials");
+  if ((e = cudaMalloc(&a->force_out, kForceSlots * sizeof(double)))) return bail(e, "force");
+  if ((e = cudaMalloc(&a->counter, sizeof(unsigned int)))) return bail(e, "counter");
+  if ((e = cudaMemset(a->counter, 0, sizeof(unsigned int)))) return bail(e, "counter");
+  if ((e = cudaMemset(a->force_out, 0, kForceSlots * sizeof(double)))) return bail(e, "force");
+  if ((e = cudaMalloc(&a->tot_partials, (size_t)kTotBlocks * 4 * sizeof(double)))) return bail(e, "totals");
+  if ((e = cudaMalloc(&a->tot_out, 4 * sizeof(double)))) return bail(e, "totals");
+  if ((e = cudaMalloc(&a->tot_counter, sizeof(unsigned int)))) return bail(e, "totals");
+  if ((e = cudaMemset(a->tot_counter, 0, sizeof(unsigned int)))) return bail(e, "totals");
+  if ((e = cudaMallocHost(&a->host_out, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
+  if ((e = cudaDeviceSynchronize())) return bail(e, "set-up");
+  p.block_slot = a->d_block_slot;
+  p.slot_to_block = a->d_slot_to_block;
+  p.iface = a->dynamic ? nullptr : a->d_iface;
+  p.iface_flag = a->d_iface_flag;
+  p.partials = a->partials;
+  p.counter = a->counter;
+  p.force_out = a->force_out;
+  *out = a;
+  return LBM_OK;
+}
+
+void lbm_amr3d_destroy(lbm_amr3d *a) {
+  if (!a) return;
+  release(a);
+  delete a;
+}
+
+int lbm_amr3d_set_stream(lbm_amr3d *a, void *cuda_stream) {
+  if (!a) return LBM_EINVAL;
+  cudaStreamSynchronize(a->stream);
+  a->stream = cuda_stream ? (cudaStream_t)cuda_stream : a->own;
+  destroy_graphs(a);
+  return LBM_OK;
+}
+
+int lbm_amr3d_init_macro(lbm_amr3d *a, const float *mac) {
+  if (!a || !mac) return a ? afail(a, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
+  const size_t bytes = (size_t)a->p.N * 16;
+  ACK(a, cudaMemcpyAsync(a->macc, mac, bytes, cudaMemcpyHostToDevice, a->stream));
+  for (int k = 0; k < 2; ++k)
+    ACK(a, launch_init_eq(a->q, LBM_STORE_FP32, a->macc, a->fc[k], a->p.N, a->sp.pk, a->stream));
+  ACK(a, launch_interp(a, a->fc[0], 0, nullptr));
+  ACK(a, launch_moments(a));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  a->cp = 0;
+  a->step_count = 0;
+  a->seeded = true;
+  return LBM_OK;
+}
+
+int lbm_amr3d_step(lbm_amr3d *a, int n) {
+  if (!a) return LBM_EINVAL;
+  if (n < 0) return afail(a, LBM_EINVAL, "step count must be >= 0");
+  if (!a->seeded) return afail(a, LBM_EINVAL, "call lbm_amr3d_init_macro first");
+  if ((n > 1 || a->dynamic) && !a->graph[0]) {
+    int rc = build_graphs(a);
+    if (rc) return rc;
+  }
+  const lbm_amr3d_config &c = a->cfg;
+  for (int k = 0; k < n; ++k) {
+    if (a->dynamic && a->step_count >= c.manage_start && (a->step_count - c.manage_start) % c.manage_every == 0)
+      ACK(a, cudaGraphLaunch(a->manage_graph[a->cp], a->stream));
+    if (k < n - 1) ACK(a, cudaGraphLaunch(a->graph[a->cp], a->stream));
+    else ACK(a, launch_macro(a, a->cp, true));
+    a->cp = 1 - a->cp;
+    a->step_count += 1;
+  }
+  return LBM_OK;
+}
+
+int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body) {
+  if (!a || !body) return a ? afail(a, LBM_EINVAL, "body is NULL") : LBM_EINVAL;
+  if (!a->cfg.root.has_body) return afail(a, LBM_EINVAL, "the hierarchy has no body");
+  lbm_config r = a->cfg.root;
+  r.body = *body;
+  std::string why;
+  if (validate_config(&r, why)) return afail(a, LBM_EINVAL, why);
+  ACK(a, cudaStreamSynchronize(a->stream));
+  a->cfg.root = r;
+  a->sp.body = *body;
+  StepParams tmp = a->sp;
+  int box[6];
+  force_cell_box(r, tmp, box);
+  a->sp.swept = tmp.swept;
+  a->sp.swept_band = tmp.swept_band;
+  a->p.c = a->sp;
+  destroy_graphs(a);
+  return LBM_OK;
+}
+
+int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]) {
+  if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  if (!a->dynamic) {
+    out[0] = a->initial; out[1] = 0; out[2] = a->capacity - a->initial; out[3] = 0;
+    return LBM_OK;
+  }
+  int counts[4];
+  ACK(a, cudaMemcpyAsync(counts, a->d_counts, sizeof(counts), cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  out[0] = a->capacity - counts[0];
+  out[1] = counts[1];
+  out[2] = counts[2];
+  out[3] = counts[3];
+  return LBM_OK;
+}
+
+int lbm_amr3d_forces(lbm_amr3d *a, double out[6]) {
+  if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  ACK(a, cudaMemcpyAsync(a->host_out, a->force_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  for (int k = 0; k < 6; ++k) out[k] = a->host_out[k];
+  return LBM_OK;
+}
+
+int lbm_amr3d_totals(lbm_amr3d *a, double out[4]) {
+  if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
+  const int64_t nb = (a->p.N + kTotThreads - 1) / kTotThreads;
+  const int grid = (int)std::min<int64_t>(kTotBlocks, nb);
+  amr3_totals<<<grid, kTotThreads, 0, a->stream>>>((const float4 *)a->macc, a->p.N, a->tot_partials, a->tot_counter,
+                                                  a->tot_out);
+  ACK(a, cudaGetLastError());
+  ACK(a, cudaMemcpyAsync(a->host_out, a->tot_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  for (int k = 0; k < 4; ++k) out[k] = a->host_out[k];
+  return LBM_OK;
+}
+
+int lbm_amr3d_read_coarse(lbm_amr3d *a, float *f, float *mac) {
+  if (!a) return LBM_EINVAL;
+  if (f) ACK(a, cudaMemcpyAsync(f, a->fc[a->cp], (size_t)a->q * a->p.N * 4, cudaMemcpyDeviceToHost, a->stream));
+  if (mac) ACK(a, cudaMemcpyAsync(mac, a->macc, (size_t)a->p.N * 16, cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr3d_read_pool(lbm_amr3d *a, float *f, float *mac) {
+  if (!a) return LBM_EINVAL;
+  const int64_t used = (int64_t)a->p.slots * a->p.T3;
+  if (f)
+    for (int i = 0; i < a->q; ++i)
+      ACK(a, cudaMemcpyAsync(f + i * used, a->fp[0] + (int64_t)i * a->p.P, used * 4, cudaMemcpyDeviceToHost, a->stream));
+  if (mac) ACK(a, cudaMemcpyAsync(mac, a->macp, used * 16, cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr3d_topology(lbm_amr3d *a, int32_t *block_slot, int32_t *slot_to_block, int32_t counts[3]) {
+  if (!a) return LBM_EINVAL;
+  if (a->dynamic) {
+    ACK(a, cudaMemcpyAsync(a->block_slot.data(), a->d_block_slot, a->block_slot.size() * sizeof(int),
+                           cudaMemcpyDeviceToHost, a->stream));
+    ACK(a, cudaMemcpyAsync(a->slot_to_block.data(), a->d_slot_to_block, a->capacity * sizeof(int),
+                           cudaMemcpyDeviceToHost, a->stream));
+    ACK(a, cudaStreamSynchronize(a->stream));
+  }
+  if (block_slot) std::memcpy(block_slot, a->block_slot.data(), a->block_slot.size() * sizeof(int32_t));
+  if (slot_to_block) std::memcpy(slot_to_block, a->slot_to_block.data(), a->capacity * sizeof(int32_t));
+  if (counts) { counts[0] = a->capacity; counts[1] = a->p.FB; counts[2] = (int32_t)a->block_slot.size(); }
+  return LBM_OK;
+}
+
+int64_t lbm_amr3d_cell_updates(lbm_amr3d *a) {
+  if (!a) return 0;
+  int32_t st[4];
+  if (lbm_amr3d_pool_stats(a, st)) return 0;
+  const int64_t rb3 = (int64_t)a->p.rb * a->p.rb * a->p.rb, fine = (int64_t)a->p.RB2 * a->p.RB2 * a->p.RB2;
+  return a->p.N - (int64_t)st[0] * rb3 + 2 * (int64_t)st[0] * fine;
+}
+
+int lbm_amr3d_sync(lbm_amr3d *a) {
+  if (!a) return LBM_EINVAL;
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+}  // extern "C"

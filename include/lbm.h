@@ -348,6 +348,91 @@ int lbm_amr2d_read_topology(lbm_amr2d *a, int32_t *block_slot, int32_t *slot_to_
 int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a);
 int lbm_amr2d_sync(lbm_amr2d *a);
 
+/* ---- 3D block-structured AMR (D3Q19 / D3Q27, FP32) -----------------------
+ * The dense L0 grid plus one pool level: blocks of RB^3 L0 cells, a refined
+ * block owning a tile of FB^3 = (2 RB + 4)^3 cells at half spacing (interior
+ * plus a two-cell ring). d3-amr.mjs (pool geometry, refineWhere,
+ * nearBodyWant) and the kernels common_d3_amr_{explode,step1,coalesce,interp}
+ * .wgsl, common_d3_force_pool.wgsl, common_d3_moments.wgsl; the macro-step
+ * order of main-3d.js:3219-3341 (force, explode, two fine substeps, coalesce,
+ * the coarse step skipping covered blocks). */
+
+typedef enum {
+  LBM_REFINE_BODY = 0,  /* blocks within `margin` of the body (nearBodyWant) */
+  LBM_REFINE_BOX = 1,   /* centred cube, `boxfrac` of each axis            */
+  LBM_REFINE_BAR = 2,   /* centred in x and y, all of z                    */
+  LBM_REFINE_SLAB = 3,  /* centred band in x                               */
+  LBM_REFINE_ALL = 4,
+  LBM_REFINE_LIST = 5   /* the caller's per-block flags                    */
+} lbm_refine;
+
+typedef struct {
+  lbm_config root;         /* L0 grid and physics; dims multiples of rb; FP32 */
+  int32_t levels;          /* 2                                               */
+  int32_t rb;              /* block edge, L0 cells (4)                        */
+  int32_t refine;          /* lbm_refine                                      */
+  float margin;            /* LBM_REFINE_BODY margin, L0 cells (2)            */
+  float boxfrac;           /* box / bar / slab fraction (0.5)                 */
+  int32_t explode_linear;  /* EXPLODE_LINEAR (1); 0 = uniform explosion       */
+  int32_t dynamic;         /* re-decide the refined set on the device (0)     */
+  int32_t manage_every;    /* macro-steps between decisions (16)              */
+  int32_t manage_start;    /* first macro-step that decides (0)               */
+  int32_t max_slots;       /* pool capacity; 0 = initial set (x slot_headroom when dynamic) */
+  float slot_headroom;     /* 1.5                                             */
+  int32_t reserved[5];     /* zero                                            */
+} lbm_amr3d_config;
+
+typedef struct lbm_amr3d lbm_amr3d;
+
+int lbm_amr3d_config_default(lbm_amr3d_config *c, int q, int nx, int ny, int nz);
+/* `block_want` (one flag per block, id = (bz*NBY + by)*NBX + bx) is read for
+ * LBM_REFINE_LIST only. Slots are handed out in ascending block id. */
+int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_amr3d **out);
+void lbm_amr3d_destroy(lbm_amr3d *a);
+const char *lbm_amr3d_last_error(const lbm_amr3d *a);
+int lbm_amr3d_set_stream(lbm_amr3d *a, void *cuda_stream);
+/* Seeds L0 at equilibrium from [rho,ux,uy,uz] per L0 cell (both buffers),
+ * every tile by trilinear interpolation of it (DC rescale
+ * 0.5 (tau_f - 1)/(tau_c - 1)), then the tiles' moments -- main-3d.js reset. */
+int lbm_amr3d_init_macro(lbm_amr3d *a, const float *mac);
+/* n macro-steps (one L0 step and two pool substeps each). With `dynamic`,
+ * macro-steps manage_start + k * manage_every first re-decide the refined
+ * set on the device (common_d3_manage.wgsl, in its order: decide, drain the
+ * dying tiles into L0, free their slots, grant slots to new blocks, fill the
+ * new tiles from L0), with slots granted in ascending block id. */
+int lbm_amr3d_step(lbm_amr3d *a, int n);
+/* Replaces the body pose (a prescribed motion); the next decision follows it. */
+int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body);
+/* {slots in use, refusals (pool exhausted), lowest free count seen, decisions}. */
+int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]);
+/* Force and torque on the body at the last macro-step (pool force, FP64). */
+int lbm_amr3d_forces(lbm_amr3d *a, double out[6]);
+/* Over the L0 macroscopic field of the last step (covered cells carry the
+ * tiles' projection): {sum(rho - 1), sum(rho ux), sum(rho uy), sum(rho uz)},
+ * FP64 -- readInterfaceDiag (main-3d.js:4660). */
+int lbm_amr3d_totals(lbm_amr3d *a, double out[4]);
+/* L0 f (Q planes of NX*NY*NZ, current time level) and mac (4 per cell). */
+int lbm_amr3d_read_coarse(lbm_amr3d *a, float *f, float *mac);
+/* Pool f (Q planes of slots*FB^3, slot-major) and mac (4 per cell). */
+int lbm_amr3d_read_pool(lbm_amr3d *a, float *f, float *mac);
+/* block_slot (NBX*NBY*NBZ), slot_to_block (capacity; -1 = free slot);
+ * counts = {capacity, FB, blocks}. Synchronous. */
+int lbm_amr3d_topology(lbm_amr3d *a, int32_t *block_slot, int32_t *slot_to_block, int32_t counts[3]);
+/* Cell updates of one macro-step at the current topology: the L0 cells
+ * outside refined blocks plus two substeps of every refined interior cell. */
+int64_t lbm_amr3d_cell_updates(lbm_amr3d *a);
+int lbm_amr3d_sync(lbm_amr3d *a);
+
+/* The block set a configuration refines (d3-amr.mjs refineWhere with the
+ * predicate of `c->refine`); `want` has NBX*NBY*NBZ entries. */
+int lbm_amr3d_refine_blocks(const lbm_amr3d_config *c, uint8_t *want);
+
+/* d3-amr.mjs resolveSource: where a tile-local source index `src` of block
+ * `block` lives. out = {slot, fx, fy, fz}; slot = -1 for the block's own
+ * tile, -2 when no tile owns it (the ring is read). Returns 0. */
+int lbm_resolve_source(int rb, const int32_t nb[3], const int32_t *block_slot, const int32_t block[3],
+                       const int32_t src[3], int32_t out[4]);
+
 /* ---- serving form -------------------------------------------------------------
  * A request loop over one device arena of `budget_bytes` allocated at
  * creation: submitted solves (a dense lbm_config + a step count) are admitted

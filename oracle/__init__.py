@@ -184,3 +184,83 @@ def run_free(cfg, f0: np.ndarray, nsteps: int, state, opts, fp32: bool = False):
     if rc:
         raise ValueError("oracle_run_free failed")
     return f, mac, forces, traj
+
+
+class Amr3D:
+    """The 3D two-level AMR restatement (FP64, or the reference's f32 order)."""
+
+    def __init__(self, cfg, block_want=None, fp32: bool = False, capacity: int = 0):
+        self._h = None
+        L = lib()
+        L.oracle_amr3d_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                          C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int]
+        L.oracle_amr3d_pool_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
+        L.oracle_amr3d_set_body.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_amr3d_create.restype = C.c_void_p
+        L.oracle_amr3d_destroy.argtypes = [C.c_void_p]
+        L.oracle_amr3d_topology.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.oracle_amr3d_seed.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.oracle_amr3d_step.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+        L.oracle_amr3d_read.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 4
+        r = cfg.root
+        self.q, self.dims, self.rb = r.q, (r.nx, r.ny, r.nz), cfg.rb
+        self.nb = tuple(d // cfg.rb for d in self.dims)
+        self.fb = 2 * cfg.rb + 4
+        lst = None
+        if block_want is not None:
+            arr = np.ascontiguousarray(block_want, np.int32)
+            self._list = arr
+            lst = arr.ctypes.data_as(C.POINTER(C.c_int32))
+        self._h = L.oracle_amr3d_create(C.addressof(r), cfg.rb, cfg.refine, cfg.margin, cfg.boxfrac, lst,
+                                        cfg.explode_linear, int(fp32), int(capacity), int(cfg.dynamic),
+                                        int(cfg.manage_every), int(cfg.manage_start))
+        if not self._h:
+            raise ValueError("oracle_amr3d_create failed")
+        nbl = int(np.prod(self.nb))
+        self.block_slot = np.zeros(nbl, np.int32)
+        s2b = np.zeros(nbl, np.int32)
+        self.slots = L.oracle_amr3d_topology(self._h, self.block_slot.ctypes.data_as(C.POINTER(C.c_int32)),
+                                             s2b.ctypes.data_as(C.POINTER(C.c_int32)))
+        self.slot_to_block = s2b[:self.slots].copy()
+
+    def pool_stats(self) -> dict:
+        out = np.zeros(4, np.int32)
+        lib().oracle_amr3d_pool_stats(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return {"in_use": int(out[0]), "refusals": int(out[1]), "min_free": int(out[2]), "decisions": int(out[3])}
+
+    def set_body(self, body):
+        lib().oracle_amr3d_set_body(self._h, C.addressof(body))
+
+    def topology(self):
+        nbl = int(np.prod(self.nb))
+        bs = np.zeros(nbl, np.int32)
+        s2b = np.zeros(max(nbl, self.slots), np.int32)
+        n = lib().oracle_amr3d_topology(self._h, bs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        s2b.ctypes.data_as(C.POINTER(C.c_int32)))
+        return bs, s2b[:n].copy()
+
+    def seed(self, mac):
+        m = np.ascontiguousarray(mac, np.float64).reshape(-1, 4)
+        lib().oracle_amr3d_seed(self._h, _d(m))
+
+    def step(self, n: int) -> np.ndarray:
+        forces = np.zeros((max(n, 1), 8))
+        lib().oracle_amr3d_step(self._h, int(n), _d(forces))
+        return forces[:n]
+
+    def read(self):
+        n = int(np.prod(self.dims))
+        p = self.slots * self.fb ** 3
+        fc, macc = np.zeros((self.q, n)), np.zeros((n, 4))
+        fp, macp = np.zeros((self.q, p)), np.zeros((p, 4))
+        lib().oracle_amr3d_read(self._h, _d(fc), _d(macc), _d(fp), _d(macp))
+        return fc, macc, fp, macp
+
+    def close(self):
+        if self._h:
+            lib().oracle_amr3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
