@@ -77,7 +77,8 @@ class Amr2DConfig(C.Structure):
                 ("solid_eq", C.c_int32), ("k_eps", C.c_float), ("sponge_w", C.c_float),
                 ("sponge_u", C.c_float * 2), ("force", C.c_float * 2), ("body", Body),
                 ("refine_every", C.c_int32), ("refine_thresh", C.c_float), ("refine_margin", C.c_float),
-                ("refine_lookahead", C.c_float), ("auto_refine", C.c_int32), ("reserved", C.c_int32 * 8)]
+                ("refine_lookahead", C.c_float), ("auto_refine", C.c_int32), ("iface", C.c_int32),
+                ("explode_linear", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class Result(C.Structure):

@@ -48,6 +48,7 @@ struct AmrParams {
   float resc_c2f, resc_f2c;
   double thr;
   int vort_on, bb, solid_eq;
+  int explode, linear;  // explode/coalesce interface; its linear explosion
   float ftarget[9];
   lbm_body body;
   int *blockSlot, *slotToBlock, *parentSlot, *freeList, *counts, *activeList;
@@ -351,6 +352,12 @@ __global__ void __launch_bounds__(kPoolThreads)
       const float ux = uxs + Fx / (2.0f * den), uy = uys + Fy / (2.0f * den);
       const float usq = ux * ux + uy * uy;
       vel1[cell] = make_float2(ux, uy);
+      if (p.explode && !(fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2)) {
+        // explode/coalesce: the ring advects without colliding (COLLIDE_RING = 0)
+#pragma unroll
+        for (int i = 0; i < 9; ++i) fout[i * p.N1 + cell] = f[i];
+        continue;
+      }
       const float dx = fminf(wx, Wf - 1.0f - wx), dy = fminf(wy, Hf - 1.0f - wy);
       const float sw = sponge_weight(fminf(dx, dy), p.sponge_w);
       const bool solid = p.solid_eq && p.bb && phi < 0.f;
@@ -461,8 +468,19 @@ __global__ void __launch_bounds__(kPoolThreads)
           float rho = 0.f, ux = 0.f, uy = 0.f;
 #pragma unroll
           for (int i = 0; i < 9; ++i) {
-            const int sx = min(max(fx - L9::ex(i), 0), p.FB - 1), sy = min(max(fy - L9::ey(i), 0), p.FB - 1);
-            const float v = __ldg(f1 + i * p.N1 + pcell(p, s, sx, sy));
+            const int sx0 = fx - L9::ex(i), sy0 = fy - L9::ey(i);
+            const int sx = min(max(sx0, 0), p.FB - 1), sy = min(max(sy0, 0), p.FB - 1);
+            int64_t src = pcell(p, s, sx, sy);
+            if (p.explode) {
+              // RING_FREE_FORCE: sources past the interior resolve as the step's do
+              const int ox = sx0 >= p.G + p.RB2 ? 1 : (sx0 < p.G ? -1 : 0);
+              const int oy = sy0 >= p.G + p.RB2 ? 1 : (sy0 < p.G ? -1 : 0);
+              if (ox || oy) {
+                const int ns = p.blockSlot[((by + oy + p.NBY) % p.NBY) * p.NBX + (bx + ox + p.NBX) % p.NBX];
+                if (ns >= 0) src = pcell(p, ns, sx0 - ox * p.RB2, sy0 - oy * p.RB2);
+              }
+            }
+            const float v = __ldg(f1 + i * p.N1 + src);
             rho += v;
             ux += v * (float)L9::ex(i);
             uy += v * (float)L9::ey(i);
@@ -483,6 +501,127 @@ __global__ void __launch_bounds__(kPoolThreads)
     }
     reduce_force<kPoolThreads>(acc, p.partials, p.counter, n, k, p.force_out);
     __syncthreads();
+  }
+}
+
+// ---- explode / coalesce interface ------------------------------------------------
+
+__device__ __forceinline__ int wrap2(int v, int n) { return ((v % n) + n) % n; }
+
+__device__ __forceinline__ bool covered2(const AmrParams &p, int x, int y) {
+  return p.blockSlot[(wrap2(y, p.H) / p.RB) * p.NBX + wrap2(x, p.W) / p.RB] >= 0;
+}
+
+__device__ __forceinline__ int64_t rcell(const AmrParams &p, int x, int y) {
+  return (int64_t)wrap2(y, p.H) * p.W + wrap2(x, p.W);
+}
+
+// amr_explode.wgsl: every ring cell whose L0 cell V is unrefined takes V's
+// time-t populations for the directions whose L0 target is covered (plus
+// the linear term orthogonal to e_i), V's population where this child's own
+// one-step destination lies in the tile (in-orphan), else 0.
+__global__ void __launch_bounds__(kPoolThreads)
+    amr_explode(const float *__restrict__ f0, float *__restrict__ f1, const __grid_constant__ AmrParams p) {
+  const int n = p.counts[1];
+  const int NFX = 2 * p.W, NFY = 2 * p.H;
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    const int G = p.G, RB2 = p.RB2, FB = p.FB;
+    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+      const int fx = c % FB, fy = c / FB;
+      if (fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2) continue;
+      const int gx = wrap2(bx * RB2 + fx - G, NFX), gy = wrap2(by * RB2 + fy - G, NFY);
+      const int vx = gx / 2, vy = gy / 2;
+      if (covered2(p, vx, vy)) continue;
+      const int64_t vc = rcell(p, vx, vy);
+      bool okx = false, oky = false;
+      if (p.linear) {
+        okx = !covered2(p, vx - 1, vy) && !covered2(p, vx + 1, vy);
+        oky = !covered2(p, vx, vy - 1) && !covered2(p, vx, vy + 1);
+      }
+      const float dx = ((float)(gx - 2 * vx) - 0.5f) * 0.5f, dy = ((float)(gy - 2 * vy) - 0.5f) * 0.5f;
+      const int64_t cell = pcell(p, s, fx, fy);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const int ex = L9::ex(i), ey = L9::ey(i);
+        const float fv = __ldg(f0 + i * p.N0 + vc);
+        float o;
+        if (covered2(p, vx + ex, vy + ey)) {
+          o = fv;
+          if (p.linear && (okx || oky)) {
+            float gxv = okx ? 0.5f * (__ldg(f0 + i * p.N0 + rcell(p, vx + 1, vy)) - __ldg(f0 + i * p.N0 + rcell(p, vx - 1, vy)))
+                            : 0.f;
+            float gyv = oky ? 0.5f * (__ldg(f0 + i * p.N0 + rcell(p, vx, vy + 1)) - __ldg(f0 + i * p.N0 + rcell(p, vx, vy - 1)))
+                            : 0.f;
+            const float ef = (gxv * (float)ex + gyv * (float)ey) / (float)(ex * ex + ey * ey);
+            gxv -= (float)ex * ef;
+            gyv -= (float)ey * ef;
+            o += dx * gxv + dy * gyv;
+          }
+        } else {
+          const int dgx = wrap2(gx + ex, NFX), dgy = wrap2(gy + ey, NFY);
+          const bool into = covered2(p, dgx / 2, dgy / 2) && dgx / RB2 == bx && dgy / RB2 == by;
+          o = into ? fv : 0.f;
+        }
+        f1[i * p.N1 + cell] = o;
+      }
+    }
+  }
+}
+
+// amr_coalesce.wgsl, one thread per L0 cell (each writes only its own cell
+// of the time-t buffer): a covered cell takes, for every direction whose
+// target is unrefined, the mean of the four fine cells of that target that
+// the L0 step will pull; an unrefined cell at the seam gets its out-orphans
+// (half-step exits of the tiles) less the in-orphans explode injected.
+__global__ void __launch_bounds__(256)
+    amr_coalesce(const float *__restrict__ f1, float *__restrict__ f0, const __grid_constant__ AmrParams p) {
+  const int64_t c = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (c >= p.N0) return;
+  const int cx = (int)(c % p.W), cy = (int)(c / p.W);
+  const int NFX = 2 * p.W, NFY = 2 * p.H;
+  const int G = p.G, RB2 = p.RB2;
+  if (covered2(p, cx, cy)) {
+    const int cbx = cx / p.RB, cby = cy / p.RB;
+    const int cs = p.blockSlot[cby * p.NBX + cbx];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const int tx = cx + L9::ex(i), ty = cy + L9::ey(i);
+      if (covered2(p, tx, ty)) continue;
+      float sum = 0.f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int px = tx * 2 + (k & 1), py = ty * 2 + (k >> 1);
+        sum += __ldg(f1 + i * p.N1 + pcell(p, cs, px - cbx * RB2 + G, py - cby * RB2 + G));
+      }
+      f0[i * p.N0 + c] = sum * 0.25f;
+    }
+    return;
+  }
+  bool nearc = false;
+#pragma unroll
+  for (int i = 1; i < 9; ++i) nearc = nearc || covered2(p, cx + L9::ex(i), cy + L9::ey(i));
+  if (!nearc) return;
+#pragma unroll
+  for (int i = 1; i < 9; ++i) {
+    const int ex = L9::ex(i), ey = L9::ey(i);
+    if (covered2(p, cx + ex, cy + ey)) continue;
+    float sum = 0.f, nin = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int ox = k & 1, oy = k >> 1;
+      const int pux = (cx + ex) * 2 + ox, puy = (cy + ey) * 2 + oy;
+      const int qx = wrap2(pux - ex, NFX), qy = wrap2(puy - ey, NFY);
+      const int qbx = qx / RB2, qby = qy / RB2;
+      const int qs = p.blockSlot[qby * p.NBX + qbx];
+      if (qs >= 0) sum += __ldg(f1 + i * p.N1 + pcell(p, qs, qx - qbx * RB2 + G + ex, qy - qby * RB2 + G + ey));
+      const int chx = wrap2(cx * 2 + ox + ex, NFX), chy = wrap2(cy * 2 + oy + ey, NFY);
+      if (covered2(p, chx / 2, chy / 2)) nin += 1.f;
+    }
+    const float own = f0[i * p.N0 + c];
+    const float net = sum - nin * own;
+    if (net != 0.f) f0[i * p.N0 + c] = own + net * 0.25f;
   }
 }
 
@@ -571,6 +710,20 @@ int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
   AmrParams &p = a->p;
   const int g = a->grid_slots;
   amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
+  if (p.explode) {
+    // amr2d-gpu.mjs:1096-1124 S_AdvanceExplode: the L0 step runs LAST
+    amr_explode<<<g, kPoolThreads, 0, st>>>(a->f0[from], a->f1[0], p);
+    amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
+    amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
+    amr_coalesce<<<(int)((p.N0 + 255) / 256), 256, 0, st>>>(a->f1[0], a->f0[from], p);
+    StepParams rp = a->root;
+    rp.write_mac = 1;
+    cudaError_t e = launch_step(9, 0, a->f0[from], a->f0[1 - from], (float *)a->mac, rp, st);
+    if (e) return afail(a, LBM_ECUDA, std::string("root step: ") + cudaGetErrorString(e));
+    amr_average<<<g, 64, 0, st>>>(a->f1[0], a->f0[1 - from], p);
+    ACK(a, cudaGetLastError());
+    return LBM_OK;
+  }
   amr_fill<<<g, kPoolThreads, 0, st>>>(a->f0[from], a->f1[0], 0, p);
   StepParams rp = a->root;
   rp.write_mac = 1;
@@ -636,6 +789,8 @@ int lbm_amr2d_config_default(lbm_amr2d_config *c, int nx, int ny) {
   c->refine_margin = 8.0f;
   c->refine_lookahead = 16.0f;
   c->auto_refine = 1;
+  c->iface = 0;
+  c->explode_linear = 1;
   return LBM_OK;
 }
 
@@ -663,6 +818,8 @@ int lbm_amr2d_create(const lbm_amr2d_config *cfg, lbm_amr2d **out) {
   p.vort_on = c.refine_thresh <= 1.0f;
   p.thr = std::exp2((double)c.refine_thresh);
   p.bb = c.use_bounceback; p.solid_eq = c.solid_eq;
+  p.explode = c.iface == 1 ? 1 : 0;
+  p.linear = c.explode_linear ? 1 : 0;
   p.body = c.body;
   for (int i = 0; i < 9; ++i) {
     const int ex = Lattice<9>::ex(i), ey = Lattice<9>::ey(i);

@@ -316,7 +316,11 @@ typedef struct {
   float refine_margin;       /* 8: refine blocks within this distance of body    */
   float refine_lookahead;    /* 16 macro-steps                                   */
   int32_t auto_refine;       /* 1                                                */
-  int32_t reserved[8];
+  int32_t iface;             /* 0: interp ring (the reference's 2D default),
+                                1: explode/coalesce (amr_explode.wgsl,
+                                amr_coalesce.wgsl; the ring advects only)       */
+  int32_t explode_linear;    /* EXPLODE_LINEAR (1), explode only                 */
+  int32_t reserved[6];
 } lbm_amr2d_config;
 
 typedef struct lbm_amr2d lbm_amr2d;

@@ -23,6 +23,14 @@
 //                                   DET_SLOTS coarsen and refine by quads
 //   common_geometry.wgsl:230-290    nearBodyBox branch and bound
 //   amr_force1.wgsl:350-496         finest-level force with dx weights
+//   amr2d-gpu.mjs:1096-1124         S_AdvanceExplode: explode, two substeps
+//                                   (the ring advects, COLLIDE_RING = 0),
+//                                   coalesce into L0's time-t buffer, the L0
+//                                   step, the restriction into L0's new buffer
+//   amr_explode.wgsl:132-203        ring <- L0 at t (linear term, in-orphans)
+//   amr_coalesce.wgsl:91-172        covered L0 cells <- mean of 4 fine cells;
+//                                   out/in-orphan balance at the seam
+//   amr_force1.wgsl:241-256         RING_FREE_FORCE gather (explode path)
 //
 // The topology path (criterion, decide, grant) is always evaluated in f32 with
 // every operation rounded, which is what the device does, so the two agree
@@ -81,6 +89,107 @@ template <class R> struct Amr2D {
   R cco() const { return R(0.5) * (R(1) - dxL); }  // CELL_CENTRE_AFFINE
   R pos(int bcoord, int fcoord) const { return R(bcoord * RB) - cco() + dxL * R(fcoord - G); }
   int64_t cell1(int slot, int fx, int fy) const { return (int64_t)slot * FB * FB + (int64_t)fy * FB + fx; }
+  static int wrapi(int v, int n) { return ((v % n) + n) % n; }
+  bool covered(int x, int y) const { return blockSlot[(wrapi(y, H) / RB) * NBX + wrapi(x, W) / RB] >= 0; }
+  int64_t rcell(int x, int y) const { return (int64_t)wrapi(y, H) * W + wrapi(x, W); }
+  bool explode_mode() const { return c.iface == 1; }
+
+  // amr_explode.wgsl: the ring of every active tile from L0 at time t.
+  void explode(const std::vector<R> &fr, std::vector<R> &dst) {
+    const Tables &T = tables(9);
+    const int NFX = 2 * W, NFY = 2 * H;
+    for (int s : activeList) {
+      const int bid = slotToBlock[s], bx = bid % NBX, by = bid / NBX;
+      for (int fy = 0; fy < FB; ++fy)
+        for (int fx = 0; fx < FB; ++fx) {
+          if (fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2) continue;
+          const int gx = wrapi(bx * RB2 + fx - G, NFX), gy = wrapi(by * RB2 + fy - G, NFY);
+          const int vx = gx / 2, vy = gy / 2;
+          if (covered(vx, vy)) continue;
+          const int64_t vc = rcell(vx, vy);
+          R fv[9];
+          for (int i = 0; i < 9; ++i) fv[i] = fr[i * N0 + vc];
+          bool okx = false, oky = false;
+          if (c.explode_linear) {
+            okx = !covered(vx - 1, vy) && !covered(vx + 1, vy);
+            oky = !covered(vx, vy - 1) && !covered(vx, vy + 1);
+          }
+          const R dx = (R(gx - 2 * vx) - R(0.5)) * R(0.5), dy = (R(gy - 2 * vy) - R(0.5)) * R(0.5);
+          const int64_t cell = cell1(s, fx, fy);
+          for (int i = 0; i < 9; ++i) {
+            const int ex = T.ex[i], ey = T.ey[i];
+            R o;
+            if (covered(vx + ex, vy + ey)) {
+              o = fv[i];
+              if (c.explode_linear && (okx || oky)) {
+                R Gx = 0, Gy = 0;
+                if (okx) Gx = R(0.5) * (fr[i * N0 + rcell(vx + 1, vy)] - fr[i * N0 + rcell(vx - 1, vy)]);
+                if (oky) Gy = R(0.5) * (fr[i * N0 + rcell(vx, vy + 1)] - fr[i * N0 + rcell(vx, vy - 1)]);
+                const R ef = (Gx * R(ex) + Gy * R(ey)) / R(ex * ex + ey * ey);
+                Gx -= R(ex) * ef;
+                Gy -= R(ey) * ef;
+                o += dx * Gx + dy * Gy;
+              }
+            } else {
+              const int dgx = wrapi(gx + ex, NFX), dgy = wrapi(gy + ey, NFY);
+              const bool into = covered(dgx / 2, dgy / 2) && dgx / RB2 == bx && dgy / RB2 == by;
+              o = into ? fv[i] : R(0);
+            }
+            dst[i * N1 + cell] = o;
+          }
+        }
+    }
+  }
+
+  // amr_coalesce.wgsl: covered L0 cells (time-t buffer) take the mean of the
+  // four fine cells the L0 step will pull; unrefined cells at the seam get
+  // the out-orphans less the in-orphans explode injected.
+  void coalesce(const std::vector<R> &fp, std::vector<R> &fr) {
+    const Tables &T = tables(9);
+    const int NFX = 2 * W, NFY = 2 * H;
+    std::vector<R> out = fr;
+    for (int cy = 0; cy < H; ++cy)
+      for (int cx = 0; cx < W; ++cx) {
+        const int64_t cc = rcell(cx, cy);
+        if (covered(cx, cy)) {
+          const int cbx = cx / RB, cby = cy / RB;
+          const int cs = blockSlot[cby * NBX + cbx];
+          for (int i = 0; i < 9; ++i) {
+            const int tx = cx + T.ex[i], ty = cy + T.ey[i];
+            if (covered(tx, ty)) continue;
+            R sum = 0;
+            for (int k = 0; k < 4; ++k) {
+              const int px = tx * 2 + (k & 1), py = ty * 2 + (k >> 1);
+              sum += fp[i * N1 + cell1(cs, px - cbx * RB2 + G, py - cby * RB2 + G)];
+            }
+            out[i * N0 + cc] = sum * R(0.25);
+          }
+          continue;
+        }
+        bool nearc = false;
+        for (int i = 1; i < 9; ++i) nearc = nearc || covered(cx + T.ex[i], cy + T.ey[i]);
+        if (!nearc) continue;
+        for (int i = 1; i < 9; ++i) {
+          const int ex = T.ex[i], ey = T.ey[i];
+          if (covered(cx + ex, cy + ey)) continue;
+          R sum = 0, nin = 0;
+          for (int k = 0; k < 4; ++k) {
+            const int ox = k & 1, oy = k >> 1;
+            const int pux = (cx + ex) * 2 + ox, puy = (cy + ey) * 2 + oy;
+            const int qx = wrapi(pux - ex, NFX), qy = wrapi(puy - ey, NFY);
+            const int qbx = qx / RB2, qby = qy / RB2;
+            const int qs = blockSlot[qby * NBX + qbx];
+            if (qs >= 0) sum += fp[i * N1 + cell1(qs, qx - qbx * RB2 + G + ex, qy - qby * RB2 + G + ey)];
+            const int chx = wrapi(cx * 2 + ox + ex, NFX), chy = wrapi(cy * 2 + oy + ey, NFY);
+            if (covered(chx / 2, chy / 2)) nin += R(1);
+          }
+          const R own = fr[i * N0 + cc];
+          const R net = sum - nin * own;
+          if (net != R(0)) out[i * N0 + cc] = own + net * R(0.25);
+        }
+      }
+    fr.swap(out);
+  }
 
   R feq(R rho, R ux, R uy, int i) const {
     const Tables &T = tables(9);
@@ -317,6 +426,10 @@ template <class R> struct Amr2D {
           const R ux = uxs + Fx / (R(2) * den), uy = uys + Fy / (R(2) * den);
           const R usq = ux * ux + uy * uy;
           vel1[2 * cell] = ux; vel1[2 * cell + 1] = uy;
+          if (explode_mode() && !(fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2)) {
+            for (int i = 0; i < 9; ++i) fout[i * N1 + cell] = f[i];  // COLLIDE_RING = 0
+            continue;
+          }
           const R dx = std::fmin(wx, fW - R(1) - wx), dy = std::fmin(wy, fH - R(1) - wy);
           const R sw = sponge(std::fmin(dx, dy), R(c.sponge_w));
           const bool solid = c.solid_eq && c.use_bounceback && phi < R(0);
@@ -413,9 +526,19 @@ template <class R> struct Amr2D {
             if (chi >= R(1e-6)) {
               R rho = 0, ux = 0, uy = 0;
               for (int i = 0; i < 9; ++i) {
-                const int sx = std::min(std::max(fx - T.ex[i], 0), FB - 1);
-                const int sy = std::min(std::max(fy - T.ey[i], 0), FB - 1);
-                const R v = f1[0][i * N1 + cell1(s, sx, sy)];
+                const int sx0 = fx - T.ex[i], sy0 = fy - T.ey[i];
+                const int sx = std::min(std::max(sx0, 0), FB - 1);
+                const int sy = std::min(std::max(sy0, 0), FB - 1);
+                int64_t src = cell1(s, sx, sy);
+                if (explode_mode()) {  // RING_FREE_FORCE: resolve as the step's gather does
+                  const int ox = sx0 >= G + RB2 ? 1 : (sx0 < G ? -1 : 0);
+                  const int oy = sy0 >= G + RB2 ? 1 : (sy0 < G ? -1 : 0);
+                  if (ox || oy) {
+                    const int ns = blockSlot[((by + oy + NBY) % NBY) * NBX + (bx + ox + NBX) % NBX];
+                    if (ns >= 0) src = cell1(ns, sx0 - ox * RB2, sy0 - oy * RB2);
+                  }
+                }
+                const R v = f1[0][i * N1 + src];
                 rho += v; ux += v * R(T.ex[i]); uy += v * R(T.ey[i]);
               }
               ux /= std::fmax(rho, R(1e-6)); uy /= std::fmax(rho, R(1e-6));
@@ -447,6 +570,18 @@ template <class R> struct Amr2D {
     if (c.auto_refine && step % c.refine_every == 0) refine_round();
     ++step;
     force_l1();
+    if (explode_mode()) {
+      explode(f0[cur], f1[0]);
+      substep(f1[0], f1[1]);
+      substep(f1[1], f1[0]);
+      coalesce(f1[0], f0[cur]);
+      std::vector<double> mac(4 * N0);
+      step2<R>(root, f0[cur], f0[1 - cur], mac.data());
+      for (int64_t k = 0; k < N0; ++k) { vel0[2 * k] = R(mac[4 * k + 1]); vel0[2 * k + 1] = R(mac[4 * k + 2]); }
+      average(f0[1 - cur]);
+      cur = 1 - cur;
+      return;
+    }
     ghost_fill();
     std::vector<double> mac(4 * N0);
     step2<R>(root, f0[cur], f0[1 - cur], mac.data());

@@ -174,3 +174,66 @@ def test_amr3d_sphere_drag_matches_dense(lbm):
     assert abs(cd_dense - 2.9436) <= 0.02 * 2.9436          # the reference's dense measurement
     assert lateral <= 0.02
     a.close()
+
+
+def test_dynamic_manager_matches_oracle_with_a_moving_body(lbm, oracle):
+    """A sphere towed across the grid by prescribed poses: every decision
+    (decide, drain, free, grant, fill) against the oracle -- topology exactly,
+    fields to FP32 rounding."""
+    dims = (40, 24, 24)
+    body = dict(shape="sphere", centre=(10.3, 11.8, 12.1), a=3.0, v=(0.25, 0.0, 0.0))
+    c = lbm.amr3d_config(19, dims, refine="body", margin=2.0, dynamic=1, manage_every=4, slot_headroom=2.0,
+                         tau=0.62, has_body=1, use_bounceback=1, body=body)
+    n = int(np.prod(dims))
+    mac = np.zeros((n, 4), np.float32)
+    mac[:, 0] = 1.0
+    mac[:, 1] = 0.03
+    a = lbm.Amr3D(c)
+    o = oracle.Amr3D(c, capacity=a.slots)
+    a.init_macro(mac)
+    o.seed(mac.astype(np.float64))
+    moved = []
+    for k in range(6):
+        for _ in range(4):
+            a.step(1)
+            o.step(1)
+        # tow the body 1 cell (4 steps x 0.25) and tell both
+        b = a.cfg.root.body
+        nb = lbm.make_body("sphere", (b.cx + 1.0, b.cy, b.cz), a=3.0, v=(0.25, 0.0, 0.0))
+        a.set_body(nb)
+        o.set_body(nb)
+        ta, to = a.topology(), o.topology()
+        assert np.array_equal(ta["block_slot"], to[0]), k
+        assert np.array_equal(ta["slot_to_block"], to[1]), k
+        moved.append(int((ta["block_slot"] >= 0).sum()))
+    assert a.pool_stats() == o.pool_stats()
+    assert a.pool_stats()["decisions"] == 6 and a.pool_stats()["refusals"] == 0
+    gfc, gmac = a.read_coarse()
+    ofc, omac, ofp, _ = o.read()
+    gfp, _ = a.read_pool()
+    assert rel_l2(gfc.astype(np.float64), ofc) <= 5e-6
+    used = np.repeat(to[1] >= 0, a.fb ** 3)
+    assert rel_l2(gfp[:, used].astype(np.float64), ofp[:, used]) <= 5e-6
+    assert rel_l2(gmac[:, 1:4].astype(np.float64), omac[:, 1:4]) <= 5e-4
+    a.close()
+
+
+def test_dynamic_manager_changes_nothing_for_a_pinned_body(lbm):
+    """sphere-amr-dynamic: the decisions re-derive the same block set, so the
+    run is bit-identical to the static one (the reference's exact gate)."""
+    from getting_air_b200 import scenarios as sc
+    s = sc.sphere(n=12, u0=0.05, re=20, dims=(96, 64, 64))
+    runs = []
+    for dyn in (0, 1):
+        c = lbm.amr3d_config(19, s["dims"], refine="body", margin=2.0, dynamic=dyn, manage_every=8, **s["kw"])
+        a = lbm.Amr3D(c)
+        a.init_macro(s["mac"])
+        a.step(64)
+        f, mac = a.read_coarse()
+        runs.append((f, mac, a.forces(), a.pool_stats(), a.topology()["block_slot"]))
+        a.close()
+    (f0, m0, F0, _, b0), (f1, m1, F1, st, b1) = runs
+    assert st["decisions"] == 8 and st["refusals"] == 0
+    assert np.array_equal(b0, b1)
+    assert np.array_equal(f0, f1) and np.array_equal(m0, m1)
+    assert np.array_equal(F0, F1)
