@@ -165,6 +165,13 @@ def _load() -> C.CDLL:
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), F, C.POINTER(C.c_uint32)], I),
         "lbm_amr2d_cell_updates": ([P], C.c_int64),
         "lbm_amr2d_sync": ([P], I),
+        "lbm_amr2d_write_pool": ([P, F, F], I),
+        "lbm_amr2d_read_parent_slots": ([P, C.POINTER(C.c_int32)], I),
+        "lbm_amr2d_write_topology": ([P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32), C.c_int32], I),
+        "lbm_amr2d_get_step": ([P], C.c_int64),
+        "lbm_amr2d_set_step": ([P, C.c_int64], I),
+        "lbm_amr2d_set_body": ([P, C.POINTER(Body)], I),
         "lbm_server_create": ([C.c_int64, C.POINTER(P)], I),
         "lbm_server_destroy": ([P], None),
         "lbm_server_last_error": ([P], C.c_char_p),
@@ -695,6 +702,33 @@ class Amr2D:
 
     def sync(self):
         self._check(lib.lbm_amr2d_sync(self._h))
+
+    def write_pool(self, f, vel):
+        f = np.ascontiguousarray(f, np.float32).reshape(9, -1)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 2)
+        self._check(lib.lbm_amr2d_write_pool(self._h, _ptr(f, C.c_float), _ptr(vel, C.c_float)))
+
+    def parent_slots(self) -> np.ndarray:
+        out = np.zeros(self.slots, np.int32)
+        self._check(lib.lbm_amr2d_read_parent_slots(self._h, _ptr(out, C.c_int32)))
+        return out
+
+    def write_topology(self, block_slot, slot_to_block, parent_slot, free_list, free_count: int):
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        bs, sb, ps, fl = i32(block_slot), i32(slot_to_block), i32(parent_slot), i32(free_list)
+        self._check(lib.lbm_amr2d_write_topology(self._h, _ptr(bs, C.c_int32), _ptr(sb, C.c_int32),
+                                                  _ptr(ps, C.c_int32), _ptr(fl, C.c_int32), int(free_count)))
+
+    @property
+    def macro_step(self) -> int:
+        return int(lib.lbm_amr2d_get_step(self._h))
+
+    @macro_step.setter
+    def macro_step(self, step: int):
+        self._check(lib.lbm_amr2d_set_step(self._h, int(step)))
+
+    def set_body(self, body: Body):
+        self._check(lib.lbm_amr2d_set_body(self._h, C.byref(body)))
 
 
 def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, boxfrac: float = 0.5,

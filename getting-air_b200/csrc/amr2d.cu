@@ -988,4 +988,83 @@ int lbm_amr2d_sync(lbm_amr2d *a) {
   return LBM_OK;
 }
 
+int lbm_amr2d_write_pool(lbm_amr2d *a, const float *f, const float *vel) {
+  if (!a || !f || !vel) return a ? afail(a, LBM_EINVAL, "NULL argument") : LBM_EINVAL;
+  const AmrParams &p = a->p;
+  ACK(a, cudaMemcpyAsync(a->f1[0], f, 9 * p.N1 * 4, cudaMemcpyHostToDevice, a->stream));
+  ACK(a, cudaMemcpyAsync(a->vel1, vel, p.N1 * 8, cudaMemcpyHostToDevice, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr2d_read_parent_slots(lbm_amr2d *a, int32_t *parent_slot) {
+  if (!a || !parent_slot) return a ? afail(a, LBM_EINVAL, "NULL argument") : LBM_EINVAL;
+  ACK(a, cudaMemcpyAsync(parent_slot, a->p.parentSlot, a->p.S * 4, cudaMemcpyDeviceToHost, a->stream));
+  ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr2d_write_topology(lbm_amr2d *a, const int32_t *block_slot, const int32_t *slot_to_block,
+                             const int32_t *parent_slot, const int32_t *free_list, int32_t free_count) {
+  if (!a || !block_slot || !slot_to_block || !parent_slot || !free_list)
+    return a ? afail(a, LBM_EINVAL, "NULL argument") : LBM_EINVAL;
+  const AmrParams &p = a->p;
+  const int nb = p.NBX * p.NBY, nq = p.S / 4;
+  if (free_count < 0 || free_count > nq) return afail(a, LBM_EINVAL, "free_count outside [0, max_slots/4]");
+  for (int b = 0; b < nb; ++b) {
+    const int s = block_slot[b];
+    if (s < -1 || s >= p.S || (s >= 0 && slot_to_block[s] != b))
+      return afail(a, LBM_EINVAL, "block_slot and slot_to_block are not inverse maps");
+  }
+  std::vector<int> quad_used(nq, 0), quad_free(nq, 0), active;
+  for (int s = 0; s < p.S; ++s) {
+    const int b = slot_to_block[s];
+    if (b < -1 || b >= nb || (b >= 0 && block_slot[b] != s))
+      return afail(a, LBM_EINVAL, "block_slot and slot_to_block are not inverse maps");
+    if (b >= 0) {
+      quad_used[s / 4] += 1;
+      active.push_back(s);
+    }
+  }
+  for (int q = 0; q < nq; ++q)
+    if (quad_used[q] != 0 && quad_used[q] != 4) return afail(a, LBM_EINVAL, "a quad is partly in use");
+  for (int k = 0; k < free_count; ++k) {
+    const int q = free_list[k];
+    if (q < 0 || q >= nq || quad_used[q] || quad_free[q]++)
+      return afail(a, LBM_EINVAL, "the free list names a quad in use, twice, or out of range");
+  }
+  const int counts[2] = {free_count, (int)active.size()};
+  active.resize(p.S, -1);
+  cudaStream_t st = a->stream;
+  ACK(a, cudaMemcpyAsync(p.blockSlot, block_slot, nb * 4, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaMemcpyAsync(p.slotToBlock, slot_to_block, p.S * 4, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaMemcpyAsync(p.parentSlot, parent_slot, p.S * 4, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaMemcpyAsync(p.freeList, free_list, nq * 4, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaMemcpyAsync(p.counts, counts, 8, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaMemcpyAsync(p.activeList, active.data(), p.S * 4, cudaMemcpyHostToDevice, st));
+  ACK(a, cudaStreamSynchronize(st));
+  return LBM_OK;
+}
+
+int64_t lbm_amr2d_get_step(const lbm_amr2d *a) { return a ? a->step : -1; }
+
+int lbm_amr2d_set_step(lbm_amr2d *a, int64_t step) {
+  if (!a || step < 0) return a ? afail(a, LBM_EINVAL, "step must be >= 0") : LBM_EINVAL;
+  a->step = step;
+  return LBM_OK;
+}
+
+int lbm_amr2d_set_body(lbm_amr2d *a, const lbm_body *body) {
+  if (!a || !body) return a ? afail(a, LBM_EINVAL, "body is NULL") : LBM_EINVAL;
+  if (body->shape != LBM_SHAPE_ELLIPSE || !(body->a > 0.f) || !(body->b > 0.f))
+    return afail(a, LBM_EINVAL, "the body must be an ellipse (a, b > 0)");
+  ACK(a, cudaStreamSynchronize(a->stream));
+  a->cfg.body = *body;
+  a->p.body = *body;
+  a->root.body = *body;
+  for (auto &g : a->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return LBM_OK;
+}
+
 }  // extern "C"

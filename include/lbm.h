@@ -352,6 +352,23 @@ int lbm_amr2d_read_topology(lbm_amr2d *a, int32_t *block_slot, int32_t *slot_to_
 int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a);
 int lbm_amr2d_sync(lbm_amr2d *a);
 
+/* State restore for checkpoints (the snapshot save/load of
+ * main-cylinder-amr.js:1524-1705, whose version-7 layout the Python host
+ * layer writes): the pool's time-t populations (9 planes of max_slots*FB^2)
+ * and velocity ([ux,uy] per cell); the pool topology -- block_slot
+ * (NBX*NBY), slot_to_block and parent_slot (max_slots), the quad free list
+ * (max_slots/4 entries, the first free_count live) -- checked for
+ * consistency (inverse maps, whole quads, no quad both free and in use) and
+ * refused with LBM_EINVAL otherwise, the active list rebuilt from it; the
+ * macro-step counter that schedules refine rounds; the body pose. */
+int lbm_amr2d_write_pool(lbm_amr2d *a, const float *f, const float *vel);
+int lbm_amr2d_read_parent_slots(lbm_amr2d *a, int32_t *parent_slot);
+int lbm_amr2d_write_topology(lbm_amr2d *a, const int32_t *block_slot, const int32_t *slot_to_block,
+                             const int32_t *parent_slot, const int32_t *free_list, int32_t free_count);
+int64_t lbm_amr2d_get_step(const lbm_amr2d *a);
+int lbm_amr2d_set_step(lbm_amr2d *a, int64_t step);
+int lbm_amr2d_set_body(lbm_amr2d *a, const lbm_body *body);
+
 /* ---- 3D block-structured AMR (D3Q19 / D3Q27, FP32) -----------------------
  * The dense L0 grid plus one pool level: blocks of RB^3 L0 cells, a refined
  * block owning a tile of FB^3 = (2 RB + 4)^3 cells at half spacing (interior
