@@ -38,7 +38,10 @@ namespace lbm {
 
 namespace {
 
-__device__ __forceinline__ int wrapi(int v, int n) { return ((v % n) + n) % n; }
+// Periodic wrap of an index at most one period outside [0, n) -- every index
+// here is a cell, block or fine coordinate a step or two past an edge --
+// without an integer division.
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 __device__ __forceinline__ bool covered(const Amr3Params &p, int x, int y, int z) {
   x = wrapi(x, p.nx); y = wrapi(y, p.ny); z = wrapi(z, p.nz);
@@ -58,15 +61,15 @@ struct TileCell {
   int64_t cell;
 };
 
+// Tile kernels run one CTA per (fz, slot) with an FB x FB thread block, so a
+// thread's tile coordinates need no division.
 __device__ __forceinline__ bool tile_cell(const Amr3Params &p, TileCell &t) {
-  const int k = blockIdx.x * kTileThreads + threadIdx.x;
-  if (k >= p.T3) return false;
   t.slot = blockIdx.y;
   const int id = p.slot_to_block[t.slot];
   if (id < 0) return false;
   t.bx = id % p.nbx; t.by = (id / p.nbx) % p.nby; t.bz = id / (p.nbx * p.nby);
-  t.fx = k % p.FB; t.fy = (k / p.FB) % p.FB; t.fz = k / (p.FB * p.FB);
-  t.cell = (int64_t)t.slot * p.T3 + k;
+  t.fx = threadIdx.x; t.fy = threadIdx.y; t.fz = blockIdx.x;
+  t.cell = (int64_t)t.slot * p.T3 + (t.fz * p.FB + t.fy) * p.FB + t.fx;
   return true;
 }
 
@@ -82,7 +85,7 @@ __device__ __forceinline__ float feq3(int i, float rho, float ux, float uy, floa
 // interpCoarseToFine3: rho and u interpolated, f = feq(rho, u) + DC-rescaled
 // interpolated fneq (common_d3_pool.wgsl:192-220).
 template <int Q>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileMaxThreads)
     amr3_interp(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p,
                 int ring_only, const unsigned char *__restrict__ only_new) {
   using L = Lattice<Q>;
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // common_d3_moments.wgsl: the tiles' mac from their f.
 template <int Q>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileMaxThreads)
     amr3_moments(const float *__restrict__ fp, float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
   using L = Lattice<Q>;
   TileCell t;
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // ---- explode ------------------------------------------------------------
 template <int Q>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileMaxThreads)
     amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p) {
   using L = Lattice<Q>;
   TileCell t;
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // ---- one pool substep ----------------------------------------------------
 template <int Q>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileMaxThreads)
     amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
                  const __grid_constant__ Amr3Params p) {
   using L = Lattice<Q>;
@@ -758,13 +761,14 @@ int afail(lbm_amr3d *a, int code, const std::string &m) {
                    std::string(#call) + ": " + cudaGetErrorString(e_));                                    \
   } while (0)
 
-dim3 tile_grid(const lbm_amr3d *a) { return dim3((a->p.T3 + kTileThreads - 1) / kTileThreads, a->p.slots); }
+dim3 tile_grid(const lbm_amr3d *a) { return dim3(a->p.FB, a->p.slots); }
+dim3 tile_block(const lbm_amr3d *a) { return dim3(a->p.FB, a->p.FB); }
 
 cudaError_t launch_interp(lbm_amr3d *a, const float *fc, int ring_only, const unsigned char *only_new) {
   if (!a->p.slots) return cudaSuccess;
   const dim3 g = tile_grid(a);
   AMR3_DISPATCH(a->q,
-                amr3_interp<Q><<<g, kTileThreads, 0, a->stream>>>(fc, a->fp[0], a->p, ring_only, only_new));
+                amr3_interp<Q><<<g, tile_block(a), 0, a->stream>>>(fc, a->fp[0], a->p, ring_only, only_new));
 }
 
 // One decision of the manager before the macro-step from L0 parity `cp`
@@ -801,7 +805,7 @@ cudaError_t launch_manage(lbm_amr3d *a, int cp) {
 cudaError_t launch_moments(lbm_amr3d *a) {
   if (!a->p.slots) return cudaSuccess;
   const dim3 g = tile_grid(a);
-  AMR3_DISPATCH(a->q, amr3_moments<Q><<<g, kTileThreads, 0, a->stream>>>(a->fp[0], a->macp, a->p));
+  AMR3_DISPATCH(a->q, amr3_moments<Q><<<g, tile_block(a), 0, a->stream>>>(a->fp[0], a->macp, a->p));
 }
 
 // One macro-step from L0 parity `cp`.
@@ -820,11 +824,11 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     auto body = [&]() -> cudaError_t {
       AMR3_DISPATCH(q, {
         if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
-        amr3_explode<Q><<<g, kTileThreads, 0, st>>>(a->fc[cp], a->fp[0], p);
+        amr3_explode<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p);
         Amr3Params pa = p;
         pa.write_mac = 0;
-        amr3_substep<Q><<<g, kTileThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
-        amr3_substep<Q><<<g, kTileThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
+        amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
+        amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
         if (gc) amr3_coalesce<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
       });
     };

@@ -16,7 +16,9 @@
 namespace lbm {
 
 constexpr int kAmrGhost = 2;
-constexpr int kTileThreads = 128;
+constexpr int kTileThreads = 128;    // 1D pool kernels (force, drain, coalesce)
+constexpr int kMaxAmrRb = 8;         // tiles up to FB = 20: FB x FB threads per CTA
+constexpr int kTileMaxThreads = (2 * kMaxAmrRb + 4) * (2 * kMaxAmrRb + 4);
 
 struct Amr3Params {
   int nx, ny, nz, rb, nbx, nby, nbz;

@@ -88,7 +88,7 @@ int amr3_validate(const lbm_amr3d_config *c, std::string &why) {
   if (r.q != 19 && r.q != 27) { why = "3D AMR runs D3Q19 or D3Q27"; return LBM_EINVAL; }
   if (r.storage != LBM_STORE_FP32) { why = "3D AMR stores FP32 populations"; return LBM_ENOTSUP; }
   if (c->levels != 2) { why = "levels must be 2 (one pool level)"; return LBM_ENOTSUP; }
-  if (c->rb < 2 || c->rb > 16) { why = "rb must be in [2, 16]"; return LBM_EINVAL; }
+  if (c->rb < 2 || c->rb > kMaxAmrRb) { why = "rb must be in [2, 8]"; return LBM_EINVAL; }
   if (r.nx % c->rb || r.ny % c->rb || r.nz % c->rb) { why = "every dimension must be a multiple of rb"; return LBM_EINVAL; }
   if (c->refine < LBM_REFINE_BODY || c->refine > LBM_REFINE_LIST) { why = "unknown refine mode"; return LBM_EINVAL; }
   if (c->refine == LBM_REFINE_BODY && !r.has_body) { why = "refine = body needs a body"; return LBM_EINVAL; }
