@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   const float ux = fmaf(Fx, hinv, uxs), uy = fmaf(Fy, hinv, uys), uz = fmaf(Fz, hinv, uzs);
   const bool in_tile = interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz);
   MemSink<float> sink{fout, p.P, (int)t.cell, c.pk};
-  if (!in_tile) {
-    // the ring advects and does not collide (COLLIDE_RING = 0)
+  if (!in_tile && !p.collide_ring) {
+    // explode/coalesce: the ring advects and does not collide (COLLIDE_RING = 0)
     if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
 #pragma unroll
     for (int i = 0; i < Q; ++i) fout[(int64_t)i * p.P + t.cell] = f[i];
@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(kTileThreads)
   if (k >= rb3) return;
   const int slot = blockIdx.y;
   const int id = p.slot_to_block[slot];
-  if (id < 0 || want[id]) return;
+  if (id < 0 || (want && want[id])) return;
   const int lc[3] = {k % p.rb, (k / p.rb) % p.rb, k / (p.rb * p.rb)};
   const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
   float rs = 0.f, ms0 = 0.f, ms1 = 0.f, ms2 = 0.f, fneq[Q];
@@ -815,6 +815,33 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
   const int q = a->q;
   cudaStream_t st = a->stream;
   cudaError_t e = cudaSuccess;
+  if (p.slots && a->cfg.iface == 1) {
+    // ?interface=interp (main-3d.js:3343-3356): the L0 step first, then the
+    // ring interpolated from L0 at t, two substeps with the ring collided,
+    // and every tile restricted into L0's new buffer.
+    StepParams sp = a->sp;
+    sp.write_mac = write_mac ? 1 : 0;
+    const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
+    const dim3 g = tile_grid(a);
+    const int rb3 = p.rb * p.rb * p.rb;
+    const dim3 gd((rb3 + kTileThreads - 1) / kTileThreads, p.slots);
+    const int r3 = p.RB2 * p.RB2 * p.RB2;
+    const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
+    const float tc = a->cfg.root.tau, tf = 2.f * tc - 0.5f;
+    const float f2c_rescale = 2.f * (tc - 1.f) / (tf - 1.f);
+    AMR3_DISPATCH(q, {
+      if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
+      amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp, a->d_block_slot, p.rb,
+                                                   p.nbx, p.nby);
+      amr3_interp<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p, 1, nullptr);
+      Amr3Params pa = p;
+      pa.write_mac = 0;
+      amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
+      amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
+      amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
+                                                 f2c_rescale);
+    });
+  }
   if (p.slots) {
     const dim3 g = tile_grid(a);
     const int r3 = p.RB2 * p.RB2 * p.RB2;
@@ -976,6 +1003,7 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
   p.rescale_c2f = 0.5f * (tf - 1.f) / (tc - 1.f);
   p.chi_eps_f = r.chi_eps * 0.5f;
   p.linear = c->explode_linear ? 1 : 0;
+  p.collide_ring = c->iface == 1 ? 1 : 0;
   fill_step_params(r, p.N, 0, a->sp);
   a->sp.force_on = 0;
   {

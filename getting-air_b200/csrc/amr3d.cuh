@@ -34,6 +34,7 @@ struct Amr3Params {
   float rescale_c2f;            // 0.5 (tau_f - 1) / (tau_c - 1)
   float chi_eps_f;              // the chi band on the fine level (CHI_EPS / 2)
   int linear;                   // linear explosion
+  int collide_ring;             // interp interface: the ring collides (COLLIDE_RING = 1)
   int write_mac;
   double *partials;             // pool force: 8 doubles per force CTA
   unsigned int *counter;

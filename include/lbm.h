@@ -400,7 +400,11 @@ typedef struct {
   int32_t manage_start;    /* first macro-step that decides (0)               */
   int32_t max_slots;       /* pool capacity; 0 = initial set (x slot_headroom when dynamic) */
   float slot_headroom;     /* 1.5                                             */
-  int32_t reserved[5];     /* zero                                            */
+  int32_t iface;           /* 0: explode/coalesce (the reference's default);
+                              1: interp -- the L0 step first, the ring
+                              interpolated from L0, ring collided, tiles
+                              restricted into L0 (main-3d.js:3343-3356)       */
+  int32_t reserved[4];     /* zero                                            */
 } lbm_amr3d_config;
 
 typedef struct lbm_amr3d lbm_amr3d;

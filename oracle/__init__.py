@@ -194,7 +194,7 @@ class Amr3D:
         L = lib()
         L.oracle_amr3d_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                           C.POINTER(C.c_int32), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                          C.c_int]
+                                          C.c_int, C.c_int]
         L.oracle_amr3d_pool_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
         L.oracle_amr3d_set_body.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_amr3d_create.restype = C.c_void_p
@@ -214,7 +214,7 @@ class Amr3D:
             lst = arr.ctypes.data_as(C.POINTER(C.c_int32))
         self._h = L.oracle_amr3d_create(C.addressof(r), cfg.rb, cfg.refine, cfg.margin, cfg.boxfrac, lst,
                                         cfg.explode_linear, int(fp32), int(capacity), int(cfg.dynamic),
-                                        int(cfg.manage_every), int(cfg.manage_start))
+                                        int(cfg.manage_every), int(cfg.manage_start), int(cfg.iface))
         if not self._h:
             raise ValueError("oracle_amr3d_create failed")
         nbl = int(np.prod(self.nb))

@@ -17,7 +17,11 @@
 //   common_d3_step.wgsl:110      coarse step skipping covered blocks
 //   common_d3_force_pool.wgsl    pool force, dx^2 and dx^3 weights
 //   main-3d.js:3219-3341         macro-step order: force, explode, two fine
-//                                substeps, coalesce, coarse step
+//                                substeps, coalesce, coarse step; with
+//                                ?interface=interp (:3343-3356) the coarse
+//                                step first, the ring interpolated
+//                                (GHOST_ONLY), substeps collide the ring,
+//                                common_d3_amr_average.wgsl into the new L0
 //   common_d3_manage.wgsl        dynamic refinement: decide (boxNearBody in
 //                                f32 with the lead of the body's motion),
 //                                drain (common_d3_amr_average.wgsl, DYING_ONLY),
@@ -123,6 +127,7 @@ template <class R> struct Amr3D {
   std::vector<double> macc, macp;
   int cp = 0;
   int linear = 1;
+  int interp = 0;  // ?interface=interp instead of explode/coalesce
   // dynamic refinement
   int dynamic = 0, manage_every = 16, manage_start = 0;
   double margin = 2.0;
@@ -584,27 +589,15 @@ template <class R> struct Amr3D {
     return false;
   }
 
-  void manage() {
-    const lbm_body &b = c.body;
-    float rc = b.shape == LBM_SHAPE_SPHERE ? b.a : (b.shape == LBM_SHAPE_SPHEROID ? std::fmax(b.a, b.c)
-                                                  : std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c));
-    const float lead = (float)manage_every * (std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
-                                              std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc);
-    const float reach = (float)margin + lead;
-    want.assign(t.nb, 0);
-    const float half = 0.5f * (float)t.rb;
-    for (int id = 0; id < t.nb; ++id) {
-      const int bx = id % t.nbx, by = (id / t.nbx) % t.nby, bz = id / (t.nbx * t.nby);
-      want[id] = box_near(b, (float)(bx * t.rb) + half, (float)(by * t.rb) + half, (float)(bz * t.rb) + half, half,
-                          reach);
-    }
-    // drain the dying tiles into the time-t L0 buffer
+  // common_d3_amr_average.wgsl: each tile restricted into its L0 cells (feq
+  // of the children's mean rho and mass-weighted u plus the F2C-rescaled
+  // mean fneq) and their mac; with `want`, only the tiles it no longer wants.
+  void restrict_tiles(std::vector<R> &fco, const uint8_t *wanted) {
     const R tc = R(c.tau), tf = R(2) * tc - R(0.5);
     const R f2c = R(2) * (tc - R(1)) / (tf - R(1));
-    std::vector<R> &fco = fc[cp];
     for (int s = 0; s < t.slots; ++s) {
       const int id = t.slot_to_block[s];
-      if (id < 0 || want[id]) continue;
+      if (id < 0 || (wanted && wanted[id])) continue;
       const int b3[3] = {id % t.nbx, (id / t.nbx) % t.nby, id / (t.nbx * t.nby)};
       for (int lz = 0; lz < t.rb; ++lz)
         for (int ly = 0; ly < t.rb; ++ly)
@@ -631,6 +624,24 @@ template <class R> struct Amr3D {
             macc[4 * dst + 1] = (double)ua; macc[4 * dst + 2] = (double)va; macc[4 * dst + 3] = (double)wa;
           }
     }
+  }
+
+  void manage() {
+    const lbm_body &b = c.body;
+    float rc = b.shape == LBM_SHAPE_SPHERE ? b.a : (b.shape == LBM_SHAPE_SPHEROID ? std::fmax(b.a, b.c)
+                                                  : std::sqrt(b.a * b.a + b.b * b.b + b.c * b.c));
+    const float lead = (float)manage_every * (std::sqrt(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
+                                              std::sqrt(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc);
+    const float reach = (float)margin + lead;
+    want.assign(t.nb, 0);
+    const float half = 0.5f * (float)t.rb;
+    for (int id = 0; id < t.nb; ++id) {
+      const int bx = id % t.nbx, by = (id / t.nbx) % t.nby, bz = id / (t.nbx * t.nby);
+      want[id] = box_near(b, (float)(bx * t.rb) + half, (float)(by * t.rb) + half, (float)(bz * t.rb) + half, half,
+                          reach);
+    }
+    // drain the dying tiles into the time-t L0 buffer
+    restrict_tiles(fc[cp], want.data());
     // coarsen then refine over the free-slot stack, ascending block id
     std::fill(slot_new.begin(), slot_new.end(), 0);
     for (int id = 0; id < t.nb; ++id) {
@@ -658,10 +669,26 @@ template <class R> struct Amr3D {
     if (dynamic && step_count >= manage_start && (step_count - manage_start) % manage_every == 0) manage();
     ++step_count;
     if (force_out) force(fp[0], force_out);
+    if (interp) {
+      // ?interface=interp (main-3d.js:3343-3356): the L0 step first, the ring
+      // interpolated from L0 at t, two substeps with the ring collided, the
+      // tiles restricted into L0's new buffer
+      l0_step(want_mac);
+      interp_fill(fc[1 - cp], fp[0], true);
+      substep(fp[0], fp[1], true);
+      substep(fp[1], fp[0], true);
+      restrict_tiles(fc[cp], nullptr);
+      return;
+    }
     explode(fc[cp], fp[0]);
     substep(fp[0], fp[1], false);
     substep(fp[1], fp[0], false);
     coalesce(fp[0], fc[cp]);
+    l0_step(want_mac);
+  }
+
+  // The L0 step from parity cp, covered blocks skipped; flips cp.
+  void l0_step(bool want_mac) {
     Cover cov;
     cov.block_slot = t.block_slot.data();
     cov.rb = t.rb; cov.nbx = t.nbx; cov.nby = t.nby;
@@ -687,7 +714,7 @@ template <class R> struct Amr3D {
 
 template <class R>
 Amr3D<R> *make(const lbm_config &c, int rb, int mode, double margin, double frac, const int32_t *list, int linear,
-               int capacity, int dynamic, int manage_every, int manage_start) {
+               int capacity, int dynamic, int manage_every, int manage_start, int interp) {
   auto *a = new Amr3D<R>();
   a->c = c;
   a->Q = c.q;
@@ -701,6 +728,7 @@ Amr3D<R> *make(const lbm_config &c, int rb, int mode, double margin, double frac
     a->t.slots = capacity;
   }
   a->dynamic = dynamic;
+  a->interp = interp;
   a->manage_every = manage_every;
   a->manage_start = manage_start;
   a->margin = margin;
@@ -730,11 +758,14 @@ extern "C" {
 
 // Builds the two-level hierarchy (topology only; oracle_amr3d_seed fills it).
 void *oracle_amr3d_create(const lbm_config *c, int rb, int mode, double margin, double frac, const int32_t *list,
-                          int linear, int fp32, int capacity, int dynamic, int manage_every, int manage_start) {
+                          int linear, int fp32, int capacity, int dynamic, int manage_every, int manage_start,
+                          int interp) {
   if (!c || c->q == 9 || rb < 1 || c->nx % rb || c->ny % rb || c->nz % rb) return nullptr;
   auto *h = new Handle{fp32, nullptr};
-  if (fp32) h->p = make<float>(*c, rb, mode, margin, frac, list, linear, capacity, dynamic, manage_every, manage_start);
-  else h->p = make<double>(*c, rb, mode, margin, frac, list, linear, capacity, dynamic, manage_every, manage_start);
+  if (fp32)
+    h->p = make<float>(*c, rb, mode, margin, frac, list, linear, capacity, dynamic, manage_every, manage_start, interp);
+  else
+    h->p = make<double>(*c, rb, mode, margin, frac, list, linear, capacity, dynamic, manage_every, manage_start, interp);
   return h;
 }
 

@@ -237,3 +237,68 @@ def test_dynamic_manager_changes_nothing_for_a_pinned_body(lbm):
     assert np.array_equal(b0, b1)
     assert np.array_equal(f0, f1) and np.array_equal(m0, m1)
     assert np.array_equal(F0, F1)
+
+
+@pytest.mark.parametrize("name", ["box-q19", "sphere-bounceback"])
+def test_amr3d_interp_interface_matches_oracle(lbm, oracle, name):
+    """?interface=interp: the L0 step first, the ring interpolated from L0,
+    the ring collided, every tile restricted into L0's new buffer."""
+    case = CASES[name]
+    q, dims = case["q"], case["dims"]
+    c = lbm.amr3d_config(q, dims, refine=case["refine"], iface=1, **case["kw"])
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(2)
+    mac = np.zeros((n, 4), np.float32)
+    mac[:, 0] = 1.0 + 0.002 * rng.standard_normal(n)
+    mac[:, 1:] = 0.01 * rng.standard_normal((n, 3))
+    a = lbm.Amr3D(c)
+    o = oracle.Amr3D(c)
+    a.init_macro(mac)
+    o.seed(mac.astype(np.float64))
+    a.step(6)
+    of = o.step(6)
+    gfc, gmac = a.read_coarse()
+    gfp, _ = a.read_pool()
+    ofc, omac, ofp, _ = o.read()
+    assert rel_l2(gfc.astype(np.float64), ofc) <= 2e-6
+    assert rel_l2(gfp.astype(np.float64), ofp) <= 2e-6
+    assert rel_l2(gmac[:, 1:4].astype(np.float64), omac[:, 1:4]) <= 2e-4
+    if c.root.has_body:
+        g = a.forces()
+        scale = max(np.abs(of[-1, :6]).max(), 1e-6)
+        assert np.abs(g - of[-1, :6]).max() <= 1e-3 * scale
+    a.close()
+
+
+def test_amr3d_interp_box_field_within_reference_bounds(lbm):
+    """amr-box-RB4 (benchmarks/d3.json amr_box_cases): the interp coupling's
+    first-order seam, scored against its own recorded values -- field L2rel
+    9.012e-3 and decay-rate error 1.024e-2 measured by the reference, bounds
+    0.012 and 0.014."""
+    N, tau, u0 = 48, 0.8, 0.04
+    nu = (tau - 0.5) / 3
+    k = 2 * math.pi / N
+    td = 1 / (nu * k * k)
+    c = lbm.amr3d_config(19, (N, N, N), refine="box", boxfrac=0.5, tau=tau, iface=1)
+    a = lbm.Amr3D(c)
+    a.init_macro(beltrami_mac(N, u0))
+    stride = max(1, N // 24)
+    sel = np.zeros((N, N, N), bool)
+    sel[::stride, ::stride, ::stride] = True
+    sel = sel.ravel()
+    samples, prev = [], 0
+    for frac in (0.25, 0.5):
+        t = round(frac * td)
+        a.step(t - prev)
+        prev = t
+        _, mac = a.read_coarse()
+        u = mac[sel, 1:4].astype(np.float64)
+        e = beltrami(N, u0, nu, t)[sel]
+        samples.append((t, rel_l2(u, e), math.sqrt((u ** 2).sum(1).mean())))
+    l2 = max(s[1] for s in samples)
+    (ta, _, ra), (tb, _, rb) = samples
+    rate_err = abs(-math.log(rb / ra) / (tb - ta) - 1 / td) * td
+    print(f"interp field L2rel {[s[1] for s in samples]}, decay-rate rel err {rate_err:.3e}")
+    assert l2 <= 0.012
+    assert rate_err <= 0.014
+    a.close()
