@@ -102,7 +102,7 @@ class Amr3DConfig(C.Structure):
                 ("margin", C.c_float), ("boxfrac", C.c_float), ("explode_linear", C.c_int32),
                 ("dynamic", C.c_int32), ("manage_every", C.c_int32), ("manage_start", C.c_int32),
                 ("max_slots", C.c_int32), ("slot_headroom", C.c_float), ("iface", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("reflux", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 REFINE = {"body": 0, "box": 1, "bar": 2, "slab": 3, "all": 4, "list": 5}
@@ -734,7 +734,8 @@ class Amr2D:
 
 def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, boxfrac: float = 0.5,
                  explode_linear: int = 1, dynamic: int = 0, manage_every: int = 16, manage_start: int = 0,
-                 max_slots: int = 0, slot_headroom: float = 1.5, iface: int = 0, **root_kw) -> Amr3DConfig:
+                 max_slots: int = 0, slot_headroom: float = 1.5, iface: int = 0, reflux: int = 0,
+                 **root_kw) -> Amr3DConfig:
     """lbm_amr3d_config: the L0 grid/physics as config_from's keywords, plus the hierarchy."""
     c = Amr3DConfig()
     rc = lib.lbm_amr3d_config_default(C.byref(c), q, *dims)
@@ -752,6 +753,7 @@ def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, 
     c.max_slots = max_slots
     c.slot_headroom = slot_headroom
     c.iface = iface
+    c.reflux = reflux
     return c
 
 

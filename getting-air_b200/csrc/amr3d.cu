@@ -406,6 +406,125 @@ __global__ void __launch_bounds__(kTileThreads)
   }
 }
 
+// ---- flux correction of the interp interface -------------------------------
+// (common_d3_amr_flux.wgsl, common_d3_amr_reflux.wgsl; opt-in, as the
+// reference's ?reflux=1.) Seam cells: unrefined L0 cells whose block touches
+// a refined block on the side (face, edge or corner) the cell sits at.
+__device__ __forceinline__ bool seam_cell(const Amr3Params &p, int x, int y, int z, int id) {
+  if (p.block_slot[id] >= 0) return false;
+  const int c3[3] = {x, y, z}, b[3] = {x / p.rb, y / p.rb, z / p.rb}, nb[3] = {p.nbx, p.nby, p.nbz};
+  int off[3];
+  for (int a = 0; a < 3; ++a) off[a] = c3[a] % p.rb == 0 ? -1 : ((c3[a] + 1) % p.rb == 0 ? 1 : 0);
+  for (int k = 1; k < 8; ++k) {
+    int q[3];
+    for (int a = 0; a < 3; ++a) q[a] = wrapi(b[a] + ((k >> a) & 1) * off[a], nb[a]);
+    if (p.block_slot[(q[2] * p.nby + q[1]) * p.nbx + q[0]] >= 0) return true;
+  }
+  return false;
+}
+
+// Thread -> L0 cell of an interface block; false when there is none.
+__device__ __forceinline__ bool iface_cell(const Amr3Params &p, int &x, int &y, int &z, int &id) {
+  const int rb3 = p.rb * p.rb * p.rb;
+  const int k = blockIdx.x * kTileThreads + threadIdx.x;
+  if (k >= p.n_iface * rb3) return false;
+  id = p.iface ? p.iface[k / rb3] : k / rb3;
+  if (!p.iface && !p.iface_flag[id]) return false;
+  const int l = k % rb3;
+  x = (id % p.nbx) * p.rb + l % p.rb;
+  y = ((id / p.nbx) % p.nby) * p.rb + (l / p.rb) % p.rb;
+  z = (id / (p.nbx * p.nby)) * p.rb + l / (p.rb * p.rb);
+  return true;
+}
+
+// The mass and momentum the fine level moves across the seam into each seam
+// cell during one substep (the buffer that substep streams), 1/8 per fine cell.
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_flux(const float *__restrict__ fp, float4 *__restrict__ acc, const __grid_constant__ Amr3Params p,
+              int accumulate) {
+  using L = Lattice<Q>;
+  int x, y, z, id;
+  if (!iface_cell(p, x, y, z, id) || !seam_cell(p, x, y, z, id)) return;
+  const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
+  float dm = 0.f, dp0 = 0.f, dp1 = 0.f, dp2 = 0.f;
+  for (int oc = 0; oc < 8; ++oc) {
+    const int pp[3] = {2 * x + (oc & 1), 2 * y + ((oc >> 1) & 1), 2 * z + ((oc >> 2) & 1)};
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+      int q[3], t[3];
+      for (int a = 0; a < 3; ++a) {
+        q[a] = wrapi(pp[a] - e[a], nf[a]);
+        t[a] = wrapi(pp[a] + e[a], nf[a]);
+      }
+      const int so = p.block_slot[((q[2] / p.RB2) * p.nby + q[1] / p.RB2) * p.nbx + q[0] / p.RB2];
+      if (so >= 0) {
+        const int lx = local_in_tile(p, q[0], q[0] / p.RB2, nf[0]), ly = local_in_tile(p, q[1], q[1] / p.RB2, nf[1]),
+                  lz = local_in_tile(p, q[2], q[2] / p.RB2, nf[2]);
+        const float f = __ldg(fp + (int64_t)i * p.P + (int64_t)so * p.T3 + (lz * p.FB + ly) * p.FB + lx);
+        dm += f; dp0 += f * (float)e[0]; dp1 += f * (float)e[1]; dp2 += f * (float)e[2];
+      }
+      const int si = p.block_slot[((t[2] / p.RB2) * p.nby + t[1] / p.RB2) * p.nbx + t[0] / p.RB2];
+      if (si >= 0) {
+        const int lx = local_in_tile(p, pp[0], t[0] / p.RB2, nf[0]), ly = local_in_tile(p, pp[1], t[1] / p.RB2, nf[1]),
+                  lz = local_in_tile(p, pp[2], t[2] / p.RB2, nf[2]);
+        const float f = __ldg(fp + (int64_t)i * p.P + (int64_t)si * p.T3 + (lz * p.FB + ly) * p.FB + lx);
+        dm -= f; dp0 -= f * (float)e[0]; dp1 -= f * (float)e[1]; dp2 -= f * (float)e[2];
+      }
+    }
+  }
+  const int64_t cell = ccell(p, x, y, z);
+  float4 v = make_float4(dm * 0.125f, dp0 * 0.125f, dp1 * 0.125f, dp2 * 0.125f);
+  if (accumulate) {
+    const float4 o = acc[cell];
+    v = make_float4(o.x + v.x, o.y + v.y, o.z + v.z, o.w + v.w);
+  }
+  acc[cell] = v;
+}
+
+// The fine flux less the one L0 computed across the same faces, added to the
+// new L0 populations as w_i (dm + 3 e_i . dp); cells within 2 of the body
+// are left alone. Rewrites the seam cells' mac.
+template <int Q>
+__global__ void __launch_bounds__(kTileThreads)
+    amr3_reflux(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macc,
+                float4 *__restrict__ acc, const __grid_constant__ Amr3Params p) {
+  using L = Lattice<Q>;
+  int x, y, z, id;
+  if (!iface_cell(p, x, y, z, id) || !seam_cell(p, x, y, z, id)) return;
+  const StepParams &c = p.c;
+  if (c.has_body && phi3({(float)x, (float)y, (float)z}, c.body) < 2.0f) return;
+  const int64_t cell = ccell(p, x, y, z);
+  const float4 a0 = acc[cell];
+  float dm = a0.x, dp0 = a0.y, dp1 = a0.z, dp2 = a0.w;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    if (covered(p, x - e[0], y - e[1], z - e[2])) {
+      const float v = __ldg(fin + (int64_t)i * p.N + ccell(p, x - e[0], y - e[1], z - e[2]));
+      dm -= v; dp0 -= v * (float)e[0]; dp1 -= v * (float)e[1]; dp2 -= v * (float)e[2];
+    }
+    if (covered(p, x + e[0], y + e[1], z + e[2])) {
+      const float v = __ldg(fin + (int64_t)i * p.N + cell);
+      dm += v; dp0 += v * (float)e[0]; dp1 += v * (float)e[1]; dp2 += v * (float)e[2];
+    }
+  }
+  acc[cell] = make_float4(dm, dp0, dp1, dp2);
+  float rho = 0.f, m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const float ex = (float)L::ex(i), ey = (float)L::ey(i), ez = (float)L::ez(i);
+    const float fo = fout[(int64_t)i * p.N + cell] + L::w(i) * (dm + 3.f * (ex * dp0 + ey * dp1 + ez * dp2));
+    fout[(int64_t)i * p.N + cell] = fo;
+    rho += fo;
+    m0 += fo * ex; m1 += fo * ey; m2 += fo * ez;
+  }
+  const float den = fmaxf(rho, 1e-6f);
+  macc[cell] = make_float4(rho, m0 / den + c.fx / (2.f * den), m1 / den + c.fy / (2.f * den),
+                           m2 / den + c.fz / (2.f * den));
+}
+
 // ---- L0 step, skipping covered blocks ------------------------------------
 template <int Q>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
@@ -741,6 +860,7 @@ struct lbm_amr3d {
   unsigned char *d_want = nullptr, *d_slot_new = nullptr, *d_iface_flag = nullptr;
   int *d_free_list = nullptr, *d_counts = nullptr;
   cudaGraphExec_t manage_graph[2] = {nullptr, nullptr};
+  float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
   std::string err;
 };
 
@@ -836,10 +956,15 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
       amr3_interp<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p, 1, nullptr);
       Amr3Params pa = p;
       pa.write_mac = 0;
+      const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
+      if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->flux, p, 0);
       amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
+      if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[1], a->flux, p, 1);
       amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
       amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
                                                  f2c_rescale);
+      if (a->flux && gc)
+        amr3_reflux<Q><<<gc, kTileThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], (float4 *)a->macc, a->flux, p);
     });
   }
   if (p.slots) {
@@ -910,7 +1035,7 @@ void release(lbm_amr3d *a) {
                     (void *)a->macp, (void *)a->d_block_slot, (void *)a->d_slot_to_block, (void *)a->d_iface,
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
-                    (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts})
+                    (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux})
     cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
@@ -1030,6 +1155,10 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
     if ((e = cudaMemset(a->fp[k], 0, fpb))) return bail(e, "memset pool f");
   }
   if ((e = cudaMalloc(&a->macc, (size_t)p.N * 16))) return bail(e, "cudaMalloc L0 mac");
+  if (c->reflux) {
+    if ((e = cudaMalloc(&a->flux, (size_t)p.N * 16))) return bail(e, "cudaMalloc flux");
+    if ((e = cudaMemset(a->flux, 0, (size_t)p.N * 16))) return bail(e, "memset flux");
+  }
   if ((e = cudaMalloc(&a->macp, (size_t)p.P * 16))) return bail(e, "cudaMalloc pool mac");
   if ((e = cudaMemset(a->macp, 0, (size_t)p.P * 16))) return bail(e, "memset pool mac");
   if ((e = cudaMalloc(&a->d_block_slot, nb * sizeof(int)))) return bail(e, "cudaMalloc block_slot");

@@ -92,6 +92,11 @@ int amr3_validate(const lbm_amr3d_config *c, std::string &why) {
   if (r.nx % c->rb || r.ny % c->rb || r.nz % c->rb) { why = "every dimension must be a multiple of rb"; return LBM_EINVAL; }
   if (c->refine < LBM_REFINE_BODY || c->refine > LBM_REFINE_LIST) { why = "unknown refine mode"; return LBM_EINVAL; }
   if (c->iface != 0 && c->iface != 1) { why = "iface must be 0 (explode/coalesce) or 1 (interp)"; return LBM_EINVAL; }
+  if (c->reflux) {
+    if (c->iface != 1) { why = "reflux needs the interp interface: explode/coalesce is conservative by construction"; return LBM_EINVAL; }
+    if (r.wall[0] || r.wall[1] || r.wall[2]) { why = "reflux is not valid with walls"; return LBM_EINVAL; }
+    if (r.nx / c->rb < 3 || r.ny / c->rb < 3 || r.nz / c->rb < 3) { why = "reflux needs at least 3 blocks per axis"; return LBM_EINVAL; }
+  }
   if (c->refine == LBM_REFINE_BODY && !r.has_body) { why = "refine = body needs a body"; return LBM_EINVAL; }
   if (std::fabs(r.tau - 1.0f) < 1e-3f) {
     why = "tau = 1 leaves no non-equilibrium part for the coarse/fine transfer to rescale";

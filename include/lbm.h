@@ -404,7 +404,11 @@ typedef struct {
                               1: interp -- the L0 step first, the ring
                               interpolated from L0, ring collided, tiles
                               restricted into L0 (main-3d.js:3343-3356)       */
-  int32_t reserved[4];     /* zero                                            */
+  int32_t reflux;          /* interp only: the flux correction of
+                              common_d3_amr_flux.wgsl / _reflux.wgsl
+                              (?reflux=1); needs no walls and >= 3 blocks
+                              per axis, as the reference requires             */
+  int32_t reserved[3];     /* zero                                            */
 } lbm_amr3d_config;
 
 typedef struct lbm_amr3d lbm_amr3d;

@@ -214,7 +214,8 @@ class Amr3D:
             lst = arr.ctypes.data_as(C.POINTER(C.c_int32))
         self._h = L.oracle_amr3d_create(C.addressof(r), cfg.rb, cfg.refine, cfg.margin, cfg.boxfrac, lst,
                                         cfg.explode_linear, int(fp32), int(capacity), int(cfg.dynamic),
-                                        int(cfg.manage_every), int(cfg.manage_start), int(cfg.iface))
+                                        int(cfg.manage_every), int(cfg.manage_start),
+                                        int(cfg.iface) | (int(cfg.reflux) << 1))
         if not self._h:
             raise ValueError("oracle_amr3d_create failed")
         nbl = int(np.prod(self.nb))

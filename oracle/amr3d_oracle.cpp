@@ -128,6 +128,8 @@ template <class R> struct Amr3D {
   int cp = 0;
   int linear = 1;
   int interp = 0;  // ?interface=interp instead of explode/coalesce
+  int reflux_on = 0;  // ?reflux=1 (interp only)
+  std::vector<R> flux_acc;
   // dynamic refinement
   int dynamic = 0, manage_every = 16, manage_start = 0;
   double margin = 2.0;
@@ -410,6 +412,110 @@ template <class R> struct Amr3D {
     return d + GH;
   }
 
+  // ---- flux / reflux (common_d3_amr_flux.wgsl, common_d3_amr_reflux.wgsl) --
+  // An unrefined L0 cell whose block touches a refined block on the side
+  // (face, edge or corner) the cell sits at.
+  bool seam_cell(int x, int y, int z) const {
+    const int c3[3] = {x, y, z};
+    const int b[3] = {x / t.rb, y / t.rb, z / t.rb};
+    if (t.block_slot[bid(b[0], b[1], b[2])] >= 0) return false;
+    int off[3];
+    for (int a = 0; a < 3; ++a) off[a] = c3[a] % t.rb == 0 ? -1 : ((c3[a] + 1) % t.rb == 0 ? 1 : 0);
+    const int nb[3] = {t.nbx, t.nby, t.nbz};
+    for (int k = 0; k < 8; ++k) {
+      int q[3];
+      for (int a = 0; a < 3; ++a) q[a] = wrapi(b[a] + ((k >> a) & 1) * off[a], nb[a]);
+      if (t.block_slot[bid(q[0], q[1], q[2])] >= 0) return true;
+    }
+    return false;
+  }
+
+  int slot_of_fine(const int g[3]) const { return t.block_slot[bid(g[0] / RB2, g[1] / RB2, g[2] / RB2)]; }
+
+  // The mass and momentum the fine level moved across the seam into each
+  // seam cell during one substep, in L0 units (1/8 per fine cell).
+  void flux(const std::vector<R> &fpo, std::vector<R> &acc, bool accumulate) {
+    const int NF[3] = {2 * t.nx, 2 * t.ny, 2 * t.nz};
+    for (int z = 0; z < t.nz; ++z)
+      for (int y = 0; y < t.ny; ++y)
+        for (int x = 0; x < t.nx; ++x) {
+          if (!seam_cell(x, y, z)) continue;
+          const int64_t cell = ccell(x, y, z);
+          R dm = 0, dp[3] = {0, 0, 0};
+          for (int oc = 0; oc < 8; ++oc) {
+            const int pp[3] = {2 * x + (oc & 1), 2 * y + ((oc >> 1) & 1), 2 * z + ((oc >> 2) & 1)};
+            for (int i = 0; i < Q; ++i) {
+              const int e[3] = {T->ex[i], T->ey[i], T->ez[i]};
+              int q[3], tt[3];
+              for (int a = 0; a < 3; ++a) {
+                q[a] = wrapi(pp[a] - e[a], NF[a]);
+                tt[a] = wrapi(pp[a] + e[a], NF[a]);
+              }
+              const int so = slot_of_fine(q);
+              if (so >= 0) {
+                const R f = fpo[i * P + pcell(so, (int)local_in_tile(q[0], q[0] / RB2, NF[0]),
+                                              (int)local_in_tile(q[1], q[1] / RB2, NF[1]),
+                                              (int)local_in_tile(q[2], q[2] / RB2, NF[2]))];
+                dm += f;
+                for (int a = 0; a < 3; ++a) dp[a] += f * R(e[a]);
+              }
+              const int si = slot_of_fine(tt);
+              if (si >= 0) {
+                const R f = fpo[i * P + pcell(si, (int)local_in_tile(pp[0], tt[0] / RB2, NF[0]),
+                                              (int)local_in_tile(pp[1], tt[1] / RB2, NF[1]),
+                                              (int)local_in_tile(pp[2], tt[2] / RB2, NF[2]))];
+                dm -= f;
+                for (int a = 0; a < 3; ++a) dp[a] -= f * R(e[a]);
+              }
+            }
+          }
+          const R v[4] = {dm * R(0.125), dp[0] * R(0.125), dp[1] * R(0.125), dp[2] * R(0.125)};
+          for (int k = 0; k < 4; ++k) acc[4 * cell + k] = accumulate ? acc[4 * cell + k] + v[k] : v[k];
+        }
+  }
+
+  // The fine flux less the flux L0 computed across the same faces, added to
+  // the new L0 populations as w_i (dm + 3 e_i . dp); cells within 2 of the
+  // body are left alone.
+  void reflux(const std::vector<R> &fin, std::vector<R> &fout, std::vector<R> &acc) {
+    for (int z = 0; z < t.nz; ++z)
+      for (int y = 0; y < t.ny; ++y)
+        for (int x = 0; x < t.nx; ++x) {
+          if (!seam_cell(x, y, z)) continue;
+          if (c.has_body && phi3<R>({R(x), R(y), R(z)}, c.body) < R(2)) continue;
+          const int64_t cell = ccell(x, y, z);
+          R dm = acc[4 * cell], dp[3] = {acc[4 * cell + 1], acc[4 * cell + 2], acc[4 * cell + 3]};
+          for (int i = 0; i < Q; ++i) {
+            const int e[3] = {T->ex[i], T->ey[i], T->ez[i]};
+            if (covered(x - e[0], y - e[1], z - e[2])) {
+              const R v = fin[i * N + ccell(x - e[0], y - e[1], z - e[2])];
+              dm -= v;
+              for (int a = 0; a < 3; ++a) dp[a] -= v * R(e[a]);
+            }
+            if (covered(x + e[0], y + e[1], z + e[2])) {
+              const R v = fin[i * N + cell];
+              dm += v;
+              for (int a = 0; a < 3; ++a) dp[a] += v * R(e[a]);
+            }
+          }
+          acc[4 * cell] = dm;
+          for (int a = 0; a < 3; ++a) acc[4 * cell + 1 + a] = dp[a];
+          R rho = 0, m[3] = {0, 0, 0};
+          for (int i = 0; i < Q; ++i) {
+            const R fo = fout[i * N + cell] +
+                         R(T->w[i]) * (dm + R(3) * (R(T->ex[i]) * dp[0] + R(T->ey[i]) * dp[1] + R(T->ez[i]) * dp[2]));
+            fout[i * N + cell] = fo;
+            rho += fo;
+            m[0] += fo * R(T->ex[i]); m[1] += fo * R(T->ey[i]); m[2] += fo * R(T->ez[i]);
+          }
+          const R den = std::fmax(rho, R(1e-6));
+          macc[4 * cell] = (double)rho;
+          macc[4 * cell + 1] = (double)(m[0] / den + R(c.force[0]) / (R(2) * den));
+          macc[4 * cell + 2] = (double)(m[1] / den + R(c.force[1]) / (R(2) * den));
+          macc[4 * cell + 3] = (double)(m[2] / den + R(c.force[2]) / (R(2) * den));
+        }
+  }
+
   void coalesce(const std::vector<R> &fpo, std::vector<R> &fco) {
     const int NF[3] = {2 * t.nx, 2 * t.ny, 2 * t.nz};
     std::vector<R> out = fco;  // each coarse cell writes only itself
@@ -675,9 +781,12 @@ template <class R> struct Amr3D {
       // tiles restricted into L0's new buffer
       l0_step(want_mac);
       interp_fill(fc[1 - cp], fp[0], true);
+      if (reflux_on) flux(fp[0], flux_acc, false);
       substep(fp[0], fp[1], true);
+      if (reflux_on) flux(fp[1], flux_acc, true);
       substep(fp[1], fp[0], true);
       restrict_tiles(fc[cp], nullptr);
+      if (reflux_on) reflux(fc[1 - cp], fc[cp], flux_acc);
       return;
     }
     explode(fc[cp], fp[0]);
@@ -728,7 +837,9 @@ Amr3D<R> *make(const lbm_config &c, int rb, int mode, double margin, double frac
     a->t.slots = capacity;
   }
   a->dynamic = dynamic;
-  a->interp = interp;
+  a->interp = interp & 1;
+  a->reflux_on = (interp >> 1) & 1;
+  a->flux_acc.assign((size_t)4 * a->t.nx * a->t.ny * a->t.nz, R(0));
   a->manage_every = manage_every;
   a->manage_start = manage_start;
   a->margin = margin;
