@@ -102,7 +102,7 @@ class Amr3DConfig(C.Structure):
                 ("margin", C.c_float), ("boxfrac", C.c_float), ("explode_linear", C.c_int32),
                 ("dynamic", C.c_int32), ("manage_every", C.c_int32), ("manage_start", C.c_int32),
                 ("max_slots", C.c_int32), ("slot_headroom", C.c_float), ("iface", C.c_int32),
-                ("reflux", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("reflux", C.c_int32), ("q_abs", C.c_float), ("q_hyst", C.c_float), ("q_lead", C.c_float)]
 
 
 REFINE = {"body": 0, "box": 1, "bar": 2, "slab": 3, "all": 4, "list": 5}
@@ -209,6 +209,7 @@ def _load() -> C.CDLL:
         "lbm_amr3d_forces": ([P, D], I),
         "lbm_amr3d_set_body": ([P, C.POINTER(Body)], I),
         "lbm_amr3d_pool_stats": ([P, C.POINTER(C.c_int32)], I),
+        "lbm_amr3d_block_q": ([P, C.c_float, C.POINTER(C.c_float)], I),
         "lbm_amr3d_totals": ([P, D], I),
         "lbm_amr3d_read_coarse": ([P, F, F], I),
         "lbm_amr3d_read_pool": ([P, F, F], I),
@@ -735,7 +736,7 @@ class Amr2D:
 def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, boxfrac: float = 0.5,
                  explode_linear: int = 1, dynamic: int = 0, manage_every: int = 16, manage_start: int = 0,
                  max_slots: int = 0, slot_headroom: float = 1.5, iface: int = 0, reflux: int = 0,
-                 **root_kw) -> Amr3DConfig:
+                 q_abs: float = 0.0, q_hyst: float = 1.0, q_lead: float = 0.0, **root_kw) -> Amr3DConfig:
     """lbm_amr3d_config: the L0 grid/physics as config_from's keywords, plus the hierarchy."""
     c = Amr3DConfig()
     rc = lib.lbm_amr3d_config_default(C.byref(c), q, *dims)
@@ -754,6 +755,9 @@ def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, 
     c.slot_headroom = slot_headroom
     c.iface = iface
     c.reflux = reflux
+    c.q_abs = q_abs
+    c.q_hyst = q_hyst
+    c.q_lead = q_lead
     return c
 
 
@@ -861,6 +865,12 @@ class Amr3D:
         out = np.zeros(4, np.int32)
         self._check(lib.lbm_amr3d_pool_stats(self._h, _ptr(out, C.c_int32)))
         return {"in_use": int(out[0]), "refusals": int(out[1]), "min_free": int(out[2]), "decisions": int(out[3])}
+
+    def block_q(self, lead: float = 0.0) -> np.ndarray:
+        """Per-block max Q-criterion of the L0 velocity, box dilated by `lead`."""
+        out = np.zeros(int(np.prod(self.nb)), np.float32)
+        self._check(lib.lbm_amr3d_block_q(self._h, float(lead), _ptr(out, C.c_float)))
+        return out
 
     def cell_updates(self) -> int:
         return int(lib.lbm_amr3d_cell_updates(self._h))

@@ -662,13 +662,92 @@ __device__ __noinline__ bool box_near_body(const lbm_body &b, float cx, float cy
   return false;
 }
 
-__global__ void amr3_decide(const __grid_constant__ Amr3Params p, unsigned char *__restrict__ want, float reach) {
+// The field half of the decision (common_d3_criterion.wgsl reduceQ): per
+// block, the max over the L0 cells of its box dilated by `lead` (floor /
+// ceil, so the box contains the region) of Q = 1/2 (|Omega|^2 - |S|^2), from
+// centred differences of the L0 velocity over the six face neighbours,
+// periodic. Products and sums are rounded one by one (no contraction), so
+// the value is the plain f32 arithmetic of the formula.
+__device__ __forceinline__ float3 mac_u(const float4 *__restrict__ mac, const Amr3Params &p, int x, int y, int z) {
+  x %= p.nx; x += x < 0 ? p.nx : 0;
+  y %= p.ny; y += y < 0 ? p.ny : 0;
+  z %= p.nz; z += z < 0 ? p.nz : 0;
+  const float4 m = __ldg(mac + ((int64_t)z * p.ny + y) * p.nx + x);
+  return make_float3(m.y, m.z, m.w);
+}
+
+__device__ float q_at(const float4 *__restrict__ mac, const Amr3Params &p, int x, int y, int z) {
+  float J[3][3];  // J[j][i] = du_i / dx_j
+  const float3 xp = mac_u(mac, p, x + 1, y, z), xm = mac_u(mac, p, x - 1, y, z);
+  const float3 yp = mac_u(mac, p, x, y + 1, z), ym = mac_u(mac, p, x, y - 1, z);
+  const float3 zp = mac_u(mac, p, x, y, z + 1), zm = mac_u(mac, p, x, y, z - 1);
+  J[0][0] = __fmul_rn(__fsub_rn(xp.x, xm.x), 0.5f); J[0][1] = __fmul_rn(__fsub_rn(xp.y, xm.y), 0.5f);
+  J[0][2] = __fmul_rn(__fsub_rn(xp.z, xm.z), 0.5f);
+  J[1][0] = __fmul_rn(__fsub_rn(yp.x, ym.x), 0.5f); J[1][1] = __fmul_rn(__fsub_rn(yp.y, ym.y), 0.5f);
+  J[1][2] = __fmul_rn(__fsub_rn(yp.z, ym.z), 0.5f);
+  J[2][0] = __fmul_rn(__fsub_rn(zp.x, zm.x), 0.5f); J[2][1] = __fmul_rn(__fsub_rn(zp.y, zm.y), 0.5f);
+  J[2][2] = __fmul_rn(__fsub_rn(zp.z, zm.z), 0.5f);
+  float s2 = 0.f, om2 = 0.f;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float a = J[j][i], b = J[i][j];
+      const float S = __fmul_rn(0.5f, __fadd_rn(a, b)), O = __fmul_rn(0.5f, __fsub_rn(a, b));
+      s2 = __fadd_rn(s2, __fmul_rn(S, S));
+      om2 = __fadd_rn(om2, __fmul_rn(O, O));
+    }
+  return __fmul_rn(0.5f, __fsub_rn(om2, s2));
+}
+
+constexpr int kCritThreads = 128;
+
+__global__ void __launch_bounds__(kCritThreads)
+    amr3_criterion(const float4 *__restrict__ mac, float *__restrict__ block_q, const __grid_constant__ Amr3Params p,
+                   float lead) {
+  const int id = blockIdx.x;
+  const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
+  int i0[3], n[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = (float)b[a] * (float)p.rb - lead;
+    const float hi = lo + (float)p.rb + 2.f * lead;
+    i0[a] = (int)floorf(lo);
+    n[a] = max((int)ceilf(hi) - i0[a], 0);
+  }
+  const int total = n[0] * n[1] * n[2];
+  float best = -1e30f;
+  for (int k = threadIdx.x; k < total; k += kCritThreads)
+    best = fmaxf(best, q_at(mac, p, i0[0] + k % n[0], i0[1] + (k / n[0]) % n[1], i0[2] + k / (n[0] * n[1])));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+  __shared__ float wq[kCritThreads / 32];
+  if ((threadIdx.x & 31) == 0) wq[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = wq[0];
+#pragma unroll
+    for (int w = 1; w < kCritThreads / 32; ++w) m = fmaxf(m, wq[w]);
+    block_q[id] = m;
+  }
+}
+
+// decide (common_d3_manage.wgsl): the union of the geometry test and, with
+// block_q, the field test -- max Q at or above q_refine for a block not yet
+// refined, at or above the one-band-lower q_hold for a block that holds a
+// tile (the refine / coarsen ladders of common_refine.wgsl at one level:
+// 1/2 log2 max(Q, 1e-30) >= 1/2 log2 Q_abs, minus the hysteresis band when
+// held, compared here in Q itself, which is monotone in the same quantity).
+__global__ void amr3_decide(const __grid_constant__ Amr3Params p, unsigned char *__restrict__ want, float reach,
+                            const float *__restrict__ block_q, float q_refine, float q_hold) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= p.nbx * p.nby * p.nbz) return;
   const int bx = id % p.nbx, by = (id / p.nbx) % p.nby, bz = id / (p.nbx * p.nby);
   const float half = 0.5f * (float)p.rb;
-  want[id] = box_near_body(p.c.body, (float)(bx * p.rb) + half, (float)(by * p.rb) + half,
-                           (float)(bz * p.rb) + half, half, reach) ? 1 : 0;
+  bool w = box_near_body(p.c.body, (float)(bx * p.rb) + half, (float)(by * p.rb) + half, (float)(bz * p.rb) + half,
+                         half, reach);
+  if (!w && block_q) w = fmaxf(block_q[id], 1e-30f) >= (p.block_slot[id] >= 0 ? q_hold : q_refine);
+  want[id] = w ? 1 : 0;
 }
 
 // drain (common_d3_amr_average.wgsl, DYING_ONLY): a tile about to be freed
@@ -860,6 +939,8 @@ struct lbm_amr3d {
   unsigned char *d_want = nullptr, *d_slot_new = nullptr, *d_iface_flag = nullptr;
   int *d_free_list = nullptr, *d_counts = nullptr;
   cudaGraphExec_t manage_graph[2] = {nullptr, nullptr};
+  float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
+  float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
   std::string err;
 };
@@ -902,7 +983,13 @@ cudaError_t launch_manage(lbm_amr3d *a, int cp) {
                      (sqrtf(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) + sqrtf(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc);
   const int nb = p.nbx * p.nby * p.nbz;
   cudaStream_t st = a->stream;
-  amr3_decide<<<(nb + 127) / 128, 128, 0, st>>>(p, a->d_want, a->cfg.margin + lead);
+  if (a->d_block_q) {
+    amr3_criterion<<<nb, kCritThreads, 0, st>>>((const float4 *)a->macc, a->d_block_q, p, a->cfg.q_lead);
+    amr3_decide<<<(nb + 127) / 128, 128, 0, st>>>(p, a->d_want, a->cfg.margin + lead, a->d_block_q, a->q_refine,
+                                                  a->q_hold);
+  } else {
+    amr3_decide<<<(nb + 127) / 128, 128, 0, st>>>(p, a->d_want, a->cfg.margin + lead, nullptr, 0.f, 0.f);
+  }
   const float tc = a->cfg.root.tau, tf = 2.f * tc - 0.5f;
   const float f2c_rescale = 2.f * (tc - 1.f) / (tf - 1.f);
   const int rb3 = p.rb * p.rb * p.rb;
@@ -1035,7 +1122,8 @@ void release(lbm_amr3d *a) {
                     (void *)a->macp, (void *)a->d_block_slot, (void *)a->d_slot_to_block, (void *)a->d_iface,
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
-                    (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux})
+                    (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux,
+                    (void *)a->d_block_q})
     cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
@@ -1183,6 +1271,14 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
     cudaMemcpy(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice);
     cudaMemcpy(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice);
+    if (c->q_abs > 0) {
+      if ((e = cudaMalloc(&a->d_block_q, nb * sizeof(float)))) return bail(e, "cudaMalloc block Q");
+      // main-3d.js: REFINE_THRESH = 1/2 log2 max(Q_ABS, 1e-30), COARSEN_THRESH
+      // one hysteresis band lower, both as thresholds on Q itself
+      const double qr = std::max((double)c->q_abs, 1e-30);
+      a->q_refine = (float)qr;
+      a->q_hold = (float)(qr * std::exp2(-2.0 * (double)c->q_hyst));
+    }
   }
   if (p.n_iface) cudaMemcpy(a->d_iface, a->iface.data(), p.n_iface * sizeof(int), cudaMemcpyHostToDevice);
   const int r3 = p.RB2 * p.RB2 * p.RB2;
@@ -1247,10 +1343,14 @@ int lbm_amr3d_step(lbm_amr3d *a, int n) {
     if (rc) return rc;
   }
   const lbm_amr3d_config &c = a->cfg;
+  auto manages = [&](int64_t s) {
+    return a->dynamic && s >= c.manage_start && (s - c.manage_start) % c.manage_every == 0;
+  };
   for (int k = 0; k < n; ++k) {
-    if (a->dynamic && a->step_count >= c.manage_start && (a->step_count - c.manage_start) % c.manage_every == 0)
-      ACK(a, cudaGraphLaunch(a->manage_graph[a->cp], a->stream));
-    if (k < n - 1) ACK(a, cudaGraphLaunch(a->graph[a->cp], a->stream));
+    if (manages(a->step_count)) ACK(a, cudaGraphLaunch(a->manage_graph[a->cp], a->stream));
+    // the field criterion reads the L0 velocity of the macro-step before it
+    if (a->d_block_q && manages(a->step_count + 1)) ACK(a, launch_macro(a, a->cp, true));
+    else if (k < n - 1) ACK(a, cudaGraphLaunch(a->graph[a->cp], a->stream));
     else ACK(a, launch_macro(a, a->cp, true));
     a->cp = 1 - a->cp;
     a->step_count += 1;
@@ -1275,6 +1375,21 @@ int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body) {
   a->sp.swept_band = tmp.swept_band;
   a->p.c = a->sp;
   destroy_graphs(a);
+  return LBM_OK;
+}
+
+int lbm_amr3d_block_q(lbm_amr3d *a, float lead, float *block_q) {
+  if (!a || !block_q) return a ? afail(a, LBM_EINVAL, "block_q is NULL") : LBM_EINVAL;
+  if (!std::isfinite(lead) || lead < 0) return afail(a, LBM_EINVAL, "lead must be finite and >= 0");
+  const int nb = a->p.nbx * a->p.nby * a->p.nbz;
+  float *d = a->d_block_q;
+  if (!d) ACK(a, cudaMallocAsync(&d, nb * sizeof(float), a->stream));
+  amr3_criterion<<<nb, kCritThreads, 0, a->stream>>>((const float4 *)a->macc, d, a->p, lead);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(block_q, d, nb * sizeof(float), cudaMemcpyDeviceToHost, a->stream);
+  if (d != a->d_block_q) cudaFreeAsync(d, a->stream);
+  ACK(a, e);
+  ACK(a, cudaStreamSynchronize(a->stream));
   return LBM_OK;
 }
 

@@ -97,6 +97,16 @@ int amr3_validate(const lbm_amr3d_config *c, std::string &why) {
     if (r.wall[0] || r.wall[1] || r.wall[2]) { why = "reflux is not valid with walls"; return LBM_EINVAL; }
     if (r.nx / c->rb < 3 || r.ny / c->rb < 3 || r.nz / c->rb < 3) { why = "reflux needs at least 3 blocks per axis"; return LBM_EINVAL; }
   }
+  if (!std::isfinite(c->q_abs) || c->q_abs < 0 || !std::isfinite(c->q_hyst) || !std::isfinite(c->q_lead) ||
+      c->q_lead < 0) {
+    why = "q_abs and q_lead must be finite and >= 0, q_hyst finite";
+    return LBM_EINVAL;
+  }
+  if (c->q_abs > 0 && !c->dynamic) {
+    why = "the Q-criterion needs dynamic refinement: a set chosen once at start would refine a flow that has not "
+          "developed yet";
+    return LBM_EINVAL;
+  }
   if (c->refine == LBM_REFINE_BODY && !r.has_body) { why = "refine = body needs a body"; return LBM_EINVAL; }
   if (std::fabs(r.tau - 1.0f) < 1e-3f) {
     why = "tau = 1 leaves no non-equilibrium part for the coarse/fine transfer to rescale";

@@ -408,7 +408,13 @@ typedef struct {
                               common_d3_amr_flux.wgsl / _reflux.wgsl
                               (?reflux=1); needs no walls and >= 3 blocks
                               per axis, as the reference requires             */
-  int32_t reserved[3];     /* zero                                            */
+  float q_abs;             /* dynamic only: also refine blocks whose max
+                              Q-criterion (common_d3_criterion.wgsl, from the
+                              L0 velocity) reaches q_abs, lattice units --
+                              the reference's qthresh x (U/D)^2; 0 = off      */
+  float q_hyst;            /* a held block keeps its tile down to
+                              q_abs * 4^-q_hyst (the reference's qhyst, 1)    */
+  float q_lead;            /* cells the Q window is dilated by (qlead)        */
 } lbm_amr3d_config;
 
 typedef struct lbm_amr3d lbm_amr3d;
@@ -434,6 +440,11 @@ int lbm_amr3d_step(lbm_amr3d *a, int n);
 int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body);
 /* {slots in use, refusals (pool exhausted), lowest free count seen, decisions}. */
 int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]);
+/* Per-block max Q-criterion of the L0 velocity of the last macro-step, over
+ * each block's box dilated by `lead` L0 cells: nb floats into host memory.
+ * Replaces the reference's criterion readback (common_d3_criterion.wgsl
+ * reduceQ into blockQ, read by main-3d.js debugCriterion). */
+int lbm_amr3d_block_q(lbm_amr3d *a, float lead, float *block_q);
 /* Force and torque on the body at the last macro-step (pool force, FP64). */
 int lbm_amr3d_forces(lbm_amr3d *a, double out[6]);
 /* Over the L0 macroscopic field of the last step (covered cells carry the

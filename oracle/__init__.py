@@ -186,6 +186,28 @@ def run_free(cfg, f0: np.ndarray, nsteps: int, state, opts, fp32: bool = False):
     return f, mac, forces, traj
 
 
+def q_cells(mac) -> np.ndarray:
+    """Q-criterion at every cell of a periodic (nz, ny, nx, 4) [rho, u] field,
+    f32 (common_d3_criterion.wgsl qAt)."""
+    m = np.ascontiguousarray(mac, np.float32)
+    nz, ny, nx = m.shape[:3]
+    out = np.zeros((nz, ny, nx), np.float32)
+    L = lib()
+    L.oracle_q_cells.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.oracle_q_cells(nx, ny, nz, m.ctypes.data_as(C.POINTER(C.c_float)), out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def q_of_grad(J) -> float:
+    """Q = 1/2 (|Omega|^2 - |S|^2) of a 3x3 gradient J[i][j] = du_i/dx_j, FP64
+    (d3-criterion.mjs qOfGrad)."""
+    j = np.ascontiguousarray(J, np.float64).reshape(9)
+    L = lib()
+    L.oracle_q_of_grad.argtypes = [C.POINTER(C.c_double)]
+    L.oracle_q_of_grad.restype = C.c_double
+    return float(L.oracle_q_of_grad(_d(j)))
+
+
 class Amr3D:
     """The 3D two-level AMR restatement (FP64, or the reference's f32 order)."""
 
@@ -218,6 +240,9 @@ class Amr3D:
                                         int(cfg.iface) | (int(cfg.reflux) << 1))
         if not self._h:
             raise ValueError("oracle_amr3d_create failed")
+        L.oracle_amr3d_set_q.argtypes = [C.c_void_p, C.c_float, C.c_float, C.c_float]
+        L.oracle_amr3d_block_q.argtypes = [C.c_void_p, C.c_float, C.POINTER(C.c_float)]
+        L.oracle_amr3d_set_q(self._h, float(cfg.q_abs), float(cfg.q_hyst), float(cfg.q_lead))
         nbl = int(np.prod(self.nb))
         self.block_slot = np.zeros(nbl, np.int32)
         s2b = np.zeros(nbl, np.int32)
@@ -240,6 +265,12 @@ class Amr3D:
         n = lib().oracle_amr3d_topology(self._h, bs.ctypes.data_as(C.POINTER(C.c_int32)),
                                         s2b.ctypes.data_as(C.POINTER(C.c_int32)))
         return bs, s2b[:n].copy()
+
+    def block_q(self, lead: float = 0.0) -> np.ndarray:
+        """Per-block max Q of the current coarse mac, box dilated by `lead`."""
+        out = np.zeros(int(np.prod(self.nb)), np.float32)
+        lib().oracle_amr3d_block_q(self._h, float(lead), out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
 
     def seed(self, mac):
         m = np.ascontiguousarray(mac, np.float64).reshape(-1, 4)

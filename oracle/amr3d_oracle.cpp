@@ -116,6 +116,31 @@ template <class R> R feq(const Tables &T, int i, R rho, R ux, R uy, R uz) {
 
 inline int wrapi(int v, int n) { return ((v % n) + n) % n; }
 
+// qAt (common_d3_criterion.wgsl): Q = 1/2 (|Omega|^2 - |S|^2) at an L0 cell
+// from centred differences of u over its six face neighbours, periodic, in
+// f32 with every product and sum rounded on its own. mac is [rho, u] per cell.
+inline float q_cell(const float *mac, int nx, int ny, int nz, int x, int y, int z) {
+  auto u = [&](int xx, int yy, int zz, int i) {
+    const int64_t c = ((int64_t)wrapi(zz, nz) * ny + wrapi(yy, ny)) * nx + wrapi(xx, nx);
+    return mac[4 * c + 1 + i];
+  };
+  float J[3][3];  // J[j][i] = du_i / dx_j
+  for (int i = 0; i < 3; ++i) {
+    J[0][i] = (u(x + 1, y, z, i) - u(x - 1, y, z, i)) * 0.5f;
+    J[1][i] = (u(x, y + 1, z, i) - u(x, y - 1, z, i)) * 0.5f;
+    J[2][i] = (u(x, y, z + 1, i) - u(x, y, z - 1, i)) * 0.5f;
+  }
+  float s2 = 0.f, om2 = 0.f;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const float a = J[j][i], b = J[i][j];
+      const float S = 0.5f * (a + b), O = 0.5f * (a - b);
+      s2 += S * S;
+      om2 += O * O;
+    }
+  return 0.5f * (om2 - s2);
+}
+
 template <class R> struct Amr3D {
   lbm_config c;
   int Q, FB, RB2, T3;
@@ -137,6 +162,9 @@ template <class R> struct Amr3D {
   std::vector<int32_t> free_list;
   std::vector<uint8_t> slot_new, want;
   int free_count = 0, refused = 0, min_free = 0, decisions = 0;
+  // the field criterion (common_d3_criterion.wgsl): off at q_abs = 0
+  float q_abs = 0.f, q_hyst = 1.f, q_lead = 0.f;
+  std::vector<float> block_q;
 
   int bid(int bx, int by, int bz) const { return (bz * t.nby + by) * t.nbx + bx; }
   bool covered(int x, int y, int z) const {
@@ -732,6 +760,30 @@ template <class R> struct Amr3D {
     }
   }
 
+  // reduceQ: per block, the max of q_cell over its L0 box dilated by `lead`
+  // (floor / ceil), read from the coarse mac as the kernel reads it, in f32.
+  void reduce_q(float lead, std::vector<float> &out) const {
+    out.assign(t.nb, 0.f);
+    std::vector<float> mac4((size_t)4 * N);
+    for (int64_t i = 0; i < 4 * N; ++i) mac4[i] = (float)macc[i];
+    for (int id = 0; id < t.nb; ++id) {
+      const int b[3] = {id % t.nbx, (id / t.nbx) % t.nby, id / (t.nbx * t.nby)};
+      int i0[3], n[3];
+      for (int a = 0; a < 3; ++a) {
+        const float lo = (float)b[a] * (float)t.rb - lead;
+        const float hi = lo + (float)t.rb + 2.f * lead;
+        i0[a] = (int)std::floor(lo);
+        n[a] = std::max((int)std::ceil(hi) - i0[a], 0);
+      }
+      float best = -1e30f;
+      for (int kz = 0; kz < n[2]; ++kz)
+        for (int ky = 0; ky < n[1]; ++ky)
+          for (int kx = 0; kx < n[0]; ++kx)
+            best = std::fmax(best, q_cell(mac4.data(), t.nx, t.ny, t.nz, i0[0] + kx, i0[1] + ky, i0[2] + kz));
+      out[id] = best;
+    }
+  }
+
   void manage() {
     const lbm_body &b = c.body;
     float rc = b.shape == LBM_SHAPE_SPHERE ? b.a : (b.shape == LBM_SHAPE_SPHEROID ? std::fmax(b.a, b.c)
@@ -745,6 +797,17 @@ template <class R> struct Amr3D {
       const int bx = id % t.nbx, by = (id / t.nbx) % t.nby, bz = id / (t.nbx * t.nby);
       want[id] = box_near(b, (float)(bx * t.rb) + half, (float)(by * t.rb) + half, (float)(bz * t.rb) + half, half,
                           reach);
+    }
+    if (q_abs > 0) {
+      // the union with the field ladder at one level (common_d3_manage.wgsl
+      // decide, common_refine.wgsl desiredLevel / desiredLevelCoarsen):
+      // 1/2 log2 max(Q, 1e-30) >= 1/2 log2 max(Q_abs, 1e-30), less q_hyst for
+      // a block that holds a tile, compared as Q >= Q_abs 4^-q_hyst
+      const double qr = std::max((double)q_abs, 1e-30);
+      const float q_refine = (float)qr, q_hold = (float)(qr * std::exp2(-2.0 * (double)q_hyst));
+      reduce_q(q_lead, block_q);
+      for (int id = 0; id < t.nb; ++id)
+        if (!want[id]) want[id] = std::fmax(block_q[id], 1e-30f) >= (t.block_slot[id] >= 0 ? q_hold : q_refine);
     }
     // drain the dying tiles into the time-t L0 buffer
     restrict_tiles(fc[cp], want.data());
@@ -924,6 +987,47 @@ int oracle_amr3d_topology(void *h, int32_t *block_slot, int32_t *slot_to_block) 
     n = a->t.slots;
   });
   return n;
+}
+
+// The field criterion of the manager: Q_abs (0 = off), hysteresis in
+// octaves of rotation rate, lead in L0 cells.
+int oracle_amr3d_set_q(void *h, float q_abs, float q_hyst, float q_lead) {
+  WITH(h, {
+    a->q_abs = q_abs;
+    a->q_hyst = q_hyst;
+    a->q_lead = q_lead;
+  });
+  return 0;
+}
+
+// Per-block max Q of the current coarse mac with the box dilated by `lead`.
+int oracle_amr3d_block_q(void *h, float lead, float *out) {
+  WITH(h, {
+    std::vector<float> q;
+    a->reduce_q(lead, q);
+    std::memcpy(out, q.data(), q.size() * sizeof(float));
+  });
+  return 0;
+}
+
+// Q at every cell of an nx*ny*nz field of [rho, ux, uy, uz] (f32, periodic).
+int oracle_q_cells(int nx, int ny, int nz, const float *mac, float *q) {
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) q[((int64_t)z * ny + y) * nx + x] = q_cell(mac, nx, ny, nz, x, y, z);
+  return 0;
+}
+
+// qOfGrad (d3-criterion.mjs) in FP64 on a 3x3 gradient J[i][j] = du_i/dx_j.
+double oracle_q_of_grad(const double *J) {
+  double om2 = 0, s2 = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double S = 0.5 * (J[3 * i + j] + J[3 * j + i]), O = 0.5 * (J[3 * i + j] - J[3 * j + i]);
+      s2 += S * S;
+      om2 += O * O;
+    }
+  return 0.5 * (om2 - s2);
 }
 
 int oracle_amr3d_seed(void *h, const double *mac) {

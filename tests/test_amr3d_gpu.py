@@ -333,3 +333,81 @@ def test_amr3d_reflux_matches_oracle_and_restores_conservation(lbm, oracle):
     assert np.abs(drift[0][1:]).max() > 1e-2            # the interp seam leaks momentum
     assert np.abs(drift[1][1:]).max() < 1e-3            # the correction holds it
     assert abs(drift[1][0]) < 1e-2
+
+
+def vortex_mac(dims, cores, u0=0.03, seed=5):
+    """[rho, u] f32: a uniform stream plus Gaussian vortex cores (x, y, z,
+    spin), periodic, with a little noise."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    u = np.zeros((nz, ny, nx, 3))
+    for cx, cy, cz, w in cores:
+        dx = (x - cx + nx / 2) % nx - nx / 2
+        dy = (y - cy + ny / 2) % ny - ny / 2
+        dz = (z - cz + nz / 2) % nz - nz / 2
+        g = np.exp(-(dx * dx + dy * dy + dz * dz) / 8.0)
+        u[..., 0] += -w * dy * g
+        u[..., 1] += w * dx * g
+    u += 1e-4 * rng.standard_normal(u.shape)
+    u[..., 0] += u0
+    mac = np.ones((nz, ny, nx, 4), np.float32)
+    mac[..., 1:] = u
+    return mac.reshape(-1, 4)
+
+
+def test_q_criterion_block_max_matches_oracle(lbm, oracle):
+    """reduceQ on the device: bit for bit against the oracle on the seeded L0
+    field at several leads, and to FP32 rounding after macro-steps."""
+    dims = (32, 24, 20)
+    c = lbm.amr3d_config(19, dims, refine="box", rb=4, tau=0.6)
+    mac = vortex_mac(dims, [(8.3, 7.1, 9.5, 0.02), (22.6, 15.2, 6.4, -0.015), (1.2, 20.5, 14.8, 0.01)])
+    a = lbm.Amr3D(c)
+    o = oracle.Amr3D(c, fp32=True)
+    a.init_macro(mac)
+    o.seed(mac.astype(np.float64))
+    for lead in (0.0, 0.5, 2.25, 5.0):
+        assert np.array_equal(a.block_q(lead), o.block_q(lead)), lead
+    a.step(4)
+    o.step(4)
+    gq, oq = a.block_q(1.0), o.block_q(1.0)
+    assert np.abs(gq - oq).max() <= 1e-4 * np.abs(oq).max()
+    assert oq.max() > 1e-5
+    a.close()
+
+
+def test_q_criterion_refines_detached_vortices_like_the_oracle(lbm, oracle):
+    """?qthresh on a dynamic run: blocks far from the body are refined because
+    a vortex core passes through them, held one hysteresis band lower, and the
+    decisions (topology, slot order) agree with the oracle exactly."""
+    dims = (40, 24, 24)
+    body = dict(shape="sphere", centre=(9.5, 12.0, 12.0), a=3.0)
+    u0 = 0.03
+    kw = dict(refine="body", margin=2.0, dynamic=1, manage_every=4, max_slots=160, tau=0.62, has_body=1,
+              use_bounceback=1, body=body)
+    c = lbm.amr3d_config(19, dims, q_abs=2e-5, q_hyst=1.0, q_lead=4 * u0, **kw)
+    geom = lbm.amr3d_refine_blocks(lbm.amr3d_config(19, dims, **kw)) > 0
+    mac = vortex_mac(dims, [(26.0, 8.0, 12.0, 0.02), (31.0, 16.5, 11.0, -0.018)], u0=u0)
+    a = lbm.Amr3D(c)
+    o = oracle.Amr3D(c, capacity=a.slots)
+    a.init_macro(mac)
+    o.seed(mac.astype(np.float64))
+    field_blocks = []
+    for k in range(6):
+        a.step(4)
+        o.step(4)
+        ta, to = a.topology(), o.topology()
+        assert np.array_equal(ta["block_slot"], to[0]), k
+        assert np.array_equal(ta["slot_to_block"], to[1]), k
+        field_blocks.append(int(((ta["block_slot"] >= 0) & ~geom).sum()))
+    print("blocks refined by the field criterion per decision:", field_blocks)
+    assert min(field_blocks) > 0
+    st = a.pool_stats()
+    assert st == o.pool_stats() and st["decisions"] == 6 and st["refusals"] == 0
+    gfc, gmac = a.read_coarse()
+    ofc, omac, ofp, _ = o.read()
+    gfp, _ = a.read_pool()
+    assert rel_l2(gfc.astype(np.float64), ofc) <= 5e-6
+    used = np.repeat(to[1] >= 0, a.fb ** 3)
+    assert rel_l2(gfp[:, used].astype(np.float64), ofp[:, used]) <= 5e-6
+    a.close()
