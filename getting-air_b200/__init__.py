@@ -94,7 +94,8 @@ class Config(C.Structure):
                 ("rho_w_local", C.c_int32), ("swept_force", C.c_int32),
                 ("chi_eps", C.c_float), ("sponge_w", C.c_float),
                 ("sponge_axis", C.c_int32 * 3), ("sponge_u", C.c_float * 3),
-                ("body", Body), ("storage", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("body", Body), ("storage", C.c_int32), ("window", C.c_int32 * 3),
+                ("win_anchor", C.c_int32 * 3), ("reserved", C.c_int32 * 1)]
 
 
 class Amr3DConfig(C.Structure):
@@ -462,13 +463,40 @@ def config_from(q: int, dims, **kw) -> Config:
             v = STORAGE[v]
         if k == "body" and isinstance(v, dict):
             v = make_body(**v)
+        if k == "window" and (v is None or isinstance(v, str)):
+            v = window_axes(v)
         if isinstance(getattr(cfg, k), C.Array):
             arr = getattr(cfg, k)
             for j, x in enumerate(v):
                 arr[j] = x
         else:
             setattr(cfg, k, v)
+    if any(cfg.window) and "win_anchor" not in kw:
+        # the anchor is the body's initial cell, so the window's offset is 0
+        # at step 0 (main-3d.js WIN_ANCHOR)
+        for j, c in enumerate((cfg.body.cx, cfg.body.cy, cfg.body.cz)):
+            cfg.win_anchor[j] = int(np.floor(c))
     return cfg
+
+
+def window_axes(spec) -> tuple:
+    """A window spec as per-axis flags (d3-window.mjs parseWindowAxes): '',
+    '0', 'none' and None are off; '1', 'all', 'xyz' all three; otherwise
+    the axes named. An unknown character is refused."""
+    if spec is None:
+        return (0, 0, 0)
+    s = str(spec).strip().lower()
+    if s in ("", "0", "none"):
+        return (0, 0, 0)
+    if s in ("1", "all", "xyz"):
+        return (1, 1, 1)
+    out = [0, 0, 0]
+    for ch in s:
+        i = "xyz".find(ch)
+        if i < 0:
+            raise ValueError(f"window={spec!r}: expected some of xyz, or 0/none/all")
+        out[i] = 1
+    return tuple(out)
 
 
 class Batch:

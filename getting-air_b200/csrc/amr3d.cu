@@ -230,8 +230,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   float phi = 1e30f;
   V3 us = {0.f, 0.f, 0.f};
   if (c.has_body) {
-    phi = phi3(pos, c.body);
-    us = body_velocity3(pos, c.body);
+    phi = phi3(pos, c.body, c.win);
+    us = body_velocity3(pos, c.body, c.win);
   }
   const bool bb = c.has_body && c.bb;
   // a fine link is sqrt(3)/2 L0 units long and phi is 1-Lipschitz
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     int s[3] = {t.fx - e[0], t.fy - e[1], t.fz - e[2]};
     if (near) {
       const V3 sp = {f2c(s[0], b[0] * p.rb), f2c(s[1], b[1] * p.rb), f2c(s[2], b[2] * p.rb)};
-      if (phi3(sp, c.body) < 0.f) {
+      if (phi3(sp, c.body, c.win) < 0.f) {
         const float corr =
             2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
         f[i] = __ldg(fin + (int64_t)L::opp(i) * p.P + t.cell) + corr;
@@ -294,9 +294,16 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   }
   float spw = 0.f;
   if (c.sponge_w > 0.f) {
-    const float dx = c.sax ? fminf(pos.x, (float)(p.nx - 1) - pos.x) : 1e30f;
-    const float dy = c.say ? fminf(pos.y, (float)(p.ny - 1) - pos.y) : 1e30f;
-    const float dz = c.saz ? fminf(pos.z, (float)(p.nz - 1) - pos.z) : 1e30f;
+    // L0 units, window coordinates (common_d3_amr_step1.wgsl:356-366)
+    V3 wp = pos;
+    if (c.win.on) {
+      wp.x = win_coord1(pos.x, win_offset1(c.body.cx, c.win.anchor[0], c.win.n[0]), c.win.n[0]);
+      wp.y = win_coord1(pos.y, win_offset1(c.body.cy, c.win.anchor[1], c.win.n[1]), c.win.n[1]);
+      wp.z = win_coord1(pos.z, win_offset1(c.body.cz, c.win.anchor[2], c.win.n[2]), c.win.n[2]);
+    }
+    const float dx = c.sax ? fminf(wp.x, (float)(p.nx - 1) - wp.x) : 1e30f;
+    const float dy = c.say ? fminf(wp.y, (float)(p.ny - 1) - wp.y) : 1e30f;
+    const float dz = c.saz ? fminf(wp.z, (float)(p.nz - 1) - wp.z) : 1e30f;
     spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), c.sponge_inv);
   }
   const bool solid = c.solid_eq && bb && phi < 0.f;
@@ -494,7 +501,7 @@ __global__ void __launch_bounds__(kTileThreads)
   int x, y, z, id;
   if (!iface_cell(p, x, y, z, id) || !seam_cell(p, x, y, z, id)) return;
   const StepParams &c = p.c;
-  if (c.has_body && phi3({(float)x, (float)y, (float)z}, c.body) < 2.0f) return;
+  if (c.has_body && phi3({(float)x, (float)y, (float)z}, c.body, c.win) < 2.0f) return;
   const int64_t cell = ccell(p, x, y, z);
   const float4 a0 = acc[cell];
   float dm = a0.x, dp0 = a0.y, dp1 = a0.z, dp2 = a0.w;
@@ -556,8 +563,8 @@ __global__ void __launch_bounds__(kTileThreads)
     const int fx = kAmrGhost + k % p.RB2, fy = kAmrGhost + (k / p.RB2) % p.RB2, fz = kAmrGhost + k / (p.RB2 * p.RB2);
     const int64_t cell = (int64_t)slot * p.T3 + (fz * p.FB + fy) * p.FB + fx;
     const V3 pos = {f2c(fx, b[0] * p.rb), f2c(fy, b[1] * p.rb), f2c(fz, b[2] * p.rb)};
-    const float phi = phi3(pos, c.body);
-    const V3 us = body_velocity3(pos, c.body);
+    const float phi = phi3(pos, c.body, c.win);
+    const V3 us = body_velocity3(pos, c.body, c.win);
     float fbx = 0.f, fby = 0.f, fbz = 0.f, fsx = 0.f, fsy = 0.f, fsz = 0.f;
     if (c.bb) {
       if (phi >= 0.f && phi < 1.0f) {
@@ -572,7 +579,7 @@ __global__ void __launch_bounds__(kTileThreads)
         for (int i = 0; i < Q; ++i) {
           const V3 sp = {f2c(fx - L::ex(i), b[0] * p.rb), f2c(fy - L::ey(i), b[1] * p.rb),
                          f2c(fz - L::ez(i), b[2] * p.rb)};
-          if (phi3(sp, c.body) < 0.f) {
+          if (phi3(sp, c.body, c.win) < 0.f) {
             const float fo = __ldg(fp + (int64_t)L::opp(i) * p.P + cell);
             const float corr =
                 2.f * L::w(i) * rhoW * ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
@@ -585,7 +592,7 @@ __global__ void __launch_bounds__(kTileThreads)
       }
       if (c.swept && fabsf(phi) < c.swept_band) {
         const bool now = phi < 0.f;
-        if (now != (phi3_ahead(pos, c.body, 1.f) < 0.f)) {
+        if (now != (phi3_ahead(pos, c.body, 1.f, c.win) < 0.f)) {
           float mcx = 0.f, mcy = 0.f, mcz = 0.f;
 #pragma unroll
           for (int i = 0; i < Q; ++i) {
@@ -615,7 +622,8 @@ __global__ void __launch_bounds__(kTileThreads)
       }
     }
     const float tx = fbx * 0.25f + fsx * 0.125f, ty = fby * 0.25f + fsy * 0.125f, tz = fbz * 0.25f + fsz * 0.125f;
-    const float rx = pos.x - c.body.cx, ry = pos.y - c.body.cy, rz = pos.z - c.body.cz;
+    const V3 r = body_delta(pos, c.body, c.win);
+    const float rx = r.x, ry = r.y, rz = r.z;
     cf.fx = tx; cf.fy = ty; cf.fz = tz;
     cf.tx = ry * tz - rz * ty;
     cf.ty = rz * tx - rx * tz;
@@ -633,29 +641,30 @@ __global__ void __launch_bounds__(kTileThreads)
 // body? One SDF evaluation brackets the minimum over a box of half-edge h as
 // phi(c) - h sqrt(3) <= min <= phi(c); undecided boxes split into octants,
 // three levels deep, accepting at the bottom. sqrt(3) rounded up.
-__device__ __noinline__ bool box_near_body(const lbm_body &b, float cx, float cy, float cz, float h0, float reach) {
+__device__ __noinline__ bool box_near_body(const lbm_body &b, const Win &w, float cx, float cy, float cz, float h0,
+                                           float reach) {
   const float S3 = 1.7320509f;
   float R0 = h0 * S3;
-  const float p0 = phi3({cx, cy, cz}, b);
+  const float p0 = phi3({cx, cy, cz}, b, w);
   if (p0 - R0 > reach) return false;
   if (p0 <= reach) return true;
   const float h1 = h0 * 0.5f, R1 = R0 * 0.5f;
   for (int i = 0; i < 8; ++i) {
     const float c1x = cx + ((i & 1) ? h1 : -h1), c1y = cy + ((i & 2) ? h1 : -h1), c1z = cz + ((i & 4) ? h1 : -h1);
-    const float p1 = phi3({c1x, c1y, c1z}, b);
+    const float p1 = phi3({c1x, c1y, c1z}, b, w);
     if (p1 - R1 > reach) continue;
     if (p1 <= reach) return true;
     const float h2 = h1 * 0.5f, R2 = R1 * 0.5f;
     for (int j = 0; j < 8; ++j) {
       const float c2x = c1x + ((j & 1) ? h2 : -h2), c2y = c1y + ((j & 2) ? h2 : -h2), c2z = c1z + ((j & 4) ? h2 : -h2);
-      const float p2 = phi3({c2x, c2y, c2z}, b);
+      const float p2 = phi3({c2x, c2y, c2z}, b, w);
       if (p2 - R2 > reach) continue;
       if (p2 <= reach) return true;
       const float h3 = h2 * 0.5f, R3 = R2 * 0.5f;
       for (int k = 0; k < 8; ++k) {
         const float c3x = c2x + ((k & 1) ? h3 : -h3), c3y = c2y + ((k & 2) ? h3 : -h3),
                     c3z = c2z + ((k & 4) ? h3 : -h3);
-        if (phi3({c3x, c3y, c3z}, b) - R3 <= reach) return true;
+        if (phi3({c3x, c3y, c3z}, b, w) - R3 <= reach) return true;
       }
     }
   }
@@ -744,7 +753,7 @@ __global__ void amr3_decide(const __grid_constant__ Amr3Params p, unsigned char 
   if (id >= p.nbx * p.nby * p.nbz) return;
   const int bx = id % p.nbx, by = (id / p.nbx) % p.nby, bz = id / (p.nbx * p.nby);
   const float half = 0.5f * (float)p.rb;
-  bool w = box_near_body(p.c.body, (float)(bx * p.rb) + half, (float)(by * p.rb) + half, (float)(bz * p.rb) + half,
+  bool w = box_near_body(p.c.body, p.c.win, (float)(bx * p.rb) + half, (float)(by * p.rb) + half, (float)(bz * p.rb) + half,
                          half, reach);
   if (!w && block_q) w = fmaxf(block_q[id], 1e-30f) >= (p.block_slot[id] >= 0 ? q_hold : q_refine);
   want[id] = w ? 1 : 0;

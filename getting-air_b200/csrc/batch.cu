@@ -279,6 +279,10 @@ int lbm_batch_create(const lbm_config *doms, int ndomains, lbm_batch **out) {
       g_batch_error = "domain " + std::to_string(d) + ": " + why;
       return LBM_EINVAL;
     }
+    if (doms[d].window[0] || doms[d].window[1] || doms[d].window[2]) {
+      g_batch_error = "domain " + std::to_string(d) + ": the moving window runs in dense sessions and 3D AMR";
+      return LBM_ENOTSUP;
+    }
     if (doms[d].q != doms[0].q || doms[d].storage != doms[0].storage) {
       g_batch_error = "all domains of a batch must share q and storage";
       return LBM_EINVAL;

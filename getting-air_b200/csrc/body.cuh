@@ -32,6 +32,16 @@
 
 namespace lbm {
 
+// The moving window (common_d3_window.wgsl, d3-window.mjs): n is the domain
+// size on a windowed axis and 0 elsewhere (WIN_N*), anchor the cell the body
+// sits in within the window (WIN_A*). The fluid never moves: the body wraps
+// through the periodic buffer and the sponge band follows it.
+struct Win {
+  float n[3];
+  float anchor[3];
+  int on;
+};
+
 // ---- reach of the body ---------------------------------------------------
 
 // Radius of the smallest sphere about the centre containing the body
@@ -50,9 +60,11 @@ LBM_HD float body_circumradius(const lbm_body &b) {
 // swept-cell term reaches one step of surface motion, and the penalty's chi
 // is below 1e-6 beyond ~6.9 band widths. `swept`/`band` are the swept-cell
 // switch and the |phi| band it applies in. Returns false when no cell of
-// the domain is within reach.
+// the domain is within reach. On a windowed axis (win[a] set) the box is
+// not clipped: it may start below 0 or end past the last cell, to be read
+// modulo the axis, and it covers the whole axis once it is that long.
 LBM_HD bool body_cell_box(const lbm_body &b, int q, int nx, int ny, int nz, int bounceback, int swept_force,
-                          float chi_eps, int box[6], int *swept, float *band) {
+                          float chi_eps, int box[6], int *swept, float *band, const int *win = nullptr) {
   const float rc = body_circumradius(b);
   const float speed = sqrtf(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz) +
                       sqrtf(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz) * rc;
@@ -66,6 +78,12 @@ LBM_HD bool body_cell_box(const lbm_body &b, int q, int nx, int ny, int nz, int 
   for (int a = 0; a < 3; ++a) {
     if (a == 2 && q == 9) { box[4] = box[5] = 0; break; }
     int lo = (int)floorf(centre[a] - reach), hi = (int)ceilf(centre[a] + reach);
+    if (win && win[a]) {
+      if (hi - lo + 1 >= len[a]) { lo = 0; hi = len[a] - 1; }
+      box[2 * a] = lo;
+      box[2 * a + 1] = hi;
+      continue;
+    }
     if (wrap2d && (lo < 0 || hi > len[a] - 1)) { lo = 0; hi = len[a] - 1; }
     box[2 * a] = lo < 0 ? 0 : lo;
     box[2 * a + 1] = hi > len[a] - 1 ? len[a] - 1 : hi;
@@ -233,7 +251,8 @@ LBM_HD lbm_body body_pose(const lbm_body &shape, const lbm_body_state &s) {
 
 struct BodyPose {
   lbm_body body;
-  int box[6];        // cells that can feel the body (inclusive)
+  int region[6];     // launch blocks that can feel the body: per axis the
+                     // first (in the grid) and first + count, read modulo it
   int swept;
   float swept_band;
 };
@@ -243,6 +262,7 @@ struct BodyDyn {
   lbm_body_opts opt;
   lbm_body shape;
   int q, nx, ny, nz, bounceback, swept_force;
+  int win[3];        // moving-window axes (the box is not clipped on them)
   float chi_eps;
   int cap[3];        // force-pass grid: the largest box, in launch blocks
   int overflow;      // steps whose box exceeded cap (clipped)

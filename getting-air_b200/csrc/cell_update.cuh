@@ -257,8 +257,8 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
   float phi = 1e30f;
   V3 us = {0.f, 0.f, 0.f};
   if (p.has_body) {
-    phi = phi3(pos, p.body);
-    us = body_velocity3(pos, p.body);
+    phi = phi3(pos, p.body, p.win);
+    us = body_velocity3(pos, p.body, p.win);
   }
   const bool bbody = p.has_body && p.bb;
   const bool at_wall = (p.wall_x && (x == 0 || x == nx - 1)) || (p.wall_y && (y == 0 || y == ny - 1)) ||
@@ -282,7 +282,7 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
       const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
       const int o = L::opp(i);
       bool solid = false;
-      if (near) solid = phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body) < 0.f;
+      if (near) solid = phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body, p.win) < 0.f;
       if (solid) {
         const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
         const float corr =
@@ -323,9 +323,17 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
 
   float spw = 0.f;
   if (p.sponge_w > 0.f) {
-    const float dx = p.sax ? fminf(pos.x, (float)(nx - 1 - x)) : 1e30f;
-    const float dy = p.say ? fminf(pos.y, (float)(ny - 1 - y)) : 1e30f;
-    const float dz = p.saz ? fminf(pos.z, (float)(nz - 1 - z)) : 1e30f;
+    // distances in window coordinates: under a moving window the band
+    // travels with the body (the identity without one)
+    V3 wp = pos;
+    if (p.win.on) {
+      wp.x = win_coord1(pos.x, win_offset1(p.body.cx, p.win.anchor[0], p.win.n[0]), p.win.n[0]);
+      wp.y = win_coord1(pos.y, win_offset1(p.body.cy, p.win.anchor[1], p.win.n[1]), p.win.n[1]);
+      wp.z = win_coord1(pos.z, win_offset1(p.body.cz, p.win.anchor[2], p.win.n[2]), p.win.n[2]);
+    }
+    const float dx = p.sax ? fminf(wp.x, (float)(nx - 1) - wp.x) : 1e30f;
+    const float dy = p.say ? fminf(wp.y, (float)(ny - 1) - wp.y) : 1e30f;
+    const float dz = p.saz ? fminf(wp.z, (float)(nz - 1) - wp.z) : 1e30f;
     spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), p.sponge_inv);
   }
 
@@ -352,7 +360,7 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
     if (bbody) {
       if (p.swept && fabsf(phi) < p.swept_band) {
         const bool solid_now = phi < 0.f;
-        const bool solid_next = phi3_ahead(pos, p.body, 1.f) < 0.f;
+        const bool solid_next = phi3_ahead(pos, p.body, 1.f, p.win) < 0.f;
         if (solid_now != solid_next) {
           float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
@@ -375,7 +383,8 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
         fbz = -(rc2 * (us.z - uzs));
       }
     }
-    const float rx = pos.x - p.body.cx, ry = pos.y - p.body.cy, rz = pos.z - p.body.cz;
+    const V3 r = body_delta(pos, p.body, p.win);
+    const float rx = r.x, ry = r.y, rz = r.z;
     cf.fx = fbx; cf.fy = fby; cf.fz = fbz;
     cf.tx = ry * fbz - rz * fby;
     cf.ty = rz * fbx - rx * fbz;

@@ -40,6 +40,7 @@ struct StepParams {
   int sax, say, saz;
   float ftarget[27];    // sponge far-field equilibrium per direction (rho = 1)
   lbm_body body;
+  Win win;              // moving window (3D); win.on = 0 without one
   int write_mac;
   // Force reduction: the blocks of the launch grid that can see the body.
   int force_on;
@@ -70,6 +71,30 @@ struct StepParams {
 #endif
 constexpr int kStepThreads = LBM_STEP_THREADS;
 constexpr int kStepMinBlocks = LBM_STEP_MIN_BLOCKS;
+
+LBM_HD int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// The launch blocks of the dense step grid (kStepThreads cells along x, one
+// row per block in y and z) that cover an inclusive cell box: per axis the
+// first block, wrapped into the grid, and first + count, read modulo the
+// grid -- the box of a windowed axis can cross the periodic seam. A box as
+// long as the grid covers all of it; a count above cap[a] is clipped to it
+// and reported (cap NULL: no limit).
+LBM_HD bool box_region(const int box[6], int nx, int ny, int nz, const int *cap, int r[6]) {
+  const int unit[3] = {kStepThreads, 1, 1};
+  const int nb[3] = {(nx + kStepThreads - 1) / kStepThreads, ny, nz};
+  bool clipped = false;
+  for (int a = 0; a < 3; ++a) {
+    const int b0 = floor_div(box[2 * a], unit[a]), b1 = floor_div(box[2 * a + 1], unit[a]);
+    int first = b0 % nb[a], count = b1 - b0 + 1;
+    if (first < 0) first += nb[a];
+    if (count >= nb[a]) { first = 0; count = nb[a]; }
+    if (cap && count > cap[a]) { count = cap[a]; clipped = true; }
+    r[2 * a] = first;
+    r[2 * a + 1] = first + count;
+  }
+  return clipped;
+}
 constexpr int kReduceThreads = 256;
 constexpr int kForceSlots = 8;
 constexpr int kTotalsSlots = 8;

@@ -42,13 +42,17 @@ __device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__re
                                               float *__restrict__ mac, const StepParams &p) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x;
   const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-  const bool region = p.force_on && bx >= p.rbx0 && bx < p.rbx1 && by >= p.rby0 && by < p.rby1 &&
-                      bz >= p.rbz0 && bz < p.rbz1;
+  // the force region, read modulo the grid (it can cross a windowed seam)
+  int dx = bx - p.rbx0, dy = by - p.rby0, dz = bz - p.rbz0;
+  dx += dx < 0 ? (int)gridDim.x : 0;
+  dy += dy < 0 ? (int)gridDim.y : 0;
+  dz += dz < 0 ? (int)gridDim.z : 0;
+  const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
+  const bool region = p.force_on && dx < rx && dy < ry && dz < rz;
   CellForce cf;
   if (x < p.nx) cell3<Q, S>(fin, fout, mac, p, x, by, bz, region, cf);
   if (region) {
-    const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
-    const int part = ((bz - p.rbz0) * ry + (by - p.rby0)) * rx + (bx - p.rbx0);
+    const int part = (dz * ry + dy) * rx + dx;
     ForceAcc acc;
     acc.add(cf);
     reduce_force<kStepThreads>(acc, p.partials, p.counter, rx * ry * rz, part, p.force_out);
@@ -68,12 +72,12 @@ __device__ __forceinline__ void stage_pose(const StepParams &p, StepParams &sp) 
     sp.body = bp.body;
     sp.swept = bp.swept;
     sp.swept_band = bp.swept_band;
-    sp.rbx0 = bp.box[0] / kStepThreads;
-    sp.rbx1 = bp.box[1] / kStepThreads + 1;
-    sp.rby0 = bp.box[2];
-    sp.rby1 = bp.box[3] + 1;
-    sp.rbz0 = bp.box[4];
-    sp.rbz1 = bp.box[5] + 1;
+    sp.rbx0 = bp.region[0];
+    sp.rbx1 = bp.region[1];
+    sp.rby0 = bp.region[2];
+    sp.rby1 = bp.region[3];
+    sp.rbz0 = bp.region[4];
+    sp.rbz1 = bp.region[5];
   }
   __syncthreads();
 }
@@ -106,7 +110,7 @@ __device__ __noinline__ void integrate_and_publish(BodyDyn *dyn, const double *f
   np.body = body_pose(dyn->shape, dyn->st);
   int box[6];
   if (!body_cell_box(np.body, dyn->q, dyn->nx, dyn->ny, dyn->nz, dyn->bounceback, dyn->swept_force, dyn->chi_eps,
-                     box, &np.swept, &np.swept_band)) {
+                     box, &np.swept, &np.swept_band, dyn->win)) {
     const float c[3] = {np.body.cx, np.body.cy, np.body.cz};
     const int len[3] = {dyn->nx, dyn->ny, dyn->nz};
     for (int a = 0; a < 3; ++a) {
@@ -114,15 +118,7 @@ __device__ __noinline__ void integrate_and_publish(BodyDyn *dyn, const double *f
       box[2 * a] = box[2 * a + 1] = v;
     }
   }
-  const int unit[3] = {kStepThreads, 1, 1};
-  for (int a = 0; a < 3; ++a) {
-    const int b0 = box[2 * a] / unit[a], b1 = box[2 * a + 1] / unit[a];
-    if (b1 - b0 + 1 > dyn->cap[a]) {
-      box[2 * a + 1] = (b0 + dyn->cap[a]) * unit[a] - 1;
-      dyn->overflow += 1;
-    }
-  }
-  for (int k = 0; k < 6; ++k) np.box[k] = box[k];
+  if (box_region(box, dyn->nx, dyn->ny, dyn->nz, dyn->cap, np.region)) dyn->overflow += 1;
   *next = np;
 }
 
@@ -135,12 +131,17 @@ __global__ void __launch_bounds__(kStepThreads)
     d3_force_pass(const S *__restrict__ fin, const __grid_constant__ StepParams p) {
   __shared__ StepParams sp;
   stage_pose(p, sp);
-  const int bx = sp.rbx0 + blockIdx.x, by = sp.rby0 + blockIdx.y, bz = sp.rbz0 + blockIdx.z;
-  if (bx >= sp.rbx1 || by >= sp.rby1 || bz >= sp.rbz1) return;
+  const int rx = sp.rbx1 - sp.rbx0, ry = sp.rby1 - sp.rby0, rz = sp.rbz1 - sp.rbz0;
+  if ((int)blockIdx.x >= rx || (int)blockIdx.y >= ry || (int)blockIdx.z >= rz) return;
+  // blocks of the region, wrapped into the grid
+  const int nbx = (sp.nx + kStepThreads - 1) / kStepThreads;
+  int bx = sp.rbx0 + blockIdx.x, by = sp.rby0 + blockIdx.y, bz = sp.rbz0 + blockIdx.z;
+  bx -= bx >= nbx ? nbx : 0;
+  by -= by >= sp.ny ? sp.ny : 0;
+  bz -= bz >= sp.nz ? sp.nz : 0;
   const int x = bx * kStepThreads + threadIdx.x;
   CellForce cf;
   if (x < sp.nx) cell3_force<Q, S>(fin, sp, x, by, bz, cf);
-  const int rx = sp.rbx1 - sp.rbx0, ry = sp.rby1 - sp.rby0, rz = sp.rbz1 - sp.rbz0;
   const int part = ((int)blockIdx.z * ry + (int)blockIdx.y) * rx + (int)blockIdx.x;
   ForceAcc acc;
   acc.add(cf);

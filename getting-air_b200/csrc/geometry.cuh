@@ -3,9 +3,9 @@
 // 3D: common_d3_geometry.wgsl:60-253 (quaternion helpers qMul/qRotInv with
 // [w,x,y,z] layout, sdSphere, sdRoundBox, sdSpheroid with 3 Newton steps on
 // the meridional ellipse, get_phi3, get_phi3Ahead, bodyVelocity3,
-// chiFromPhiEps3). Without a moving window bodyDelta3 is exactly p - c
-// (common_d3_window.wgsl:43-52 at WIN_N* = 0), which is the only mode this
-// library runs.
+// chiFromPhiEps3). bodyDelta3 takes the nearest periodic image on the
+// axes of a moving window (common_d3_window.wgsl winWrapDelta) and is
+// exactly p - c without one.
 // 2D: common_geometry.wgsl:84-160 (get_phi: exact circle, far-field
 // algebraic early-out at SDF_FAR = 64, otherwise 3 Newton steps) with the
 // periodic nearest-image wrap `d -= N * round(d / N)`.
@@ -16,11 +16,30 @@
 
 #include <cuda_runtime.h>
 #include "../../include/lbm.h"
+#include "body.cuh"
 
 namespace lbm {
 
 struct V3 { float x, y, z; };
 struct Q4 { float w, x, y, z; };
+
+// winWrap1: d - n round(d / n), round to nearest even as WGSL's round, each
+// operation rounded on its own; the identity at n = 0.
+__device__ __forceinline__ float win_wrap1(float d, float n) {
+  return n > 0.f ? __fsub_rn(d, __fmul_rn(n, rintf(__fdiv_rn(d, n)))) : d;
+}
+
+// winOffset: whole cells the window has travelled, floor(c) - anchor.
+__device__ __forceinline__ float win_offset1(float c, float anchor, float n) {
+  return n > 0.f ? __fsub_rn(floorf(c), anchor) : 0.f;
+}
+
+// winCoord1: a buffer position as a window coordinate in [0, n).
+__device__ __forceinline__ float win_coord1(float p, float off, float n) {
+  if (!(n > 0.f)) return p;
+  const float w = __fsub_rn(p, off);
+  return __fsub_rn(w, __fmul_rn(n, floorf(__fdiv_rn(w, n))));
+}
 
 __device__ __forceinline__ Q4 q_mul(Q4 p, Q4 q) {
   return {p.w * q.w - p.x * q.x - p.y * q.y - p.z * q.z,
@@ -76,24 +95,34 @@ __device__ __forceinline__ float sdf_local3(V3 lp, const lbm_body &b) {
   return sd_round_box(lp, {b.a, b.b, b.c}, b.r);
 }
 
-__device__ __forceinline__ float phi3_inline(V3 p, const lbm_body &b) {
+// bodyDelta3: p relative to the body centre, nearest image on windowed axes.
+__device__ __forceinline__ V3 body_delta(V3 p, const lbm_body &b, const Win &w) {
   V3 d = {p.x - b.cx, p.y - b.cy, p.z - b.cz};
-  return sdf_local3(q_rot_inv({b.qw, b.qx, b.qy, b.qz}, d), b);
+  if (w.on) {
+    d.x = win_wrap1(d.x, w.n[0]);
+    d.y = win_wrap1(d.y, w.n[1]);
+    d.z = win_wrap1(d.z, w.n[2]);
+  }
+  return d;
+}
+
+__device__ __forceinline__ float phi3_inline(V3 p, const lbm_body &b, const Win &w) {
+  return sdf_local3(q_rot_inv({b.qw, b.qx, b.qy, b.qz}, body_delta(p, b, w)), b);
 }
 
 // Out of line: called per bounce-back link candidate, which only the thin
 // shell of cells next to the body evaluates; inlining it at 19-27 sites
 // bloats the step kernel past the instruction cache.
-static __device__ __noinline__ float phi3_call(float x, float y, float z, const lbm_body *b) {
-  return phi3_inline({x, y, z}, *b);
+static __device__ __noinline__ float phi3_call(float x, float y, float z, const lbm_body *b, const Win *w) {
+  return phi3_inline({x, y, z}, *b, *w);
 }
 
 // A sphere's distance does not depend on its orientation, so the per-cell
 // evaluation skips the rotation (bit-identical to the rotated form for the
 // identity quaternion, the only orientation a pinned sphere has).
-__device__ __forceinline__ float phi3(V3 p, const lbm_body &b) {
-  if (b.shape == LBM_SHAPE_SPHERE) return len3({p.x - b.cx, p.y - b.cy, p.z - b.cz}) - b.a;
-  return phi3_call(p.x, p.y, p.z, &b);
+__device__ __forceinline__ float phi3(V3 p, const lbm_body &b, const Win &w) {
+  if (b.shape == LBM_SHAPE_SPHERE) return len3(body_delta(p, b, w)) - b.a;
+  return phi3_call(p.x, p.y, p.z, &b, &w);
 }
 
 // exp map of an angular velocity over dt, common_d3_geometry.wgsl:86-91.
@@ -107,14 +136,20 @@ __device__ __forceinline__ Q4 exp_map(V3 w, float dt) {
 
 // The same body one step ahead at its current velocities,
 // common_d3_geometry.wgsl:199-203.
-__device__ __forceinline__ float phi3_ahead(V3 p, const lbm_body &b, float dt) {
+__device__ __forceinline__ float phi3_ahead(V3 p, const lbm_body &b, float dt, const Win &w) {
   V3 c = {b.cx + b.vx * dt, b.cy + b.vy * dt, b.cz + b.vz * dt};
   Q4 q = q_mul(exp_map({b.wx, b.wy, b.wz}, dt), {b.qw, b.qx, b.qy, b.qz});
-  return sdf_local3(q_rot_inv(q, {p.x - c.x, p.y - c.y, p.z - c.z}), b);
+  V3 d = {p.x - c.x, p.y - c.y, p.z - c.z};
+  if (w.on) {
+    d.x = win_wrap1(d.x, w.n[0]);
+    d.y = win_wrap1(d.y, w.n[1]);
+    d.z = win_wrap1(d.z, w.n[2]);
+  }
+  return sdf_local3(q_rot_inv(q, d), b);
 }
 
-__device__ __forceinline__ V3 body_velocity3(V3 p, const lbm_body &b) {
-  V3 r = {p.x - b.cx, p.y - b.cy, p.z - b.cz};
+__device__ __forceinline__ V3 body_velocity3(V3 p, const lbm_body &b, const Win &w) {
+  const V3 r = body_delta(p, b, w);
   // v + w x r
   return {b.vx + (b.wy * r.z - b.wz * r.y), b.vy + (b.wz * r.x - b.wx * r.z),
           b.vz + (b.wx * r.y - b.wy * r.x)};

@@ -36,6 +36,23 @@ int validate_config(const lbm_config *c, std::string &why) {
     if (!(c->body.a > 0.f)) { why = "body size must be positive"; return LBM_EINVAL; }
     if (!c->use_bounceback && !(c->chi_eps > 0.f)) { why = "chi_eps must be positive"; return LBM_EINVAL; }
   }
+  // the moving window's refusals (main-3d.js:316-348)
+  const bool win = c->window[0] || c->window[1] || c->window[2];
+  for (int a = 0; a < 3; ++a)
+    if (c->window[a] != 0 && c->window[a] != 1) { why = "window flags must be 0 or 1"; return LBM_EINVAL; }
+  if (win) {
+    if (c->q == 9) { why = "the moving window is 3D (the D2Q9 body already takes the nearest image)"; return LBM_EINVAL; }
+    if (!c->has_body) { why = "the moving window needs a body to follow"; return LBM_EINVAL; }
+    for (int a = 0; a < 3; ++a)
+      if (c->window[a] && c->wall[a]) {
+        why = "the moving window needs a periodic axis for the body to cross: no wall on a windowed axis";
+        return LBM_EINVAL;
+      }
+    if (!(c->sponge_w > 0.f)) {
+      why = "the moving window needs a sponge: without one the wake wraps around the periodic buffer";
+      return LBM_EINVAL;
+    }
+  }
   return LBM_OK;
 }
 
@@ -80,6 +97,16 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
   }
   p.pk = make_pack(c);
   p.body = c.body;
+  p.win = Win{};
+  if (c.q != 9) {
+    const int len[3] = {c.nx, c.ny, c.nz};
+    for (int a = 0; a < 3; ++a)
+      if (c.window[a]) {
+        p.win.n[a] = (float)len[a];
+        p.win.anchor[a] = (float)c.win_anchor[a];
+        p.win.on = 1;
+      }
+  }
   p.write_mac = 0;
   p.force_on = 0;
   p.swept = 0;
@@ -89,7 +116,7 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
 bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]) {
   if (!c.has_body) return false;
   return body_cell_box(c.body, c.q, c.nx, c.ny, c.nz, c.use_bounceback, c.swept_force, c.chi_eps, box, &p.swept,
-                       &p.swept_band);
+                       &p.swept_band, c.q != 9 ? c.window : nullptr);
 }
 
 }  // namespace lbm

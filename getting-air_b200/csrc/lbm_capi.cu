@@ -84,12 +84,11 @@ void set_force_region(lbm_session *s) {
   int box[6];
   p.force_on = force_cell_box(s->cfg, p, box) ? 1 : 0;
   if (!p.force_on) return;
-  p.rbx0 = box[0] / kStepThreads;
-  p.rbx1 = box[1] / kStepThreads + 1;
-  p.rby0 = box[2];
-  p.rby1 = box[3] + 1;
-  p.rbz0 = box[4];
-  p.rbz1 = box[5] + 1;
+  int r[6];
+  box_region(box, p.nx, p.ny, p.nz, nullptr, r);
+  p.rbx0 = r[0]; p.rbx1 = r[1];
+  p.rby0 = r[2]; p.rby1 = r[3];
+  p.rbz0 = r[4]; p.rbz1 = r[5];
 }
 
 int ensure_force_scratch(lbm_session *s) {
@@ -353,6 +352,12 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   if (!ok || !(qn > 0.5 && qn < 2.0)) return fail(s, LBM_EINVAL, "body state must be finite, massive and unit-quaternion");
   lbm_body_opts o;
   if (opts) o = *opts; else lbm_body_opts_default(&o);
+  {
+    // a windowed axis wraps the body at the domain length (winWrapPos)
+    const int len[3] = {c.nx, c.ny, c.nz};
+    for (int k = 0; k < 3; ++k)
+      if (c.window[k]) o.wrap[k] = len[k];
+  }
   BodyDyn d{};
   d.st = st;
   d.opt = o;
@@ -361,6 +366,7 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   d.bounceback = c.use_bounceback;
   d.swept_force = c.swept_force;
   d.chi_eps = c.chi_eps;
+  for (int k = 0; k < 3; ++k) d.win[k] = c.window[k];
   // Largest force box the body can need: its reach at the clamped speeds
   // (the whole domain when a clamp is off).
   const double rc = body_circumradius(c.body);
@@ -377,7 +383,7 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   p0.body = body_pose(c.body, st);
   int box[6];
   if (!body_cell_box(p0.body, c.q, c.nx, c.ny, c.nz, c.use_bounceback, c.swept_force, c.chi_eps, box, &p0.swept,
-                     &p0.swept_band)) {
+                     &p0.swept_band, c.window)) {
     const float ctr[3] = {p0.body.cx, p0.body.cy, p0.body.cz};
     const int len[3] = {c.nx, c.ny, c.nz};
     for (int a = 0; a < 3; ++a) {
@@ -385,12 +391,7 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
       box[2 * a] = box[2 * a + 1] = v;
     }
   }
-  const int unit[3] = {kStepThreads, 1, 1};
-  for (int a = 0; a < 3; ++a) {
-    const int b0 = box[2 * a] / unit[a], b1 = box[2 * a + 1] / unit[a];
-    if (b1 - b0 + 1 > d.cap[a]) box[2 * a + 1] = (b0 + d.cap[a]) * unit[a] - 1;
-  }
-  for (int k = 0; k < 6; ++k) p0.box[k] = box[k];
+  box_region(box, c.nx, c.ny, c.nz, d.cap, p0.region);
   const int need = d.cap[0] * d.cap[1] * d.cap[2];
   if (need > s->force_nparts) {
     cudaStreamSynchronize(s->stream);

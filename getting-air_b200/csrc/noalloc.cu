@@ -88,12 +88,11 @@ int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float
   int box[6];
   p.force_on = (force_out && lbm::force_cell_box(*cfg, p, box)) ? 1 : 0;
   if (p.force_on) {
-    p.rbx0 = box[0] / lbm::kStepThreads;
-    p.rbx1 = box[1] / lbm::kStepThreads + 1;
-    p.rby0 = box[2];
-    p.rby1 = box[3] + 1;
-    p.rbz0 = box[4];
-    p.rbz1 = box[5] + 1;
+    int r[6];
+    lbm::box_region(box, p.nx, p.ny, p.nz, nullptr, r);
+    p.rbx0 = r[0]; p.rbx1 = r[1];
+    p.rby0 = r[2]; p.rby1 = r[3];
+    p.rbz0 = r[4]; p.rbz1 = r[5];
     const int64_t parts = (int64_t)(p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0);
     if (parts > kNoAllocMaxParts)
       return nfail(LBM_ENOSPC, "the body's force region spans " + std::to_string(parts) +

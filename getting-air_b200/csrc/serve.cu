@@ -402,6 +402,8 @@ int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const fl
   if (!s) return LBM_EINVAL;
   std::string why;
   if (validate_config(cfg, why)) return sfail(s, LBM_EINVAL, why);
+  if (cfg->window[0] || cfg->window[1] || cfg->window[2])
+    return sfail(s, LBM_ENOTSUP, "the moving window runs in dense sessions and 3D AMR");
   if (steps < 1) return sfail(s, LBM_EINVAL, "steps must be >= 1");
   if (s->reqs.count(id)) return sfail(s, LBM_EINVAL, "request id already in use");
   StepParams tmp{};

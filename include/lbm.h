@@ -105,7 +105,13 @@ typedef struct {
   float sponge_u[3];      /* SPONGE_UX/UY/UZ far-field velocity              */
   lbm_body body;
   int32_t storage;        /* lbm_storage                                     */
-  int32_t reserved[7];    /* zero                                            */
+  int32_t window[3];      /* moving window per axis (3D, common_d3_window.wgsl
+                             WIN_N*): the body wraps through the periodic
+                             buffer and the sponge band follows it; needs a
+                             body, a sponge and no wall on the axis          */
+  int32_t win_anchor[3];  /* WIN_AX/AY/AZ: the cell the body sits in within
+                             the window, the floor of its initial centre    */
+  int32_t reserved[1];    /* zero                                            */
 } lbm_config;
 
 typedef struct lbm_session lbm_session;
@@ -133,7 +139,9 @@ typedef struct {
 typedef struct {
   double gravity[3];       /* uniform acceleration                             */
   double v_max, o_max;     /* magnitude clamps; <= 0 (or inf) = none           */
-  double wrap[3];          /* per-axis wrap length of the position, 0 = none   */
+  double wrap[3];          /* per-axis wrap length of the position, 0 = none;
+                              a session sets it to the domain length on the
+                              axes of its moving window                     */
   int32_t planar;          /* no z translation, rotation about z only          */
   int32_t no_fluid_force;  /* integrate without the fluid load (it is still recorded) */
   int32_t pinned;          /* record the load, do not move                     */

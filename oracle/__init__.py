@@ -296,3 +296,30 @@ class Amr3D:
 
     def __del__(self):
         self.close()
+
+
+def _win_fn(name, nargs):
+    f = getattr(lib(), name)
+    f.argtypes = [C.c_double] * nargs
+    f.restype = C.c_double
+    return f
+
+
+def win_wrap_delta(d: float, n: float) -> float:
+    """Nearest periodic image of a delta on an axis of length n (0 = no window)."""
+    return _win_fn("oracle_win_wrap_delta", 2)(d, n)
+
+
+def win_offset(c: float, anchor: float, n: float) -> float:
+    """Whole cells the window has travelled: floor(c) - anchor (0 = no window)."""
+    return _win_fn("oracle_win_offset", 3)(c, anchor, n)
+
+
+def win_coord(p: float, off: float, n: float) -> float:
+    """A buffer position as a window coordinate in [0, n)."""
+    return _win_fn("oracle_win_coord", 3)(p, off, n)
+
+
+def win_wrap_position(c: float, n: float) -> float:
+    """A body position wrapped into the buffer [0, n)."""
+    return _win_fn("oracle_win_wrap_position", 2)(c, n)

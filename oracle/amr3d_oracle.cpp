@@ -162,6 +162,7 @@ template <class R> struct Amr3D {
   std::vector<int32_t> free_list;
   std::vector<uint8_t> slot_new, want;
   int free_count = 0, refused = 0, min_free = 0, decisions = 0;
+  Win win;  // the moving window of the L0 configuration
   // the field criterion (common_d3_criterion.wgsl): off at q_abs = 0
   float q_abs = 0.f, q_hyst = 1.f, q_lead = 0.f;
   std::vector<float> block_q;
@@ -341,8 +342,8 @@ template <class R> struct Amr3D {
             };
             const int64_t cell = pcell(s, fx, fy, fz);
             const V3<R> p{f2c(fx, b[0] * t.rb), f2c(fy, b[1] * t.rb), f2c(fz, b[2] * t.rb)};
-            const R phi = hb ? phi3(p, bd) : R(1e30f);
-            const V3<R> us = hb ? body_vel3(p, bd) : V3<R>{0, 0, 0};
+            const R phi = hb ? phi3(p, bd, &win) : R(1e30f);
+            const V3<R> us = hb ? body_vel3(p, bd, &win) : V3<R>{0, 0, 0};
             R rhoW = R(1);
             if (bb && c.rho_w_local && phi < R(2)) {
               R sum = 0;
@@ -355,7 +356,7 @@ template <class R> struct Amr3D {
               int sc[3] = {fx - e[0], fy - e[1], fz - e[2]};
               if (bb) {
                 const V3<R> sp{f2c(sc[0], b[0] * t.rb), f2c(sc[1], b[1] * t.rb), f2c(sc[2], b[2] * t.rb)};
-                if (phi3(sp, bd) < R(0)) {
+                if (phi3(sp, bd, &win) < R(0)) {
                   const R corr = R(2) * R(T->w[i]) * rhoW * (R(e[0]) * us.x + R(e[1]) * us.y + R(e[2]) * us.z) / CS2;
                   f[i] = fin[T->opp[i] * P + cell] + corr;
                   continue;
@@ -394,9 +395,10 @@ template <class R> struct Amr3D {
             }
             R sw = R(0);
             if (c.sponge_w > 0) {
-              const R dx = c.sponge_axis[0] ? std::fmin(p.x, R(t.nx - 1) - p.x) : R(1e30f);
-              const R dy = c.sponge_axis[1] ? std::fmin(p.y, R(t.ny - 1) - p.y) : R(1e30f);
-              const R dz = c.sponge_axis[2] ? std::fmin(p.z, R(t.nz - 1) - p.z) : R(1e30f);
+              const V3<R> wp = win_coord(p, bd, &win);  // common_d3_amr_step1.wgsl:362
+              const R dx = c.sponge_axis[0] ? std::fmin(wp.x, R(t.nx - 1) - wp.x) : R(1e30f);
+              const R dy = c.sponge_axis[1] ? std::fmin(wp.y, R(t.ny - 1) - wp.y) : R(1e30f);
+              const R dz = c.sponge_axis[2] ? std::fmin(wp.z, R(t.nz - 1) - wp.z) : R(1e30f);
               sw = sponge(std::fmin(dx, std::fmin(dy, dz)), R(c.sponge_w));
             }
             const R usq = ux * ux + uy * uy + uz * uz, ufar = SUX * SUX + SUY * SUY + SUZ * SUZ;
@@ -510,7 +512,7 @@ template <class R> struct Amr3D {
       for (int y = 0; y < t.ny; ++y)
         for (int x = 0; x < t.nx; ++x) {
           if (!seam_cell(x, y, z)) continue;
-          if (c.has_body && phi3<R>({R(x), R(y), R(z)}, c.body) < R(2)) continue;
+          if (c.has_body && phi3<R>({R(x), R(y), R(z)}, c.body, &win) < R(2)) continue;
           const int64_t cell = ccell(x, y, z);
           R dm = acc[4 * cell], dp[3] = {acc[4 * cell + 1], acc[4 * cell + 2], acc[4 * cell + 3]};
           for (int i = 0; i < Q; ++i) {
@@ -631,9 +633,9 @@ template <class R> struct Amr3D {
           for (int fx = GH; fx < GH + RB2; ++fx) {
             const int64_t cell = pcell(s, fx, fy, fz);
             const V3<R> p{f2c(fx, b[0] * t.rb), f2c(fy, b[1] * t.rb), f2c(fz, b[2] * t.rb)};
-            const R phi = phi3(p, bd);
-            const V3<R> r{p.x - R(bd.cx), p.y - R(bd.cy), p.z - R(bd.cz)};
-            const V3<R> us = body_vel3(p, bd);
+            const R phi = phi3(p, bd, &win);
+            const V3<R> r = bdelta(p, bd, &win);
+            const V3<R> us = body_vel3(p, bd, &win);
             V3<R> fb{0, 0, 0}, fs{0, 0, 0};
             if (c.use_bounceback) {
               if (phi >= R(0)) {
@@ -646,7 +648,7 @@ template <class R> struct Amr3D {
                 for (int i = 0; i < Q; ++i) {
                   const V3<R> sp{f2c(fx - T->ex[i], b[0] * t.rb), f2c(fy - T->ey[i], b[1] * t.rb),
                                  f2c(fz - T->ez[i], b[2] * t.rb)};
-                  if (phi3(sp, bd) < R(0)) {
+                  if (phi3(sp, bd, &win) < R(0)) {
                     const R fo = f[T->opp[i] * P + cell];
                     const R corr = R(2) * R(T->w[i]) * rhoW *
                                    (R(T->ex[i]) * us.x + R(T->ey[i]) * us.y + R(T->ez[i]) * us.z) / CS2;
@@ -657,7 +659,7 @@ template <class R> struct Amr3D {
               }
               if (c.swept_force) {
                 const bool now = phi < R(0);
-                if (now != (phi3_ahead(p, bd, R(1)) < R(0))) {
+                if (now != (phi3_ahead(p, bd, R(1), &win) < R(0))) {
                   V3<R> mc{0, 0, 0};
                   for (int i = 0; i < Q; ++i) {
                     const R v = f[i * P + cell];
@@ -695,28 +697,28 @@ template <class R> struct Amr3D {
   }
 
   // ---- dynamic refinement (common_d3_manage.wgsl), in f32 as the kernel --
-  static bool box_near(const lbm_body &b, float cx, float cy, float cz, float h0, float reach) {
+  static bool box_near(const lbm_body &b, const Win *w, float cx, float cy, float cz, float h0, float reach) {
     const float S3 = 1.7320509f;
     const float R0 = h0 * S3;
-    const float p0 = phi3<float>({cx, cy, cz}, b);
+    const float p0 = phi3<float>({cx, cy, cz}, b, w);
     if (p0 - R0 > reach) return false;
     if (p0 <= reach) return true;
     const float h1 = h0 * 0.5f, R1 = R0 * 0.5f;
     for (int i = 0; i < 8; ++i) {
       const float c1x = cx + ((i & 1) ? h1 : -h1), c1y = cy + ((i & 2) ? h1 : -h1), c1z = cz + ((i & 4) ? h1 : -h1);
-      const float p1 = phi3<float>({c1x, c1y, c1z}, b);
+      const float p1 = phi3<float>({c1x, c1y, c1z}, b, w);
       if (p1 - R1 > reach) continue;
       if (p1 <= reach) return true;
       const float h2 = h1 * 0.5f, R2 = R1 * 0.5f;
       for (int j = 0; j < 8; ++j) {
         const float c2x = c1x + ((j & 1) ? h2 : -h2), c2y = c1y + ((j & 2) ? h2 : -h2), c2z = c1z + ((j & 4) ? h2 : -h2);
-        const float p2 = phi3<float>({c2x, c2y, c2z}, b);
+        const float p2 = phi3<float>({c2x, c2y, c2z}, b, w);
         if (p2 - R2 > reach) continue;
         if (p2 <= reach) return true;
         const float h3 = h2 * 0.5f, R3 = R2 * 0.5f;
         for (int k = 0; k < 8; ++k) {
           const float c3x = c2x + ((k & 1) ? h3 : -h3), c3y = c2y + ((k & 2) ? h3 : -h3), c3z = c2z + ((k & 4) ? h3 : -h3);
-          if (phi3<float>({c3x, c3y, c3z}, b) - R3 <= reach) return true;
+          if (phi3<float>({c3x, c3y, c3z}, b, w) - R3 <= reach) return true;
         }
       }
     }
@@ -795,7 +797,7 @@ template <class R> struct Amr3D {
     const float half = 0.5f * (float)t.rb;
     for (int id = 0; id < t.nb; ++id) {
       const int bx = id % t.nbx, by = (id / t.nbx) % t.nby, bz = id / (t.nbx * t.nby);
-      want[id] = box_near(b, (float)(bx * t.rb) + half, (float)(by * t.rb) + half, (float)(bz * t.rb) + half, half,
+      want[id] = box_near(b, &win, (float)(bx * t.rb) + half, (float)(by * t.rb) + half, (float)(bz * t.rb) + half, half,
                           reach);
     }
     if (q_abs > 0) {
@@ -889,6 +891,7 @@ Amr3D<R> *make(const lbm_config &c, int rb, int mode, double margin, double frac
                int capacity, int dynamic, int manage_every, int manage_start, int interp) {
   auto *a = new Amr3D<R>();
   a->c = c;
+  a->win = window_of(c);
   a->Q = c.q;
   a->T = &tables(c.q);
   a->t.nx = c.nx; a->t.ny = c.ny; a->t.nz = c.nz; a->t.rb = rb;

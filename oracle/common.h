@@ -130,12 +130,61 @@ template <class R> R sdf_local(V3<R> lp, const lbm_body &b) {
 
 template <class R> Q4<R> bquat(const lbm_body &b) { return {R(b.qw), R(b.qx), R(b.qy), R(b.qz)}; }
 
-template <class R> R phi3(V3<R> p, const lbm_body &b) {
-  V3<R> d{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
-  return sdf_local<R>(qrotinv(bquat<R>(b), d), b);
+// The moving window (common_d3_window.wgsl, d3-window.mjs:90-150): n is the
+// domain size on a windowed axis, 0 elsewhere; anchor the body's cell in the
+// window. winWrap1 takes the nearest image (round half to even, as WGSL),
+// winOffset the whole cells travelled, winCoord a buffer position in [0, n).
+struct Win {
+  double n[3] = {0, 0, 0};
+  double anchor[3] = {0, 0, 0};
+  bool on = false;
+};
+
+inline Win window_of(const lbm_config &c) {
+  Win w;
+  if (c.q == 9) return w;
+  const int len[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; ++a)
+    if (c.window[a]) {
+      w.n[a] = len[a];
+      w.anchor[a] = c.win_anchor[a];
+      w.on = true;
+    }
+  return w;
 }
 
-template <class R> R phi3_ahead(V3<R> p, const lbm_body &b, R dt) {
+template <class R> R win_wrap1(R d, double n) { return n > 0 ? d - R(n) * std::nearbyint(d / R(n)) : d; }
+template <class R> R win_offset1(R c, double anchor, double n) { return n > 0 ? std::floor(c) - R(anchor) : R(0); }
+template <class R> R win_coord1(R p, R off, double n) {
+  if (!(n > 0)) return p;
+  const R w = p - off;
+  return w - R(n) * std::floor(w / R(n));
+}
+
+// bodyDelta3: p relative to the body centre, nearest image on windowed axes.
+template <class R> V3<R> bdelta(V3<R> p, const lbm_body &b, const Win *w) {
+  V3<R> d{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
+  if (w && w->on) {
+    d.x = win_wrap1(d.x, w->n[0]);
+    d.y = win_wrap1(d.y, w->n[1]);
+    d.z = win_wrap1(d.z, w->n[2]);
+  }
+  return d;
+}
+
+// The sponge's view of a position: window coordinates (identity without one).
+template <class R> V3<R> win_coord(V3<R> p, const lbm_body &b, const Win *w) {
+  if (!w || !w->on) return p;
+  return {win_coord1(p.x, win_offset1(R(b.cx), w->anchor[0], w->n[0]), w->n[0]),
+          win_coord1(p.y, win_offset1(R(b.cy), w->anchor[1], w->n[1]), w->n[1]),
+          win_coord1(p.z, win_offset1(R(b.cz), w->anchor[2], w->n[2]), w->n[2])};
+}
+
+template <class R> R phi3(V3<R> p, const lbm_body &b, const Win *w = nullptr) {
+  return sdf_local<R>(qrotinv(bquat<R>(b), bdelta(p, b, w)), b);
+}
+
+template <class R> R phi3_ahead(V3<R> p, const lbm_body &b, R dt, const Win *win = nullptr) {
   V3<R> w{R(b.wx), R(b.wy), R(b.wz)};
   R m = len3(w);
   Q4<R> e{R(1), R(0), R(0), R(0)};
@@ -146,11 +195,17 @@ template <class R> R phi3_ahead(V3<R> p, const lbm_body &b, R dt) {
   }
   V3<R> c{R(b.cx) + R(b.vx) * dt, R(b.cy) + R(b.vy) * dt, R(b.cz) + R(b.vz) * dt};
   Q4<R> q = qmul(e, bquat<R>(b));
-  return sdf_local<R>(qrotinv(q, V3<R>{p.x - c.x, p.y - c.y, p.z - c.z}), b);
+  V3<R> d{p.x - c.x, p.y - c.y, p.z - c.z};
+  if (win && win->on) {
+    d.x = win_wrap1(d.x, win->n[0]);
+    d.y = win_wrap1(d.y, win->n[1]);
+    d.z = win_wrap1(d.z, win->n[2]);
+  }
+  return sdf_local<R>(qrotinv(q, d), b);
 }
 
-template <class R> V3<R> body_vel3(V3<R> p, const lbm_body &b) {
-  V3<R> r{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
+template <class R> V3<R> body_vel3(V3<R> p, const lbm_body &b, const Win *w = nullptr) {
+  const V3<R> r = bdelta(p, b, w);
   return {R(b.vx) + (R(b.wy) * r.z - R(b.wz) * r.y), R(b.vy) + (R(b.wz) * r.x - R(b.wx) * r.z),
           R(b.vz) + (R(b.wx) * r.y - R(b.wy) * r.x)};
 }

@@ -21,6 +21,7 @@ void force3(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
   const int NX = c.nx, NY = c.ny, NZ = c.nz, Q = c.q;
   const int64_t N = (int64_t)NX * NY * NZ;
   const lbm_body &b = c.body;
+  const Win win = window_of(c);
   const R CS2 = R(1) / R(3);
   std::vector<double> rows((size_t)NY * NZ * 7, 0.0);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -30,9 +31,9 @@ void force3(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
       for (int x = 0; x < NX; ++x) {
         const int64_t cell = ((int64_t)z * NY + y) * NX + x;
         V3<R> p{R(x), R(y), R(z)};
-        R phi = phi3(p, b);
-        V3<R> r{p.x - R(b.cx), p.y - R(b.cy), p.z - R(b.cz)};
-        V3<R> us = body_vel3(p, b);
+        R phi = phi3(p, b, &win);
+        V3<R> r = bdelta(p, b, &win);
+        V3<R> us = body_vel3(p, b, &win);
         V3<R> fb{0, 0, 0}, tb{0, 0, 0};
         if (c.use_bounceback) {
           if (phi >= R(0)) {
@@ -44,7 +45,7 @@ void force3(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
             }
             for (int i = 0; i < Q; ++i) {
               V3<R> sp{p.x - R(T.ex[i]), p.y - R(T.ey[i]), p.z - R(T.ez[i])};
-              if (phi3(sp, b) < R(0)) {
+              if (phi3(sp, b, &win) < R(0)) {
                 R fo = fin[T.opp[i] * N + cell];
                 R corr = R(2) * R(T.w[i]) * rhoW *
                          (R(T.ex[i]) * us.x + R(T.ey[i]) * us.y + R(T.ez[i]) * us.z) / CS2;
@@ -57,7 +58,7 @@ void force3(const lbm_config &c, const std::vector<R> &fin, double out[8]) {
           }
           if (c.swept_force) {
             bool now = phi < R(0);
-            if (now != (phi3_ahead(p, b, R(1)) < R(0))) {
+            if (now != (phi3_ahead(p, b, R(1), &win) < R(0))) {
               V3<R> mc{0, 0, 0};
               for (int i = 0; i < Q; ++i) {
                 R v = fin[i * N + cell];
@@ -114,6 +115,7 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
   const int NX = c.nx, NY = c.ny, NZ = c.nz, Q = c.q;
   const int64_t N = (int64_t)NX * NY * NZ;
   const lbm_body &b = c.body;
+  const Win win = window_of(c);
   const R CS2 = R(1) / R(3);
   const R OMEGA = R(1) / R(c.tau);
   const R FX = R(c.force[0]), FY = R(c.force[1]), FZ = R(c.force[2]);
@@ -125,8 +127,8 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
         if (cover.at(x, y, z)) continue;
         const int64_t cell = ((int64_t)z * NY + y) * NX + x;
         V3<R> p{R(x), R(y), R(z)};
-        R phi = c.has_body ? phi3(p, b) : R(1e30f);
-        V3<R> us = c.has_body ? body_vel3(p, b) : V3<R>{0, 0, 0};
+        R phi = c.has_body ? phi3(p, b, &win) : R(1e30f);
+        V3<R> us = c.has_body ? body_vel3(p, b, &win) : V3<R>{0, 0, 0};
         const bool bb = c.has_body && c.use_bounceback;
         R rhoW = R(1);
         if (bb && c.rho_w_local && phi < R(2)) {
@@ -137,7 +139,7 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
         R f[27];
         for (int i = 0; i < Q; ++i) {
           int sxi = x - T.ex[i], syi = y - T.ey[i], szi = z - T.ez[i];
-          if (bb && phi3(V3<R>{R(sxi), R(syi), R(szi)}, b) < R(0)) {
+          if (bb && phi3(V3<R>{R(sxi), R(syi), R(szi)}, b, &win) < R(0)) {
             R corr = R(2) * R(T.w[i]) * rhoW *
                      (R(T.ex[i]) * us.x + R(T.ey[i]) * us.y + R(T.ez[i]) * us.z) / CS2;
             f[i] = fin[T.opp[i] * N + cell] + corr;
@@ -164,9 +166,10 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
         R usq = ux * ux + uy * uy + uz * uz;
         R sw = R(0);
         if (c.sponge_w > 0) {
-          R dx = c.sponge_axis[0] ? std::fmin(p.x, R(NX - 1) - p.x) : R(1e30f);
-          R dy = c.sponge_axis[1] ? std::fmin(p.y, R(NY - 1) - p.y) : R(1e30f);
-          R dz = c.sponge_axis[2] ? std::fmin(p.z, R(NZ - 1) - p.z) : R(1e30f);
+          const V3<R> wp = win_coord(p, b, &win);  // common_d3_step.wgsl:316
+          R dx = c.sponge_axis[0] ? std::fmin(wp.x, R(NX - 1) - wp.x) : R(1e30f);
+          R dy = c.sponge_axis[1] ? std::fmin(wp.y, R(NY - 1) - wp.y) : R(1e30f);
+          R dz = c.sponge_axis[2] ? std::fmin(wp.z, R(NZ - 1) - wp.z) : R(1e30f);
           sw = sponge(std::fmin(dx, std::fmin(dy, dz)), R(c.sponge_w));
         }
         const bool solid = c.solid_eq && bb && phi < R(0);

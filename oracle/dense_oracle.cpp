@@ -180,11 +180,22 @@ int oracle_run_free(const lbm_config *c, int fp32, double *f, int nsteps, lbm_bo
                     const lbm_body_opts *o, double *mac, double *forces, double *traj) {
   if (!c || !f || !state || !o || c->q == 9 || nsteps < 0) return -1;
   RigidBody r = from_state(*state);
-  if (fp32) run_free<float>(*c, f, nsteps, r, *o, mac, forces, traj);
-  else run_free<double>(*c, f, nsteps, r, *o, mac, forces, traj);
+  lbm_body_opts oo = *o;
+  const int len[3] = {c->nx, c->ny, c->nz};
+  for (int k = 0; k < 3; ++k)
+    if (c->window[k]) oo.wrap[k] = len[k];  // a windowed axis wraps the body (winWrapPos)
+  if (fp32) run_free<float>(*c, f, nsteps, r, oo, mac, forces, traj);
+  else run_free<double>(*c, f, nsteps, r, oo, mac, forces, traj);
   to_state(r, *state);
   return 0;
 }
+
+// The moving window's scalar maps (d3-window.mjs wrapDelta, windowOffset,
+// windowCoord, wrapPosition), FP64; n = 0 is an unwindowed axis.
+double oracle_win_wrap_delta(double d, double n) { return win_wrap1<double>(d, n); }
+double oracle_win_offset(double c, double anchor, double n) { return win_offset1<double>(c, anchor, n); }
+double oracle_win_coord(double p, double off, double n) { return win_coord1<double>(p, off, n); }
+double oracle_win_wrap_position(double c, double n) { return wrap_pos(c, n); }
 
 // Derived lattice tables (weights as exact f32 values).
 int oracle_tables(int q, int32_t *ex, int32_t *ey, int32_t *ez, float *w, int32_t *opp) {
