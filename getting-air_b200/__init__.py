@@ -109,6 +109,20 @@ class Amr3DConfig(C.Structure):
 REFINE = {"body": 0, "box": 1, "bar": 2, "slab": 3, "all": 4, "list": 5}
 
 
+class VolumeSpec(C.Structure):
+    _fields_ = [("origin", C.c_float * 3), ("shape", C.c_int32 * 3), ("h", C.c_float * 3), ("fp16", C.c_int32),
+                ("device", C.c_int32)]
+
+
+class SliceSpec(C.Structure):
+    _fields_ = [("axis", C.c_int32), ("slice", C.c_int32), ("mode", C.c_int32), ("rot", C.c_int32),
+                ("u_scale", C.c_float), ("v_scale", C.c_float), ("vort_scale", C.c_float),
+                ("vort_gamma", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("device", C.c_int32)]
+
+
+SLICE_MODES = {"speed": 0, "vorticity": 1, "normal": 2}
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is missing: build it with getting-air_b200/build.py "
@@ -130,6 +144,12 @@ def _load() -> C.CDLL:
         "lbm_write_f_raw": ([P, P], I),
         "lbm_read_f_raw": ([P, P], I),
         "lbm_read_mac": ([P, F], I),
+        "lbm_volume_spec_default": ([C.POINTER(VolumeSpec), I, I, I], I),
+        "lbm_slice_spec_default": ([C.POINTER(SliceSpec), I, I, I], I),
+        "lbm_resample": ([P, C.POINTER(VolumeSpec), P, P], I),
+        "lbm_render_slice": ([P, C.POINTER(SliceSpec), P], I),
+        "lbm_amr3d_resample": ([P, C.POINTER(VolumeSpec), P, P], I),
+        "lbm_amr3d_render_slice": ([P, C.POINTER(SliceSpec), P], I),
         "lbm_step": ([P, I], I),
         "lbm_set_body": ([P, C.POINTER(Body)], I),
         "lbm_forces": ([P, D], I),
@@ -382,6 +402,14 @@ class Solver:
     def step(self, n: int = 1):
         self._check(lib.lbm_step(self._h, int(n)))
 
+    def resample(self, **kw):
+        """The field on a voxel box (volume_spec keywords; `level`, `out`)."""
+        return _resample(lib.lbm_resample, self._h, self._check, self.dims, **kw)
+
+    def render_slice(self, **kw) -> np.ndarray:
+        """An axis-aligned slice picture, (height, width, 4) RGBA8."""
+        return _render(lib.lbm_render_slice, self._h, self._check, self.dims, **kw)
+
     def set_body(self, body: Body):
         self._check(lib.lbm_set_body(self._h, C.byref(body)))
 
@@ -452,6 +480,65 @@ def body_advance(state: BodyState, opts: BodyOpts, n: int = 1, force=(0.0, 0.0, 
     if rc:
         raise LbmError(rc, "invalid body state or options")
     return state
+
+
+def volume_spec(dims, origin=(0.0, 0.0, 0.0), shape=None, h=(1.0, 1.0, 1.0), fp16=False) -> VolumeSpec:
+    """A voxel box in L0 cell units (cell centres at integers): `shape`
+    voxels of `h` L0 cells from `origin`; the whole L0 grid by default."""
+    v = VolumeSpec()
+    lib.lbm_volume_spec_default(C.byref(v), *dims)
+    for k in range(3):
+        v.origin[k] = float(origin[k])
+        v.h[k] = float(h[k])
+        if shape is not None:
+            v.shape[k] = int(shape[k])
+    v.fp16 = int(bool(fp16))
+    return v
+
+
+def slice_spec(dims, axis=2, slice=None, mode="speed", rot=0, width=None, height=None, u_scale=0.05,
+               v_scale=0.01, vort_scale=1.0, vort_gamma=1.2) -> SliceSpec:
+    """An axis-aligned slice picture (common_d3_render_slice.wgsl RParams);
+    one pixel per L0 cell of the plane by default."""
+    v = SliceSpec()
+    lib.lbm_slice_spec_default(C.byref(v), *dims)
+    v.axis = int(axis)
+    v.slice = int(dims[axis] // 2 if slice is None else slice)
+    v.mode = SLICE_MODES[mode] if isinstance(mode, str) else int(mode)
+    v.rot = int(rot)
+    pa, pb = dims[(axis + 1) % 3], dims[(axis + 2) % 3]
+    if rot % 2:
+        pa, pb = pb, pa
+    v.width = int(pa if width is None else width)
+    v.height = int(pb if height is None else height)
+    v.u_scale, v.v_scale = float(u_scale), float(v_scale)
+    v.vort_scale, v.vort_gamma = float(vort_scale), float(vort_gamma)
+    return v
+
+
+def _resample(fn, handle, check, dims, out=None, level=False, **kw):
+    """Host arrays (nz, ny, nx, 4) float16/float32 and (nz, ny, nx) uint8, or
+    into a device tensor `out` (its data pointer, no copy)."""
+    spec = volume_spec(dims, **kw)
+    shp = (spec.shape[2], spec.shape[1], spec.shape[0])
+    if out is not None and hasattr(out, "data_ptr"):
+        spec.device = 1
+        lv = level if (level is not False and hasattr(level, "data_ptr")) else None
+        check(fn(handle, C.byref(spec), C.c_void_p(out.data_ptr()),
+                 C.c_void_p(lv.data_ptr() if lv is not None else 0)))
+        return out, lv
+    arr = np.empty(shp + (4,), np.float16 if spec.fp16 else np.float32)
+    lv = np.empty(shp, np.uint8) if level else None
+    check(fn(handle, C.byref(spec), arr.ctypes.data_as(C.c_void_p),
+             lv.ctypes.data_as(C.c_void_p) if lv is not None else None))
+    return arr, lv
+
+
+def _render(fn, handle, check, dims, **kw):
+    spec = slice_spec(dims, **kw)
+    img = np.empty((spec.height, spec.width, 4), np.uint8)
+    check(fn(handle, C.byref(spec), img.ctypes.data_as(C.c_void_p)))
+    return img
 
 
 def config_from(q: int, dims, **kw) -> Config:
@@ -893,6 +980,14 @@ class Amr3D:
         out = np.zeros(4, np.int32)
         self._check(lib.lbm_amr3d_pool_stats(self._h, _ptr(out, C.c_int32)))
         return {"in_use": int(out[0]), "refusals": int(out[1]), "min_free": int(out[2]), "decisions": int(out[3])}
+
+    def resample(self, **kw):
+        """The hierarchy on a voxel box, finest level wins (volume_spec keywords)."""
+        return _resample(lib.lbm_amr3d_resample, self._h, self._check, self.dims, **kw)
+
+    def render_slice(self, **kw) -> np.ndarray:
+        """An axis-aligned slice picture of the hierarchy, (height, width, 4)."""
+        return _render(lib.lbm_amr3d_render_slice, self._h, self._check, self.dims, **kw)
 
     def block_q(self, lead: float = 0.0) -> np.ndarray:
         """Per-block max Q-criterion of the L0 velocity, box dilated by `lead`."""

@@ -33,6 +33,7 @@
 #include "amr3d.cuh"
 #include "cell_update.cuh"
 #include "host_params.cuh"
+#include "sample.cuh"
 
 namespace lbm {
 
@@ -1399,6 +1400,35 @@ int lbm_amr3d_block_q(lbm_amr3d *a, float lead, float *block_q) {
   if (d != a->d_block_q) cudaFreeAsync(d, a->stream);
   ACK(a, e);
   ACK(a, cudaStreamSynchronize(a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr3d_resample(lbm_amr3d *a, const lbm_volume_spec *spec, void *out, uint8_t *level) {
+  if (!a) return LBM_EINVAL;
+  std::string why;
+  if (validate_volume(spec, why)) return afail(a, LBM_EINVAL, why);
+  if (!out) return afail(a, LBM_EINVAL, "out is NULL");
+  const Amr3Params &p = a->p;
+  const TreeView t{(const float4 *)a->macc, p.nx, p.ny, p.nz, p.slots ? 1 : 0, (const float4 *)a->macp,
+                   a->d_block_slot, p.rb, p.FB, p.T3};
+  ACK(a, run_resample(t, *spec, out, level, a->stream));
+  return LBM_OK;
+}
+
+int lbm_amr3d_render_slice(lbm_amr3d *a, const lbm_slice_spec *spec, uint8_t *rgba) {
+  if (!a) return LBM_EINVAL;
+  const Amr3Params &p = a->p;
+  std::string why;
+  if (validate_slice(spec, p.nx, p.ny, p.nz, why)) return afail(a, LBM_EINVAL, why);
+  if (!rgba) return afail(a, LBM_EINVAL, "rgba is NULL");
+  const lbm_config &c = a->cfg.root;
+  ViewOffset off{{0.f, 0.f, 0.f}};
+  const float ctr[3] = {c.body.cx, c.body.cy, c.body.cz};
+  for (int k = 0; k < 3; ++k)
+    if (c.window[k]) off.v[k] = ctr[k] - (float)c.win_anchor[k];
+  const TreeView t{(const float4 *)a->macc, p.nx, p.ny, p.nz, p.slots ? 1 : 0, (const float4 *)a->macp,
+                   a->d_block_slot, p.rb, p.FB, p.T3};
+  ACK(a, run_slice(t, *spec, off, rgba, a->stream));
   return LBM_OK;
 }
 

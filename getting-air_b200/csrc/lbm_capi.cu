@@ -17,6 +17,7 @@
 #include "dense.cuh"
 #include "host_params.cuh"
 #include "lattice.cuh"
+#include "sample.cuh"
 
 using namespace lbm;
 
@@ -415,6 +416,43 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   for (int k = 0; k < 3; ++k) s->cap[k] = d.cap[k];
   s->body_par = 0;
   s->free_body = true;
+  return LBM_OK;
+}
+
+int lbm_resample(lbm_session *s, const lbm_volume_spec *spec, void *out, uint8_t *level) {
+  if (!s) return LBM_EINVAL;
+  std::string why;
+  if (validate_volume(spec, why)) return fail(s, LBM_EINVAL, why);
+  if (!out) return fail(s, LBM_EINVAL, "out is NULL");
+  if (s->q == 9) return fail(s, LBM_ENOTSUP, "the headless views are 3D");
+  const lbm_config &c = s->cfg;
+  const TreeView t{(const float4 *)s->mac, c.nx, c.ny, c.nz, 0, nullptr, nullptr, 1, 1, 1};
+  CK(s, run_resample(t, *spec, out, level, s->stream));
+  return LBM_OK;
+}
+
+int lbm_render_slice(lbm_session *s, const lbm_slice_spec *spec, uint8_t *rgba) {
+  if (!s) return LBM_EINVAL;
+  const lbm_config &c = s->cfg;
+  std::string why;
+  if (validate_slice(spec, c.nx, c.ny, c.nz, why)) return fail(s, LBM_EINVAL, why);
+  if (!rgba) return fail(s, LBM_EINVAL, "rgba is NULL");
+  if (s->q == 9) return fail(s, LBM_ENOTSUP, "the headless views are 3D");
+  // winViewOffset: the view pans with the body under a moving window
+  ViewOffset off{{0.f, 0.f, 0.f}};
+  if (c.window[0] || c.window[1] || c.window[2]) {
+    float ctr[3] = {c.body.cx, c.body.cy, c.body.cz};
+    if (s->free_body) {
+      lbm_body_state st;
+      CK(s, cudaMemcpyAsync(&st, &s->dyn->st, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+      CK(s, cudaStreamSynchronize(s->stream));
+      for (int k = 0; k < 3; ++k) ctr[k] = (float)st.x[k];
+    }
+    for (int k = 0; k < 3; ++k)
+      if (c.window[k]) off.v[k] = ctr[k] - (float)c.win_anchor[k];
+  }
+  const TreeView t{(const float4 *)s->mac, c.nx, c.ny, c.nz, 0, nullptr, nullptr, 1, 1, 1};
+  CK(s, run_slice(t, *spec, off, rgba, s->stream));
   return LBM_OK;
 }
 

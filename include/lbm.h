@@ -195,6 +195,43 @@ int lbm_read_f_raw(lbm_session *s, void *planes);
 /* Reads the macroscopic field of the last step (4 floats per cell). */
 int lbm_read_mac(lbm_session *s, float *mac);
 
+/* ---- headless views of the field (no graphics API) ----------------------
+ * The reference resamples its hierarchy onto a 3D texture
+ * (common_d3_resample.wgsl over common_d3_tree_sample.wgsl sampleTree:
+ * nearest sample, finest level present wins) and draws axis-aligned slices
+ * (common_d3_render_slice.wgsl fs_main with common_vortcolor.wgsl). Here
+ * both are compute kernels writing into a buffer. */
+typedef struct {
+  float origin[3];    /* volOrigin: L0 cell units, cell centres at integers  */
+  int32_t shape[3];   /* VOL_NX/NY/NZ voxels                                  */
+  float h[3];         /* VOL_HX/HY/HZ: L0 cells per voxel                     */
+  int32_t fp16;       /* 1: texels as IEEE binary16 (the rgba16float texture),
+                         0: f32. Texel = (ux, uy, uz, rho), x fastest          */
+  int32_t device;     /* 1: out / level are device pointers (no copy, no sync) */
+} lbm_volume_spec;
+
+typedef struct {
+  int32_t axis;       /* slice normal: 0 x, 1 y, 2 z (in-plane axes cyclic)   */
+  int32_t slice;      /* index along the normal, window coordinates           */
+  int32_t mode;       /* 0 speed, 1 out-of-plane vorticity, 2 normal velocity */
+  int32_t rot;        /* quarter turns of the picture, clockwise              */
+  float u_scale;      /* velocity reference of modes 0 and 2                  */
+  float v_scale;      /* vorticity reference of mode 1                        */
+  float vort_scale;   /* common_vortcolor.wgsl VORT_SCALE (the 3D page: 1)    */
+  float vort_gamma;   /* VORT_GAMMA (1.2)                                     */
+  int32_t width, height;  /* pixels; RGBA8 rows top to bottom                 */
+  int32_t device;     /* 1: rgba is a device pointer                          */
+} lbm_slice_spec;
+
+/* Defaults: full-domain L0 volume (origin 0, h 1, f32, host) / a z slice
+ * through the middle, speed, 1:1 pixels, VORT_SCALE 1, VORT_GAMMA 1.2. */
+int lbm_volume_spec_default(lbm_volume_spec *v, int nx, int ny, int nz);
+int lbm_slice_spec_default(lbm_slice_spec *v, int nx, int ny, int nz);
+/* The dense session's field (level 0 only) resampled / drawn; `level` (one
+ * byte per voxel, may be NULL) receives the level each voxel came from. */
+int lbm_resample(lbm_session *s, const lbm_volume_spec *spec, void *out, uint8_t *level);
+int lbm_render_slice(lbm_session *s, const lbm_slice_spec *spec, uint8_t *rgba);
+
 /* Advances n fused stream-collide steps (common_d3_step.wgsl:224 `step`,
  * lbm_step.wgsl:137 `main`), each fused with the body force/torque sum of
  * common_d3_force.wgsl / lbm_force.wgsl over the pre-streaming f. mac is
@@ -453,6 +490,11 @@ int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]);
  * Replaces the reference's criterion readback (common_d3_criterion.wgsl
  * reduceQ into blockQ, read by main-3d.js debugCriterion). */
 int lbm_amr3d_block_q(lbm_amr3d *a, float lead, float *block_q);
+/* The hierarchy's field of the last macro-step resampled onto a voxel box /
+ * drawn as a slice, each point answered by the finest level present there
+ * (common_d3_resample.wgsl, common_d3_render_slice.wgsl). */
+int lbm_amr3d_resample(lbm_amr3d *a, const lbm_volume_spec *spec, void *out, uint8_t *level);
+int lbm_amr3d_render_slice(lbm_amr3d *a, const lbm_slice_spec *spec, uint8_t *rgba);
 /* Force and torque on the body at the last macro-step (pool force, FP64). */
 int lbm_amr3d_forces(lbm_amr3d *a, double out[6]);
 /* Over the L0 macroscopic field of the last step (covered cells carry the

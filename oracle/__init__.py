@@ -323,3 +323,50 @@ def win_coord(p: float, off: float, n: float) -> float:
 def win_wrap_position(c: float, n: float) -> float:
     """A body position wrapped into the buffer [0, n)."""
     return _win_fn("oracle_win_wrap_position", 2)(c, n)
+
+
+def _tree_args(mac, dims, levels, macp, block_slot, rb, fb):
+    nx, ny, nz = dims
+    mac = np.ascontiguousarray(mac, np.float32).reshape(-1, 4)
+    if levels:
+        macp = np.ascontiguousarray(macp, np.float32).reshape(-1, 4)
+        bs = np.ascontiguousarray(block_slot, np.int32)
+    else:
+        macp = np.zeros((1, 4), np.float32)
+        bs = np.zeros(1, np.int32)
+    keep = (mac, macp, bs)
+    F, I32 = C.POINTER(C.c_float), C.POINTER(C.c_int32)
+    return keep, [nx, ny, nz, mac.ctypes.data_as(F), int(levels), macp.ctypes.data_as(F), bs.ctypes.data_as(I32),
+                  int(rb), int(fb)]
+
+
+def tree_resample(mac, dims, origin, shape, h, levels=0, macp=None, block_slot=None, rb=1, fb=1):
+    """The voxel box sampled from the hierarchy (finest level wins): (nvox, 4)
+    f32 texels (ux, uy, uz, rho), x fastest, and the level per voxel."""
+    keep, args = _tree_args(mac, dims, levels, macp, block_slot, rb, fb)
+    nvox = int(np.prod(shape))
+    out = np.zeros((nvox, 4), np.float32)
+    lvl = np.zeros(nvox, np.uint8)
+    o = np.ascontiguousarray(origin, np.float32)
+    s = np.ascontiguousarray(shape, np.int32)
+    hh = np.ascontiguousarray(h, np.float32)
+    F = C.POINTER(C.c_float)
+    lib().oracle_tree_resample(*args, o.ctypes.data_as(F), s.ctypes.data_as(C.POINTER(C.c_int32)),
+                               hh.ctypes.data_as(F), out.ctypes.data_as(F), lvl.ctypes.data_as(C.POINTER(C.c_uint8)))
+    del keep
+    return out, lvl
+
+
+def tree_slice(mac, dims, axis, slice, mode, rot, width, height, u_scale, v_scale, vort_scale=1.0, vort_gamma=1.2,
+               off=(0.0, 0.0, 0.0), levels=0, macp=None, block_slot=None, rb=1, fb=1):
+    """One slice picture (height, width, 4) uint8, rows top to bottom."""
+    keep, args = _tree_args(mac, dims, levels, macp, block_slot, rb, fb)
+    params = np.array([axis, slice, mode, rot, width, height], np.int32)
+    scales = np.array([u_scale, v_scale, vort_scale, vort_gamma], np.float32)
+    o = np.ascontiguousarray(off, np.float32)
+    img = np.zeros((height, width, 4), np.uint8)
+    F = C.POINTER(C.c_float)
+    lib().oracle_tree_slice(*args, params.ctypes.data_as(C.POINTER(C.c_int32)), scales.ctypes.data_as(F),
+                            o.ctypes.data_as(F), img.ctypes.data_as(C.POINTER(C.c_uint8)))
+    del keep
+    return img

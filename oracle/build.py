@@ -12,7 +12,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_build" / "liboracle.so"
-SOURCES = ["dense_oracle.cpp", "amr2d_oracle.cpp", "amr3d_oracle.cpp"]
+SOURCES = ["dense_oracle.cpp", "amr2d_oracle.cpp", "amr3d_oracle.cpp", "sample_oracle.cpp"]
 FLAGS = ["-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared"]
 
 
