@@ -376,14 +376,22 @@ def time_amr3d(lbm, steps, warmup, world):
 def time_served(lbm, world, count=48, budget_gb=48):
     """Serving: a seeded Poisson stream (200 req/s) of D3Q19/D3Q27 sphere or
     rounded-box solves, N^3 with N log-uniform in [32, 192], 500-2000 steps,
+    a quarter of them two-level AMR solves (blocks near the body refined),
     admitted by HBM budget into one device arena and batched continuously.
     Latency = completion - arrival on the host clock. Against it, the plain
-    form: the same requests one after another as dense sessions (FIFO)."""
+    form: the same requests one after another as single sessions (FIFO).
+    Work = lattice updates (an AMR macro-step counts its L0 cells outside
+    refined blocks plus two substeps of every fine cell)."""
     import torch
     from getting_air_b200 import scenarios as sc
-    reqs = sc.serving_stream(count=count, seed=2024, rate=200.0)
-    cfgs = {r["id"]: lbm.config_from(r["q"], r["dims"], **r["kw"]) for r in reqs}
-    work = sum(int(np.prod(r["dims"])) * r["steps"] for r in reqs)
+    reqs = sc.serving_stream(count=count, seed=2024, rate=200.0, amr_frac=0.25)
+    cfgs = {r["id"]: sc.serving_config(lbm, r) for r in reqs}
+
+    def submit(srv, r):
+        if r["levels"] == 2:
+            srv.submit_amr3d(r["id"], cfgs[r["id"]], r["steps"])
+        else:
+            srv.submit(r["id"], cfgs[r["id"]], r["steps"])
     # warm the kernels of both lattices
     w = lbm.Server(1 << 30)
     for k, q in enumerate((19, 27)):
@@ -399,8 +407,7 @@ def time_served(lbm, world, count=48, budget_gb=48):
     while len(done) < len(reqs):
         now = time.perf_counter() - t0
         while nxt < len(reqs) and reqs[nxt]["t"] <= now:
-            r = reqs[nxt]
-            srv.submit(r["id"], cfgs[r["id"]], r["steps"])
+            submit(srv, reqs[nxt])
             nxt += 1
         st = srv.stats()
         if st["resident"] == 0 and st["queued"] == 0:
@@ -413,9 +420,11 @@ def time_served(lbm, world, count=48, budget_gb=48):
             lat[r["id"]] = tdone - reqs[r["id"]]["t"]
             srv.release(r["id"])
     total = time.perf_counter() - t0
+    work = srv.stats()["lattice_updates"]
     srv.close()
     L = np.array(sorted(lat.values()))
     served = {"mlups": work / total / 1e6, "wall_s": total, "requests": len(reqs),
+              "amr_requests": sum(r["levels"] == 2 for r in reqs),
               "lattice_updates": work, "p50_latency_ms": 1e3 * float(np.percentile(L, 50)),
               "p99_latency_ms": 1e3 * float(np.percentile(L, 99)), "budget_gb": budget_gb,
               "arrivals": "Poisson 200/s, seed 2024", "timing": "host wall clock, first arrival to last completion"}
@@ -426,7 +435,7 @@ def time_served(lbm, world, count=48, budget_gb=48):
         now = time.perf_counter() - t0
         if now < r["t"]:
             time.sleep(r["t"] - now)
-        s = lbm.Solver(cfgs[r["id"]])
+        s = lbm.Amr3D(cfgs[r["id"]]) if r["levels"] == 2 else lbm.Solver(cfgs[r["id"]])
         s.init_macro(sc.uniform_macro(int(np.prod(r["dims"])), (0.05, 0.0, 0.0)))
         s.step(r["steps"])
         s.forces()
@@ -436,7 +445,7 @@ def time_served(lbm, world, count=48, budget_gb=48):
     P = np.array(plat)
     plain = {"mlups": work / ptotal / 1e6, "wall_s": ptotal, "p50_latency_ms": 1e3 * float(np.percentile(P, 50)),
              "p99_latency_ms": 1e3 * float(np.percentile(P, 99)),
-             "timing": "host wall clock; requests one after another as dense sessions"}
+             "timing": "host wall clock; requests one after another as single sessions"}
     return served, plain
 
 

@@ -231,6 +231,9 @@ def _load() -> C.CDLL:
         "lbm_amr3d_set_body": ([P, C.POINTER(Body)], I),
         "lbm_amr3d_pool_stats": ([P, C.POINTER(C.c_int32)], I),
         "lbm_amr3d_block_q": ([P, C.c_float, C.POINTER(C.c_float)], I),
+        "lbm_amr3d_device_bytes": ([C.POINTER(Amr3DConfig), P, C.POINTER(C.c_int64)], I),
+        "lbm_amr3d_create_in": ([C.POINTER(Amr3DConfig), P, P, C.c_int64, C.POINTER(P)], I),
+        "lbm_server_submit_amr3d": ([P, C.c_int64, C.POINTER(Amr3DConfig), F, I], I),
         "lbm_amr3d_totals": ([P, D], I),
         "lbm_amr3d_read_coarse": ([P, F, F], I),
         "lbm_amr3d_read_pool": ([P, F, F], I),
@@ -876,6 +879,15 @@ def amr3d_config(q: int, dims, refine="body", rb: int = 4, margin: float = 2.0, 
     return c
 
 
+def amr3d_device_bytes(cfg: Amr3DConfig) -> int:
+    """Device bytes the hierarchy holds (no GPU needed)."""
+    out = C.c_int64()
+    rc = lib.lbm_amr3d_device_bytes(C.byref(cfg), None, C.byref(out))
+    if rc:
+        raise LbmError(rc, lib.lbm_amr3d_last_error(None).decode())
+    return int(out.value)
+
+
 def amr3d_refine_blocks(cfg: Amr3DConfig) -> np.ndarray:
     nb = (cfg.root.nx // cfg.rb) * (cfg.root.ny // cfg.rb) * (cfg.root.nz // cfg.rb)
     out = np.zeros(nb, np.uint8)
@@ -1045,6 +1057,14 @@ class Server:
             ptr = _ptr(mac, C.c_float)
         self._check(lib.lbm_server_submit(self._h, int(rid), C.byref(cfg), ptr, int(steps)))
 
+    def submit_amr3d(self, rid: int, cfg: Amr3DConfig, steps: int, mac=None):
+        """Queues a 3D two-level AMR solve of `steps` macro-steps."""
+        ptr = None
+        if mac is not None:
+            mac = np.ascontiguousarray(mac, np.float32)
+            ptr = _ptr(mac, C.c_float)
+        self._check(lib.lbm_server_submit_amr3d(self._h, int(rid), C.byref(cfg), ptr, int(steps)))
+
     def poll(self, max_steps: int = 64):
         n = C.c_int()
         self._check(lib.lbm_server_poll(self._h, int(max_steps), self._results, len(self._results), C.byref(n)))
@@ -1055,7 +1075,10 @@ class Server:
                         "admit_s": r.admit_s, "done_s": r.done_s})
         return out
 
-    def read(self, rid: int, cfg: Config, f: bool = True):
+    def read(self, rid: int, cfg, f: bool = True):
+        """Final f and mac of a finished solve (an AMR solve's L0 level)."""
+        if isinstance(cfg, Amr3DConfig):
+            cfg = cfg.root
         n = cfg.nx * cfg.ny * cfg.nz
         mac = np.empty((n, 4), np.float32)
         ff = np.empty((cfg.q, n), np.float32) if f else None

@@ -74,6 +74,61 @@ __device__ __forceinline__ bool tile_cell(const Amr3Params &p, TileCell &t) {
   return true;
 }
 
+// The D3Q27 directions (D3Q19 their first 19), as a table in constant
+// memory for loops over a runtime direction index.
+struct DirTable {
+  signed char ex[27], ey[27], ez[27];
+};
+constexpr DirTable make_dirs() {
+  DirTable t{};
+  for (int i = 0; i < 27; ++i) {
+    t.ex[i] = (signed char)detail::ex27(i);
+    t.ey[i] = (signed char)detail::ey27(i);
+    t.ez[i] = (signed char)detail::ez27(i);
+  }
+  return t;
+}
+__constant__ DirTable c_dirs = make_dirs();
+
+// Cell-list kernels: one CTA of kListThreads per (chunk, slot) walking a
+// per-session list of the tile's cells -- the interior first, then the
+// ring -- so that a warp holds interior cells or ring cells, not both, and
+// a ring-only pass launches no interior threads. Sets up the CTA's
+// neighbour table; false for a thread with no cell (after the barrier).
+constexpr int kListThreads = 128;
+
+__device__ __forceinline__ bool list_cell(const Amr3Params &p, const uint32_t *__restrict__ cells, int first,
+                                          int count, int *nb27, TileCell &t) {
+  t.slot = blockIdx.y;
+  const int id = p.slot_to_block[t.slot];
+  if (id < 0) return false;  // the whole CTA: a free slot
+  t.bx = id % p.nbx; t.by = (id / p.nbx) % p.nby; t.bz = id / (p.nbx * p.nby);
+  if (threadIdx.x < 27) {
+    const int k = threadIdx.x, dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+    nb27[k] = k == 13 ? t.slot
+                      : p.block_slot[(wrapi(t.bz + dz, p.nbz) * p.nby + wrapi(t.by + dy, p.nby)) * p.nbx +
+                                     wrapi(t.bx + dx, p.nbx)];
+  }
+  __syncthreads();
+  const int k = blockIdx.x * kListThreads + threadIdx.x;
+  if (k >= count) return false;
+  const uint32_t c = __ldg(cells + first + k);
+  t.fx = c & 0xff; t.fy = (c >> 8) & 0xff; t.fz = c >> 16;
+  t.cell = (int64_t)t.slot * p.T3 + (t.fz * p.FB + t.fy) * p.FB + t.fx;
+  return true;
+}
+
+// Is L0 cell (x, y, z) -- within one L0 cell of block b's 3 x 3 x 3
+// neighbourhood -- under a refined block? From the CTA's neighbour table.
+__device__ __forceinline__ bool covered_near(const Amr3Params &p, const int *nb27, const int b[3], int x, int y,
+                                             int z) {
+  const int r[3] = {x - b[0] * p.rb, y - b[1] * p.rb, z - b[2] * p.rb};
+  int k[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) k[a] = r[a] < 0 ? 0 : (r[a] >= p.rb ? 2 : 1);
+  return nb27[k[2] * 9 + k[1] * 3 + k[0]] >= 0;
+}
+
 template <int Q>
 __device__ __forceinline__ float feq3(int i, float rho, float ux, float uy, float uz) {
   using L = Lattice<Q>;
@@ -140,30 +195,36 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 
 // ---- explode ------------------------------------------------------------
 template <int Q>
-__global__ void __launch_bounds__(kTileMaxThreads)
-    amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p) {
+__global__ void __launch_bounds__(kListThreads)
+    amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p,
+                 const uint32_t *__restrict__ cells, int first, int count) {
   using L = Lattice<Q>;
   TileCell t;
-  if (!tile_cell(p, t)) return;
-  if (interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz)) return;
+  // the ring cells only; coverage of the L0 cells around the tile from the
+  // neighbour table
+  __shared__ int nb27[27];
+  if (!list_cell(p, cells, first, count, nb27, t)) return;
   const int b[3] = {t.bx, t.by, t.bz};
   const int fi[3] = {t.fx, t.fy, t.fz};
   const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
-  int g[3], v[3];
+  // g: the fine coordinate (wrapped), v: its L0 cell; vu the same unwrapped
+  int g[3], v[3], vu[3];
   for (int a = 0; a < 3; ++a) {
-    g[a] = wrapi(b[a] * p.RB2 + fi[a] - kAmrGhost, nf[a]);
+    const int gu = b[a] * p.RB2 + fi[a] - kAmrGhost;
+    g[a] = wrapi(gu, nf[a]);
     v[a] = g[a] / 2;
+    vu[a] = gu >= 0 ? gu / 2 : -((1 - gu) / 2);
   }
   // A ring cell inside a covered L0 cell is never read (DIRECT_GHOST).
-  if (covered(p, v[0], v[1], v[2])) return;
+  if (covered_near(p, nb27, b, vu[0], vu[1], vu[2])) return;
   const int64_t vc = ccell(p, v[0], v[1], v[2]);
   bool ok[3];
   int64_t vm[3], vp[3];
   for (int a = 0; a < 3; ++a) {
-    int m[3] = {v[0], v[1], v[2]}, q[3] = {v[0], v[1], v[2]};
+    int m[3] = {vu[0], vu[1], vu[2]}, q[3] = {vu[0], vu[1], vu[2]};
     m[a] -= 1;
     q[a] += 1;
-    ok[a] = !covered(p, m[0], m[1], m[2]) && !covered(p, q[0], q[1], q[2]);
+    ok[a] = !covered_near(p, nb27, b, m[0], m[1], m[2]) && !covered_near(p, nb27, b, q[0], q[1], q[2]);
     vm[a] = ccell(p, m[0], m[1], m[2]);
     vp[a] = ccell(p, q[0], q[1], q[2]);
   }
@@ -173,11 +234,15 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   for (int i = 0; i < Q; ++i) {
     const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
     float out;
-    if (!covered(p, v[0] + e[0], v[1] + e[1], v[2] + e[2])) {
+    if (!covered_near(p, nb27, b, vu[0] + e[0], vu[1] + e[1], vu[2] + e[2])) {
       // in-orphan: this child's own one-step destination is in this tile
-      int dg[3];
-      for (int a = 0; a < 3; ++a) dg[a] = wrapi(g[a] + e[a], nf[a]);
-      const bool into = covered(p, dg[0] / 2, dg[1] / 2, dg[2] / 2) && dg[0] / p.RB2 == b[0] &&
+      int dg[3], dv[3];
+      for (int a = 0; a < 3; ++a) {
+        dg[a] = wrapi(g[a] + e[a], nf[a]);
+        const int du = b[a] * p.RB2 + fi[a] - kAmrGhost + e[a];
+        dv[a] = du >= 0 ? du / 2 : -((1 - du) / 2);
+      }
+      const bool into = covered_near(p, nb27, b, dv[0], dv[1], dv[2]) && dg[0] / p.RB2 == b[0] &&
                         dg[1] / p.RB2 == b[1] && dg[2] / p.RB2 == b[2];
       out = into ? __ldg(fc + (int64_t)i * p.N + vc) : 0.f;
     } else {
@@ -201,31 +266,30 @@ __global__ void __launch_bounds__(kTileMaxThreads)
 
 // ---- one pool substep ----------------------------------------------------
 template <int Q>
-__global__ void __launch_bounds__(kTileMaxThreads)
+__global__ void __launch_bounds__(kListThreads)
     amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
-                 const __grid_constant__ Amr3Params p) {
+                 const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells, int count) {
   using L = Lattice<Q>;
   TileCell t;
-  if (!tile_cell(p, t)) return;
+  // the tile's 26 same-level neighbours, loaded once per CTA
+  __shared__ int nb27[27];
+  if (!list_cell(p, cells, 0, count, nb27, t)) return;
   const StepParams &c = p.c;
   const int G = kAmrGhost, RB2 = p.RB2, FB = p.FB;
   const int b[3] = {t.bx, t.by, t.bz};
   const int fi[3] = {t.fx, t.fy, t.fz};
-  const int nb[3] = {p.nbx, p.nby, p.nbz};
-  int off[3], bn[3];
-  for (int a = 0; a < 3; ++a) {
-    off[a] = fi[a] <= G ? -1 : (fi[a] + 1 >= G + RB2 ? 1 : 0);
-    bn[a] = wrapi(b[a] + off[a], nb[a]);
-  }
-  // Same-level neighbour tiles, indexed by which axes step off the tile.
-  int nbr[8];
-  nbr[0] = t.slot;
+  // Per axis and per e in {-1, 0, +1}: the neighbour step of the source --
+  // toward the tile edge this cell sits at, when the source leaves the
+  // interior (DIRECT_GHOST reads the neighbour's interior there).
+  int oa[3][3];
 #pragma unroll
-  for (int m = 1; m < 8; ++m) {
-    const bool sx = m & 1, sy = m & 2, sz = m & 4;
-    const bool need = (!sx || off[0]) && (!sy || off[1]) && (!sz || off[2]);
-    nbr[m] = need ? p.block_slot[((sz ? bn[2] : b[2]) * p.nby + (sy ? bn[1] : b[1])) * p.nbx + (sx ? bn[0] : b[0])]
-                  : -1;
+  for (int a = 0; a < 3; ++a) {
+    const int off = fi[a] <= G ? -1 : (fi[a] + 1 >= G + RB2 ? 1 : 0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int sa = fi[a] - (k - 1);
+      oa[a][k] = (sa < G || sa >= G + RB2) ? off : 0;
+    }
   }
   const V3 pos = {f2c(t.fx, b[0] * p.rb), f2c(t.fy, b[1] * p.rb), f2c(t.fz, b[2] * p.rb)};
   float phi = 1e30f;
@@ -235,6 +299,19 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     us = body_velocity3(pos, c.body, c.win);
   }
   const bool bb = c.has_body && c.bb;
+  const bool in_tile = interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz);
+  // A cell that collides inside the body (SOLID_EQ) is held at feq(1, u_body),
+  // whatever it pulls: write that and skip the pull.
+  if ((in_tile || p.collide_ring) && c.solid_eq && bb && phi < 0.f) {
+    const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
+      fout[(int64_t)i * p.P + t.cell] = L::w(i) * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq);
+    }
+    if (p.write_mac) macp[t.cell] = make_float4(1.f, us.x, us.y, us.z);
+    return;
+  }
   // a fine link is sqrt(3)/2 L0 units long and phi is 1-Lipschitz
   const bool near = bb && phi < 1.0f;
   float rhoW = 1.f;
@@ -244,34 +321,50 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     for (int i = 0; i < Q; ++i) s += __ldg(fin + (int64_t)i * p.P + t.cell);
     rhoW = s;
   }
+  // Which links bounce back: the source is inside the body. A rolled loop
+  // (one SDF instance), and none at all where every source must be solid
+  // (deeper than a link's length plus rounding). The rest direction's
+  // source is the cell itself (phi); for a ring cell its regular pull would
+  // read the neighbour tile, so it is decided like any other link.
+  uint32_t solid_links = 0;
+  if (near) {
+    if (phi < -0.87f) {
+      solid_links = (1u << Q) - 1u;
+    } else {
+      solid_links = phi < 0.f ? 1u : 0u;
+#pragma unroll 1
+      for (int i = 1; i < Q; ++i) {
+        const V3 sp = {f2c(t.fx - c_dirs.ex[i], b[0] * p.rb), f2c(t.fy - c_dirs.ey[i], b[1] * p.rb),
+                       f2c(t.fz - c_dirs.ez[i], b[2] * p.rb)};
+        if (phi3(sp, c.body, c.win) < 0.f) solid_links |= 1u << i;
+      }
+    }
+  }
   float f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    if (solid_links & (1u << i)) {
+      const float corr =
+          2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
+      f[i] = __ldg(fin + (int64_t)L::opp(i) * p.P + t.cell) + corr;
+      continue;
+    }
     int s[3] = {t.fx - e[0], t.fy - e[1], t.fz - e[2]};
-    if (near) {
-      const V3 sp = {f2c(s[0], b[0] * p.rb), f2c(s[1], b[1] * p.rb), f2c(s[2], b[2] * p.rb)};
-      if (phi3(sp, c.body, c.win) < 0.f) {
-        const float corr =
-            2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
-        f[i] = __ldg(fin + (int64_t)L::opp(i) * p.P + t.cell) + corr;
-        continue;
-      }
-    }
-    int m = 0, o[3];
-    for (int a = 0; a < 3; ++a) {
-      o[a] = (s[a] < G || s[a] >= G + RB2) ? off[a] : 0;
-      if (o[a]) m |= 1 << a;
-    }
+    const int o0 = oa[0][e[0] + 1], o1 = oa[1][e[1] + 1], o2 = oa[2][e[2] + 1];
     int src = t.slot;
-    if (m) {
-      const int ns = nbr[m];
+    if (o0 | o1 | o2) {
+      const int ns = nb27[(o2 + 1) * 9 + (o1 + 1) * 3 + (o0 + 1)];
       if (ns >= 0) {
         src = ns;
-        for (int a = 0; a < 3; ++a) s[a] -= o[a] * RB2;
+        s[0] -= o0 * RB2;
+        s[1] -= o1 * RB2;
+        s[2] -= o2 * RB2;
+      } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s[a] = min(max(s[a], 0), FB - 1);
       }
     }
-    for (int a = 0; a < 3; ++a) s[a] = min(max(s[a], 0), FB - 1);
     f[i] = __ldg(fin + (int64_t)i * p.P + (int64_t)src * p.T3 + (s[2] * FB + s[1]) * FB + s[0]);
   }
   float rho, mx, my, mz;
@@ -284,7 +377,6 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   const float Fx = rc * (us.x - uxs) + c.fx, Fy = rc * (us.y - uys) + c.fy, Fz = rc * (us.z - uzs) + c.fz;
   const float hinv = 0.5f * inv;
   const float ux = fmaf(Fx, hinv, uxs), uy = fmaf(Fy, hinv, uys), uz = fmaf(Fz, hinv, uzs);
-  const bool in_tile = interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz);
   MemSink<float> sink{fout, p.P, (int)t.cell, c.pk};
   if (!in_tile && !p.collide_ring) {
     // explode/coalesce: the ring advects and does not collide (COLLIDE_RING = 0)
@@ -307,19 +399,8 @@ __global__ void __launch_bounds__(kTileMaxThreads)
     const float dz = c.saz ? fminf(wp.z, (float)(p.nz - 1) - wp.z) : 1e30f;
     spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), c.sponge_inv);
   }
-  const bool solid = c.solid_eq && bb && phi < 0.f;
-  if (!solid) {
-    collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega_f, spw, c.ftarget, sink);
-    if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
-  } else {
-    const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
-      fout[(int64_t)i * p.P + t.cell] = L::w(i) * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq);
-    }
-    if (p.write_mac) macp[t.cell] = make_float4(1.f, us.x, us.y, us.z);
-  }
+  collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega_f, spw, c.ftarget, sink);
+  if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
 }
 
 // ---- coalesce -------------------------------------------------------------
@@ -949,6 +1030,8 @@ struct lbm_amr3d {
   unsigned char *d_want = nullptr, *d_slot_new = nullptr, *d_iface_flag = nullptr;
   int *d_free_list = nullptr, *d_counts = nullptr;
   cudaGraphExec_t manage_graph[2] = {nullptr, nullptr};
+  bool carved = false;          // device memory carved from a caller's block
+  uint32_t *d_cells = nullptr;  // tile cells: interior (RB2^3) then ring, packed x | y << 8 | z << 16
   float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
   float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
@@ -1040,6 +1123,7 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     sp.write_mac = write_mac ? 1 : 0;
     const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
     const dim3 g = tile_grid(a);
+    const dim3 gl((p.T3 + kListThreads - 1) / kListThreads, p.slots);
     const int rb3 = p.rb * p.rb * p.rb;
     const dim3 gd((rb3 + kTileThreads - 1) / kTileThreads, p.slots);
     const int r3 = p.RB2 * p.RB2 * p.RB2;
@@ -1055,9 +1139,9 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
       pa.write_mac = 0;
       const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->flux, p, 0);
-      amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
+      amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa, a->d_cells, p.T3);
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[1], a->flux, p, 1);
-      amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
+      amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p, a->d_cells, p.T3);
       amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
                                                  f2c_rescale);
       if (a->flux && gc)
@@ -1065,7 +1149,7 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     });
   }
   if (p.slots) {
-    const dim3 g = tile_grid(a);
+    const dim3 gl((p.T3 + kListThreads - 1) / kListThreads, p.slots);
     const int r3 = p.RB2 * p.RB2 * p.RB2;
     const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
     const int rb3 = p.rb * p.rb * p.rb;
@@ -1073,11 +1157,13 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     auto body = [&]() -> cudaError_t {
       AMR3_DISPATCH(q, {
         if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
-        amr3_explode<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p);
+        const int r3i = p.RB2 * p.RB2 * p.RB2, nring = p.T3 - r3i;
+        const dim3 gr((nring + kListThreads - 1) / kListThreads, p.slots);
+        amr3_explode<Q><<<gr, kListThreads, 0, st>>>(a->fc[cp], a->fp[0], p, a->d_cells, r3i, nring);
         Amr3Params pa = p;
         pa.write_mac = 0;
-        amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[0], a->fp[1], a->macp, pa);
-        amr3_substep<Q><<<g, tile_block(a), 0, st>>>(a->fp[1], a->fp[0], a->macp, p);
+        amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa, a->d_cells, p.T3);
+        amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p, a->d_cells, p.T3);
         if (gc) amr3_coalesce<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
       });
     };
@@ -1125,6 +1211,23 @@ int build_graphs(lbm_amr3d *a) {
   return LBM_OK;
 }
 
+// Device memory of a hierarchy: its own allocations, or carved in order
+// from a caller's block (256-byte granules); `measure` only adds up the bytes.
+struct DevCarve {
+  char *base = nullptr;
+  size_t cap = 0, used = 0;
+  bool measure = false;
+  template <class T> cudaError_t take(T **ptr, size_t bytes) {
+    const size_t b = (bytes + 255) & ~size_t(255);
+    if (measure) { *ptr = nullptr; used += b; return cudaSuccess; }
+    if (!base) return cudaMalloc(ptr, bytes);
+    if (used + b > cap) return cudaErrorMemoryAllocation;
+    *ptr = reinterpret_cast<T *>(base + used);
+    used += b;
+    return cudaSuccess;
+  }
+};
+
 void release(lbm_amr3d *a) {
   if (a->stream) cudaStreamSynchronize(a->stream);
   destroy_graphs(a);
@@ -1133,8 +1236,8 @@ void release(lbm_amr3d *a) {
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
                     (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux,
-                    (void *)a->d_block_q})
-    cudaFree(ptr);
+                    (void *)a->d_block_q, (void *)a->d_cells})
+    if (!a->carved) cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
 }
@@ -1161,7 +1264,14 @@ int lbm_amr3d_config_default(lbm_amr3d_config *c, int q, int nx, int ny, int nz)
 
 const char *lbm_amr3d_last_error(const lbm_amr3d *a) { return a ? a->err.c_str() : g_amr3_error.c_str(); }
 
-int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_amr3d **out) {
+}  // extern "C"
+
+namespace {
+
+// Builds the hierarchy with its device memory from `mem`; with mem.measure
+// nothing touches the GPU and *bytes receives the device bytes it needs.
+int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCarve &mem, lbm_amr3d **out,
+                     size_t *bytes) {
   if (!out) return afail(nullptr, LBM_EINVAL, "out is NULL");
   *out = nullptr;
   std::string why;
@@ -1244,45 +1354,78 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
     return afail(nullptr, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA, m);
   };
   cudaError_t e;
+  const bool live = !mem.measure;
+  a->carved = mem.base != nullptr;
+  const size_t fcb = (size_t)a->q * p.N * sizeof(float), fpb = (size_t)a->q * p.P * sizeof(float);
+  const int nfree = a->capacity - a->initial;
+  const size_t nfl = (size_t)std::max(1, a->capacity);
+  // every device allocation, in one order for measuring and for carving
+  {
+    for (int k = 0; k < 2; ++k) {
+      if ((e = mem.take(&a->fc[k], fcb))) return bail(e, "L0 f");
+      if ((e = mem.take(&a->fp[k], fpb))) return bail(e, "pool f");
+    }
+    if ((e = mem.take(&a->macc, (size_t)p.N * 16))) return bail(e, "L0 mac");
+    if (c->reflux && (e = mem.take(&a->flux, (size_t)p.N * 16))) return bail(e, "flux");
+    if ((e = mem.take(&a->macp, (size_t)p.P * 16))) return bail(e, "pool mac");
+    if ((e = mem.take(&a->d_block_slot, nb * sizeof(int)))) return bail(e, "block_slot");
+    if ((e = mem.take(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "slots");
+    if ((e = mem.take(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "iface");
+    if ((e = mem.take(&a->d_cells, (size_t)p.T3 * sizeof(uint32_t)))) return bail(e, "cell list");
+    if (a->dynamic) {
+      if ((e = mem.take(&a->d_want, nb))) return bail(e, "want");
+      if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
+      if ((e = mem.take(&a->d_slot_new, a->capacity))) return bail(e, "new");
+      if ((e = mem.take(&a->d_free_list, nfl * sizeof(int)))) return bail(e, "free list");
+      if ((e = mem.take(&a->d_counts, 4 * sizeof(int)))) return bail(e, "counts");
+      if (c->q_abs > 0 && (e = mem.take(&a->d_block_q, nb * sizeof(float)))) return bail(e, "block Q");
+    }
+    const int r3 = p.RB2 * p.RB2 * p.RB2;
+    a->force_parts = std::max(1, ((r3 + kTileThreads - 1) / kTileThreads) * p.slots);
+    if ((e = mem.take(&a->partials, (size_t)a->force_parts * kForceSlots * sizeof(double)))) return bail(e, "partials");
+    if ((e = mem.take(&a->force_out, kForceSlots * sizeof(double)))) return bail(e, "force");
+    if ((e = mem.take(&a->counter, sizeof(unsigned int)))) return bail(e, "counter");
+    if ((e = mem.take(&a->tot_partials, (size_t)kTotBlocks * 4 * sizeof(double)))) return bail(e, "totals");
+    if ((e = mem.take(&a->tot_out, 4 * sizeof(double)))) return bail(e, "totals");
+    if ((e = mem.take(&a->tot_counter, sizeof(unsigned int)))) return bail(e, "totals");
+  }
+  if (!live) {
+    *bytes = mem.used;
+    delete a;
+    return LBM_OK;
+  }
   if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
   a->stream = a->own;
-  const size_t fcb = (size_t)a->q * p.N * sizeof(float), fpb = (size_t)a->q * p.P * sizeof(float);
-  for (int k = 0; k < 2; ++k) {
-    if ((e = cudaMalloc(&a->fc[k], fcb))) return bail(e, "cudaMalloc L0 f");
-    if ((e = cudaMalloc(&a->fp[k], fpb))) return bail(e, "cudaMalloc pool f");
+  for (int k = 0; k < 2; ++k)
     if ((e = cudaMemset(a->fp[k], 0, fpb))) return bail(e, "memset pool f");
-  }
-  if ((e = cudaMalloc(&a->macc, (size_t)p.N * 16))) return bail(e, "cudaMalloc L0 mac");
-  if (c->reflux) {
-    if ((e = cudaMalloc(&a->flux, (size_t)p.N * 16))) return bail(e, "cudaMalloc flux");
-    if ((e = cudaMemset(a->flux, 0, (size_t)p.N * 16))) return bail(e, "memset flux");
-  }
-  if ((e = cudaMalloc(&a->macp, (size_t)p.P * 16))) return bail(e, "cudaMalloc pool mac");
+  if (a->flux && (e = cudaMemset(a->flux, 0, (size_t)p.N * 16))) return bail(e, "memset flux");
   if ((e = cudaMemset(a->macp, 0, (size_t)p.P * 16))) return bail(e, "memset pool mac");
-  if ((e = cudaMalloc(&a->d_block_slot, nb * sizeof(int)))) return bail(e, "cudaMalloc block_slot");
-  if ((e = cudaMalloc(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "cudaMalloc slots");
-  if ((e = cudaMalloc(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "cudaMalloc iface");
   cudaMemcpy(a->d_block_slot, a->block_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(a->d_slot_to_block, a->slot_to_block.data(), a->capacity * sizeof(int), cudaMemcpyHostToDevice);
+  {
+    std::vector<uint32_t> cl;
+    cl.reserve(p.T3);
+    for (int pass = 0; pass < 2; ++pass)
+      for (int z = 0; z < p.FB; ++z)
+        for (int y = 0; y < p.FB; ++y)
+          for (int x = 0; x < p.FB; ++x) {
+            auto in = [&](int j) { return j >= kAmrGhost && j < kAmrGhost + p.RB2; };
+            if ((in(x) && in(y) && in(z)) == (pass == 0)) cl.push_back(x | (y << 8) | (z << 16));
+          }
+    cudaMemcpy(a->d_cells, cl.data(), cl.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  }
   if (a->dynamic) {
     std::vector<unsigned char> flag(nb, 0);
     for (int id : a->iface) flag[id] = 1;
-    const int nfree = a->capacity - a->initial;
-    std::vector<int> fl(std::max(1, a->capacity), 0);
+    std::vector<int> fl(nfl, 0);
     for (int i = 0; i < nfree; ++i) fl[i] = a->initial + i;
     const int counts[4] = {nfree, 0, nfree, 0};
-    if ((e = cudaMalloc(&a->d_want, nb))) return bail(e, "cudaMalloc want");
-    if ((e = cudaMalloc(&a->d_iface_flag, nb))) return bail(e, "cudaMalloc flags");
-    if ((e = cudaMalloc(&a->d_slot_new, a->capacity))) return bail(e, "cudaMalloc new");
-    if ((e = cudaMalloc(&a->d_free_list, fl.size() * sizeof(int)))) return bail(e, "cudaMalloc free list");
-    if ((e = cudaMalloc(&a->d_counts, 4 * sizeof(int)))) return bail(e, "cudaMalloc counts");
     cudaMemset(a->d_want, 0, nb);
     cudaMemset(a->d_slot_new, 0, a->capacity);
     cudaMemcpy(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice);
     cudaMemcpy(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice);
     if (c->q_abs > 0) {
-      if ((e = cudaMalloc(&a->d_block_q, nb * sizeof(float)))) return bail(e, "cudaMalloc block Q");
       // main-3d.js: REFINE_THRESH = 1/2 log2 max(Q_ABS, 1e-30), COARSEN_THRESH
       // one hysteresis band lower, both as thresholds on Q itself
       const double qr = std::max((double)c->q_abs, 1e-30);
@@ -1291,16 +1434,8 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
     }
   }
   if (p.n_iface) cudaMemcpy(a->d_iface, a->iface.data(), p.n_iface * sizeof(int), cudaMemcpyHostToDevice);
-  const int r3 = p.RB2 * p.RB2 * p.RB2;
-  a->force_parts = std::max(1, ((r3 + kTileThreads - 1) / kTileThreads) * p.slots);
-  if ((e = cudaMalloc(&a->partials, (size_t)a->force_parts * kForceSlots * sizeof(double)))) return bail(e, "partials");
-  if ((e = cudaMalloc(&a->force_out, kForceSlots * sizeof(double)))) return bail(e, "force");
-  if ((e = cudaMalloc(&a->counter, sizeof(unsigned int)))) return bail(e, "counter");
   if ((e = cudaMemset(a->counter, 0, sizeof(unsigned int)))) return bail(e, "counter");
   if ((e = cudaMemset(a->force_out, 0, kForceSlots * sizeof(double)))) return bail(e, "force");
-  if ((e = cudaMalloc(&a->tot_partials, (size_t)kTotBlocks * 4 * sizeof(double)))) return bail(e, "totals");
-  if ((e = cudaMalloc(&a->tot_out, 4 * sizeof(double)))) return bail(e, "totals");
-  if ((e = cudaMalloc(&a->tot_counter, sizeof(unsigned int)))) return bail(e, "totals");
   if ((e = cudaMemset(a->tot_counter, 0, sizeof(unsigned int)))) return bail(e, "totals");
   if ((e = cudaMallocHost(&a->host_out, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
   if ((e = cudaDeviceSynchronize())) return bail(e, "set-up");
@@ -1313,6 +1448,37 @@ int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_a
   p.force_out = a->force_out;
   *out = a;
   return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_amr3d **out) {
+  DevCarve mem;
+  return amr3_create_impl(c, block_want, mem, out, nullptr);
+}
+
+int lbm_amr3d_device_bytes(const lbm_amr3d_config *c, const uint8_t *block_want, int64_t *bytes) {
+  if (!bytes) return LBM_EINVAL;
+  DevCarve mem;
+  mem.measure = true;
+  lbm_amr3d *a = nullptr;
+  size_t b = 0;
+  const int rc = amr3_create_impl(c, block_want, mem, &a, &b);
+  if (rc) return rc;
+  *bytes = (int64_t)b;
+  return LBM_OK;
+}
+
+int lbm_amr3d_create_in(const lbm_amr3d_config *c, const uint8_t *block_want, void *device_base, int64_t capacity,
+                        lbm_amr3d **out) {
+  if (!device_base || capacity <= 0) return afail(nullptr, LBM_EINVAL, "device block is NULL or empty");
+  if ((uintptr_t)device_base % 256) return afail(nullptr, LBM_EINVAL, "device block must be 256-byte aligned");
+  DevCarve mem;
+  mem.base = (char *)device_base;
+  mem.cap = (size_t)capacity;
+  return amr3_create_impl(c, block_want, mem, out, nullptr);
 }
 
 void lbm_amr3d_destroy(lbm_amr3d *a) {

@@ -121,7 +121,7 @@ static __device__ __noinline__ float phi3_call(float x, float y, float z, const 
 // evaluation skips the rotation (bit-identical to the rotated form for the
 // identity quaternion, the only orientation a pinned sphere has).
 __device__ __forceinline__ float phi3(V3 p, const lbm_body &b, const Win &w) {
-  if (b.shape == LBM_SHAPE_SPHERE) return len3(body_delta(p, b, w)) - b.a;
+  if (b.shape == LBM_SHAPE_SPHERE && !w.on) return len3({p.x - b.cx, p.y - b.cy, p.z - b.cz}) - b.a;
   return phi3_call(p.x, p.y, p.z, &b, &w);
 }
 

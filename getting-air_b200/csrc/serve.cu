@@ -13,6 +13,12 @@
 // requests are retired (force read back, memory returned to the arena) and
 // queued ones admitted into the freed space before the next tick.
 //
+// A request may also be a 3D two-level AMR solve (lbm_server_submit_amr3d):
+// its hierarchy is built inside its share of the arena
+// (lbm_amr3d_create_in), it advances on a stream of its own -- graph-launched
+// macro-steps that overlap the persistent dense launches -- and it is the
+// same solve, bit for bit, as an lbm_amr3d session of the same config.
+//
 // The reference has no serving form (one page steps one domain).
 
 #include <algorithm>
@@ -164,7 +170,15 @@ struct Request {
   int nparts = 0;
   int state = 0;  // 0 queued, 1 resident, 2 finished (resident until released)
   double force[8] = {};
+  // a 3D two-level AMR solve (kind 1): its hierarchy and stream
+  int kind = 0;
+  lbm_amr3d_config acfg{};
+  lbm_amr3d *amr = nullptr;
+  cudaStream_t amr_stream = nullptr;
 };
+
+// Lattice cells of a request's domain (L0 for an AMR solve).
+int64_t request_cells(const Request &r) { return (int64_t)r.cfg.nx * r.cfg.ny * r.cfg.nz; }
 
 int64_t request_bytes(const lbm_config &c, int nparts) {
   const int64_t n = (int64_t)c.nx * c.ny * c.nz;
@@ -258,7 +272,47 @@ int ensure_staging(lbm_server *s, int ndoms, int ntiles) {
 
 // Places a queued request into the arena and seeds it; false when it does
 // not fit right now.
+int admit_amr(lbm_server *s, Request &r, bool &ok) {
+  ok = false;
+  int64_t bytes = 0;
+  int rc = lbm_amr3d_device_bytes(&r.acfg, nullptr, &bytes);
+  if (rc) return sfail(s, rc, lbm_amr3d_last_error(nullptr));
+  const int64_t off = s->arena.alloc(bytes);
+  if (off < 0) return LBM_OK;
+  r.off = off;
+  r.bytes = bytes;
+  rc = lbm_amr3d_create_in(&r.acfg, nullptr, s->arena_ptr + off, bytes, &r.amr);
+  if (rc) {
+    s->arena.release(off, bytes);
+    return sfail(s, rc, lbm_amr3d_last_error(nullptr));
+  }
+  SCK(s, cudaStreamCreateWithFlags(&r.amr_stream, cudaStreamNonBlocking));
+  lbm_amr3d_set_stream(r.amr, r.amr_stream);
+  const int64_t n = request_cells(r);
+  std::vector<float> seed;
+  const float *src = r.mac_seed.empty() ? nullptr : r.mac_seed.data();
+  if (!src) {
+    const lbm_config &c = r.cfg;
+    const float ux = c.sponge_u[0], uy = c.sponge_u[1], uz = c.sponge_u[2];
+    const float rho = 1.0f - (ux * ux + uy * uy + uz * uz) * 1.5f;
+    seed.resize(4 * n);
+    for (int64_t k = 0; k < n; ++k) {
+      seed[4 * k] = rho; seed[4 * k + 1] = ux; seed[4 * k + 2] = uy; seed[4 * k + 3] = uz;
+    }
+    src = seed.data();
+  }
+  rc = lbm_amr3d_init_macro(r.amr, src);
+  if (rc) return sfail(s, rc, lbm_amr3d_last_error(r.amr));
+  r.mac_seed.clear();
+  r.mac_seed.shrink_to_fit();
+  r.state = 1;
+  r.t_admit = now_s(s);
+  ok = true;
+  return LBM_OK;
+}
+
 int admit(lbm_server *s, Request &r, bool &ok) {
+  if (r.kind == 1) return admit_amr(s, r, ok);
   ok = false;
   StepParams tmp{};
   fill_step_params(r.cfg, 1, 0, tmp);
@@ -310,11 +364,17 @@ int admit(lbm_server *s, Request &r, bool &ok) {
 
 // Runs `k` steps of every resident, unfinished request.
 int run_steps(lbm_server *s, const std::vector<Request *> &act, int k) {
+  // the AMR solves first: k macro-steps each, queued on their own streams
+  for (Request *r : act) {
+    if (r->kind != 1) continue;
+    const int rc = lbm_amr3d_step(r->amr, k);
+    if (rc) return sfail(s, rc, lbm_amr3d_last_error(r->amr));
+  }
   for (int q : {9, 19, 27})
     for (int st = 0; st <= 2; ++st) {
       std::vector<Request *> group;
       for (Request *r : act)
-        if (r->cfg.q == q && r->cfg.storage == st) group.push_back(r);
+        if (r->kind == 0 && r->cfg.q == q && r->cfg.storage == st) group.push_back(r);
       if (group.empty()) continue;
       int ntiles = 0;
       for (Request *r : group) {
@@ -354,7 +414,20 @@ int run_steps(lbm_server *s, const std::vector<Request *> &act, int k) {
       // The staging buffers are rewritten by the next group: wait for the copies.
       SCK(s, cudaStreamSynchronize(s->stream));
     }
+  for (Request *r : act) {
+    if (r->kind != 1) continue;
+    SCK(s, cudaStreamSynchronize(r->amr_stream));
+    r->done += k;
+    s->lattice_updates += (int64_t)k * lbm_amr3d_cell_updates(r->amr);
+  }
   return LBM_OK;
+}
+
+void drop_amr(Request &r) {
+  if (r.amr) lbm_amr3d_destroy(r.amr);
+  if (r.amr_stream) cudaStreamDestroy(r.amr_stream);
+  r.amr = nullptr;
+  r.amr_stream = nullptr;
 }
 
 }  // namespace
@@ -387,6 +460,7 @@ int lbm_server_create(int64_t budget_bytes, lbm_server **out) {
 void lbm_server_destroy(lbm_server *s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto &kv : s->reqs) drop_amr(kv.second);
   cudaFree(s->arena_ptr);
   cudaFree(s->d_doms);
   cudaFree(s->d_tiles);
@@ -422,6 +496,30 @@ int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const fl
   return LBM_OK;
 }
 
+int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *cfg, const float *mac, int steps) {
+  if (!s) return LBM_EINVAL;
+  if (!cfg) return sfail(s, LBM_EINVAL, "config is NULL");
+  if (cfg->refine == LBM_REFINE_LIST) return sfail(s, LBM_EINVAL, "a served hierarchy is refined by a rule, not a list");
+  int64_t bytes = 0;
+  const int rc = lbm_amr3d_device_bytes(cfg, nullptr, &bytes);
+  if (rc) return sfail(s, rc, lbm_amr3d_last_error(nullptr));
+  if (steps < 1) return sfail(s, LBM_EINVAL, "steps must be >= 1");
+  if (s->reqs.count(id)) return sfail(s, LBM_EINVAL, "request id already in use");
+  if (bytes > s->budget)
+    return sfail(s, LBM_ENOSPC, "request needs " + std::to_string(bytes) + " bytes, more than the whole budget");
+  Request r;
+  r.id = id;
+  r.kind = 1;
+  r.acfg = *cfg;
+  r.cfg = cfg->root;
+  r.steps = steps;
+  r.t_submit = now_s(s);
+  if (mac) r.mac_seed.assign(mac, mac + 4 * request_cells(r));
+  s->reqs.emplace(id, std::move(r));
+  s->queue.push_back(id);
+  return LBM_OK;
+}
+
 int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done, int *n_done) {
   if (!s || max_steps < 1) return s ? sfail(s, LBM_EINVAL, "max_steps must be >= 1") : LBM_EINVAL;
   if (n_done) *n_done = 0;
@@ -451,7 +549,12 @@ int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done
   for (Request *r : act) {
     if (r->done < r->steps) continue;
     if (done && nd >= max_done) break;  // the rest retire on the next poll
-    SCK(s, cudaMemcpy(r->force, r->force_out, kForceSlots * 8, cudaMemcpyDeviceToHost));
+    if (r->kind == 1) {
+      const int rc = lbm_amr3d_forces(r->amr, r->force);
+      if (rc) return sfail(s, rc, lbm_amr3d_last_error(r->amr));
+    } else {
+      SCK(s, cudaMemcpy(r->force, r->force_out, kForceSlots * 8, cudaMemcpyDeviceToHost));
+    }
     r->state = 2;
     r->t_done = now_s(s);
     if (done && nd < max_done) {
@@ -476,6 +579,14 @@ int lbm_server_read(lbm_server *s, int64_t id, float *f, float *mac) {
   if (it == s->reqs.end() || it->second.state != 2) return sfail(s, LBM_ESTATE, "request is not finished");
   Request &r = it->second;
   const int64_t n = (int64_t)r.cfg.nx * r.cfg.ny * r.cfg.nz;
+  if (r.kind == 1) {
+    // the L0 level: f of the current time level and the mac
+    const int64_t qn = (int64_t)r.cfg.q * n;
+    std::vector<float> fb(f ? 0 : qn), mb(mac ? 0 : 4 * n);
+    const int rc = lbm_amr3d_read_coarse(r.amr, f ? f : fb.data(), mac ? mac : mb.data());
+    if (rc) return sfail(s, rc, lbm_amr3d_last_error(r.amr));
+    return LBM_OK;
+  }
   if (f) {
     if (r.cfg.storage == LBM_STORE_FP32) {
       SCK(s, cudaMemcpyAsync(f, r.f[r.cur], (size_t)r.cfg.q * n * 4, cudaMemcpyDeviceToHost, s->stream));
@@ -498,6 +609,7 @@ int lbm_server_release(lbm_server *s, int64_t id) {
   if (it->second.state == 0) {
     s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), id), s->queue.end());
   } else {
+    drop_amr(it->second);
     s->arena.release(it->second.off, it->second.bytes);
   }
   s->reqs.erase(it);

@@ -174,19 +174,26 @@ def cylinder_amr(W: int = 1024, H: int = 256, r: float = 20.0, centre=(256.0, 12
 
 
 def serving_stream(count: int = 48, seed: int = 2024, rate: float = 200.0, nmin: int = 32, nmax: int = 192,
-                   steps=(500, 2000)):
+                   steps=(500, 2000), amr_frac: float = 0.0):
     """Seeded Poisson stream of 3D obstacle solves: arrival times with mean
     rate `rate`/s, cubic domains N^3 with N log-uniform in [nmin, nmax],
     D3Q19 or D3Q27, a pinned sphere (radius N/8) or rounded box (half-extent
     N/8), bounce-back, sponge (width max(6, N/16)) toward u0 = 0.05 along x,
-    tau uniform in [0.55, 0.7], steps uniform in the given range. Returns a
-    list of dicts: t (arrival, s), q, dims, kw (Solver keywords), steps."""
+    tau uniform in [0.55, 0.7], steps uniform in the given range. A fraction
+    `amr_frac` are two-level AMR solves (levels = 2, RB = 4, the blocks near
+    the body refined, N rounded to a multiple of 4; steps are macro-steps).
+    Returns a list of dicts: t (arrival, s), q, dims, kw (Solver keywords),
+    steps, levels."""
     rng = mulberry32(seed)
+    amr_rng = mulberry32(seed ^ 0x5EED)
     t = 0.0
     out = []
     for k in range(count):
         t += -math.log(1.0 - rng()) / rate
         n = int(round(nmin * (nmax / nmin) ** rng()))
+        levels = 2 if amr_rng() < amr_frac else 1
+        if levels == 2:
+            n = max(16, 4 * (n // 4))
         q = 19 if rng() < 0.5 else 27
         box = rng() < 0.5
         tau = float(np.float32(0.55 + 0.15 * rng()))
@@ -197,5 +204,13 @@ def serving_stream(count: int = 48, seed: int = 2024, rate: float = 200.0, nmin:
                 dict(shape="sphere", centre=centre, a=a))
         kw = dict(tau=tau, has_body=1, use_bounceback=1, body=body, sponge_w=float(max(6, n // 16)),
                   sponge_u=(0.05, 0.0, 0.0))
-        out.append({"t": t, "q": q, "dims": (n, n, n), "kw": kw, "steps": nsteps, "id": k})
+        out.append({"t": t, "q": q, "dims": (n, n, n), "kw": kw, "steps": nsteps, "id": k, "levels": levels})
     return out
+
+
+def serving_config(lbm, r):
+    """The request's config: an lbm_config, or for levels = 2 an
+    lbm_amr3d_config refining the blocks within 2 cells of the body."""
+    if r.get("levels", 1) == 2:
+        return lbm.amr3d_config(r["q"], r["dims"], refine="body", rb=4, margin=2.0, **r["kw"])
+    return lbm.config_from(r["q"], r["dims"], **r["kw"])

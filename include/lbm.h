@@ -468,6 +468,13 @@ int lbm_amr3d_config_default(lbm_amr3d_config *c, int q, int nx, int ny, int nz)
 /* `block_want` (one flag per block, id = (bz*NBY + by)*NBX + bx) is read for
  * LBM_REFINE_LIST only. Slots are handed out in ascending block id. */
 int lbm_amr3d_create(const lbm_amr3d_config *c, const uint8_t *block_want, lbm_amr3d **out);
+/* Device bytes the hierarchy of `c` holds (256-byte granules), computed
+ * without touching the GPU; and the same hierarchy built inside a caller's
+ * device block of at least that many bytes (256-byte aligned), which the
+ * caller keeps and frees after lbm_amr3d_destroy (the server's arena). */
+int lbm_amr3d_device_bytes(const lbm_amr3d_config *c, const uint8_t *block_want, int64_t *bytes);
+int lbm_amr3d_create_in(const lbm_amr3d_config *c, const uint8_t *block_want, void *device_base, int64_t capacity,
+                        lbm_amr3d **out);
 void lbm_amr3d_destroy(lbm_amr3d *a);
 const char *lbm_amr3d_last_error(const lbm_amr3d *a);
 int lbm_amr3d_set_stream(lbm_amr3d *a, void *cuda_stream);
@@ -549,6 +556,12 @@ const char *lbm_server_last_error(const lbm_server *s);
 /* Queues a solve; `mac` (host, 4 floats per cell) seeds it, or NULL for the
  * uniform freestream at cfg->sponge_u. LBM_ENOSPC when it can never fit. */
 int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const float *mac, int steps);
+/* Queues a 3D two-level AMR solve of `steps` macro-steps (refine = body,
+ * box, bar, slab or all; static or dynamic), seeded like lbm_server_submit
+ * on L0. Its hierarchy lives in the server's arena (lbm_amr3d_create_in) and
+ * advances on its own stream beside the dense launches; lbm_server_read
+ * returns its L0 f and mac, the result its pool force. */
+int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *cfg, const float *mac, int steps);
 /* Admits what fits, runs one tick of at most max_steps steps, and returns up
  * to max_done finished solves. Finished solves keep their device state until
  * lbm_server_release. */

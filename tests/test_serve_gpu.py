@@ -88,3 +88,71 @@ def test_oversized_request_is_refused(lbm):
     with pytest.raises(lbm.LbmError, match="budget"):
         srv.submit(1, cfg, 10)
     srv.close()
+
+
+def test_amr_solves_same_alone_and_in_mix(lbm):
+    """Two-level AMR requests beside dense ones: each AMR result equals an
+    lbm_amr3d session of the same config, bit for bit (L0 f and mac, force),
+    and its hierarchy lives inside the server's arena."""
+    from getting_air_b200 import scenarios as sc
+    reqs = sc.serving_stream(count=8, seed=11, nmin=16, nmax=40, steps=(10, 30), amr_frac=0.5)
+    assert {r["levels"] for r in reqs} == {1, 2}
+    cfgs = {r["id"]: sc.serving_config(lbm, r) for r in reqs}
+    srv = lbm.Server(2 << 30)
+    for r in reqs:
+        if r["levels"] == 2:
+            srv.submit_amr3d(r["id"], cfgs[r["id"]], r["steps"])
+        else:
+            srv.submit(r["id"], cfgs[r["id"]], r["steps"])
+    st = srv.stats()
+    got = drain(srv, [r["id"] for r in reqs])
+    used = srv.stats()["bytes_used"]
+    amr_bytes = sum(lbm.amr3d_device_bytes(cfgs[r["id"]]) for r in reqs if r["levels"] == 2)
+    assert used >= amr_bytes
+    for r in reqs:
+        rid, cfg, steps = r["id"], cfgs[r["id"]], r["steps"]
+        f, mac = srv.read(rid, cfg)
+        root = cfg.root if r["levels"] == 2 else cfg
+        ux, uy, uz = (np.float32(v) for v in root.sponge_u)
+        rho = np.float32(1) - (ux * ux + uy * uy + uz * uz) * np.float32(1.5)
+        seed = np.tile(np.array([rho, ux, uy, uz], np.float32), (root.nx * root.ny * root.nz, 1))
+        if r["levels"] == 2:
+            alone = lbm.Amr3D(cfg)
+            alone.init_macro(seed)
+            alone.step(steps)
+            af, amac = alone.read_coarse()
+        else:
+            alone = lbm.Solver(cfg)
+            alone.init_macro(seed)
+            alone.step(steps)
+            af, amac = alone.read_f(), alone.read_mac()
+        assert got[rid]["steps"] == steps
+        assert np.array_equal(f, af), rid
+        assert np.array_equal(mac, amac), rid
+        want = alone.forces()
+        assert np.array_equal(np.array(got[rid]["forces"]), np.array(want)), rid
+        alone.close()
+        srv.release(rid)
+    assert srv.stats()["bytes_used"] == 0
+    srv.close()
+
+
+def test_amr_budget_refusal_and_queueing(lbm):
+    from getting_air_b200 import scenarios as sc
+    r = sc.serving_stream(count=1, seed=3, nmin=32, nmax=32, amr_frac=1.0)[0]
+    cfg = sc.serving_config(lbm, r)
+    need = lbm.amr3d_device_bytes(cfg)
+    srv = lbm.Server(need // 2)
+    with pytest.raises(lbm.LbmError, match="budget"):
+        srv.submit_amr3d(1, cfg, 5)
+    srv.close()
+    # room for one at a time: the second queues until the first is released
+    srv = lbm.Server(need + (need // 2))
+    srv.submit_amr3d(1, cfg, 5)
+    srv.submit_amr3d(2, cfg, 5)
+    first = drain(srv, [1])
+    assert srv.stats()["queued"] == 1
+    srv.release(1)
+    drain(srv, [2])
+    srv.release(2)
+    srv.close()
