@@ -413,52 +413,75 @@ __device__ __forceinline__ int local_in_tile(const Amr3Params &p, int g, int b, 
   return d + kAmrGhost;
 }
 
+// One CTA per interface block, one thread per L0 cell of it (rb^3 threads);
+// the 3 x 3 x 3 neighbour blocks' slots come from a shared table, so no
+// coverage or slot lookup goes to global memory or divides.
+__device__ __forceinline__ int rel_block(int q, int b, int nb) {
+  int d = q - b;
+  if (d > 1) d -= nb;
+  if (d < -1) d += nb;
+  return d;
+}
+
 template <int Q>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
     amr3_coalesce(const float *__restrict__ fp, float *__restrict__ fc, float4 *__restrict__ macc,
                   const float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
   using L = Lattice<Q>;
-  const int rb3 = p.rb * p.rb * p.rb;
-  const int k = blockIdx.x * kTileThreads + threadIdx.x;
-  if (k >= p.n_iface * rb3) return;
-  const int id = p.iface ? p.iface[k / rb3] : k / rb3, l = k % rb3;
-  if (!p.iface && !p.iface_flag[id]) return;
+  const int id = p.iface ? p.iface[blockIdx.x] : (int)blockIdx.x;
+  if (!p.iface && !p.iface_flag[id]) return;  // the whole CTA
   const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
+  __shared__ int nb27[27];
+  for (int k = threadIdx.x; k < 27; k += blockDim.x) {
+    const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+    nb27[k] = p.block_slot[(wrapi(b[2] + dz, p.nbz) * p.nby + wrapi(b[1] + dy, p.nby)) * p.nbx +
+                           wrapi(b[0] + dx, p.nbx)];
+  }
+  __syncthreads();
+  const int l = threadIdx.x;
   const int x = b[0] * p.rb + l % p.rb, y = b[1] * p.rb + (l / p.rb) % p.rb, z = b[2] * p.rb + l / (p.rb * p.rb);
   const int cc[3] = {x, y, z};
   const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
+  const int nbk[3] = {p.nbx, p.nby, p.nbz};
   const int64_t cell = ccell(p, x, y, z);
-  const int slot = p.block_slot[id];
+  const int slot = nb27[13];
   if (slot < 0) {
     // out-orphans (half-step exits no coarse bucket absorbs) against
     // in-orphans (what explode injected into this cell's own children)
     bool nearc = false;
 #pragma unroll
-    for (int i = 1; i < Q; ++i) nearc = nearc || covered(p, x + L::ex(i), y + L::ey(i), z + L::ez(i));
+    for (int i = 1; i < Q; ++i) nearc = nearc || covered_near(p, nb27, b, x + L::ex(i), y + L::ey(i), z + L::ez(i));
     if (!nearc) return;
 #pragma unroll 1
     for (int i = 1; i < Q; ++i) {
-      const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+      const int e[3] = {c_dirs.ex[i], c_dirs.ey[i], c_dirs.ez[i]};
       const int tc[3] = {x + e[0], y + e[1], z + e[2]};
-      if (covered(p, tc[0], tc[1], tc[2])) continue;
+      if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
       float sacc = 0.f, nin = 0.f;
       for (int q = 0; q < 8; ++q) {
         const int o[3] = {q & 1, (q >> 1) & 1, (q >> 2) & 1};
-        int pp[3], qq[3], qb[3];
+        int pp[3], qb[3], rel[3];
         for (int a = 0; a < 3; ++a) {
-          pp[a] = wrapi(wrapi(tc[a], a == 0 ? p.nx : (a == 1 ? p.ny : p.nz)) * 2 + o[a], nf[a]);
-          qq[a] = wrapi(pp[a] - e[a], nf[a]);
-          qb[a] = qq[a] / p.RB2;
+          // the child of the target and its fine source, one step upstream;
+          // the source's block relative to b from the unwrapped coordinate
+          const int ppu = 2 * tc[a] + o[a], qqu = ppu - e[a];
+          const int d = qqu - b[a] * p.RB2;
+          rel[a] = d < 0 ? -1 : (d >= p.RB2 ? 1 : 0);
+          pp[a] = wrapi(ppu, nf[a]);
+          qb[a] = wrapi(b[a] + rel[a], nbk[a]);
         }
-        const int qs = p.block_slot[(qb[2] * p.nby + qb[1]) * p.nbx + qb[0]];
+        const int qs = nb27[(rel[2] + 1) * 9 + (rel[1] + 1) * 3 + (rel[0] + 1)];
         if (qs >= 0) {
           const int lx = local_in_tile(p, pp[0], qb[0], nf[0]), ly = local_in_tile(p, pp[1], qb[1], nf[1]),
                     lz = local_in_tile(p, pp[2], qb[2], nf[2]);
           sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)qs * p.T3 + (lz * p.FB + ly) * p.FB + lx);
         }
         int ch[3];
-        for (int a = 0; a < 3; ++a) ch[a] = wrapi(cc[a] * 2 + o[a] + e[a], nf[a]);
-        if (covered(p, ch[0] / 2, ch[1] / 2, ch[2] / 2)) nin += 1.f;
+        for (int a = 0; a < 3; ++a) {
+          const int chu = cc[a] * 2 + o[a] + e[a];
+          ch[a] = chu >= 0 ? chu / 2 : -((1 - chu) / 2);
+        }
+        if (covered_near(p, nb27, b, ch[0], ch[1], ch[2])) nin += 1.f;
       }
       const float own = fc[(int64_t)i * p.N + cell];
       const float net = sacc - nin * own;
@@ -483,7 +506,7 @@ __global__ void __launch_bounds__(kTileThreads)
   for (int i = 0; i < Q; ++i) {
     const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
     const int tc[3] = {x + e[0], y + e[1], z + e[2]};
-    if (covered(p, tc[0], tc[1], tc[2])) continue;
+    if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
     float sacc = 0.f;
     for (int q = 0; q < 8; ++q) {
       const int lx = local_in_tile(p, tc[0] * 2 + (q & 1), b[0], nf[0]);
@@ -1164,7 +1187,8 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
         pa.write_mac = 0;
         amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa, a->d_cells, p.T3);
         amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p, a->d_cells, p.T3);
-        if (gc) amr3_coalesce<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
+        if (p.n_iface)
+          amr3_coalesce<Q><<<p.n_iface, rb3, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
       });
     };
     e = body();
