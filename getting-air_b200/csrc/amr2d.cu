@@ -33,6 +33,7 @@
 
 #include "../../include/lbm.h"
 #include "cell_update.cuh"
+#include "scan.cuh"
 #include "dense.cuh"
 #include "host_params.cuh"
 
@@ -40,6 +41,10 @@ namespace lbm {
 namespace {
 
 constexpr int kPoolThreads = 256;
+// Cell-parallel tile kernels (substep, fill, explode): one CTA per
+// (active tile, chunk of kChunk cells), so that a few tiles still spread
+// over every SM.
+constexpr int kChunk = 128;
 
 struct AmrParams {
   int W, H, RB, G, FB, RB2, NBX, NBY, PNX, PNY, S;
@@ -158,41 +163,78 @@ __global__ void amr_decide(const __grid_constant__ AmrParams p) {
 // (amr_manage_pool.wgsl coarsen/refine), then compact the active list
 // (amr_active_list.wgsl). One thread: a few thousand integer steps once per
 // refine round.
-__global__ void amr_coarsen_refine(const __grid_constant__ AmrParams p) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One CTA of kManageThreads, the serial order kept exactly: dying quads
+// pushed on the free stack in ascending slot order, parents wanting
+// refinement served in ascending parent id from the top of the stack (the
+// rest refused), then the active list compacted in ascending slot order --
+// each a block-wide prefix sum over the candidates.
+constexpr int kManageThreads = 1024;
+
+__global__ void __launch_bounds__(kManageThreads) amr_coarsen_refine(const __grid_constant__ AmrParams p) {
+  __shared__ int sm[64];
   int count = p.counts[0];
-  for (int s = 0; s < p.S; s += 4) {
-    const int b = p.slotToBlock[s];
-    if (b < 0 || p.want[b]) continue;
-    p.freeList[count++] = s / 4;
-    for (int q = 0; q < 4; ++q) {
-      const int bb = p.slotToBlock[s + q];
-      if (bb >= 0) p.blockSlot[bb] = -1;
-      p.slotToBlock[s + q] = -1;
+  // coarsen: quads whose first block is no longer wanted
+  const int nquads = p.S / 4;
+  for (int base = 0; base < nquads; base += kManageThreads) {
+    const int q = base + threadIdx.x;
+    int dying = 0;
+    if (q < nquads) {
+      const int b = p.slotToBlock[4 * q];
+      dying = (b >= 0 && !p.want[b]) ? 1 : 0;
     }
-  }
-  for (int ps = 0; ps < p.PNX * p.PNY; ++ps) {
-    const int bxP = ps % p.PNX, byP = ps / p.PNX;
-    const int b0 = (byP * 2) * p.NBX + bxP * 2;
-    if (p.blockSlot[b0] >= 0 || !p.want[b0]) continue;
-    if (count <= 0) continue;
-    count -= 1;
-    const int quad = p.freeList[count];
-    for (int qy = 0; qy < 2; ++qy)
-      for (int qx = 0; qx < 2; ++qx) {
-        const int slot = quad * 4 + qx + 2 * qy;
-        const int bid = (byP * 2 + qy) * p.NBX + bxP * 2 + qx;
-        p.blockSlot[bid] = slot;
-        p.slotToBlock[slot] = bid;
-        p.parentSlot[slot] = ps;
-        p.newly[slot] = 1u;
+    int total;
+    const int r = block_scan(dying, sm, total);
+    if (dying) {
+      p.freeList[count + r] = q;
+      for (int k = 0; k < 4; ++k) {
+        const int bb = p.slotToBlock[4 * q + k];
+        if (bb >= 0) p.blockSlot[bb] = -1;
+        p.slotToBlock[4 * q + k] = -1;
       }
+    }
+    count += total;
   }
-  p.counts[0] = count;
+  __syncthreads();
+  // refine: parents whose first child is unrefined and wanted
+  const int np = p.PNX * p.PNY;
+  for (int base = 0; base < np; base += kManageThreads) {
+    const int ps = base + threadIdx.x;
+    int need = 0, bxP = 0, byP = 0;
+    if (ps < np) {
+      bxP = ps % p.PNX;
+      byP = ps / p.PNX;
+      const int b0 = (byP * 2) * p.NBX + bxP * 2;
+      need = (p.blockSlot[b0] < 0 && p.want[b0]) ? 1 : 0;
+    }
+    int total;
+    const int r = block_scan(need, sm, total);
+    if (need && r < count) {
+      const int quad = p.freeList[count - 1 - r];
+      for (int qy = 0; qy < 2; ++qy)
+        for (int qx = 0; qx < 2; ++qx) {
+          const int slot = quad * 4 + qx + 2 * qy;
+          const int bid = (byP * 2 + qy) * p.NBX + bxP * 2 + qx;
+          p.blockSlot[bid] = slot;
+          p.slotToBlock[slot] = bid;
+          p.parentSlot[slot] = ps;
+          p.newly[slot] = 1u;
+        }
+    }
+    count -= min(total, count);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) p.counts[0] = count;
+  // the active list
   int n = 0;
-  for (int s = 0; s < p.S; ++s)
-    if (p.slotToBlock[s] >= 0) p.activeList[n++] = s;
-  p.counts[1] = n;
+  for (int base = 0; base < p.S; base += kManageThreads) {
+    const int s = base + threadIdx.x;
+    const int act = (s < p.S && p.slotToBlock[s] >= 0) ? 1 : 0;
+    int total;
+    const int r = block_scan(act, sm, total);
+    if (act) p.activeList[n + r] = s;
+    n += total;
+  }
+  if (threadIdx.x == 0) p.counts[1] = n;
 }
 
 // ---- transfers ------------------------------------------------------------------
@@ -247,17 +289,19 @@ __device__ void interp_cell(const AmrParams &p, const float *__restrict__ f0, fl
 
 // mode 0: ring of every active tile (same-level neighbour copy, else root
 // interpolation); mode 1: every cell of the tiles activated this round.
-__global__ void __launch_bounds__(kPoolThreads)
+__global__ void __launch_bounds__(kChunk)
     amr_fill(const float *__restrict__ f0, float *__restrict__ f1, int mode, const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
-  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+  const int FB2 = p.FB * p.FB, nch = (FB2 + kChunk - 1) / kChunk;
+  for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
+    const int k = w / nch, c0 = (w % nch) * kChunk, c1 = min(c0 + kChunk, FB2);
     const int s = p.activeList[k];
     if (mode == 1 && !p.newly[s]) continue;
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
     const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
     const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
     const int G = p.G, RB2 = p.RB2, FB = p.FB;
-    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+    for (int c = c0 + threadIdx.x; c < c1; c += kChunk) {
       const int fx = c % FB, fy = c / FB;
       const bool inX = fx >= G && fx < G + RB2, inY = fy >= G && fy < G + RB2;
       if (mode == 1) {
@@ -290,18 +334,20 @@ __global__ void __launch_bounds__(kPoolThreads)
 // that neighbour is refined, else from this tile's ring), BGK + Guo at
 // tau_f with the chi penalty on this level's band, sponge, SOLID_EQ. Every
 // cell of the tile, ring included, collides (COLLIDE_RING = 1).
-__global__ void __launch_bounds__(kPoolThreads)
+__global__ void __launch_bounds__(kChunk)
     amr_substep(const float *__restrict__ fin, float *__restrict__ fout, float2 *__restrict__ vel1,
                 const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
   const float Wf = (float)p.W, Hf = (float)p.H;
-  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+  const int FB2 = p.FB * p.FB, nch = (FB2 + kChunk - 1) / kChunk;
+  for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
+    const int k = w / nch, c0 = (w % nch) * kChunk, c1 = min(c0 + kChunk, FB2);
     const int s = p.activeList[k];
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
     const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
     const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
     const int G = p.G, RB2 = p.RB2, FB = p.FB;
-    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+    for (int c = c0 + threadIdx.x; c < c1; c += kChunk) {
       const int fx = c % FB, fy = c / FB;
       const int offX = fx <= G ? -1 : (fx + 1 >= G + RB2 ? 1 : 0);
       const int offY = fy <= G ? -1 : (fy + 1 >= G + RB2 ? 1 : 0);
@@ -520,15 +566,17 @@ __device__ __forceinline__ int64_t rcell(const AmrParams &p, int x, int y) {
 // time-t populations for the directions whose L0 target is covered (plus
 // the linear term orthogonal to e_i), V's population where this child's own
 // one-step destination lies in the tile (in-orphan), else 0.
-__global__ void __launch_bounds__(kPoolThreads)
+__global__ void __launch_bounds__(kChunk)
     amr_explode(const float *__restrict__ f0, float *__restrict__ f1, const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
   const int NFX = 2 * p.W, NFY = 2 * p.H;
-  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+  const int FB2 = p.FB * p.FB, nch = (FB2 + kChunk - 1) / kChunk;
+  for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
+    const int k = w / nch, c0 = (w % nch) * kChunk, c1 = min(c0 + kChunk, FB2);
     const int s = p.activeList[k];
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
     const int G = p.G, RB2 = p.RB2, FB = p.FB;
-    for (int c = threadIdx.x; c < FB * FB; c += kPoolThreads) {
+    for (int c = c0 + threadIdx.x; c < c1; c += kChunk) {
       const int fx = c % FB, fy = c / FB;
       if (fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2) continue;
       const int gx = wrap2(bx * RB2 + fx - G, NFX), gy = wrap2(by * RB2 + fy - G, NFY);
@@ -712,9 +760,9 @@ int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
   amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
   if (p.explode) {
     // amr2d-gpu.mjs:1096-1124 S_AdvanceExplode: the L0 step runs LAST
-    amr_explode<<<g, kPoolThreads, 0, st>>>(a->f0[from], a->f1[0], p);
-    amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
-    amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
+    amr_explode<<<g, kChunk, 0, st>>>(a->f0[from], a->f1[0], p);
+    amr_substep<<<g, kChunk, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
+    amr_substep<<<g, kChunk, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
     amr_coalesce<<<(int)((p.N0 + 255) / 256), 256, 0, st>>>(a->f1[0], a->f0[from], p);
     StepParams rp = a->root;
     rp.write_mac = 1;
@@ -724,13 +772,13 @@ int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
     ACK(a, cudaGetLastError());
     return LBM_OK;
   }
-  amr_fill<<<g, kPoolThreads, 0, st>>>(a->f0[from], a->f1[0], 0, p);
+  amr_fill<<<g, kChunk, 0, st>>>(a->f0[from], a->f1[0], 0, p);
   StepParams rp = a->root;
   rp.write_mac = 1;
   cudaError_t e = launch_step(9, 0, a->f0[from], a->f0[1 - from], (float *)a->mac, rp, st);
   if (e) return afail(a, LBM_ECUDA, std::string("root step: ") + cudaGetErrorString(e));
-  amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
-  amr_substep<<<g, kPoolThreads, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
+  amr_substep<<<g, kChunk, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
+  amr_substep<<<g, kChunk, 0, st>>>(a->f1[1], a->f1[0], a->vel1, p);
   amr_average<<<g, 64, 0, st>>>(a->f1[0], a->f0[1 - from], p);
   ACK(a, cudaGetLastError());
   return LBM_OK;
@@ -743,8 +791,8 @@ int refine_round(lbm_amr2d *a) {
   amr_criterion<<<p.NBX * p.NBY, 64, 0, st>>>(a->mac, p);
   ACK(a, cudaMemsetAsync(p.want, 0, (size_t)p.NBX * p.NBY * sizeof(unsigned), st));
   amr_decide<<<(p.PNX * p.PNY + 127) / 128, 128, 0, st>>>(p);
-  amr_coarsen_refine<<<1, 1, 0, st>>>(p);
-  amr_fill<<<a->grid_slots, kPoolThreads, 0, st>>>(a->f0[a->cur], a->f1[0], 1, p);
+  amr_coarsen_refine<<<1, kManageThreads, 0, st>>>(p);
+  amr_fill<<<a->grid_slots, kChunk, 0, st>>>(a->f0[a->cur], a->f1[0], 1, p);
   ACK(a, cudaGetLastError());
   return LBM_OK;
 }

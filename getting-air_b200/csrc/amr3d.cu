@@ -33,6 +33,7 @@
 #include "amr3d.cuh"
 #include "cell_update.cuh"
 #include "host_params.cuh"
+#include "scan.cuh"
 #include "sample.cuh"
 
 namespace lbm {
@@ -904,33 +905,6 @@ __global__ void __launch_bounds__(kTileThreads)
 #pragma unroll
   for (int i = 0; i < Q; ++i) fc[(int64_t)i * p.N + dst] = feq3<Q>(i, ra, ua, va, wa) + rescale_f2c * (fneq[i] * 0.125f);
   macc[dst] = make_float4(ra, ua, va, wa);
-}
-
-// Exclusive prefix sum of one flag per thread over a 1024-thread CTA.
-__device__ __forceinline__ int block_scan(int v, int *sm, int &total) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) sm[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int w = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    sm[32 + lane] = w;
-  }
-  __syncthreads();
-  total = sm[32 + (blockDim.x >> 5) - 1];
-  const int before = (warp ? sm[32 + warp - 1] : 0) + x - v;
-  __syncthreads();
-  return before;
 }
 
 constexpr int kManageThreads = 1024;
