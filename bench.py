@@ -605,6 +605,26 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_form(args):
+    """One side form alone, one GPU: the same timing as inside the full run."""
+    lbm = load_package()
+    world, rank, local = dist_setup(1)
+    if args.form in ("fp16", "bf16"):
+        wl = workload(args.form)
+        cells = int(np.prod(wl["dims"]))
+        tm, lm, _, fo, _ = time_device(lbm, wl, args.steps, args.warmup, world)
+        out = {"mlups": cells * args.steps / (tm * 1e-3) / 1e6, "ms_per_step": tm / args.steps}
+    elif args.form == "batched":
+        out = dict(zip(("batched", "batched_plain"), time_batched(lbm, args.steps, args.warmup, world)))
+    elif args.form == "amr2d_cylinder":
+        out = time_amr(lbm, args.steps, args.warmup, world)
+    elif args.form == "amr3d_sphere":
+        out = time_amr3d(lbm, args.steps, args.warmup, world)
+    else:
+        out = dict(zip(("served", "served_plain"), time_served(lbm, world)))
+    print(json.dumps({"form": args.form, "steps": args.steps, "warmup": args.warmup, **out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,9 +634,14 @@ def main():
     ap.add_argument("--skip-forms", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--form", choices=("fp16", "bf16", "batched", "amr2d_cylinder", "amr3d_sphere", "served"),
+                    help="run one of the side forms alone (for profiling) and print its JSON line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.form:
+        run_form(args)
+        return
     if args.impl == "reference":
         # The CPU arm is bounded to a few minutes: its steps are capped.
         args.steps = min(args.steps, 20)
