@@ -609,8 +609,12 @@ def run_form(args):
     """One side form alone, one GPU: the same timing as inside the full run."""
     lbm = load_package()
     world, rank, local = dist_setup(1)
-    if args.form in ("fp16", "bf16"):
-        wl = workload(args.form)
+    if args.form in ("fp32", "fp16", "bf16"):
+        if args.dims:
+            dims = tuple(int(v) for v in args.dims.split(","))
+            wl = workload(args.form, dims=dims, n=max(4, round(32 * dims[0] / DIMS[0])))
+        else:
+            wl = workload(args.form)
         cells = int(np.prod(wl["dims"]))
         tm, lm, _, fo, _ = time_device(lbm, wl, args.steps, args.warmup, world)
         out = {"mlups": cells * args.steps / (tm * 1e-3) / 1e6, "ms_per_step": tm / args.steps}
@@ -634,8 +638,10 @@ def main():
     ap.add_argument("--skip-forms", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--form", choices=("fp16", "bf16", "batched", "amr2d_cylinder", "amr3d_sphere", "served"),
+    ap.add_argument("--form", choices=("fp32", "fp16", "bf16", "batched", "amr2d_cylinder", "amr3d_sphere", "served"),
                     help="run one of the side forms alone (for profiling) and print its JSON line")
+    ap.add_argument("--dims", type=str, default=None,
+                    help="with --form fp32/fp16/bf16: a smaller sphere domain NX,NY,NZ (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
