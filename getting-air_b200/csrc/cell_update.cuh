@@ -256,7 +256,15 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
   const V3 pos = {(float)x, (float)y, (float)z};
   float phi = 1e30f;
   V3 us = {0.f, 0.f, 0.f};
-  if (p.has_body) {
+  bool see = p.has_body;
+  if (see && p.nbox_on) {
+    int dx = x - p.nbox[0], dy = y - p.nbox[2], dz = z - p.nbox[4];
+    dx += dx < 0 ? nx : 0;
+    dy += dy < 0 ? ny : 0;
+    dz += dz < 0 ? nz : 0;
+    see = dx <= p.nbox[1] - p.nbox[0] && dy <= p.nbox[3] - p.nbox[2] && dz <= p.nbox[5] - p.nbox[4];
+  }
+  if (see) {
     phi = phi3(pos, p.body, p.win);
     us = body_velocity3(pos, p.body, p.win);
   }

@@ -41,6 +41,11 @@ struct StepParams {
   float ftarget[27];    // sponge far-field equilibrium per direction (rho = 1)
   lbm_body body;
   Win win;              // moving window (3D); win.on = 0 without one
+  // Bounce-back body only: the cell box (read modulo the grid) outside which
+  // no cell is within a link of the body, so the SDF and the body velocity
+  // need not be evaluated there (nbox_on = 0: evaluate everywhere).
+  int nbox_on;
+  int nbox[6];
   int write_mac;
   // Force reduction: the blocks of the launch grid that can see the body.
   int force_on;

@@ -70,6 +70,7 @@ __device__ __forceinline__ void stage_pose(const StepParams &p, StepParams &sp) 
   if (threadIdx.x == 0) {
     const BodyPose &bp = *p.pose_in;
     sp.body = bp.body;
+    sp.nbox_on = 0;  // the pose moves on the device: evaluate the SDF everywhere
     sp.swept = bp.swept;
     sp.swept_band = bp.swept_band;
     sp.rbx0 = bp.region[0];

@@ -107,6 +107,7 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
         p.win.on = 1;
       }
   }
+  p.nbox_on = 0;
   p.write_mac = 0;
   p.force_on = 0;
   p.swept = 0;
