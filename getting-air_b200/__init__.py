@@ -234,6 +234,7 @@ def _load() -> C.CDLL:
         "lbm_amr3d_device_bytes": ([C.POINTER(Amr3DConfig), P, C.POINTER(C.c_int64)], I),
         "lbm_amr3d_create_in": ([C.POINTER(Amr3DConfig), P, P, C.c_int64, C.POINTER(P)], I),
         "lbm_server_submit_amr3d": ([P, C.c_int64, C.POINTER(Amr3DConfig), F, I], I),
+        "lbm_server_set_policy": ([P, I, C.c_int64], I),
         "lbm_amr3d_totals": ([P, D], I),
         "lbm_amr3d_read_coarse": ([P, F, F], I),
         "lbm_amr3d_read_pool": ([P, F, F], I),
@@ -1056,6 +1057,12 @@ class Server:
             mac = np.ascontiguousarray(mac, np.float32)
             ptr = _ptr(mac, C.c_float)
         self._check(lib.lbm_server_submit(self._h, int(rid), C.byref(cfg), ptr, int(steps)))
+
+    def set_policy(self, policy: str = "fifo", max_resident_cells: int = 0):
+        """Admission order ("fifo" or "sjf": least cells x steps first) and a
+        cap on the resident requests' cells (0: the budget alone)."""
+        p = {"fifo": 0, "sjf": 1}[policy]
+        self._check(lib.lbm_server_set_policy(self._h, p, int(max_resident_cells)))
 
     def submit_amr3d(self, rid: int, cfg: Amr3DConfig, steps: int, mac=None):
         """Queues a 3D two-level AMR solve of `steps` macro-steps."""

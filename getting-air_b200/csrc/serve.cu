@@ -220,6 +220,8 @@ struct lbm_server {
   ServeDom *h_doms = nullptr;        // pinned staging
   int2 *h_tiles = nullptr;
   int sms = 148;
+  int policy = 0;                    // 0 FIFO, 1 shortest work first
+  int64_t max_resident_cells = 0;    // 0: no cap besides the budget
   std::chrono::steady_clock::time_point t0;
   int64_t lattice_updates = 0;
   std::string err;
@@ -496,6 +498,15 @@ int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const fl
   return LBM_OK;
 }
 
+int lbm_server_set_policy(lbm_server *s, int policy, int64_t max_resident_cells) {
+  if (!s) return LBM_EINVAL;
+  if (policy != 0 && policy != 1) return sfail(s, LBM_EINVAL, "policy must be 0 (FIFO) or 1 (shortest work first)");
+  if (max_resident_cells < 0) return sfail(s, LBM_EINVAL, "max_resident_cells must be >= 0");
+  s->policy = policy;
+  s->max_resident_cells = max_resident_cells;
+  return LBM_OK;
+}
+
 int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *cfg, const float *mac, int steps) {
   if (!s) return LBM_EINVAL;
   if (!cfg) return sfail(s, LBM_EINVAL, "config is NULL");
@@ -523,13 +534,29 @@ int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *c
 int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done, int *n_done) {
   if (!s || max_steps < 1) return s ? sfail(s, LBM_EINVAL, "max_steps must be >= 1") : LBM_EINVAL;
   if (n_done) *n_done = 0;
-  // 1. admit in FIFO order while the head fits
+  // 1. admit: FIFO while the head fits, or the least total work first;
+  // the resident-cell cap keeps the GPU busy without making every request
+  // share it (continuous batching's latency cost)
+  int64_t resident = 0;
+  for (auto &kv : s->reqs)
+    if (kv.second.state == 1) resident += request_cells(kv.second);
+  auto capped = [&](const Request &r) {
+    return s->max_resident_cells > 0 && resident > 0 && resident + request_cells(r) > s->max_resident_cells;
+  };
+  if (s->policy == 1) {
+    std::stable_sort(s->queue.begin(), s->queue.end(), [&](int64_t x, int64_t y) {
+      const Request &a = s->reqs[x], &b = s->reqs[y];
+      return request_cells(a) * a.steps < request_cells(b) * b.steps;
+    });
+  }
   while (!s->queue.empty()) {
     Request &r = s->reqs[s->queue.front()];
+    if (capped(r)) break;
     bool ok = false;
     int rc = admit(s, r, ok);
     if (rc) return rc;
     if (!ok) break;
+    resident += request_cells(r);
     s->queue.pop_front();
   }
   // 2. one tick: every resident unfinished request, up to the soonest finish

@@ -562,6 +562,13 @@ int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const fl
  * advances on its own stream beside the dense launches; lbm_server_read
  * returns its L0 f and mac, the result its pool force. */
 int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *cfg, const float *mac, int steps);
+/* Admission policy: 0 = FIFO (the default; a request waits while the one
+ * ahead of it does not fit), 1 = the queued request with the least total
+ * work (cells x steps) first. max_resident_cells > 0 caps the resident
+ * requests' cells (a single request is always admitted when the device is
+ * idle): enough to fill the GPU, so that short requests do not share it with
+ * every long one. */
+int lbm_server_set_policy(lbm_server *s, int policy, int64_t max_resident_cells);
 /* Admits what fits, runs one tick of at most max_steps steps, and returns up
  * to max_done finished solves. Finished solves keep their device state until
  * lbm_server_release. */

@@ -156,3 +156,43 @@ def test_amr_budget_refusal_and_queueing(lbm):
     drain(srv, [2])
     srv.release(2)
     srv.close()
+
+
+def test_shortest_work_first_with_a_resident_cap(lbm):
+    """Policy 1 admits the least cells x steps first; the resident-cell cap
+    holds the rest back while the device is busy; results are unchanged."""
+    from getting_air_b200 import scenarios as sc
+    reqs = sc.serving_stream(count=6, seed=9, nmin=16, nmax=40, steps=(10, 40))
+    cfgs = {r["id"]: lbm.config_from(r["q"], r["dims"], **r["kw"]) for r in reqs}
+    work = {r["id"]: int(np.prod(r["dims"])) * r["steps"] for r in reqs}
+    biggest = max(int(np.prod(r["dims"])) for r in reqs)
+    srv = lbm.Server(2 << 30)
+    srv.set_policy("sjf", biggest)
+    for r in reqs:
+        srv.submit(r["id"], cfgs[r["id"]], r["steps"])
+    held_back = False
+    done = {}
+    for _ in range(10000):
+        for d in srv.poll(8):
+            done[d["id"]] = d
+        st = srv.stats()
+        held_back |= st["resident"] > 0 and st["queued"] > 0
+        if len(done) == len(reqs):
+            break
+    assert len(done) == len(reqs)
+    # admitted in ascending total work (ties keep submission order)
+    order = sorted(done, key=lambda i: done[i]["admit_s"])
+    assert [work[i] for i in order] == sorted(work.values())
+    # 2 GiB would hold all six at once: the cap is what queued some
+    assert held_back
+    for r in reqs:
+        f, mac = srv.read(r["id"], cfgs[r["id"]])
+        alone = lbm.Solver(cfgs[r["id"]])
+        ux, uy, uz = (np.float32(v) for v in cfgs[r["id"]].sponge_u)
+        rho = np.float32(1) - (ux * ux + uy * uy + uz * uz) * np.float32(1.5)
+        alone.init_macro(np.tile(np.array([rho, ux, uy, uz], np.float32), (int(np.prod(r["dims"])), 1)))
+        alone.step(r["steps"])
+        assert np.array_equal(f, alone.read_f())
+        alone.close()
+        srv.release(r["id"])
+    srv.close()
