@@ -34,8 +34,10 @@ namespace lbm {
 
 namespace {
 
+// Register budget for 768 resident threads per SM (85 per thread): the
+// loop over a tile's cells is latency-bound, and occupancy is what hides it.
 template <int Q, typename S, int THREADS>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 768 / THREADS)
     batch_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
                const StepParams *__restrict__ doms, const int2 *__restrict__ tiles, int ntiles,
                int cells_per_tile, int write_mac) {
@@ -55,15 +57,33 @@ __global__ void __launch_bounds__(THREADS)
     const int lt = t - sp.tile0;
     const bool region = sp.force_on && lt >= sp.ft0 && lt < sp.ft1;
     ForceAcc acc;
-    for (int c = td.y + threadIdx.x; c < end; c += THREADS) {
-      const int x = c % nx, r = c / nx;
-      CellForce cf;
-      if constexpr (Q == 9) {
-        cell2<S>(fin, fout, mac, sp, x, r, region, cf);
-      } else {
-        cell3<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, region, cf);
+    if constexpr (Q == 9) {
+      // two cells per pass, both gathers issued before either update, so a
+      // thread keeps 18 loads in flight
+      for (int c = td.y + threadIdx.x; c < end; c += 2 * THREADS) {
+        const int c2 = c + THREADS;
+        const bool two = c2 < end;
+        const int x = c % nx, r = c / nx;
+        const int x2 = two ? c2 % nx : 0, r2 = two ? c2 / nx : 0;
+        float f[9], g[9];
+        gather2<S>(fin + sp.base, sp, x, r, f);
+        if (two) gather2<S>(fin + sp.base, sp, x2, r2, g);
+        CellForce cf;
+        cell2_core<S>(fin, f, fout, mac, sp, x, r, region, cf);
+        if (region) acc.add(cf);
+        if (two) {
+          CellForce cf2;
+          cell2_core<S>(fin, g, fout, mac, sp, x2, r2, region, cf2);
+          if (region) acc.add(cf2);
+        }
       }
-      if (region) acc.add(cf);
+    } else {
+      for (int c = td.y + threadIdx.x; c < end; c += THREADS) {
+        const int x = c % nx, r = c / nx;
+        CellForce cf;
+        cell3<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, region, cf);
+        if (region) acc.add(cf);
+      }
     }
     if (region)
       reduce_force<THREADS>(acc, sp.partials, sp.counter, sp.ft1 - sp.ft0, lt - sp.ft0, sp.force_out);

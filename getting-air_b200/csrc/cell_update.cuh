@@ -448,25 +448,49 @@ __device__ __forceinline__ void cell3_force(const S *__restrict__ fin, const Ste
 
 // ---- 2D cell update (D2Q9) ---------------------------------------------------
 
+// Pull gather of one D2Q9 cell from its periodic sources.
 template <typename S>
-__device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__ fout,
-                                      float *__restrict__ mac, const StepParams &p, int x, int y,
-                                      bool force, CellForce &cf) {
+__device__ __forceinline__ void gather2(const S *__restrict__ fi, const StepParams &p, int x, int y, float (&f)[9]) {
   using L = Lattice<9>;
   const int W = p.nx, H = p.ny;
   const int64_t n = p.n;
-  const S *fi = fin + p.base;
-  S *fo_ = fout + p.base;
   const int cell = y * W + x;
   const int xo_p = x == 0 ? W - 1 : -1, xo_m = x == W - 1 ? 1 - W : 1;
   const int yo_p = y == 0 ? (H - 1) * W : -W, yo_m = y == H - 1 ? (1 - H) * W : W;
-  float f[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const int ex = L::ex(i), ey = L::ey(i);
     const int off = (ex == 1 ? xo_p : (ex == -1 ? xo_m : 0)) + (ey == 1 ? yo_p : (ey == -1 ? yo_m : 0));
     f[i] = Codec<S>::ld(fi + (int64_t)i * n + (cell + off), i, p.pk);
   }
+}
+
+template <typename S>
+__device__ __forceinline__ void cell2_core(const S *__restrict__ fin, float (&f)[9], S *__restrict__ fout,
+                                           float *__restrict__ mac, const StepParams &p, int x, int y, bool force,
+                                           CellForce &cf);
+
+template <typename S>
+__device__ __forceinline__ void cell2(const S *__restrict__ fin, S *__restrict__ fout,
+                                      float *__restrict__ mac, const StepParams &p, int x, int y,
+                                      bool force, CellForce &cf) {
+  float f[9];
+  gather2<S>(fin + p.base, p, x, y, f);
+  cell2_core<S>(fin, f, fout, mac, p, x, y, force, cf);
+}
+
+// Everything after the gather for one D2Q9 cell: bounce-back and wall
+// patches, moments, forcing, collision, mac, force.
+template <typename S>
+__device__ __forceinline__ void cell2_core(const S *__restrict__ fin, float (&f)[9], S *__restrict__ fout,
+                                           float *__restrict__ mac, const StepParams &p, int x, int y, bool force,
+                                           CellForce &cf) {
+  using L = Lattice<9>;
+  const int W = p.nx, H = p.ny;
+  const int64_t n = p.n;
+  const S *fi = fin + p.base;
+  S *fo_ = fout + p.base;
+  const int cell = y * W + x;
   const float fW = (float)W, fH = (float)H;
   const float px = (float)x, py = (float)y;
   float rx = 0.f, ry = 0.f, usx = 0.f, usy = 0.f, phi = 1e30f;
