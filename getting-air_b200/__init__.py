@@ -231,6 +231,9 @@ def _load() -> C.CDLL:
         "lbm_amr3d_set_body": ([P, C.POINTER(Body)], I),
         "lbm_amr3d_pool_stats": ([P, C.POINTER(C.c_int32)], I),
         "lbm_amr3d_block_q": ([P, C.c_float, C.POINTER(C.c_float)], I),
+        "lbm_amr3d_manage_now": ([P], I),
+        "lbm_amr2d_refine_round": ([P], I),
+        "lbm_amr2d_set_auto_refine": ([P, I], I),
         "lbm_amr3d_device_bytes": ([C.POINTER(Amr3DConfig), P, C.POINTER(C.c_int64)], I),
         "lbm_amr3d_create_in": ([C.POINTER(Amr3DConfig), P, P, C.c_int64, C.POINTER(P)], I),
         "lbm_server_submit_amr3d": ([P, C.c_int64, C.POINTER(Amr3DConfig), F, I], I),
@@ -802,6 +805,13 @@ class Amr2D:
     def step(self, n: int = 1):
         self._check(lib.lbm_amr2d_step(self._h, int(n)))
 
+    def refine_round(self):
+        """One refine round now (criterion, decide, coarsen, refine, fill)."""
+        self._check(lib.lbm_amr2d_refine_round(self._h))
+
+    def set_auto_refine(self, on: bool):
+        self._check(lib.lbm_amr2d_set_auto_refine(self._h, int(bool(on))))
+
     def forces(self):
         out = np.zeros(4, np.float64)
         self._check(lib.lbm_amr2d_forces(self._h, _ptr(out, C.c_double)))
@@ -1001,6 +1011,10 @@ class Amr3D:
     def render_slice(self, **kw) -> np.ndarray:
         """An axis-aligned slice picture of the hierarchy, (height, width, 4)."""
         return _render(lib.lbm_amr3d_render_slice, self._h, self._check, self.dims, **kw)
+
+    def manage_now(self):
+        """One decision of the dynamic manager before the next macro-step."""
+        self._check(lib.lbm_amr3d_manage_now(self._h))
 
     def block_q(self, lead: float = 0.0) -> np.ndarray:
         """Per-block max Q-criterion of the L0 velocity, box dilated by `lead`."""

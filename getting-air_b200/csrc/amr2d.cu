@@ -996,6 +996,17 @@ int lbm_amr2d_step(lbm_amr2d *a, int n) {
   return LBM_OK;
 }
 
+int lbm_amr2d_refine_round(lbm_amr2d *a) {
+  if (!a) return LBM_EINVAL;
+  return refine_round(a);
+}
+
+int lbm_amr2d_set_auto_refine(lbm_amr2d *a, int on) {
+  if (!a) return LBM_EINVAL;
+  a->cfg.auto_refine = on ? 1 : 0;
+  return LBM_OK;
+}
+
 int lbm_amr2d_forces(lbm_amr2d *a, double out[4]) {
   if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
   ACK(a, cudaMemcpyAsync(a->host, a->p.force_out, kForceSlots * 8, cudaMemcpyDeviceToHost, a->stream));

@@ -1532,6 +1532,18 @@ int lbm_amr3d_step(lbm_amr3d *a, int n) {
   return LBM_OK;
 }
 
+int lbm_amr3d_manage_now(lbm_amr3d *a) {
+  if (!a) return LBM_EINVAL;
+  if (!a->dynamic) return afail(a, LBM_EINVAL, "the hierarchy is static (dynamic = 0)");
+  if (!a->seeded) return afail(a, LBM_EINVAL, "call lbm_amr3d_init_macro first");
+  if (!a->graph[0]) {
+    int rc = build_graphs(a);
+    if (rc) return rc;
+  }
+  ACK(a, cudaGraphLaunch(a->manage_graph[a->cp], a->stream));
+  return LBM_OK;
+}
+
 int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body) {
   if (!a || !body) return a ? afail(a, LBM_EINVAL, "body is NULL") : LBM_EINVAL;
   if (!a->cfg.root.has_body) return afail(a, LBM_EINVAL, "the hierarchy has no body");

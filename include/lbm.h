@@ -385,6 +385,12 @@ int lbm_amr2d_read_root(lbm_amr2d *a, float *f, float *vel);
 int lbm_amr2d_read_pool(lbm_amr2d *a, float *f, float *vel);
 /* n macro-steps. */
 int lbm_amr2d_step(lbm_amr2d *a, int n);
+/* One refine round now -- criterion over the root velocity of the last
+ * macro-step, decide, coarsen, refine, fill the new tiles (amr2d-gpu.mjs
+ * refineRound, the page's debug refine) -- and the switch of the rounds the
+ * step runs every refine_every macro-steps (setAutoRefine). */
+int lbm_amr2d_refine_round(lbm_amr2d *a);
+int lbm_amr2d_set_auto_refine(lbm_amr2d *a, int on);
 /* Drag/lift/torque of the last macro-step, FP64: {fx, fy, tz, nonfinite}. */
 int lbm_amr2d_forces(lbm_amr2d *a, double out[4]);
 /* Level-1 topology: block_slot[nbx*nby], slot_to_block[max_slots],
@@ -490,6 +496,9 @@ int lbm_amr3d_init_macro(lbm_amr3d *a, const float *mac);
 int lbm_amr3d_step(lbm_amr3d *a, int n);
 /* Replaces the body pose (a prescribed motion); the next decision follows it. */
 int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body);
+/* One decision of the dynamic manager now, before the next macro-step
+ * (the step runs them every manage_every macro-steps from manage_start). */
+int lbm_amr3d_manage_now(lbm_amr3d *a);
 /* {slots in use, refusals (pool exhausted), lowest free count seen, decisions}. */
 int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]);
 /* Per-block max Q-criterion of the L0 velocity of the last macro-step, over

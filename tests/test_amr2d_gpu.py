@@ -146,3 +146,27 @@ def test_explode_and_interp_interfaces_agree_on_drag(lbm):
         a.close()
     print("drag interp %.5f explode %.5f" % tuple(drags))
     assert abs(drags[1] - drags[0]) <= 0.05 * abs(drags[0])
+
+
+def test_manual_refine_rounds_equal_automatic_ones(lbm):
+    """refineRound called by hand at the same macro-steps as the automatic
+    schedule (every 16, from step 0) gives the same run, bit for bit."""
+    s, cfg = make(lbm)
+    runs = []
+    for manual in (False, True):
+        a = lbm.Amr2D(cfg)
+        a.write_root(s["f"], s["vel"])
+        if manual:
+            a.set_auto_refine(False)
+            for _ in range(3):
+                a.refine_round()
+                a.step(16)
+        else:
+            a.step(48)
+        f, vel = a.read_root()
+        runs.append((f, a.topology(), a.forces()))
+        a.close()
+    (f0, t0, F0), (f1, t1, F1) = runs
+    assert np.array_equal(f0, f1)
+    assert np.array_equal(t0["block_slot"], t1["block_slot"]) and np.array_equal(t0["active"], t1["active"])
+    assert np.array_equal(F0, F1)

@@ -411,3 +411,37 @@ def test_q_criterion_refines_detached_vortices_like_the_oracle(lbm, oracle):
     used = np.repeat(to[1] >= 0, a.fb ** 3)
     assert rel_l2(gfp[:, used].astype(np.float64), ofp[:, used]) <= 5e-6
     a.close()
+
+
+def test_manual_manager_decisions_equal_scheduled_ones(lbm):
+    """lbm_amr3d_manage_now before every fourth macro-step equals the
+    manager the step schedules with manage_every = 4, bit for bit."""
+    dims = (40, 24, 24)
+    body = dict(shape="sphere", centre=(10.3, 11.8, 12.1), a=3.0, v=(0.25, 0.0, 0.0))
+    n = int(np.prod(dims))
+    mac = np.zeros((n, 4), np.float32)
+    mac[:, 0] = 1.0
+    mac[:, 1] = 0.03
+    runs = []
+    for manual in (False, True):
+        # the lead of the decision is manage_every x speed in both runs; the
+        # manual run only moves the schedule out of reach
+        c = lbm.amr3d_config(19, dims, refine="body", margin=2.0, dynamic=1, manage_every=4,
+                             manage_start=10 ** 6 if manual else 0, slot_headroom=2.0,
+                             tau=0.62, has_body=1, use_bounceback=1, body=body)
+        a = lbm.Amr3D(c)
+        a.init_macro(mac)
+        cx = body["centre"][0]
+        for k in range(5):
+            if manual:
+                a.manage_now()
+            a.step(4)
+            cx += 1.0
+            a.set_body(lbm.make_body("sphere", (cx, 11.8, 12.1), a=3.0, v=(0.25, 0.0, 0.0)))
+        fc, mc = a.read_coarse()
+        runs.append((fc, a.topology()["block_slot"], a.forces()))
+        a.close()
+    (f0, b0, F0), (f1, b1, F1) = runs
+    assert np.array_equal(b0, b1)
+    assert np.array_equal(f0, f1)
+    assert np.array_equal(F0, F1)
