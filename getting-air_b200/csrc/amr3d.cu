@@ -681,11 +681,18 @@ __global__ void __launch_bounds__(kTileThreads)
           for (int i = 0; i < Q; ++i) s += __ldg(fp + (int64_t)i * p.P + cell);
           rhoW = s;
         }
+        // solid sources from one rolled SDF loop (the cell itself, phi >= 0
+        // here, is not one)
+        uint32_t solid = 0;
+#pragma unroll 1
+        for (int i = 1; i < Q; ++i) {
+          const V3 sp = {f2c(fx - c_dirs.ex[i], b[0] * p.rb), f2c(fy - c_dirs.ey[i], b[1] * p.rb),
+                         f2c(fz - c_dirs.ez[i], b[2] * p.rb)};
+          if (phi3(sp, c.body, c.win) < 0.f) solid |= 1u << i;
+        }
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
-          const V3 sp = {f2c(fx - L::ex(i), b[0] * p.rb), f2c(fy - L::ey(i), b[1] * p.rb),
-                         f2c(fz - L::ez(i), b[2] * p.rb)};
-          if (phi3(sp, c.body, c.win) < 0.f) {
+          if (solid & (1u << i)) {
             const float fo = __ldg(fp + (int64_t)L::opp(i) * p.P + cell);
             const float corr =
                 2.f * L::w(i) * rhoW * ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
