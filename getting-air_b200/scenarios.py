@@ -107,6 +107,56 @@ def cylinder2d(W: int = 256, H: int = 128, r: float = 10.0, u0: float = 0.05, ta
     return {"q": 9, "dims": (W, H, 1), "kw": kw, "mac": uniform_macro(W * H, (u0, 0, 0))}
 
 
+def cylinder_page(res: int = 9, re: float = 100.0, u0: float = 0.04, blockage: float = 24.0, upstream: float = 12.0,
+                  bounceback: bool = True, perturb: float = 0.02, seed: int = 12345, k_eps: float = 1.5) -> dict:
+    """The dense 2D cylinder page's configuration (main-cylinder.js): a square
+    W = H = 2^res domain, R = W / (2 blockage) at (upstream * 2R, H/2), tau from
+    Re on the diameter (tau = 0.5 + 3 nu, nu = u0 D / Re), sponge width 4
+    toward (u0, 0), SOLID_EQ, bounce-back or the chi penalty with K_EPS, and
+    the seed of initF: every cell at feq(1, u0, uy) with a per-cell
+    transverse uy = (rng * 2 - 1) * perturb * u0 from mulberry32(seed)."""
+    W = H = 1 << res
+    R = W / (2.0 * blockage)
+    D = 2.0 * R
+    nu = u0 * D / re
+    tau = float(np.float32(0.5 + 3.0 * nu))
+    rng = mulberry32(seed)
+    n = W * H
+    uy = np.array([(rng() * 2 - 1) * perturb * u0 for _ in range(n)], np.float64)
+    ex = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1], np.float64)
+    ey = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1], np.float64)
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    f = np.empty((9, n), np.float32)
+    usq = u0 * u0 + uy * uy
+    for i in range(9):
+        eu = ex[i] * u0 + ey[i] * uy
+        f[i] = (w[i] * (1 + 3 * eu + 4.5 * eu * eu - 1.5 * usq)).astype(np.float32)
+    body = dict(shape="ellipse", centre=(upstream * D, H / 2.0, 0.0), a=R, b=R)
+    kw = dict(tau=tau, has_body=1, use_bounceback=int(bounceback), chi_eps=k_eps, solid_eq=1, body=body,
+              sponge_w=4.0, sponge_u=(u0, 0.0, 0.0))
+    return {"q": 9, "dims": (W, H, 1), "kw": kw, "f": f, "u0": u0, "D": D, "re": re}
+
+
+def cylinder_analyze(history, transient: int, D: float, u0: float) -> dict:
+    """Cd mean over the post-transient samples and St from the zero crossings
+    of the mean-removed Cl (linear interpolation), as tools/lib/cylinder-
+    metrics.js analyze(); history rows are (step, Cd, Cl)."""
+    win = [r for r in history if r[0] > transient]
+    cd = float(np.mean([r[1] for r in win]))
+    cl = np.array([r[2] for r in win])
+    c = cl - cl.mean()
+    cross = []
+    for i in range(1, len(c)):
+        if c[i - 1] < 0 <= c[i]:
+            a, b = win[i - 1][0], win[i][0]
+            cross.append(a + (-c[i - 1] / (c[i] - c[i - 1])) * (b - a))
+    st = None
+    if len(cross) >= 3:
+        period = float(np.mean(np.diff(cross)))
+        st = D / period / u0
+    return {"cd": cd, "st": st, "samples": len(win), "crossings": len(cross)}
+
+
 def batched_domains(count: int = 512, seed: int = 12345, nmin: int = 64, nmax: int = 512,
                     tau_range=(0.55, 0.9), u0: float = 0.04):
     """The batched D2Q9 workload: `count` square domains with N = round(nmin *
