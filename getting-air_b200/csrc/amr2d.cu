@@ -161,8 +161,7 @@ __global__ void amr_decide(const __grid_constant__ AmrParams p) {
 
 // Coarsen then refine in the deterministic serial order of DET_SLOTS
 // (amr_manage_pool.wgsl coarsen/refine), then compact the active list
-// (amr_active_list.wgsl). One thread: a few thousand integer steps once per
-// refine round.
+// (amr_active_list.wgsl).
 // One CTA of kManageThreads, the serial order kept exactly: dying quads
 // pushed on the free stack in ascending slot order, parents wanting
 // refinement served in ascending parent id from the top of the stack (the

@@ -90,3 +90,48 @@ def test_cylinder_gates(lbm, re, cd, cd_tol, st, st_tol, ref_cd, ref_st):
     if st is not None:
         assert abs(r["st"] - st) <= st_tol
         assert abs(r["st"] - ref_st) <= 0.02 * ref_st
+
+
+# The reference's recorded two-level AMR bounce-back run of the same page
+# (main-cylinder-amr.js at res 9, levels 2): (Re, Cd, St), and its recorded
+# dense Cd for the same Re.
+AMR_RECORDED = [(20.0, 2.003906120080501, None, 2.179687508032657),
+                (100.0, 1.285, 0.16394208475416622, 1.326993803887924)]
+
+
+@pytest.mark.parametrize("re,ref_cd,ref_st,dense_cd", AMR_RECORDED, ids=lambda v: str(v))
+def test_amr2d_cylinder_gates(lbm, re, ref_cd, ref_st, dense_cd):
+    """The 2D AMR cylinder page (root 512^2 in 16^2 root tiles, RB 8, one 2:1
+    level by vorticity and geometry, bounce-back): Cd / St inside the
+    literature bands, St close to the reference's recorded AMR run, and Cd
+    within 3 % of the dense result (the recorded AMR Cd sits 3-8 % below the
+    recorded dense one; this build's fine level reproduces the dense drag,
+    which a 1024^2 dense run confirms is resolution-converged: Cd 2.1779 at
+    Re 20)."""
+    from getting_air_b200 import scenarios as sc
+    W = 512
+    r = W / 48.0
+    s = sc.cylinder_amr(W=W, H=W, r=r, centre=(W / 2.0, W / 2.0), u0=0.04, re=re, bounceback=True)
+    cfg = lbm.amr2d_config(W, W, **s["kw"])
+    a = lbm.Amr2D(cfg)
+    a.write_root(s["f"], s["vel"])
+    D, u0 = 2 * r, 0.04
+    rnd = lambda n: int(np.ceil(n / 64) * 64)
+    st_lit = {20.0: None, 100.0: 0.165}[re]
+    transient = rnd(40 * D / u0)
+    measure = rnd(15 * D / (st_lit * u0)) if st_lit else rnd(5 * D / u0)
+    rows = []
+    scale = 2.0 / (u0 * u0 * D)
+    for k in range((transient + measure) // 64):
+        a.step(64)
+        f = a.forces()
+        rows.append(((k + 1) * 64, f[0] * scale, f[1] * scale))
+    a.close()
+    res = sc.cylinder_analyze(rows, transient, D, u0)
+    print(f"AMR Re {re:g}: {res}")
+    cd_lit, cd_tol = {20.0: (2.05, 0.15), 100.0: (1.35, 0.15)}[re]
+    assert abs(res["cd"] - cd_lit) <= cd_tol
+    assert abs(res["cd"] - dense_cd) <= 0.03 * dense_cd
+    if st_lit:
+        assert abs(res["st"] - st_lit) <= 0.015
+        assert abs(res["st"] - ref_st) <= 0.02 * ref_st
