@@ -81,30 +81,37 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm) {
 }
 
 // Writes this block's partial (thread 0 holds it), and if this block is the
-// last of `nparts` to do so, sums all partials in index order into `out` and
-// re-arms the ticket counter for the next step.
+// last of `nparts` to do so, sums all partials in a fixed order into `out`
+// and re-arms the ticket counter for the next step. Only warp 0 takes part:
+// the other warps leave as soon as their share is in `sm`, so they do not
+// hold the SM while thread 0 waits on its fence and ticket. Returns true in
+// warp 0 of the last block.
 template <int NV, int THREADS>
 __device__ bool finish_sum(const double (&v)[NV], double *partials, unsigned int *counter,
-                           int nparts, int part, double *out, double *sm) {
-  __shared__ bool s_last;
-  if (threadIdx.x == 0) {
+                           int nparts, int part, double *out, double *) {
+  if (threadIdx.x >= 32) return false;
+  const int lane = threadIdx.x;
+  unsigned int last = 0u;
+  if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) partials[(int64_t)part * NV + k] = v[k];
     __threadfence();
-    unsigned int ticket = atomicAdd(counter, 1u);
-    s_last = (ticket == (unsigned int)(nparts - 1));
+    const unsigned int ticket = atomicAdd(counter, 1u);
+    last = ticket == (unsigned int)(nparts - 1) ? 1u : 0u;
   }
-  __syncthreads();
-  if (!s_last) return false;
+  if (!__shfl_sync(0xffffffffu, last, 0)) return false;
   __threadfence();
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-  for (int j = threadIdx.x; j < nparts; j += THREADS)
+  for (int j = lane; j < nparts; j += 32)
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(int64_t)j * NV + k]);
-  block_sum<NV, THREADS>(acc, sm);
-  if (threadIdx.x == 0) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+  if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) out[k] = acc[k];
     *counter = 0u;
@@ -144,6 +151,42 @@ struct ForceAcc {
     v[5] += finite_or_zero(c.tz, bad);
   }
 };
+
+// The block's FP64 partial of the force, written by thread 0 to
+// partials[part]; the caller's stream sums the partials after the launch.
+template <int THREADS>
+__device__ __forceinline__ void publish_force(const ForceAcc &a, double *partials, int part) {
+  __shared__ double sm[kForceSlots * (THREADS / 32)];
+  double v[kForceSlots];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) v[k] = a.v[k];
+  v[6] = a.bad;
+  v[7] = 0.0;
+  block_sum<kForceSlots, THREADS>(v, sm);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < kForceSlots; ++k) partials[(int64_t)part * kForceSlots + k] = v[k];
+}
+
+// The sum of a launch's force partials, spread over the first blocks of a
+// later launch so that no block waits on more than one round of loads:
+// block b adds the partials of group b (kSumGroup consecutive ones, one per
+// thread, then the block tree) into groups[b]; the last group to finish
+// (a ticket behind one fence per group, not per partial) sums the groups in
+// order into out. The order depends only on nparts, so every launch that
+// sums the same partials with THREADS = kSumGroup gets the same bits.
+template <int THREADS>
+__device__ __forceinline__ bool sum_partials_grouped(const double *partials, int nparts, double *groups,
+                                                     unsigned int *counter, double *out, int b) {
+  static_assert(THREADS == kSumGroup, "one partial per thread");
+  __shared__ double sm[kForceSlots * (THREADS / 32)];
+  double acc[kForceSlots];
+  const int j = b * kSumGroup + (int)threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < kForceSlots; ++k) acc[k] = j < nparts ? partials[(int64_t)j * kForceSlots + k] : 0.0;
+  block_sum<kForceSlots, THREADS>(acc, sm);
+  return finish_sum<kForceSlots, THREADS>(acc, groups, counter, sum_groups(nparts), b, out, sm);
+}
 
 // Returns true in the block that summed the partials (the last to finish).
 template <int THREADS>
@@ -276,37 +319,56 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
   const bool near = bbody && phi < 2.5f;
   float fbx = 0.f, fby = 0.f, fbz = 0.f;
 
-  // 1b. Bounce-back links.
+  // 1b. Bounce-back links. Every link is classified first (SDF and wall
+  // tests, no memory access), then the cell's own populations that the
+  // patches read are loaded together: a near cell waits for one memory
+  // latency instead of one per solid link. (The rest direction never
+  // patches: its source is the cell itself.)
   if (near || at_wall) {
-    float rhoW = 1.f;
-    if (bbody && p.rho_w_local && phi < 2.f) {
-      float s = 0.f;
+    unsigned solid = 0u, wall = 0u;
 #pragma unroll
-      for (int i = 0; i < Q; ++i) s += Codec<S>::ld(fi + (int64_t)i * n + cell, i, p.pk);
-      rhoW = s;
-    }
-#pragma unroll
-    for (int i = 0; i < Q; ++i) {
+    for (int i = 1; i < Q; ++i) {
       const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
-      const int o = L::opp(i);
-      bool solid = false;
-      if (near) solid = phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body, p.win) < 0.f;
-      if (solid) {
-        const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
-        const float corr =
-            2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) / kCS2;
-        f[i] = fopp + corr;
-        if (phi >= 0.f) {
-          const float m = 2.f * fopp + corr;
-          fbx += -(float)ex * m;
-          fby += -(float)ey * m;
-          fbz += -(float)ez * m;
-        }
+      if (near && phi3({pos.x - (float)ex, pos.y - (float)ey, pos.z - (float)ez}, p.body, p.win) < 0.f) {
+        solid |= 1u << i;
       } else if (at_wall) {
         const int sx = x - ex, sy = y - ey, sz = z - ez;
         const bool out = (p.wall_x && (sx < 0 || sx >= nx)) || (p.wall_y && (sy < 0 || sy >= ny)) ||
                          (p.wall_z && (sz < 0 || sz >= nz));
-        if (out) f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
+        if (out) wall |= 1u << i;
+      }
+    }
+    if (solid | wall) {
+      const bool all = bbody && p.rho_w_local && phi < 2.f;  // rho_w sums every population
+      float own[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i)
+        own[i] = (all || (((solid | wall) >> L::opp(i)) & 1u)) ? Codec<S>::ld(fi + (int64_t)i * n + cell, i, p.pk)
+                                                                 : 0.f;
+      float rhoW = 1.f;
+      if (all) {
+        float s = 0.f;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) s += own[i];
+        rhoW = s;
+      }
+#pragma unroll
+      for (int i = 1; i < Q; ++i) {
+        const int ex = L::ex(i), ey = L::ey(i), ez = L::ez(i);
+        const float fopp = own[L::opp(i)];
+        if ((solid >> i) & 1u) {
+          const float corr =
+              2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) / kCS2;
+          f[i] = fopp + corr;
+          if (phi >= 0.f) {
+            const float m = 2.f * fopp + corr;
+            fbx += -(float)ex * m;
+            fby += -(float)ey * m;
+            fbz += -(float)ez * m;
+          }
+        } else if ((wall >> i) & 1u) {
+          f[i] = fopp;
+        }
       }
     }
   }

@@ -53,6 +53,15 @@ struct StepParams {
   double *partials;        // 8 doubles per region block
   unsigned int *counter;   // last-block ticket, returns to 0 after each step
   double *force_out;       // 8 doubles: fx fy fz tx ty tz nonfinite 0
+  // Dense steps sum their partials after the launch (sum_partials_grouped,
+  // with `counter` as its ticket and `groups` as its first-level sums): with
+  // defer_force = 0 launch_step() follows the step with a launch that does
+  // it; with defer_force = 1 it is left to the next launch on the stream,
+  // whose first blocks sum the prev_parts partials at prev_partials.
+  double *groups;
+  int defer_force;
+  int prev_parts;
+  const double *prev_partials;
   Pack pk;                 // 16-bit storage encoding
   // Multi-domain launches: the domain's first tile, and the tile range
   // [ft0, ft1) (relative to tile0) whose cells can see the body.
@@ -99,6 +108,15 @@ LBM_HD bool box_region(const int box[6], int nx, int ny, int nz, const int *cap,
     r[2 * a + 1] = first + count;
   }
   return clipped;
+}
+// Force partials summed per block by sum_partials_grouped (one per thread),
+// and the number of such groups.
+constexpr int kSumGroup = 64;
+LBM_HD int sum_groups(int nparts) { return (nparts + kSumGroup - 1) / kSumGroup; }
+
+// Number of force partials (launch blocks of the force region) of a dense step.
+inline int force_parts(int q, const StepParams &p) {
+  return (p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (q == 9 ? 1 : p.rbz1 - p.rbz0);
 }
 constexpr int kReduceThreads = 256;
 constexpr int kForceSlots = 8;

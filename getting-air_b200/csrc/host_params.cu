@@ -112,6 +112,10 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
   p.force_on = 0;
   p.swept = 0;
   p.swept_band = 0.f;
+  p.groups = nullptr;
+  p.defer_force = 0;
+  p.prev_parts = 0;
+  p.prev_partials = nullptr;
 }
 
 bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]) {

@@ -29,6 +29,7 @@ struct lbm_session {
   int cur = 0;
   float *mac = nullptr;
   double *force_partials = nullptr;
+  double *force_groups = nullptr;  // first-level sums of the partials
   unsigned int *force_counter = nullptr;
   double *force_out = nullptr;
   int force_nparts = 0;
@@ -109,26 +110,40 @@ void set_force_region(lbm_session *s) {
   p.rbz0 = r[4]; p.rbz1 = r[5];
 }
 
+// Force scratch for `need` partials per step (grown, never shrunk; the
+// stream is drained first since launches in flight may still read it).
+int grow_force_scratch(lbm_session *s, int need) {
+  if (need <= s->force_nparts) return LBM_OK;
+  if (s->force_partials) {
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->force_partials);
+    cudaFree(s->force_groups);
+    s->bytes -= (int64_t)(2 * s->force_nparts + sum_groups(s->force_nparts)) * kForceSlots * 8;
+  }
+  s->force_partials = nullptr;
+  s->force_groups = nullptr;
+  s->force_nparts = 0;
+  // two sets of partials: consecutive steps of one lbm_step() alternate
+  CK(s, cudaMalloc(&s->force_partials, (size_t)2 * need * kForceSlots * sizeof(double)));
+  CK(s, cudaMalloc(&s->force_groups, (size_t)sum_groups(need) * kForceSlots * sizeof(double)));
+  s->force_nparts = need;
+  s->bytes += (int64_t)(2 * need + sum_groups(need)) * kForceSlots * 8;
+  s->sp.partials = s->force_partials;
+  s->sp.groups = s->force_groups;
+  return LBM_OK;
+}
+
 int ensure_force_scratch(lbm_session *s) {
   const StepParams &p = s->sp;
   if (!p.force_on) return LBM_OK;
-  const int need = (p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0);
-  if (need <= s->force_nparts) return LBM_OK;
-  if (s->force_partials) {
-    cudaFree(s->force_partials);
-    s->bytes -= (int64_t)s->force_nparts * kForceSlots * 8;
-  }
-  s->force_partials = nullptr;
-  CK(s, cudaMalloc(&s->force_partials, (size_t)need * kForceSlots * sizeof(double)));
-  s->force_nparts = need;
-  s->bytes += (int64_t)need * kForceSlots * 8;
-  return LBM_OK;
+  return grow_force_scratch(s, (p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0));
 }
 
 void fill_params(lbm_session *s) {
   StepParams &p = s->sp;
   fill_step_params(s->cfg, s->n, 0, p);
   p.partials = s->force_partials;
+  p.groups = s->force_groups;
   p.counter = s->force_counter;
   p.force_out = s->force_out;
   set_force_region(s);
@@ -141,6 +156,7 @@ void release(lbm_session *s) {
   cudaFree(s->f[1]);
   cudaFree(s->mac);
   cudaFree(s->force_partials);
+  cudaFree(s->force_groups);
   cudaFree(s->force_counter);
   cudaFree(s->force_out);
   cudaFree(s->tot_partials);
@@ -329,11 +345,23 @@ int lbm_step(lbm_session *s, int n) {
     }
     return LBM_OK;
   }
+  // Each step's force partials are summed by the next step's first block;
+  // the last step's by the one-CTA sum launch_step() adds after it.
+  const int64_t half = (int64_t)s->force_nparts * kForceSlots;
+  const int parts = s->sp.force_on ? force_parts(s->q, s->sp) : 0;
   for (int k = 0; k < n; ++k) {
-    s->sp.write_mac = (k == n - 1);
-    CK(s, launch_step(s->q, s->storage, s->f[s->cur], s->f[1 - s->cur], s->mac, s->sp, s->stream));
+    StepParams &sp = s->sp;
+    sp.write_mac = (k == n - 1);
+    sp.partials = s->force_partials + (k & 1) * half;
+    sp.defer_force = k < n - 1;
+    sp.prev_parts = k > 0 ? parts : 0;
+    sp.prev_partials = s->force_partials + ((k + 1) & 1) * half;
+    CK(s, launch_step(s->q, s->storage, s->f[s->cur], s->f[1 - s->cur], s->mac, sp, s->stream));
     s->cur = 1 - s->cur;
   }
+  s->sp.partials = s->force_partials;
+  s->sp.defer_force = 0;
+  s->sp.prev_parts = 0;
   return LBM_OK;
 }
 
@@ -411,17 +439,7 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   }
   box_region(box, c.nx, c.ny, c.nz, d.cap, p0.region);
   const int need = d.cap[0] * d.cap[1] * d.cap[2];
-  if (need > s->force_nparts) {
-    cudaStreamSynchronize(s->stream);
-    cudaFree(s->force_partials);
-    s->bytes -= (int64_t)s->force_nparts * kForceSlots * 8;
-    s->force_partials = nullptr;
-    s->force_nparts = 0;
-    CK(s, cudaMalloc(&s->force_partials, (size_t)need * kForceSlots * sizeof(double)));
-    s->force_nparts = need;
-    s->bytes += (int64_t)need * kForceSlots * 8;
-    s->sp.partials = s->force_partials;
-  }
+  if (int rc = grow_force_scratch(s, need)) return rc;
   if (!s->pose) {
     CK(s, cudaMalloc(&s->pose, 2 * sizeof(BodyPose)));
     CK(s, cudaMalloc(&s->dyn, sizeof(BodyDyn)));

@@ -7,8 +7,10 @@
 // streams are busy, or code that runs under a fixed memory budget decided
 // up front. They already hold the populations; what the step additionally
 // needs is scratch for the deterministic FP64 body-force reduction (one
-// partial per launch block near the body plus a ticket counter). Here that
-// scratch is a file-scope device array, so the entry point only launches.
+// partial per launch block near the body, first-level group sums and a
+// ticket counter, used by the sum launched after the step on the same
+// stream). Here that scratch is a file-scope device array, so the entry
+// point only launches.
 //
 // Limits and rules of use:
 //  * the scratch holds kNoAllocMaxParts block partials (512 KiB); a body
@@ -20,8 +22,8 @@
 //    (cudaGetSymbolAddress) with that device current and caches it; make
 //    that first call before any stream capture;
 //  * all calls on a device share the one array, which keeps the last call's
-//    contents: the ticket counter is cleared on the caller's stream before
-//    every launch, and two calls whose kernels overlap on the GPU race.
+//    partials; the ticket returns to zero at the end of every sum; two
+//    calls whose kernels overlap on the GPU race.
 //
 // The step itself is the dense kernel of dense_kernels.cu, unchanged.
 
@@ -38,9 +40,10 @@
 namespace {
 
 constexpr int kNoAllocMaxParts = 8192;
-// Partials (kForceSlots doubles per block), then one slot whose first four
-// bytes are the ticket counter.
-constexpr int kScratchDoubles = kNoAllocMaxParts * lbm::kForceSlots + 32;
+// Partials (kForceSlots doubles per block), the group sums, then one slot
+// whose first four bytes are the ticket (zero at load, and after every sum).
+constexpr int kMaxGroups = (kNoAllocMaxParts + lbm::kSumGroup - 1) / lbm::kSumGroup;
+constexpr int kScratchDoubles = (kNoAllocMaxParts + kMaxGroups) * lbm::kForceSlots + 32;
 
 static __device__ __align__(256) double g_step_scratch[kScratchDoubles];
 
@@ -103,13 +106,12 @@ int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float
   int rc = scratch_for_current_device(&scratch);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  unsigned int *ticket = reinterpret_cast<unsigned int *>(scratch + kNoAllocMaxParts * lbm::kForceSlots);
   p.partials = scratch;
-  p.counter = ticket;
+  p.groups = scratch + kNoAllocMaxParts * lbm::kForceSlots;
+  p.counter = reinterpret_cast<unsigned int *>(p.groups + kMaxGroups * lbm::kForceSlots);
   p.force_out = force_out;
   p.write_mac = mac ? 1 : 0;
-  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned int), st);
-  if (e == cudaSuccess) e = lbm::launch_step(cfg->q, cfg->storage, f_in, f_out, mac, p, st);
+  const cudaError_t e = lbm::launch_step(cfg->q, cfg->storage, f_in, f_out, mac, p, st);
   if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("step: ") + cudaGetErrorString(e));
   return LBM_OK;
 }

@@ -238,8 +238,35 @@ def test_step_in_pieces_equals_one_call(lbm, oracle):
         b.step(3)
     assert np.array_equal(a.read_f(), b.read_f())
     assert np.array_equal(a.read_mac(), b.read_mac())
+    assert np.array_equal(a.forces(), b.forces())
     a.close()
     b.close()
+
+
+def test_chained_force_sums_equal_per_step_sums(lbm, oracle):
+    """Within one step(n) each step's force partials are summed by the next
+    step's first block, the last step's by a sum launched after it, with the
+    partials alternating between two sets: an even count ends on the second
+    set. The last force equals the one of n calls of step(1), whichever set
+    the call ended on."""
+    from getting_air_b200 import scenarios as sc
+    s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40)
+    f0 = oracle.init_eq(19, s["mac"], fp32=True).astype(np.float32)
+    a = lbm.Solver.create(19, s["dims"], **s["kw"])
+    c = lbm.Solver.create(19, s["dims"], **s["kw"])
+    a.write_f(f0)
+    c.write_f(f0)
+    a.step(8)
+    for _ in range(8):
+        c.step(1)
+    assert np.array_equal(a.read_f(), c.read_f())
+    assert np.array_equal(a.forces(), c.forces())
+    a.step(3)
+    c.step(2)
+    c.step(1)
+    assert np.array_equal(a.forces(), c.forces())
+    a.close()
+    c.close()
 
 
 def test_init_macro_matches_oracle_init(lbm, oracle):
