@@ -13,9 +13,9 @@
 // point only launches.
 //
 // Limits and rules of use:
-//  * the scratch holds kNoAllocMaxParts block partials (512 KiB); a body
-//    whose force region needs more launch blocks is refused with
-//    LBM_ENOSPC;
+//  * the scratch holds kNoAllocMaxParts block partials (520 KiB with their
+//    group sums); a body whose force region needs more launch blocks is
+//    refused with LBM_ENOSPC;
 //  * every GPU that loads this library holds the array until the process
 //    exits;
 //  * the first call on a device looks up the array's device address

@@ -289,7 +289,7 @@ int64_t lbm_device_bytes(const lbm_session *s);
  * optionally writing mac (4 floats per cell, device) and the body's
  * force/torque (8 doubles, device: fx fy fz tx ty tz nonfinite 0), launched
  * on cuda_stream. Allocates nothing: the force reduction's scratch is a fixed
- * 512 KiB device array inside the library (8192 launch blocks of partials);
+ * 520 KiB device array inside the library (8192 launch blocks of partials);
  * a force region needing more returns LBM_ENOSPC. The first call on a device
  * looks up that array's address and must come before any stream capture.
  * All calls share the array: calls whose kernels overlap on the GPU race.
