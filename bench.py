@@ -201,9 +201,9 @@ def time_device(lbm, wl, steps, warmup, world):
             torch.cuda.synchronize()
         barrier(world)
     total_ms = start.elapsed_time(end)
-    # Per step the stream runs the step kernel and, with the body in the
-    # domain, the one-CTA force sum after it: total / steps bounds the step
-    # kernel's mean duration from above (the sum and the gaps included).
+    # The stream runs one step kernel per step (each also sums the previous
+    # step's force partials) and one force-sum launch after the last:
+    # total / steps bounds the step kernel's mean duration from above.
     launch_ms = [total_ms / steps]
     forces = s.forces()
     totals = s.totals()
@@ -558,7 +558,7 @@ def run_ours(args):
                      "kernel_ms": kern_ms},
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps},
-        "gpu_launches": 2 * args.steps,  # step kernel + force sum per step
+        "gpu_launches": args.steps + 1,  # a step kernel per step, a force sum after the last
         "clocks": clocks,
         "forms": forms,
         "drag_lift_last_step": {"fx": forces[0], "fy": forces[1], "fz": forces[2]},
