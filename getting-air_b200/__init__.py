@@ -401,8 +401,14 @@ class Solver:
         self._check(lib.lbm_read_f_raw(self._h, out.ctypes.data_as(C.c_void_p)))
         return out
 
-    def read_mac(self) -> np.ndarray:
-        out = np.empty((self.ncells, 4), np.float32)
+    def read_mac(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The mac field (rho, ux, uy, uz per cell). `out`, if given, is a
+        C-contiguous float32 array of ncells x 4 values to fill in place (a
+        pinned one makes the copy a direct DMA)."""
+        if out is None:
+            out = np.empty((self.ncells, 4), np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.ncells * 4:
+            raise ValueError("out must be a C-contiguous float32 array of ncells x 4 values")
         self._check(lib.lbm_read_mac(self._h, _ptr(out, C.c_float)))
         return out
 

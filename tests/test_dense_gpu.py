@@ -239,6 +239,10 @@ def test_step_in_pieces_equals_one_call(lbm, oracle):
     assert np.array_equal(a.read_f(), b.read_f())
     assert np.array_equal(a.read_mac(), b.read_mac())
     assert np.array_equal(a.forces(), b.forces())
+    buf = np.full((a.ncells, 4), np.nan, np.float32)
+    assert a.read_mac(out=buf) is buf and np.array_equal(buf, b.read_mac())
+    with pytest.raises(ValueError):
+        a.read_mac(out=np.empty((a.ncells, 4), np.float64))
     a.close()
     b.close()
 
