@@ -341,16 +341,15 @@ __global__ void __launch_bounds__(kListThreads)
       }
     }
   }
+  // One load per direction, its address chosen without a branch (the
+  // cell's own opposite population for a solid link, else the pull
+  // source), so that all Q loads are in flight together rather than one
+  // round trip per solid link.
   float f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
-    if (solid_links & (1u << i)) {
-      const float corr =
-          2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
-      f[i] = __ldg(fin + (int64_t)L::opp(i) * p.P + t.cell) + corr;
-      continue;
-    }
+    const bool solid = (solid_links >> i) & 1u;
     int s[3] = {t.fx - e[0], t.fy - e[1], t.fz - e[2]};
     const int o0 = oa[0][e[0] + 1], o1 = oa[1][e[1] + 1], o2 = oa[2][e[2] + 1];
     int src = t.slot;
@@ -366,7 +365,15 @@ __global__ void __launch_bounds__(kListThreads)
         for (int a = 0; a < 3; ++a) s[a] = min(max(s[a], 0), FB - 1);
       }
     }
-    f[i] = __ldg(fin + (int64_t)i * p.P + (int64_t)src * p.T3 + (s[2] * FB + s[1]) * FB + s[0]);
+    const int64_t pull = (int64_t)i * p.P + (int64_t)src * p.T3 + (s[2] * FB + s[1]) * FB + s[0];
+    const float v = __ldg(fin + (solid ? (int64_t)L::opp(i) * p.P + t.cell : pull));
+    if (solid) {
+      const float corr =
+          2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
+      f[i] = v + corr;
+    } else {
+      f[i] = v;
+    }
   }
   float rho, mx, my, mz;
   moments<L, Q>(f, rho, mx, my, mz);
