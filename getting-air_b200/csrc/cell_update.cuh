@@ -154,8 +154,18 @@ struct ForceAcc {
 
 // The block's FP64 partial of the force, written by thread 0 to
 // partials[part]; the caller's stream sums the partials after the launch.
+// Most blocks of a force region hold no cell with a contribution (the
+// region is the body's box; only its shell touches the body): when every
+// thread's sums are +0 the block writes its zero partial directly instead
+// of running the FP64 tree, whose result would be the same +0s.
 template <int THREADS>
 __device__ __forceinline__ void publish_force(const ForceAcc &a, double *partials, int part) {
+  const bool mine = a.v[0] != 0.0 || a.v[1] != 0.0 || a.v[2] != 0.0 || a.v[3] != 0.0 || a.v[4] != 0.0 ||
+                    a.v[5] != 0.0 || a.bad != 0.0;
+  if (!__syncthreads_or(mine)) {
+    if (threadIdx.x < kForceSlots) partials[(int64_t)part * kForceSlots + threadIdx.x] = 0.0;
+    return;
+  }
   __shared__ double sm[kForceSlots * (THREADS / 32)];
   double v[kForceSlots];
 #pragma unroll
@@ -494,6 +504,40 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   gather3<Q, S>(fi, p, x, y, z, f);
   MemSink<S> sink{fout + p.base, p.n, (z * p.ny + y) * p.nx + x, p.pk};
   cell3_core<Q, S>(fi, f, mac, p, x, y, z, force, cf, sink);
+}
+
+// A cell that only fluid can reach: no body link within reach (or no body),
+// no wall on any of its links, no moving window, and not in the force
+// reduction. For such a cell cell3() finds phi = 1e30, u_s = 0 and chi = 0,
+// so its Guo force is the body force alone (rho chi (u_s - u*) = +-0, and
+// +-0 + F = F) and nothing is patched; this is that path with the dead
+// tests taken out, to the bit.
+template <int Q, typename S>
+__device__ __forceinline__ void cell3_fluid(const S *__restrict__ fin, S *__restrict__ fout,
+                                            float *__restrict__ mac, const StepParams &p, int x, int y, int z) {
+  using L = Lattice<Q>;
+  const S *fi = fin + p.base;
+  float f[Q];
+  gather3<Q, S>(fi, p, x, y, z, f);
+  float rho, mx, my, mz;
+  moments<L, Q>(f, rho, mx, my, mz);
+  const float inv = 1.0f / fmaxf(rho, 1e-6f);
+  const float uxs = mx * inv, uys = my * inv, uzs = mz * inv;
+  const float hinv = 0.5f * inv;
+  const float ux = fmaf(p.fx, hinv, uxs);
+  const float uy = fmaf(p.fy, hinv, uys);
+  const float uz = fmaf(p.fz, hinv, uzs);
+  float spw = 0.f;
+  if (p.sponge_w > 0.f) {
+    const float dx = p.sax ? fminf((float)x, (float)(p.nx - 1) - (float)x) : 1e30f;
+    const float dy = p.say ? fminf((float)y, (float)(p.ny - 1) - (float)y) : 1e30f;
+    const float dz = p.saz ? fminf((float)z, (float)(p.nz - 1) - (float)z) : 1e30f;
+    spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), p.sponge_inv);
+  }
+  const int cell = (z * p.ny + y) * p.nx + x;
+  MemSink<S> sink{fout + p.base, p.n, cell, p.pk};
+  collide_store<L, Q>(f, rho, ux, uy, uz, p.fx, p.fy, p.fz, p.omega, spw, p.ftarget, sink);
+  if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, uz);
 }
 
 // Force contribution of one cell without the collision (a free body's

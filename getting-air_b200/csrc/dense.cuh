@@ -17,6 +17,7 @@ namespace lbm {
 // noff[i] = -off[i] * scale (exact: scale is a power of two), so that the
 // encode is one fused multiply-add, fma(f, scale, noff[i]) = (f - off) *
 // scale to the bit.
+constexpr float kF16Scale = 1024.0f;  // 2^10, the FP16 storage scale
 struct Pack {
   float off[27];
   float noff[27];

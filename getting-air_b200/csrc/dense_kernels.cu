@@ -34,6 +34,8 @@
 // every step costs its launch gaps (measured at 256x128x128: +9 %, +10 %
 // and +7 % of the step against no force at all, and +1 % for this form).
 
+#include <type_traits>
+
 #include "cell_update.cuh"
 
 namespace lbm {
@@ -41,8 +43,9 @@ namespace lbm {
 namespace {
 
 // ---- dense fused steps -------------------------------------------------------
-// One thread per cell, 128-thread CTAs along x, grid (NX/128, NY, NZ): the
-// row and plane come straight from blockIdx, no division.
+// One thread per cell, kStepThreads (64) cells of a row per CTA, grid
+// (NX/64, NY, NZ): the row and plane come straight from blockIdx, no
+// division.
 
 // The previous step's force, in this launch's first blocks (before their
 // own cells, so that the group's fence has no stores of theirs to wait on).
@@ -50,6 +53,40 @@ __device__ __forceinline__ void sum_previous(const StepParams &p) {
   const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (p.prev_parts && b < sum_groups(p.prev_parts))
     sum_partials_grouped<kStepThreads>(p.prev_partials, p.prev_parts, p.groups, p.counter, p.force_out, b);
+}
+
+// Whether a cell of [lo, hi] lies in the interval [a, a + len] read modulo
+// n (a in [0, n); len < 0 is empty): the reach-box test of cell3_core for a
+// whole span of cells.
+__device__ __forceinline__ bool span_hits(int lo, int hi, int a, int len, int n) {
+  if (len >= n - 1) return true;
+  const int b = a + len;
+  return (lo <= b && hi >= a) || (lo + n <= b && hi + n >= a);
+}
+
+// What a launch block of the 3D step must evaluate, decided once per block
+// (warp-uniform): kGeneral runs cell3 for every cell; kFluid runs
+// cell3_fluid, for blocks that take no part in the force reduction, have no
+// cell within reach of a bounce-back body (or no body), touch no wall and
+// are not windowed. Penalty bodies reach every cell through chi and always
+// take kGeneral. (A third kind without the sponge blend, for blocks beyond
+// the sponge band, had fewer instructions per update but a slower step: a
+// third hot copy of the update raised instruction-fetch and memory stalls.)
+enum BlockKind { kGeneral = 0, kFluid = 1 };
+
+__device__ __forceinline__ int block_kind(const StepParams &p, int lo, int hi, int y, int z, bool region) {
+  if (region || p.win.on) return kGeneral;
+  if (p.has_body) {
+    if (!p.bb || !p.nbox_on) return kGeneral;
+    if (span_hits(lo, hi, p.nbox[0], p.nbox[1] - p.nbox[0], p.nx) &&
+        span_hits(y, y, p.nbox[2], p.nbox[3] - p.nbox[2], p.ny) &&
+        span_hits(z, z, p.nbox[4], p.nbox[5] - p.nbox[4], p.nz))
+      return kGeneral;
+  }
+  if ((p.wall_x && (lo == 0 || hi == p.nx - 1)) || (p.wall_y && (y == 0 || y == p.ny - 1)) ||
+      (p.wall_z && (z == 0 || z == p.nz - 1)))
+    return kGeneral;
+  return kFluid;
 }
 
 template <int Q, typename S>
@@ -65,6 +102,16 @@ __device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__re
   dz += dz < 0 ? (int)gridDim.z : 0;
   const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
   const bool region = p.force_on && dx < rx && dy < ry && dz < rz;
+  // The fluid path pays for 16-bit storage (issue-bound: 0.1106 against
+  // 0.1167 ms per step on the 256x128x128 sphere) but not for FP32, whose
+  // step is bound by memory latency and ran 0.1123 against 0.1110 ms with
+  // it: FP32 takes the general path everywhere.
+  const int lo = bx * kStepThreads, hi = min(lo + kStepThreads, p.nx) - 1;
+  const int kind = std::is_same<S, float>::value ? kGeneral : block_kind(p, lo, hi, by, bz, region);
+  if (kind == kFluid) {
+    if (x < p.nx) cell3_fluid<Q, S>(fin, fout, mac, p, x, by, bz);
+    return;
+  }
   CellForce cf;
   if (x < p.nx) cell3<Q, S>(fin, fout, mac, p, x, by, bz, region, cf);
   if (region) {

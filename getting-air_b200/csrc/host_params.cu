@@ -66,7 +66,7 @@ Pack make_pack(const lbm_config &c) {
     const float eu = (float)ex * ux + (float)ey * uy + (float)ez * uz;
     k.off[i] = lattice_weight(c.q, i) * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * usq);
   }
-  k.scale = c.storage == LBM_STORE_FP16 ? 1024.0f : 1.0f;
+  k.scale = c.storage == LBM_STORE_FP16 ? kF16Scale : 1.0f;
   k.inv = 1.0f / k.scale;
   for (int i = 0; i < 27; ++i) k.noff[i] = -k.off[i] * k.scale;
   return k;
@@ -122,6 +122,35 @@ bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]) {
   if (!c.has_body) return false;
   return body_cell_box(c.body, c.q, c.nx, c.ny, c.nz, c.use_bounceback, c.swept_force, c.chi_eps, box, &p.swept,
                        &p.swept_band, c.q != 9 ? c.window : nullptr);
+}
+
+bool set_body_regions(const lbm_config &c, StepParams &p, bool force) {
+  int box[6];
+  const bool any = force_cell_box(c, p, box);
+  p.nbox_on = 0;
+  if (c.q != 9 && c.has_body && c.use_bounceback) {
+    const int len[3] = {c.nx, c.ny, c.nz};
+    p.nbox_on = 1;
+    for (int a = 0; a < 3; ++a) {
+      if (!any) {  // no cell within reach: an empty box
+        p.nbox[2 * a] = 0;
+        p.nbox[2 * a + 1] = -1;
+        continue;
+      }
+      int lo = box[2 * a] % len[a];
+      if (lo < 0) lo += len[a];
+      p.nbox[2 * a] = lo;
+      p.nbox[2 * a + 1] = lo + (box[2 * a + 1] - box[2 * a]);
+    }
+  }
+  p.force_on = (force && any) ? 1 : 0;
+  if (!p.force_on) return false;
+  int r[6];
+  box_region(box, p.nx, p.ny, p.nz, nullptr, r);
+  p.rbx0 = r[0]; p.rbx1 = r[1];
+  p.rby0 = r[2]; p.rby1 = r[3];
+  p.rbz0 = r[4]; p.rbz1 = r[5];
+  return true;
 }
 
 }  // namespace lbm

@@ -25,6 +25,13 @@ void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &
 // false when the body has no cell in the domain (force off).
 bool force_cell_box(const lbm_config &c, StepParams &p, int box[6]);
 
+// The body's regions of a dense step, from force_cell_box(): the reach box
+// p.nbox of a 3D bounce-back body (cells outside it are beyond every link,
+// so the step skips the SDF there; an empty box when the body has no cell
+// in the domain), and with `force` the launch blocks that reduce the force
+// (p.rb*). Returns p.force_on.
+bool set_body_regions(const lbm_config &c, StepParams &p, bool force);
+
 float lattice_weight(int q, int i);
 
 // 16-bit storage encoding of a domain (far-field equilibrium offsets).

@@ -79,36 +79,9 @@ template <int Q> void tables(int32_t *ex, int32_t *ey, int32_t *ez, float *w, in
   }
 }
 
-// Which launch blocks can receive a force contribution: the blocks covering
-// the cell box of force_cell_box().
-void set_force_region(lbm_session *s) {
-  StepParams &p = s->sp;
-  int box[6];
-  p.force_on = force_cell_box(s->cfg, p, box) ? 1 : 0;
-  // a bounce-back body: cells outside the force box are beyond any link of it
-  p.nbox_on = 0;
-  if (s->cfg.q != 9 && s->cfg.has_body && s->cfg.use_bounceback) {
-    const int len[3] = {s->cfg.nx, s->cfg.ny, s->cfg.nz};
-    p.nbox_on = 1;
-    for (int a = 0; a < 3; ++a) {
-      if (!p.force_on) {  // no cell within reach: an empty box
-        p.nbox[2 * a] = 0;
-        p.nbox[2 * a + 1] = -1;
-        continue;
-      }
-      int lo = box[2 * a] % len[a];
-      if (lo < 0) lo += len[a];
-      p.nbox[2 * a] = lo;
-      p.nbox[2 * a + 1] = lo + (box[2 * a + 1] - box[2 * a]);
-    }
-  }
-  if (!p.force_on) return;
-  int r[6];
-  box_region(box, p.nx, p.ny, p.nz, nullptr, r);
-  p.rbx0 = r[0]; p.rbx1 = r[1];
-  p.rby0 = r[2]; p.rby1 = r[3];
-  p.rbz0 = r[4]; p.rbz1 = r[5];
-}
+// Which launch blocks can receive a force contribution (the blocks covering
+// the cell box of force_cell_box()) and the bounce-back reach box.
+void set_force_region(lbm_session *s) { set_body_regions(s->cfg, s->sp, true); }
 
 // Force scratch for `need` partials per step (grown, never shrunk; the
 // stream is drained first since launches in flight may still read it).

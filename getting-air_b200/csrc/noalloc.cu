@@ -14,16 +14,26 @@
 //
 // Limits and rules of use:
 //  * the scratch holds kNoAllocMaxParts block partials (520 KiB with their
-//    group sums); a body whose force region needs more launch blocks is
-//    refused with LBM_ENOSPC;
+//    group sums and the ticket); a body whose force region needs more
+//    launch blocks is refused with LBM_ENOSPC before anything is launched;
 //  * every GPU that loads this library holds the array until the process
 //    exits;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current and caches it; make
-//    that first call before any stream capture;
+//  * a call outside stream capture looks up the array's device address
+//    (cudaGetSymbolAddress) with the calling device current and keeps it
+//    for that device; a call made while its stream is capturing uses the
+//    kept address, so the first call on a device must come before any
+//    capture. The lookup on every uncaptured call also means that a context
+//    torn down by cudaDeviceReset is followed by a fresh address, not a
+//    stale one; a graph captured before such a reset must not be replayed;
 //  * all calls on a device share the one array, which keeps the last call's
-//    partials; the ticket returns to zero at the end of every sum; two
-//    calls whose kernels overlap on the GPU race.
+//    contents. Each call clears the sum's ticket on its stream before the
+//    step (the only scratch that must start at zero; partials and group
+//    sums are written before they are read), so a sum that an earlier call
+//    left unfinished cannot skew a later one. Two calls whose kernels
+//    overlap on the GPU still race on the array: serialise them (one stream,
+//    or events between streams);
+//  * force_out, when given, is always written on the stream: the body's
+//    force, or zeros when no cell of the domain can reach the body.
 //
 // The step itself is the dense kernel of dense_kernels.cu, unchanged.
 
@@ -57,19 +67,25 @@ int nfail(int code, const std::string &m) {
   return code;
 }
 
-// Device address of the scratch array on the current device, looked up once.
-int scratch_for_current_device(double **out) {
+// Device address of the scratch array on the current device: looked up
+// (and kept) when the stream is not capturing, the kept one otherwise.
+int scratch_for_current_device(cudaStream_t st, double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return nfail(LBM_ENOTSUP, "device index beyond the scratch cache");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cs);
+  if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_addr[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void *ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_step_scratch);
     if (e != cudaSuccess || !ptr)
       return nfail(LBM_ECUDA, std::string("cudaGetSymbolAddress(step scratch): ") + cudaGetErrorString(e));
     g_scratch_addr[dev] = (double *)ptr;
+  } else if (!g_scratch_addr[dev]) {
+    return nfail(LBM_ESTATE, "the first lbm_step_noalloc call on a device must come before any stream capture");
   }
   *out = g_scratch_addr[dev];
   return LBM_OK;
@@ -88,29 +104,29 @@ int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float
   const int64_t n = (int64_t)cfg->nx * cfg->ny * cfg->nz;
   lbm::StepParams p{};
   lbm::fill_step_params(*cfg, n, 0, p);
-  int box[6];
-  p.force_on = (force_out && lbm::force_cell_box(*cfg, p, box)) ? 1 : 0;
-  if (p.force_on) {
-    int r[6];
-    lbm::box_region(box, p.nx, p.ny, p.nz, nullptr, r);
-    p.rbx0 = r[0]; p.rbx1 = r[1];
-    p.rby0 = r[2]; p.rby1 = r[3];
-    p.rbz0 = r[4]; p.rbz1 = r[5];
+  // the reach box and force region exactly as a session sets them
+  if (lbm::set_body_regions(*cfg, p, force_out != nullptr)) {
     const int64_t parts = (int64_t)(p.rbx1 - p.rbx0) * (p.rby1 - p.rby0) * (p.rbz1 - p.rbz0);
     if (parts > kNoAllocMaxParts)
       return nfail(LBM_ENOSPC, "the body's force region spans " + std::to_string(parts) +
                                    " launch blocks; the fixed scratch holds " + std::to_string(kNoAllocMaxParts));
   }
   if (!f_in || !f_out || f_in == f_out) return nfail(LBM_EINVAL, "f_in and f_out must be distinct device buffers");
-  double *scratch = nullptr;
-  int rc = scratch_for_current_device(&scratch);
-  if (rc) return rc;
   cudaStream_t st = (cudaStream_t)cuda_stream;
+  double *scratch = nullptr;
+  int rc = scratch_for_current_device(st, &scratch);
+  if (rc) return rc;
   p.partials = scratch;
   p.groups = scratch + kNoAllocMaxParts * lbm::kForceSlots;
   p.counter = reinterpret_cast<unsigned int *>(p.groups + kMaxGroups * lbm::kForceSlots);
   p.force_out = force_out;
   p.write_mac = mac ? 1 : 0;
+  cudaError_t z = cudaSuccess;
+  if (p.force_on)
+    z = cudaMemsetAsync(p.counter, 0, sizeof(unsigned int), st);
+  else if (force_out)
+    z = cudaMemsetAsync(force_out, 0, lbm::kForceSlots * sizeof(double), st);
+  if (z != cudaSuccess) return nfail(LBM_ECUDA, std::string("clear: ") + cudaGetErrorString(z));
   const cudaError_t e = lbm::launch_step(cfg->q, cfg->storage, f_in, f_out, mac, p, st);
   if (e != cudaSuccess) return nfail(LBM_ECUDA, std::string("step: ") + cudaGetErrorString(e));
   return LBM_OK;

@@ -58,8 +58,11 @@ typedef enum {
 /* On-device storage of f. The wire format is always f32 planes. */
 typedef enum {
   LBM_STORE_FP32 = 0, /* plain f32 planes                                   */
-  LBM_STORE_FP16 = 1, /* binary16 planes holding f_i - w_i (f-pack mode 2)  */
-  LBM_STORE_BF16 = 2  /* bfloat16 planes holding f_i - w_i                  */
+  LBM_STORE_FP16 = 1, /* binary16 planes holding (f_i - feq_i(1, U_far)) * 2^10:
+                         the deviation from the far-field (sponge) equilibrium,
+                         f-pack mode 2 with the rest state replaced by the free
+                         stream; w_i when there is no far-field velocity      */
+  LBM_STORE_BF16 = 2  /* bfloat16 planes holding f_i - feq_i(1, U_far)         */
 } lbm_storage;
 
 /* Body shapes. 3D: common_d3_geometry.wgsl:40-42. D2Q9 uses ELLIPSE
@@ -289,11 +292,17 @@ int64_t lbm_device_bytes(const lbm_session *s);
  * optionally writing mac (4 floats per cell, device) and the body's
  * force/torque (8 doubles, device: fx fy fz tx ty tz nonfinite 0), launched
  * on cuda_stream. Allocates nothing: the force reduction's scratch is a fixed
- * 520 KiB device array inside the library (8192 launch blocks of partials);
- * a force region needing more returns LBM_ENOSPC. The first call on a device
- * looks up that array's address and must come before any stream capture.
- * All calls share the array: calls whose kernels overlap on the GPU race.
- * Errors are reported by lbm_noalloc_last_error(). */
+ * 520 KiB device array inside the library (8192 launch blocks of partials
+ * plus their group sums and a ticket); a force region needing more returns
+ * LBM_ENOSPC before anything is launched. force_out, when given, is always
+ * written: zeros when no cell can reach the body. A call whose stream is not
+ * capturing looks up the array's device address for the current device and
+ * keeps it; a call during stream capture uses the kept one, so the first
+ * call on a device must come before any capture (and a graph captured
+ * before a cudaDeviceReset must not be replayed after it). All calls share
+ * the array; each clears the ticket on its stream first, and calls whose
+ * kernels overlap on the GPU race. Errors are reported by
+ * lbm_noalloc_last_error(). */
 int lbm_step_noalloc(const lbm_config *cfg, const void *f_in, void *f_out, float *mac, double *force_out,
                      void *cuda_stream);
 const char *lbm_noalloc_last_error(void);
