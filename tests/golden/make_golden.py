@@ -13,7 +13,7 @@ executed; its JavaScript cannot run here):
 * benchmarks.json -- the analytic gates of benchmarks/tgv.json (cases and
                     tolerances) used by the physics tests.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py <path of the reference checkout>
 """
 from __future__ import annotations
 
@@ -96,4 +96,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    main(Path(sys.argv[1]))

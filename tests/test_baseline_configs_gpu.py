@@ -1,0 +1,175 @@
+"""GPU parity at the benchmark's own configurations, full size.
+
+The other GPU tests check every kernel on reduced grids; these run the
+shapes the benchmark times, where the force region, the bounce-back reach
+box, the sponge band and the 64-bit plane offsets all take their full-size
+values:
+
+* the D3Q19 sphere, 256 x 128 x 128 (r = 16, tau 0.56, u0 0.05, bounce-back,
+  sponge, Guo force), in FP32, FP16 and BF16 storage, against ONE FP64
+  oracle run from the same f32 start (SPHERE_STEPS steps): velocity and
+  density relative L2 and drag, each within its storage's stated bound;
+* the 2D AMR cylinder, 1024 x 256 root (r = 20 at (256, 128), Re 100,
+  u0 0.08): every refine round's topology bit-identical to the oracle's
+  round applied to the device's own pre-round state, and the fields and
+  drag after two refine rounds within the AMR tolerances;
+* a 32-domain slice (every 16th) of the seeded 512-domain batch, at the
+  domains' full sizes, each domain against the FP64 oracle.
+
+Bounds. FP32 storage computes in f32 with FMAs against the oracle's f64:
+1e-5 in velocity. The 16-bit storages round every population to the
+format's quantum of its deviation from the far-field equilibrium each
+step: FP16 (11 significand bits at scale 2^10) and BF16 (8 bits). Their
+velocity bound is the north star's 1e-3. The drag after 100 steps from an
+impulsive start is a transient sum with heavy cancellation; measured on
+B200: FP32 1.3e-4, FP16 7.9e-4, BF16 2.5e-3 relative (velocity 3.6e-6,
+5.4e-5, 2.3e-4), so the drag bounds below are 1e-3, 1e-2 and 2e-2.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SPHERE_DIMS = (256, 128, 128)
+SPHERE_STEPS = 100
+# storage: (velocity relL2, density relL2, relative drag error)
+SPHERE_BOUNDS = {"fp32": (1e-5, 1e-6, 1e-3), "fp16": (1e-3, 1e-4, 1e-2), "bf16": (1e-3, 1e-3, 2e-2)}
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def sphere_workload(storage):
+    from getting_air_b200 import scenarios as sc
+    return sc.sphere(n=32, dims=SPHERE_DIMS, u0=0.05, tau=0.56, q=19, bounceback=True,
+                     force=(1e-6, 0.0, 0.0), storage=storage)
+
+
+@pytest.fixture(scope="module")
+def sphere_fp64(lbm, oracle):
+    """The FP64 oracle's state after SPHERE_STEPS from the f32 equilibrium
+    seed (one run shared by the three storages)."""
+    s = sphere_workload("fp32")
+    cfg = lbm.config_from(19, s["dims"], **s["kw"])
+    f0 = oracle.init_eq(19, s["mac"], fp32=True).astype(np.float32)
+    _, mac, forces = oracle.run(cfg, f0.astype(np.float64), SPHERE_STEPS)
+    return f0, mac, forces[-1]
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+def test_sphere_256x128x128_against_fp64(lbm, sphere_fp64, storage):
+    f0, omac, oforce = sphere_fp64
+    s = sphere_workload(storage)
+    sol = lbm.Solver.create(19, s["dims"], **s["kw"])
+    sol.write_f(f0)
+    sol.step(SPHERE_STEPS)
+    mac = sol.read_mac().astype(np.float64)
+    force = sol.forces()
+    sol.close()
+    u_tol, rho_tol, drag_tol = SPHERE_BOUNDS[storage]
+    eu = rel_l2(mac[:, 1:4], omac[:, 1:4])
+    er = rel_l2(mac[:, 0], omac[:, 0])
+    ed = abs(force[0] - oforce[0]) / abs(oforce[0])
+    print(f"{storage}: u relL2 {eu:.3e}, rho relL2 {er:.3e}, drag rel {ed:.3e}")
+    assert np.isfinite(mac).all()
+    assert eu <= u_tol, f"{storage}: u relL2 {eu:.3e} > {u_tol}"
+    assert er <= rho_tol, f"{storage}: rho relL2 {er:.3e} > {rho_tol}"
+    assert ed <= drag_tol, f"{storage}: drag error {ed:.3e} > {drag_tol}"
+    assert abs(oforce[0]) > 0
+
+
+def _topo_equal(t, o):
+    assert np.array_equal(t["block_slot"], o["block_slot"])
+    assert np.array_equal(t["slot_to_block"], o["slot_to_block"])
+    assert t["free_count"] == o["free_count"]
+    n = t["free_count"]
+    assert np.array_equal(t["free_list"][:n], o["free_list"][:n])
+    assert np.array_equal(t["active"], o["active"])
+    assert np.array_equal(t["want"], o["want"])
+
+
+def _cylinder(lbm):
+    from getting_air_b200 import scenarios as sc
+    s = sc.cylinder_amr(W=1024, H=256, r=20.0, centre=(256.0, 128.0), u0=0.08, re=100.0)
+    return s, lbm.amr2d_config(1024, 256, **s["kw"])
+
+
+def test_amr_cylinder_1024x256_refine_rounds_bit_exact(lbm, oracle):
+    s, cfg = _cylinder(lbm)
+    a = lbm.Amr2D(cfg)
+    a.write_root(s["f"], s["vel"])
+    o = oracle.Amr2D(cfg, fp32=True)
+    a.step(1)
+    o.refine_from_vel(s["vel"])
+    t, r = a.topology(), o.read()
+    assert np.array_equal(t["criterion"], r["criterion"])
+    _topo_equal(t, r)
+    assert len(t["active"]) > 0
+    for _ in range(2):
+        a.step(15)
+        before = a.topology()
+        _, vel = a.read_root()
+        a.step(1)
+        after = a.topology()
+        o.set_topology(before["block_slot"], before["slot_to_block"], before["free_list"], before["free_count"])
+        o.refine_from_vel(vel)
+        ro = o.read()
+        assert np.array_equal(after["criterion"], ro["criterion"])
+        _topo_equal(after, ro)
+    a.close()
+    o.close()
+
+
+def test_amr_cylinder_1024x256_fields_and_drag_against_fp64(lbm, oracle):
+    s, cfg = _cylinder(lbm)
+    a = lbm.Amr2D(cfg)
+    a.write_root(s["f"], s["vel"])
+    o = oracle.Amr2D(cfg)
+    o.write_root(s["f"].astype(np.float64), s["vel"].astype(np.float64))
+    n = 20  # refine rounds at macro-steps 0 and 16
+    a.step(n)
+    o.step(n)
+    ro = o.read()
+    t = a.topology()
+    _topo_equal(t, ro)
+    f0, vel0 = a.read_root()
+    f1, vel1 = a.read_pool()
+    fb2 = (cfg.rb * 2 + 4) ** 2
+    idx = np.concatenate([np.arange(k * fb2, (k + 1) * fb2) for k in t["active"]])  # live tiles only
+    eu0 = rel_l2(vel0.astype(np.float64), ro["vel0"])
+    eu1 = rel_l2(vel1[idx].astype(np.float64), ro["vel1"][idx])
+    ef = rel_l2(f0.astype(np.float64), ro["f0"])
+    force = a.forces()
+    ed = abs(force[0] - ro["force"][0]) / abs(ro["force"][0])
+    print(f"AMR 1024x256: root u {eu0:.3e}, pool u {eu1:.3e}, root f {ef:.3e}, drag {ed:.3e}")
+    a.close()
+    o.close()
+    assert eu0 <= 1e-4 and eu1 <= 1e-4
+    assert ef <= 1e-6
+    assert ed <= 1e-3
+
+
+def test_batch_slice_of_the_512_domain_workload_against_fp64(lbm, oracle):
+    from getting_air_b200 import scenarios as sc
+    doms = sc.batched_domains(count=512, seed=12345)[::16]
+    assert len(doms) == 32
+    w = lbm.lattice_tables(9)["w"]
+    cfgs = [lbm.config_from(9, d["dims"], **d["kw"]) for d in doms]
+    seeds = [sc.seed_domain(d, w) for d in doms]
+    b = lbm.Batch(cfgs)
+    for k, f0 in enumerate(seeds):
+        b.write_f(k, f0)
+    steps = 50
+    b.step(steps)
+    worst = 0.0
+    for k, (cfg, f0) in enumerate(zip(cfgs, seeds)):
+        m = b.read_mac(k).astype(np.float64)
+        _, om, _ = oracle.run(cfg, f0.astype(np.float64), steps)
+        e = rel_l2(m[:, 1:3], om[:, 1:3])
+        worst = max(worst, e)
+        assert e <= 1e-5, f"domain {k} ({doms[k]['kind']} {doms[k]['dims'][0]}^2): u relL2 {e:.3e}"
+        assert rel_l2(m[:, 0], om[:, 0]) <= 1e-6
+    b.close()
+    print(f"batch slice: worst u relL2 {worst:.3e} over {len(doms)} domains, sizes "
+          f"{min(d['dims'][0] for d in doms)}..{max(d['dims'][0] for d in doms)}")
