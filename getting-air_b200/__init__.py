@@ -95,7 +95,7 @@ class Config(C.Structure):
                 ("chi_eps", C.c_float), ("sponge_w", C.c_float),
                 ("sponge_axis", C.c_int32 * 3), ("sponge_u", C.c_float * 3),
                 ("body", Body), ("storage", C.c_int32), ("window", C.c_int32 * 3),
-                ("win_anchor", C.c_int32 * 3), ("reserved", C.c_int32 * 1)]
+                ("win_anchor", C.c_int32 * 3), ("trt", C.c_int32), ("trt_lambda", C.c_float)]
 
 
 class Amr3DConfig(C.Structure):
@@ -135,6 +135,10 @@ def _load() -> C.CDLL:
         "lbm_abi_version": ([], I),
         "lbm_config_default": ([C.POINTER(Config), I, I, I, I], I),
         "lbm_create": ([C.POINTER(Config), C.POINTER(P)], I),
+        "lbm_create_slab": ([C.POINTER(Config), I, I, C.POINTER(P)], I),
+        "lbm_slab_halo_bytes": ([P], C.c_int64),
+        "lbm_slab_pack": ([P, P, P], I),
+        "lbm_slab_unpack": ([P, P, P], I),
         "lbm_destroy": ([P], None),
         "lbm_last_error": ([P], C.c_char_p),
         "lbm_set_stream": ([P, P], I),
@@ -205,6 +209,8 @@ def _load() -> C.CDLL:
         "lbm_step_noalloc": ([C.POINTER(Config), P, P, P, P, P], I),
         "lbm_noalloc_last_error": ([], C.c_char_p),
         "lbm_tau_at_level": ([C.c_double, I], C.c_double),
+        "lbm_trt_tau_minus": ([C.c_double, C.c_double], C.c_double),
+        "lbm_trt_lambda": ([C.c_double, C.c_double], C.c_double),
         "lbm_dc_rescale_c2f": ([C.c_double, C.c_double], C.c_double),
         "lbm_dc_rescale_f2c": ([C.c_double, C.c_double], C.c_double),
         "lbm_tau_chain_singularity": ([C.c_double, I, C.c_double], I),
@@ -213,6 +219,7 @@ def _load() -> C.CDLL:
         "lbm_release_assignment": ([C.POINTER(C.c_int32), I, I, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], I),
         "lbm_active_slot_list": ([C.POINTER(C.c_int32), I, C.POINTER(C.c_int32)], I),
         "lbm_cascade21": ([C.POINTER(C.POINTER(C.c_uint8)), I, I, I], I),
+        "lbm_cascade21_device": ([C.POINTER(C.POINTER(C.c_uint8)), I, I, I, P], I),
         "lbm_lattice_tables": ([I, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), F, C.POINTER(C.c_int32)], I),
         "lbm_set_free_body": ([P, C.POINTER(BodyState), C.POINTER(BodyOpts)], I),
@@ -332,13 +339,20 @@ class Solver:
     ``totals`` (readConservedTotals / readStats), ``read_mac``, ``read_f``.
     """
 
-    def __init__(self, cfg: Config):
+    def __init__(self, cfg: Config, slab: tuple | None = None):
+        """slab = (z0, nz_local): planes [z0, z0 + nz_local) of the domain
+        (lbm_create_slab); its arrays then cover those planes only."""
         self.cfg = cfg
         self.q = cfg.q
-        self.dims = (cfg.nx, cfg.ny, cfg.nz)
-        self.ncells = cfg.nx * cfg.ny * cfg.nz
+        self.slab = slab
+        nz = cfg.nz if slab is None else int(slab[1])
+        self.dims = (cfg.nx, cfg.ny, nz)
+        self.ncells = cfg.nx * cfg.ny * nz
         h = C.c_void_p()
-        rc = lib.lbm_create(C.byref(cfg), C.byref(h))
+        if slab is None:
+            rc = lib.lbm_create(C.byref(cfg), C.byref(h))
+        else:
+            rc = lib.lbm_create_slab(C.byref(cfg), int(slab[0]), int(slab[1]), C.byref(h))
         if rc:
             raise LbmError(rc, lib.lbm_last_error(None).decode())
         self._h = h
@@ -414,6 +428,18 @@ class Solver:
 
     def step(self, n: int = 1):
         self._check(lib.lbm_step(self._h, int(n)))
+
+    # ---- slabs (lbm_create_slab) ----
+    def halo_bytes(self) -> int:
+        return int(lib.lbm_slab_halo_bytes(self._h))
+
+    def pack(self, send_lo_ptr: int, send_hi_ptr: int):
+        """The populations leaving through the bottom / top face into device buffers."""
+        self._check(lib.lbm_slab_pack(self._h, C.c_void_p(send_lo_ptr), C.c_void_p(send_hi_ptr)))
+
+    def unpack(self, recv_lo_ptr: int, recv_hi_ptr: int):
+        """The neighbours' populations into the ghost planes below / above."""
+        self._check(lib.lbm_slab_unpack(self._h, C.c_void_p(recv_lo_ptr), C.c_void_p(recv_hi_ptr)))
 
     def resample(self, **kw):
         """The field on a voxel box (volume_spec keywords; `level`, `out`)."""
@@ -687,6 +713,16 @@ def tau_at_level(tau0: float, m: int) -> float:
     return float(lib.lbm_tau_at_level(tau0, m))
 
 
+def trt_tau_minus(tau_plus: float, lam: float) -> float:
+    """tau_- of the TRT collision for a given Lambda (plans/TRT.md sec 8.1 tauMinusOf)."""
+    return float(lib.lbm_trt_tau_minus(tau_plus, lam))
+
+
+def trt_lambda(tau_plus: float, tau_minus: float) -> float:
+    """Lambda = (tau_+ - 1/2)(tau_- - 1/2) (plans/TRT.md sec 8.1 lambdaOf)."""
+    return float(lib.lbm_trt_lambda(tau_plus, tau_minus))
+
+
 def dc_rescale_c2f(tc: float, tf: float) -> float:
     return float(lib.lbm_dc_rescale_c2f(tc, tf))
 
@@ -739,6 +775,19 @@ def cascade21(want_levels, levels: int, nbx1: int, nby1: int):
     n = lib.lbm_cascade21(ptrs, levels, nbx1, nby1)
     if n < 0:
         raise LbmError(n, "cascade21")
+    return masks, int(n)
+
+
+def cascade21_device(want_levels, levels: int, nbx1: int, nby1: int, stream_ptr: int | None = None):
+    """cascade21 run by the device kernels (amr_cascade.wgsl's completeQuads
+    and balance). Same arguments and result as cascade21."""
+    masks = [None] + [np.ascontiguousarray(want_levels[m], np.uint8).ravel().copy() for m in range(1, levels)]
+    ptrs = (C.POINTER(C.c_uint8) * levels)()
+    for m in range(1, levels):
+        ptrs[m] = masks[m].ctypes.data_as(C.POINTER(C.c_uint8))
+    n = lib.lbm_cascade21_device(ptrs, levels, nbx1, nby1, C.c_void_p(stream_ptr or 0))
+    if n < 0:
+        raise LbmError(n, "cascade21_device")
     return masks, int(n)
 
 

@@ -1290,6 +1290,9 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   int rc = amr3_validate(c, why);
   if (rc) return afail(nullptr, rc, why);
   if (validate_config(&c->root, why)) return afail(nullptr, LBM_EINVAL, why);
+  // the pool's transfers rescale one relaxation time (plans/TRT.md sec 8.0(4)
+  // splits them per parity): the hierarchy stays BGK
+  if (c->root.trt) return afail(nullptr, LBM_ENOTSUP, "the TRT collision runs in dense, batched and served domains, not in AMR hierarchies");
   if (c->refine == LBM_REFINE_LIST && !block_want) return afail(nullptr, LBM_EINVAL, "refine = list needs block flags");
   auto *a = new lbm_amr3d();
   a->cfg = *c;
@@ -1409,11 +1412,12 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
   a->stream = a->own;
   for (int k = 0; k < 2; ++k)
-    if ((e = cudaMemset(a->fp[k], 0, fpb))) return bail(e, "memset pool f");
-  if (a->flux && (e = cudaMemset(a->flux, 0, (size_t)p.N * 16))) return bail(e, "memset flux");
-  if ((e = cudaMemset(a->macp, 0, (size_t)p.P * 16))) return bail(e, "memset pool mac");
-  cudaMemcpy(a->d_block_slot, a->block_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice);
-  cudaMemcpy(a->d_slot_to_block, a->slot_to_block.data(), a->capacity * sizeof(int), cudaMemcpyHostToDevice);
+    if ((e = cudaMemsetAsync(a->fp[k], 0, fpb, a->own))) return bail(e, "memset pool f");
+  if (a->flux && (e = cudaMemsetAsync(a->flux, 0, (size_t)p.N * 16, a->own))) return bail(e, "memset flux");
+  if ((e = cudaMemsetAsync(a->macp, 0, (size_t)p.P * 16, a->own))) return bail(e, "memset pool mac");
+  cudaMemcpyAsync(a->d_block_slot, a->block_slot.data(), nb * sizeof(int), cudaMemcpyHostToDevice, a->own);
+  cudaMemcpyAsync(a->d_slot_to_block, a->slot_to_block.data(), a->capacity * sizeof(int), cudaMemcpyHostToDevice,
+                  a->own);
   {
     std::vector<uint32_t> cl;
     cl.reserve(p.T3);
@@ -1424,7 +1428,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
             auto in = [&](int j) { return j >= kAmrGhost && j < kAmrGhost + p.RB2; };
             if ((in(x) && in(y) && in(z)) == (pass == 0)) cl.push_back(x | (y << 8) | (z << 16));
           }
-    cudaMemcpy(a->d_cells, cl.data(), cl.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(a->d_cells, cl.data(), cl.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, a->own);
   }
   if (a->dynamic) {
     std::vector<unsigned char> flag(nb, 0);
@@ -1432,11 +1436,11 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     std::vector<int> fl(nfl, 0);
     for (int i = 0; i < nfree; ++i) fl[i] = a->initial + i;
     const int counts[4] = {nfree, 0, nfree, 0};
-    cudaMemset(a->d_want, 0, nb);
-    cudaMemset(a->d_slot_new, 0, a->capacity);
-    cudaMemcpy(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice);
-    cudaMemcpy(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice);
-    cudaMemcpy(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice);
+    cudaMemsetAsync(a->d_want, 0, nb, a->own);
+    cudaMemsetAsync(a->d_slot_new, 0, a->capacity, a->own);
+    cudaMemcpyAsync(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice, a->own);
+    cudaMemcpyAsync(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice, a->own);
+    cudaMemcpyAsync(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, a->own);
     if (c->q_abs > 0) {
       // main-3d.js: REFINE_THRESH = 1/2 log2 max(Q_ABS, 1e-30), COARSEN_THRESH
       // one hysteresis band lower, both as thresholds on Q itself
@@ -1445,12 +1449,15 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
       a->q_hold = (float)(qr * std::exp2(-2.0 * (double)c->q_hyst));
     }
   }
-  if (p.n_iface) cudaMemcpy(a->d_iface, a->iface.data(), p.n_iface * sizeof(int), cudaMemcpyHostToDevice);
-  if ((e = cudaMemset(a->counter, 0, sizeof(unsigned int)))) return bail(e, "counter");
-  if ((e = cudaMemset(a->force_out, 0, kForceSlots * sizeof(double)))) return bail(e, "force");
-  if ((e = cudaMemset(a->tot_counter, 0, sizeof(unsigned int)))) return bail(e, "totals");
+  if (p.n_iface)
+    cudaMemcpyAsync(a->d_iface, a->iface.data(), p.n_iface * sizeof(int), cudaMemcpyHostToDevice, a->own);
+  if ((e = cudaMemsetAsync(a->counter, 0, sizeof(unsigned int), a->own))) return bail(e, "counter");
+  if ((e = cudaMemsetAsync(a->force_out, 0, kForceSlots * sizeof(double), a->own))) return bail(e, "force");
+  if ((e = cudaMemsetAsync(a->tot_counter, 0, sizeof(unsigned int), a->own))) return bail(e, "totals");
   if ((e = cudaMallocHost(&a->host_out, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
-  if ((e = cudaDeviceSynchronize())) return bail(e, "set-up");
+  // set-up is ordered on the hierarchy's own stream: it waits for nothing
+  // else on the device (a server admits hierarchies while ticks run)
+  if ((e = cudaStreamSynchronize(a->own))) return bail(e, "set-up");
   p.block_slot = a->d_block_slot;
   p.slot_to_block = a->d_slot_to_block;
   p.iface = a->dynamic ? nullptr : a->d_iface;

@@ -3,13 +3,47 @@
 // deterministic free-list grant/release order, the active-slot list and the
 // 2:1 cascade closure. The device manager (amr2d.cu) applies the same grant
 // and release order; these are the specification it is tested against.
+// The cascade closure also runs on the device (lbm_cascade21_device), as the
+// reference's amr_cascade.wgsl does, and is tested against the host rule.
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/lbm.h"
+
+namespace {
+
+// amr_cascade.wgsl:114-129 completeQuads: a wanted block at level m >= 2
+// wants its whole quad (tiles are granted in quads). Every write is "= 1",
+// so threads writing the same byte agree and the order does not matter.
+__global__ void cascade_complete_quads(uint8_t *__restrict__ want, int nbx, int nby) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbx * nby || !want[b]) return;
+  const int bx = b % nbx, by = b / nbx;
+  const int qx0 = bx & ~1, qy0 = by & ~1;
+  for (int k = 0; k < 4; ++k) want[(qy0 + (k >> 1)) * nbx + qx0 + (k & 1)] = 1;
+}
+
+// amr_cascade.wgsl:138-157 balance: a wanted block at level m wants the
+// parents of itself and of its 8 periodic neighbours at level m - 1 (a
+// different array, so the pass has no read/write hazard).
+__global__ void cascade_balance(const uint8_t *__restrict__ want, uint8_t *__restrict__ parent, int nbx, int nby) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbx * nby || !want[b]) return;
+  const int bx = b % nbx, by = b / nbx;
+  const int pbx = nbx >> 1;
+  for (int k = 0; k < 9; ++k) {
+    const int nx = (bx + nbx + k % 3 - 1) % nbx, ny = (by + nby + k / 3 - 1) % nby;
+    parent[(ny >> 1) * pbx + (nx >> 1)] = 1;
+  }
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -18,6 +52,10 @@ double lbm_tau_at_level(double tau0, int m) {
   for (int i = 0; i < m; ++i) t = 2.0 * t - 0.5;
   return t;
 }
+
+double lbm_trt_tau_minus(double tau_plus, double lambda) { return 0.5 + lambda / (tau_plus - 0.5); }
+
+double lbm_trt_lambda(double tau_plus, double tau_minus) { return (tau_plus - 0.5) * (tau_minus - 0.5); }
 
 double lbm_dc_rescale_c2f(double tau_coarse, double tau_fine) {
   return 0.5 * (tau_fine - 1.0) / (tau_coarse - 1.0);
@@ -106,6 +144,44 @@ int lbm_cascade21(uint8_t **want, int levels, int nbx1, int nby1) {
         }
     }
   }
+  return added;
+}
+
+int lbm_cascade21_device(uint8_t **want, int levels, int nbx1, int nby1, void *cuda_stream) {
+  if (!want || levels < 2 || nbx1 <= 0 || nby1 <= 0) return LBM_EINVAL;
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  std::vector<size_t> off(levels + 1, 0);
+  for (int m = 1; m < levels; ++m) {
+    if (!want[m]) return LBM_EINVAL;
+    off[m + 1] = off[m] + (size_t)(nbx1 << (m - 1)) * (size_t)(nby1 << (m - 1));
+  }
+  const size_t total = off[levels];
+  uint8_t *d = nullptr;
+  if (cudaMallocAsync((void **)&d, total, st) != cudaSuccess) return LBM_ENOMEM;
+  cudaError_t e = cudaSuccess;
+  for (int m = 1; m < levels && !e; ++m)
+    e = cudaMemcpyAsync(d + off[m], want[m], off[m + 1] - off[m], cudaMemcpyHostToDevice, st);
+  // one sweep, deepest first (amr_cascade.wgsl: the rule only propagates
+  // down the levels, so this is the fixed point)
+  for (int m = levels - 1; m >= 2 && !e; --m) {
+    const int W = nbx1 << (m - 1), H = nby1 << (m - 1);
+    const int grid = (W * H + 127) / 128;
+    cascade_complete_quads<<<grid, 128, 0, st>>>(d + off[m], W, H);
+    cascade_balance<<<grid, 128, 0, st>>>(d + off[m], d + off[m - 1], W, H);
+    e = cudaGetLastError();
+  }
+  std::vector<uint8_t> out(total);
+  if (!e) e = cudaMemcpyAsync(out.data(), d, total, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) return LBM_ECUDA;
+  int added = 0;
+  for (int m = 1; m < levels; ++m)
+    for (size_t i = 0; i < off[m + 1] - off[m]; ++i) {
+      const uint8_t v = out[off[m] + i] ? 1 : 0;
+      added += v && !want[m][i];
+      want[m][i] = v;
+    }
   return added;
 }
 

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
       for (int c = td.y + threadIdx.x; c < end; c += THREADS) {
         const int x = c % nx, r = c / nx;
         CellForce cf;
-        cell3<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, region, cf);
+        cell3_any<Q, S>(fin, fout, mac, sp, x, r % ny, r / ny, region, cf);
         if (region) acc.add(cf);
       }
     }

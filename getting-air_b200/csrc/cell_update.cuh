@@ -238,10 +238,19 @@ struct NullSink {
   __device__ __forceinline__ void put(int, float) {}
 };
 
-template <class L, int Q, class Sink>
+// TRT (dw = omega_- - omega != 0): the odd part of each pair relaxes at
+// omega_- instead, in the reference's delta form (plans/TRT.md sec 8.0(1)):
+//   f_i += -dw (f_i^- - feq_i^-) - dw/2 S_i^-,
+//   f_i^- = (f_i - f_j)/2, feq_i^- = 3 w rho e.u, S_i^- = 3 w e.F,
+// the odd forcing prefactor becoming (1 - omega_-/2); the sponge blend
+// scales it by (1 - s) like the rest of the collided value, and f_j takes
+// the negative. TRT = false is the BGK loop alone (dw ignored); the kernels
+// pick the instantiation from dw != 0 per launch, so the BGK code keeps its
+// register allocation.
+template <class L, int Q, class Sink, bool TRT = false>
 __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, float ux, float uy, float uz, float Fx,
                                               float Fy, float Fz, float omg, float spw, const float *ftarget,
-                                              Sink &sink) {
+                                              Sink &sink, float dw = 0.f) {
   const float usq = ux * ux + uy * uy + uz * uz;
   const float uF = ux * Fx + uy * Fy + uz * Fz;
   const float ks = 1.0f - spw;
@@ -250,19 +259,39 @@ __device__ __forceinline__ void collide_store(const float (&f)[Q], float rho, fl
   const float keep = (1.0f - omg) * ks;
   const float c0 = fmaf(a, fmaf(-1.5f, usq, 1.0f), -3.0f * b * uF);
   sink.put(0, fmaf(keep, f[0], fmaf(spw, ftarget[0], L::w(0) * c0)));
+  if (!TRT) {
 #pragma unroll
-  for (int i = 1; i < Q; ++i) {
-    const int j = L::opp(i);
-    if (j < i) continue;
-    const float ex = (float)L::ex(i), ey = (float)L::ey(i), ez = (float)L::ez(i);
-    const float w = L::w(i);
-    const float eu = ex * ux + ey * uy + ez * uz;
-    const float eF = ex * Fx + ey * Fy + ez * Fz;
-    const float t = fmaf((9.0f * w) * b, eF, ((4.5f * w) * a) * eu);
-    const float A = fmaf(eu, t, w * c0);
-    const float B = fmaf((3.0f * w) * a, eu, ((3.0f * w) * b) * eF);
-    sink.put(i, fmaf(keep, f[i], fmaf(spw, ftarget[i], A + B)));
-    sink.put(j, fmaf(keep, f[j], fmaf(spw, ftarget[j], A - B)));
+    for (int i = 1; i < Q; ++i) {
+      const int j = L::opp(i);
+      if (j < i) continue;
+      const float ex = (float)L::ex(i), ey = (float)L::ey(i), ez = (float)L::ez(i);
+      const float w = L::w(i);
+      const float eu = ex * ux + ey * uy + ez * uz;
+      const float eF = ex * Fx + ey * Fy + ez * Fz;
+      const float t = fmaf((9.0f * w) * b, eF, ((4.5f * w) * a) * eu);
+      const float A = fmaf(eu, t, w * c0);
+      const float B = fmaf((3.0f * w) * a, eu, ((3.0f * w) * b) * eF);
+      sink.put(i, fmaf(keep, f[i], fmaf(spw, ftarget[i], A + B)));
+      sink.put(j, fmaf(keep, f[j], fmaf(spw, ftarget[j], A - B)));
+    }
+  } else {
+    const float kd = -ks * dw;
+    const float rho3 = 3.0f * rho;
+#pragma unroll
+    for (int i = 1; i < Q; ++i) {
+      const int j = L::opp(i);
+      if (j < i) continue;
+      const float ex = (float)L::ex(i), ey = (float)L::ey(i), ez = (float)L::ez(i);
+      const float w = L::w(i);
+      const float eu = ex * ux + ey * uy + ez * uz;
+      const float eF = ex * Fx + ey * Fy + ez * Fz;
+      const float t = fmaf((9.0f * w) * b, eF, ((4.5f * w) * a) * eu);
+      const float A = fmaf(eu, t, w * c0);
+      const float B = fmaf((3.0f * w) * a, eu, ((3.0f * w) * b) * eF);
+      const float D = kd * fmaf(0.5f, f[i] - f[j], w * fmaf(1.5f, eF, -rho3 * eu));
+      sink.put(i, fmaf(keep, f[i], fmaf(spw, ftarget[i], A + B)) + D);
+      sink.put(j, fmaf(keep, f[j], fmaf(spw, ftarget[j], A - B)) - D);
+    }
   }
 }
 
@@ -288,6 +317,34 @@ __device__ __forceinline__ float sponge_weight_inv(float d, float inv_sw) {
   return w * w * (3.0f - 2.0f * w);
 }
 
+// ---- row-major walks without divisions --------------------------------------
+// A thread of a multi-domain launch visits cells c0, c0 + step, c0 + 2 step,
+// ... of one domain. Its first cell takes the divisions; every later one
+// adds the step's own decomposition (dx, dy, dz) with one carry per axis
+// (x + dx < 2 nx and y + dy + 1 < 2 ny, so a single subtraction suffices).
+struct CellWalk {
+  int x, y, z;
+  int dx, dy, dz;
+  int nx, ny;
+  __device__ __forceinline__ CellWalk(int c0, int step, int nx_, int ny_) : nx(nx_), ny(ny_) {
+    const int r = c0 / nx;
+    x = c0 - r * nx;
+    y = r % ny;
+    z = r / ny;
+    const int rs = step / nx;
+    dx = step - rs * nx;
+    dy = rs % ny;
+    dz = rs / ny;
+  }
+  __device__ __forceinline__ void advance() {
+    x += dx;
+    y += dy;
+    z += dz;
+    if (x >= nx) { x -= nx; ++y; }
+    if (y >= ny) { y -= ny; ++z; }
+  }
+};
+
 // ---- 3D cell update ---------------------------------------------------------
 // Pull-stream (periodic sources, then bounce-back patches: body first with
 // Ladd's correction at local rho_w, then walls), moments, Guo forcing with
@@ -298,14 +355,18 @@ __device__ __forceinline__ float sponge_weight_inv(float d, float inv_sw) {
 // Everything after the pull gather, for one cell: bounce-back patches,
 // moments, forcing, collision into `sink`, mac, force. `fi` is the domain's
 // base in the input arena (own-cell loads of the bounce-back patches).
-template <int Q, typename S, class Sink>
+template <int Q, typename S, class Sink, bool TRT = false>
 __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[Q], float *__restrict__ mac,
                                            const StepParams &p, int x, int y, int z, bool force, CellForce &cf,
                                            Sink &sink) {
   using L = Lattice<Q>;
-  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  // z indexes the stored planes; the physics (body, walls, sponge, reach
+  // box) sees the domain's own z, which for a slab is offset by p.zoff in a
+  // domain p.nzg planes deep (both the identity for a whole domain)
+  const int nx = p.nx, ny = p.ny, nz = p.nzg;
   const int64_t n = p.n;
   const int cell = (z * ny + y) * nx + x;
+  z += p.zoff;
   const V3 pos = {(float)x, (float)y, (float)z};
   float phi = 1e30f;
   V3 us = {0.f, 0.f, 0.f};
@@ -420,7 +481,7 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
   // 4. Collide + sponge blend, 5. solid interior held at feq(1, u_body).
   const bool in_solid = p.solid_eq && bbody && phi < 0.f;
   if (!in_solid) {
-    collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, sink);
+    collide_store<L, Q, Sink, TRT>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega, spw, p.ftarget, sink, p.trt_dw);
   } else {
     const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
 #pragma unroll
@@ -495,7 +556,9 @@ __device__ __forceinline__ void gather3(const S *__restrict__ fi, const StepPara
   }
 }
 
-template <int Q, typename S>
+// TRT: the collision is the two-relaxation-time one; callers pass
+// p.trt_dw != 0 (see collide_store).
+template <int Q, typename S, bool TRT = false>
 __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__ fout,
                                       float *__restrict__ mac, const StepParams &p, int x, int y,
                                       int z, bool force, CellForce &cf) {
@@ -503,7 +566,17 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
   float f[Q];
   gather3<Q, S>(fi, p, x, y, z, f);
   MemSink<S> sink{fout + p.base, p.n, (z * p.ny + y) * p.nx + x, p.pk};
-  cell3_core<Q, S>(fi, f, mac, p, x, y, z, force, cf, sink);
+  cell3_core<Q, S, MemSink<S>, TRT>(fi, f, mac, p, x, y, z, force, cf, sink);
+}
+
+// cell3 with the collision picked from the launch's parameters (a
+// warp-uniform branch), for kernels that do not instantiate per collision.
+template <int Q, typename S>
+__device__ __forceinline__ void cell3_any(const S *__restrict__ fin, S *__restrict__ fout,
+                                          float *__restrict__ mac, const StepParams &p, int x, int y,
+                                          int z, bool force, CellForce &cf) {
+  if (p.trt_dw != 0.f) cell3<Q, S, true>(fin, fout, mac, p, x, y, z, force, cf);
+  else cell3<Q, S, false>(fin, fout, mac, p, x, y, z, force, cf);
 }
 
 // A cell that only fluid can reach: no body link within reach (or no body),
@@ -512,7 +585,7 @@ __device__ __forceinline__ void cell3(const S *__restrict__ fin, S *__restrict__
 // so its Guo force is the body force alone (rho chi (u_s - u*) = +-0, and
 // +-0 + F = F) and nothing is patched; this is that path with the dead
 // tests taken out, to the bit.
-template <int Q, typename S>
+template <int Q, typename S, bool TRT = false>
 __device__ __forceinline__ void cell3_fluid(const S *__restrict__ fin, S *__restrict__ fout,
                                             float *__restrict__ mac, const StepParams &p, int x, int y, int z) {
   using L = Lattice<Q>;
@@ -531,12 +604,14 @@ __device__ __forceinline__ void cell3_fluid(const S *__restrict__ fin, S *__rest
   if (p.sponge_w > 0.f) {
     const float dx = p.sax ? fminf((float)x, (float)(p.nx - 1) - (float)x) : 1e30f;
     const float dy = p.say ? fminf((float)y, (float)(p.ny - 1) - (float)y) : 1e30f;
-    const float dz = p.saz ? fminf((float)z, (float)(p.nz - 1) - (float)z) : 1e30f;
+    const float zg = (float)(z + p.zoff);
+    const float dz = p.saz ? fminf(zg, (float)(p.nzg - 1) - zg) : 1e30f;
     spw = sponge_weight_inv(fminf(dx, fminf(dy, dz)), p.sponge_inv);
   }
   const int cell = (z * p.ny + y) * p.nx + x;
   MemSink<S> sink{fout + p.base, p.n, cell, p.pk};
-  collide_store<L, Q>(f, rho, ux, uy, uz, p.fx, p.fy, p.fz, p.omega, spw, p.ftarget, sink);
+  collide_store<L, Q, MemSink<S>, TRT>(f, rho, ux, uy, uz, p.fx, p.fy, p.fz, p.omega, spw, p.ftarget, sink,
+                                       p.trt_dw);
   if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, uz);
 }
 

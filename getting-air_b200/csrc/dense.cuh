@@ -27,10 +27,17 @@ struct Pack {
 // Per-step constants of the fused stream-collide kernels. Mirrors the
 // override constants of common_d3_step.wgsl:125-213 / lbm_step.wgsl:36-135.
 struct StepParams {
-  int nx, ny, nz;
+  int nx, ny, nz;       // stored extent (a slab's nz counts its two ghost planes)
+  // A z-slab of a larger domain (lbm_create_slab): stored plane z is the
+  // domain's plane z + zoff, the domain is nzg planes deep, and the step
+  // covers the stored planes [zlo, nz - zlo) (zlo = 1: the ghost planes
+  // below and above are filled by the halo exchange). A whole domain has
+  // zoff = 0, nzg = nz, zlo = 0.
+  int zoff, nzg, zlo;
   int64_t n;            // plane stride of the arena the domain lives in (cells)
   int64_t base;         // arena index of the domain's cell 0
   float omega;          // 1 / tau
+  float trt_dw;         // omega_- - omega of the TRT collision; 0 = BGK
   float fx, fy, fz;     // uniform Guo body force
   int wall_x, wall_y, wall_z;
   float wall_u0, wall_u1;  // D2Q9 moving y-walls
@@ -133,6 +140,10 @@ cudaError_t launch_force_pass(int q, int storage, const void *f_in, const StepPa
                               cudaStream_t st);
 cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out, int64_t n, const Pack &pk,
                            cudaStream_t st);
+// The equilibrium of one state (rho, ux, uy, uz) in every cell, with that
+// state written to mac: the same bits as launch_init_eq of a uniform field.
+cudaError_t launch_init_uniform(int q, int storage, const float rho_u[4], float *mac_out, void *f_out, int64_t n,
+                                const Pack &pk, cudaStream_t st);
 cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n, const Pack &pk,
                         cudaStream_t st);
 cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, int64_t n, const Pack &pk,
@@ -140,8 +151,9 @@ cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, i
 // Totals over the current f, FP64; `partials` holds totals_partials() * 8
 // doubles, `counter` one zeroed unsigned int.
 int totals_blocks();
+// n cells from f (a plane stride of `stride` cells, n when 0).
 cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, const Pack &pk, double *partials,
-                          unsigned int *counter, double *out, cudaStream_t st);
+                          unsigned int *counter, double *out, cudaStream_t st, int64_t stride = 0);
 
 // One step of every domain of a batch (batch.cu).
 cudaError_t launch_batch_step(int q, int storage, int threads, int ctas, cudaStream_t st, const void *fin,

@@ -80,26 +80,30 @@ __device__ __forceinline__ int block_kind(const StepParams &p, int lo, int hi, i
     if (!p.bb || !p.nbox_on) return kGeneral;
     if (span_hits(lo, hi, p.nbox[0], p.nbox[1] - p.nbox[0], p.nx) &&
         span_hits(y, y, p.nbox[2], p.nbox[3] - p.nbox[2], p.ny) &&
-        span_hits(z, z, p.nbox[4], p.nbox[5] - p.nbox[4], p.nz))
+        span_hits(z, z, p.nbox[4], p.nbox[5] - p.nbox[4], p.nzg))
       return kGeneral;
   }
   if ((p.wall_x && (lo == 0 || hi == p.nx - 1)) || (p.wall_y && (y == 0 || y == p.ny - 1)) ||
-      (p.wall_z && (z == 0 || z == p.nz - 1)))
+      (p.wall_z && (z == 0 || z == p.nzg - 1)))
     return kGeneral;
   return kFluid;
 }
 
-template <int Q, typename S>
+template <int Q, typename S, bool TRT>
 __device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__restrict__ fout,
                                               float *__restrict__ mac, const StepParams &p) {
   sum_previous(p);
   const int x = blockIdx.x * kStepThreads + threadIdx.x;
-  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-  // the force region, read modulo the grid (it can cross a windowed seam)
-  int dx = bx - p.rbx0, dy = by - p.rby0, dz = bz - p.rbz0;
+  // bz: the stored plane (a slab skips its ghost plane below); zg: the
+  // domain's plane, which the force region and the block kind are in
+  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z + p.zlo;
+  const int zg = bz + p.zoff;
+  // the force region, read modulo the grid (it can cross a windowed seam;
+  // a slab's region is its own share, with no seam)
+  int dx = bx - p.rbx0, dy = by - p.rby0, dz = zg - p.rbz0;
   dx += dx < 0 ? (int)gridDim.x : 0;
   dy += dy < 0 ? (int)gridDim.y : 0;
-  dz += dz < 0 ? (int)gridDim.z : 0;
+  dz += (dz < 0 && p.zlo == 0) ? p.nzg : 0;
   const int rx = p.rbx1 - p.rbx0, ry = p.rby1 - p.rby0, rz = p.rbz1 - p.rbz0;
   const bool region = p.force_on && dx < rx && dy < ry && dz < rz;
   // The fluid path pays for 16-bit storage (issue-bound: 0.1106 against
@@ -107,13 +111,13 @@ __device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__re
   // step is bound by memory latency and ran 0.1123 against 0.1110 ms with
   // it: FP32 takes the general path everywhere.
   const int lo = bx * kStepThreads, hi = min(lo + kStepThreads, p.nx) - 1;
-  const int kind = std::is_same<S, float>::value ? kGeneral : block_kind(p, lo, hi, by, bz, region);
+  const int kind = std::is_same<S, float>::value ? kGeneral : block_kind(p, lo, hi, by, zg, region);
   if (kind == kFluid) {
-    if (x < p.nx) cell3_fluid<Q, S>(fin, fout, mac, p, x, by, bz);
+    if (x < p.nx) cell3_fluid<Q, S, TRT>(fin, fout, mac, p, x, by, bz);
     return;
   }
   CellForce cf;
-  if (x < p.nx) cell3<Q, S>(fin, fout, mac, p, x, by, bz, region, cf);
+  if (x < p.nx) cell3<Q, S, TRT>(fin, fout, mac, p, x, by, bz, region, cf);
   if (region) {
     ForceAcc acc;
     acc.add(cf);
@@ -145,22 +149,22 @@ __device__ __forceinline__ void stage_pose(const StepParams &p, StepParams &sp) 
   __syncthreads();
 }
 
-template <int Q, typename S>
+template <int Q, typename S, bool TRT>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     d3_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
             const __grid_constant__ StepParams p) {
-  d3_step_block<Q, S>(fin, fout, mac, p);
+  d3_step_block<Q, S, TRT>(fin, fout, mac, p);
 }
 
 // The step of a free body: the pose comes from the device (written by the
 // force pass just before); no force reduction.
-template <int Q, typename S>
+template <int Q, typename S, bool TRT>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     d3_step_free(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
                  const __grid_constant__ StepParams p) {
   __shared__ StepParams sp;
   stage_pose(p, sp);
-  d3_step_block<Q, S>(fin, fout, mac, sp);
+  d3_step_block<Q, S, TRT>(fin, fout, mac, sp);
 }
 
 // Integrates the free body under the force just summed and publishes the
@@ -240,12 +244,16 @@ __global__ void __launch_bounds__(kStepThreads)
 
 // ---- seeding and storage conversion ----------------------------------------
 
-template <int Q, typename S>
-__global__ void init_eq(const float4 *__restrict__ mac, S *__restrict__ f, int64_t n, const Pack pk) {
+// f at equilibrium of the mac field; UNIFORM: of the one state `mu`, which
+// is also written to every cell of mac (a uniform seed needs no host data).
+template <int Q, typename S, bool UNIFORM = false>
+__global__ void init_eq(const float4 *__restrict__ mac, S *__restrict__ f, int64_t n, const Pack pk,
+                        float4 mu = {}, float4 *__restrict__ mac_out = nullptr) {
   using L = Lattice<Q>;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
-    const float4 m = mac[c];
+    const float4 m = UNIFORM ? mu : mac[c];
+    if (UNIFORM) mac_out[c] = mu;
     const float rho = m.x, ux = m.y, uy = m.z, uz = Q == 9 ? 0.f : m.w;
     const float usq = Q == 9 ? (ux * ux + uy * uy) : (ux * ux + uy * uy + uz * uz);
 #pragma unroll
@@ -284,8 +292,8 @@ constexpr int kTotalsBlocks = 148 * 4;
 
 template <int Q, typename S>
 __global__ void __launch_bounds__(kReduceThreads)
-    totals_kernel(const S *__restrict__ f, int64_t n, const Pack pk, double *partials, unsigned int *counter,
-                  double *out) {
+    totals_kernel(const S *__restrict__ f, int64_t n, int64_t stride, const Pack pk, double *partials,
+                  unsigned int *counter, double *out) {
   using L = Lattice<Q>;
   double mass = 0.0, px = 0.0, py = 0.0, pz = 0.0, bad = 0.0;
   double rmin = 1e300, rmax = -1e300, u2max = 0.0;
@@ -294,7 +302,7 @@ __global__ void __launch_bounds__(kReduceThreads)
     double rho = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const double v = (double)Codec<S>::ld(f + (int64_t)i * n + c, i, pk);
+      const double v = (double)Codec<S>::ld(f + (int64_t)i * stride + c, i, pk);
       rho += v;
       mx += v * L::ex(i);
       my += v * L::ey(i);
@@ -386,14 +394,18 @@ int grid_for(int64_t n, int threads) {
 namespace {
 cudaError_t launch_step_kernel(int q, int storage, const void *f_in, void *f_out, float *mac, const StepParams &p,
                                cudaStream_t st) {
-  dim3 grid((p.nx + kStepThreads - 1) / kStepThreads, p.ny, q == 9 ? 1 : p.nz);
+  dim3 grid((p.nx + kStepThreads - 1) / kStepThreads, p.ny, q == 9 ? 1 : p.nz - 2 * p.zlo);
   LBM_DISPATCH(q, storage, {
     if constexpr (Q == 9)
       d2_step<S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+    else if (p.pose_in && p.trt_dw != 0.f)
+      d3_step_free<Q, S, true><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
     else if (p.pose_in)
-      d3_step_free<Q, S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+      d3_step_free<Q, S, false><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+    else if (p.trt_dw != 0.f)
+      d3_step<Q, S, true><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
     else
-      d3_step<Q, S><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+      d3_step<Q, S, false><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
   });
 }
 }  // namespace
@@ -425,6 +437,13 @@ cudaError_t launch_init_eq(int q, int storage, const float *mac_in, void *f_out,
   LBM_DISPATCH(q, storage, init_eq<Q, S><<<grid_for(n, 256), 256, 0, st>>>((const float4 *)mac_in, (S *)f_out, n, pk));
 }
 
+cudaError_t launch_init_uniform(int q, int storage, const float rho_u[4], float *mac_out, void *f_out, int64_t n,
+                                const Pack &pk, cudaStream_t st) {
+  const float4 mu = make_float4(rho_u[0], rho_u[1], rho_u[2], rho_u[3]);
+  LBM_DISPATCH(q, storage, (init_eq<Q, S, true><<<grid_for(n, 256), 256, 0, st>>>(nullptr, (S *)f_out, n, pk, mu,
+                                                                                 (float4 *)mac_out)));
+}
+
 cudaError_t launch_pack(int q, int storage, const float *f32, void *f_store, int64_t n, const Pack &pk,
                         cudaStream_t st) {
   LBM_DISPATCH(q, storage, pack_planes<Q, S><<<grid_for(n, 256), 256, 0, st>>>(f32, (S *)f_store, n, pk));
@@ -438,8 +457,9 @@ cudaError_t launch_unpack(int q, int storage, const void *f_store, float *f32, i
 int totals_blocks() { return kTotalsBlocks; }
 
 cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, const Pack &pk, double *partials,
-                          unsigned int *counter, double *out, cudaStream_t st) {
-  LBM_DISPATCH(q, storage, (totals_kernel<Q, S><<<kTotalsBlocks, kReduceThreads, 0, st>>>((const S *)f, n, pk, partials, counter, out)));
+                          unsigned int *counter, double *out, cudaStream_t st, int64_t stride) {
+  if (stride <= 0) stride = n;
+  LBM_DISPATCH(q, storage, (totals_kernel<Q, S><<<kTotalsBlocks, kReduceThreads, 0, st>>>((const S *)f, n, stride, pk, partials, counter, out)));
 }
 
 }  // namespace lbm

@@ -29,6 +29,15 @@ int validate_config(const lbm_config *c, std::string &why) {
   if (n > 0x7fffffffLL) { why = "grid exceeds 2^31-1 cells"; return LBM_EINVAL; }
   if (!(c->tau > 0.5f) || !std::isfinite(c->tau)) { why = "tau must be finite and > 0.5"; return LBM_EINVAL; }
   if (c->storage < 0 || c->storage > 2) { why = "unknown storage"; return LBM_EINVAL; }
+  if (c->trt != 0 && c->trt != 1) { why = "trt must be 0 or 1"; return LBM_EINVAL; }
+  if (c->trt) {
+    // plans/TRT.md sec 8.0(7): the 2D solver stays BGK
+    if (c->q == 9) { why = "the TRT collision is 3D (the D2Q9 solver stays BGK)"; return LBM_EINVAL; }
+    if (!(c->trt_lambda > 0.f) || !std::isfinite(c->trt_lambda)) {
+      why = "trt_lambda must be finite and > 0";
+      return LBM_EINVAL;
+    }
+  }
   if (c->has_body) {
     const int sh = c->body.shape;
     if (c->q == 9 && sh != LBM_SHAPE_ELLIPSE) { why = "D2Q9 bodies are ellipses"; return LBM_EINVAL; }
@@ -74,7 +83,16 @@ Pack make_pack(const lbm_config &c) {
 
 void fill_step_params(const lbm_config &c, int64_t n, int64_t base, StepParams &p) {
   p.nx = c.nx; p.ny = c.ny; p.nz = c.nz; p.n = n; p.base = base;
+  p.zoff = 0; p.nzg = c.nz; p.zlo = 0;
   p.omega = 1.0f / c.tau;
+  // TRT: omega_- from tau_- = 1/2 + Lambda / (tau - 1/2), both in double and
+  // rounded once to f32 as the reference's OMEGA_M override is; the kernels
+  // take the difference (the delta form, plans/TRT.md sec 8.0(1)).
+  p.trt_dw = 0.f;
+  if (c.trt) {
+    const float omega_m = (float)(1.0 / lbm_trt_tau_minus((double)c.tau, (double)c.trt_lambda));
+    p.trt_dw = omega_m - p.omega;
+  }
   p.fx = c.force[0]; p.fy = c.force[1]; p.fz = c.q == 9 ? 0.f : c.force[2];
   p.wall_x = c.q == 9 ? 0 : c.wall[0];
   p.wall_y = c.wall[1];

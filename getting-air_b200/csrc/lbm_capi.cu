@@ -47,6 +47,12 @@ struct lbm_session {
   int cap[3] = {0, 0, 0};
   BodyPose *pose = nullptr;
   BodyDyn *dyn = nullptr;
+  // A z-slab of the domain cfg describes (lbm_create_slab): planes
+  // [z0, z0 + nzl) stored as planes 1..nzl between two ghost planes, so n
+  // counts nzl + 2 planes and `cells` the nzl the caller sees.
+  bool slab = false;
+  int z0 = 0, nzl = 0;
+  int64_t nxy = 0, cells = 0;
 };
 
 namespace {
@@ -119,7 +125,31 @@ void fill_params(lbm_session *s) {
   p.groups = s->force_groups;
   p.counter = s->force_counter;
   p.force_out = s->force_out;
-  set_force_region(s);
+  set_force_region(s);  // in the whole domain's planes
+  if (!s->slab) return;
+  // a slab: stored plane z is domain plane z + z0 - 1; its force region is
+  // its own share of the domain's (slabs take no window, so no seam)
+  p.nz = s->nzl + 2;
+  p.zoff = s->z0 - 1;
+  p.nzg = s->cfg.nz;
+  p.zlo = 1;
+  if (p.force_on) {
+    p.rbz0 = std::max(p.rbz0, s->z0);
+    p.rbz1 = std::min(p.rbz1, s->z0 + s->nzl);
+    if (p.rbz0 >= p.rbz1) p.force_on = 0;
+  }
+}
+
+// Copies between the caller's array of the session's cells (Q planes of
+// `cells`, or 4 floats per cell with planes = 1, width 16) and a device
+// array of the stored layout: a slab skips its ghost plane below and above.
+cudaError_t copy_cells(lbm_session *s, void *dst, const void *src, size_t elem, int planes, cudaMemcpyKind kind) {
+  if (!s->slab)
+    return cudaMemcpyAsync(dst, src, elem * (size_t)planes * s->n, kind, s->stream);
+  const size_t w = elem * (size_t)s->cells, skip = elem * (size_t)s->nxy, stored = elem * (size_t)s->n;
+  if (kind == cudaMemcpyDeviceToHost)
+    return cudaMemcpy2DAsync(dst, w, (const char *)src + skip, stored, w, planes, kind, s->stream);
+  return cudaMemcpy2DAsync((char *)dst + skip, stored, src, w, w, planes, kind, s->stream);
 }
 
 void release(lbm_session *s) {
@@ -166,18 +196,31 @@ int lbm_config_default(lbm_config *cfg, int q, int nx, int ny, int nz) {
   return LBM_OK;
 }
 
-int lbm_create(const lbm_config *cfg, lbm_session **out) {
+namespace {
+int create_session(const lbm_config *cfg, int z0, int nzl, bool slab, lbm_session **out) {
   if (!out) return fail(nullptr, LBM_EINVAL, "out is NULL");
   *out = nullptr;
   std::string why;
   int rc = validate_config(cfg, why);
   if (rc) return fail(nullptr, rc, why);
+  if (slab) {
+    if (cfg->q == 9) return fail(nullptr, LBM_EINVAL, "slabs split a 3D domain along z");
+    if (cfg->window[0] || cfg->window[1] || cfg->window[2])
+      return fail(nullptr, LBM_ENOTSUP, "a slab takes no moving window");
+    if (nzl < 1 || z0 < 0 || z0 + nzl > cfg->nz)
+      return fail(nullptr, LBM_EINVAL, "the slab [z0, z0 + nz_local) must lie in [0, nz)");
+  }
   lbm_session *s = new lbm_session();
   s->cfg = *cfg;
   s->q = cfg->q;
   s->storage = cfg->storage;
   s->elem = cfg->storage == LBM_STORE_FP32 ? 4 : 2;
-  s->n = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+  s->slab = slab;
+  s->z0 = slab ? z0 : 0;
+  s->nzl = slab ? nzl : cfg->nz;
+  s->nxy = (int64_t)cfg->nx * cfg->ny;
+  s->cells = s->nxy * s->nzl;
+  s->n = s->nxy * (slab ? nzl + 2 : cfg->nz);
   auto bail = [&](cudaError_t e, const char *what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(e);
     release(s);
@@ -216,6 +259,70 @@ int lbm_create(const lbm_config *cfg, lbm_session **out) {
   *out = s;
   return LBM_OK;
 }
+}  // namespace
+
+int lbm_create(const lbm_config *cfg, lbm_session **out) { return create_session(cfg, 0, 0, false, out); }
+
+int lbm_create_slab(const lbm_config *cfg, int z0, int nz_local, lbm_session **out) {
+  return create_session(cfg, z0, nz_local, true, out);
+}
+
+int64_t lbm_slab_halo_bytes(const lbm_session *s) {
+  if (!s || !s->slab) return 0;
+  return s->nxy * (s->q == 19 ? 5 : 9) * s->elem;
+}
+
+namespace {
+// The populations that cross a slab's z faces: ez = +1 leave through the top
+// (the slab above pulls them from its ghost plane below), ez = -1 through
+// the bottom; in ascending direction order on every slab.
+int crossing(int q, int ez, int idx[9]) {
+  int k = 0;
+  for (int i = 0; i < q; ++i) {
+    const int e = q == 19 ? Lattice<19>::ez(i) : Lattice<27>::ez(i);
+    if (e == ez) idx[k++] = i;
+  }
+  return k;
+}
+}  // namespace
+
+int lbm_slab_pack(lbm_session *s, void *send_lo, void *send_hi) {
+  if (!s || !s->slab) return s ? fail(s, LBM_EINVAL, "not a slab session") : LBM_EINVAL;
+  if (!send_lo || !send_hi) return fail(s, LBM_EINVAL, "send buffers are NULL");
+  const size_t plane = (size_t)s->nxy * s->elem;
+  const char *f = (const char *)s->f[s->cur];
+  int idx[9];
+  // the first stored plane's downward populations, the last one's upward
+  int k = crossing(s->q, -1, idx);
+  for (int j = 0; j < k; ++j)
+    CK(s, cudaMemcpyAsync((char *)send_lo + j * plane, f + ((size_t)idx[j] * s->n + s->nxy) * s->elem, plane,
+                          cudaMemcpyDeviceToDevice, s->stream));
+  k = crossing(s->q, 1, idx);
+  for (int j = 0; j < k; ++j)
+    CK(s, cudaMemcpyAsync((char *)send_hi + j * plane,
+                          f + ((size_t)idx[j] * s->n + (size_t)s->nzl * s->nxy) * s->elem, plane,
+                          cudaMemcpyDeviceToDevice, s->stream));
+  return LBM_OK;
+}
+
+int lbm_slab_unpack(lbm_session *s, const void *recv_lo, const void *recv_hi) {
+  if (!s || !s->slab) return s ? fail(s, LBM_EINVAL, "not a slab session") : LBM_EINVAL;
+  if (!recv_lo || !recv_hi) return fail(s, LBM_EINVAL, "receive buffers are NULL");
+  const size_t plane = (size_t)s->nxy * s->elem;
+  char *f = (char *)s->f[s->cur];
+  int idx[9];
+  // from the slab below: its upward populations, into the ghost plane below
+  int k = crossing(s->q, 1, idx);
+  for (int j = 0; j < k; ++j)
+    CK(s, cudaMemcpyAsync(f + (size_t)idx[j] * s->n * s->elem, (const char *)recv_lo + j * plane, plane,
+                          cudaMemcpyDeviceToDevice, s->stream));
+  // from the slab above: its downward populations, into the ghost plane above
+  k = crossing(s->q, -1, idx);
+  for (int j = 0; j < k; ++j)
+    CK(s, cudaMemcpyAsync(f + ((size_t)idx[j] * s->n + (size_t)(s->nzl + 1) * s->nxy) * s->elem,
+                          (const char *)recv_hi + j * plane, plane, cudaMemcpyDeviceToDevice, s->stream));
+  return LBM_OK;
+}
 
 void lbm_destroy(lbm_session *s) {
   release(s);
@@ -235,7 +342,9 @@ int lbm_set_stream(lbm_session *s, void *stream) {
 
 int lbm_init_macro(lbm_session *s, const float *mac) {
   if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
-  CK(s, cudaMemcpyAsync(s->mac, mac, (size_t)s->n * 16, cudaMemcpyHostToDevice, s->stream));
+  // (a slab's ghost planes keep a zero mac: their populations are only read
+  // after a halo exchange has written them)
+  CK(s, copy_cells(s, s->mac, mac, 16, 1, cudaMemcpyHostToDevice));
   CK(s, launch_init_eq(s->q, s->storage, s->mac, s->f[s->cur], s->n, s->sp.pk, s->stream));
   CK(s, cudaStreamSynchronize(s->stream));
   return LBM_OK;
@@ -245,11 +354,11 @@ int lbm_write_f(lbm_session *s, const float *f) {
   if (!s || !f) return s ? fail(s, LBM_EINVAL, "f is NULL") : LBM_EINVAL;
   const size_t bytes = (size_t)s->q * s->n * 4;
   if (s->storage == LBM_STORE_FP32) {
-    CK(s, cudaMemcpyAsync(s->f[s->cur], f, bytes, cudaMemcpyHostToDevice, s->stream));
+    CK(s, copy_cells(s, s->f[s->cur], f, 4, s->q, cudaMemcpyHostToDevice));
   } else {
     float *tmp = nullptr;
     CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
-    cudaError_t e = cudaMemcpyAsync(tmp, f, bytes, cudaMemcpyHostToDevice, s->stream);
+    cudaError_t e = copy_cells(s, tmp, f, 4, s->q, cudaMemcpyHostToDevice);
     if (!e) e = launch_pack(s->q, s->storage, tmp, s->f[s->cur], s->n, s->sp.pk, s->stream);
     cudaFreeAsync(tmp, s->stream);
     if (e) return cuda_fail(s, e, "pack f");
@@ -262,12 +371,12 @@ int lbm_read_f(lbm_session *s, float *f) {
   if (!s || !f) return s ? fail(s, LBM_EINVAL, "f is NULL") : LBM_EINVAL;
   const size_t bytes = (size_t)s->q * s->n * 4;
   if (s->storage == LBM_STORE_FP32) {
-    CK(s, cudaMemcpyAsync(f, s->f[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(s, copy_cells(s, f, s->f[s->cur], 4, s->q, cudaMemcpyDeviceToHost));
   } else {
     float *tmp = nullptr;
     CK(s, cudaMallocAsync(&tmp, bytes, s->stream));
     cudaError_t e = launch_unpack(s->q, s->storage, s->f[s->cur], tmp, s->n, s->sp.pk, s->stream);
-    if (!e) e = cudaMemcpyAsync(f, tmp, bytes, cudaMemcpyDeviceToHost, s->stream);
+    if (!e) e = copy_cells(s, f, tmp, 4, s->q, cudaMemcpyDeviceToHost);
     cudaFreeAsync(tmp, s->stream);
     if (e) return cuda_fail(s, e, "unpack f");
   }
@@ -277,21 +386,21 @@ int lbm_read_f(lbm_session *s, float *f) {
 
 int lbm_write_f_raw(lbm_session *s, const void *planes) {
   if (!s || !planes) return s ? fail(s, LBM_EINVAL, "planes is NULL") : LBM_EINVAL;
-  CK(s, cudaMemcpyAsync(s->f[s->cur], planes, (size_t)s->q * s->n * s->elem, cudaMemcpyHostToDevice, s->stream));
+  CK(s, copy_cells(s, s->f[s->cur], planes, s->elem, s->q, cudaMemcpyHostToDevice));
   CK(s, cudaStreamSynchronize(s->stream));
   return LBM_OK;
 }
 
 int lbm_read_f_raw(lbm_session *s, void *planes) {
   if (!s || !planes) return s ? fail(s, LBM_EINVAL, "planes is NULL") : LBM_EINVAL;
-  CK(s, cudaMemcpyAsync(planes, s->f[s->cur], (size_t)s->q * s->n * s->elem, cudaMemcpyDeviceToHost, s->stream));
+  CK(s, copy_cells(s, planes, s->f[s->cur], s->elem, s->q, cudaMemcpyDeviceToHost));
   CK(s, cudaStreamSynchronize(s->stream));
   return LBM_OK;
 }
 
 int lbm_read_mac(lbm_session *s, float *mac) {
   if (!s || !mac) return s ? fail(s, LBM_EINVAL, "mac is NULL") : LBM_EINVAL;
-  CK(s, cudaMemcpyAsync(mac, s->mac, (size_t)s->n * 16, cudaMemcpyDeviceToHost, s->stream));
+  CK(s, copy_cells(s, mac, s->mac, 16, 1, cudaMemcpyDeviceToHost));
   CK(s, cudaStreamSynchronize(s->stream));
   return LBM_OK;
 }
@@ -361,6 +470,7 @@ int lbm_set_free_body(lbm_session *s, const lbm_body_state *state, const lbm_bod
   }
   const lbm_config &c = s->cfg;
   if (c.q == 9) return fail(s, LBM_ENOTSUP, "free bodies are 3D only");
+  if (s->slab) return fail(s, LBM_ENOTSUP, "a free body moves across slabs: it runs in a whole domain");
   if (!c.has_body) return fail(s, LBM_EINVAL, "the session has no body");
   const lbm_body_state &st = *state;
   bool ok = st.mass > 0.0 && std::isfinite(st.mass);
@@ -431,6 +541,7 @@ int lbm_resample(lbm_session *s, const lbm_volume_spec *spec, void *out, uint8_t
   if (!s) return LBM_EINVAL;
   std::string why;
   if (validate_volume(spec, why)) return fail(s, LBM_EINVAL, why);
+  if (s->slab) return fail(s, LBM_ENOTSUP, "the headless views read a whole domain");
   if (!out) return fail(s, LBM_EINVAL, "out is NULL");
   if (s->q == 9) return fail(s, LBM_ENOTSUP, "the headless views are 3D");
   const lbm_config &c = s->cfg;
@@ -445,6 +556,7 @@ int lbm_render_slice(lbm_session *s, const lbm_slice_spec *spec, uint8_t *rgba) 
   std::string why;
   if (validate_slice(spec, c.nx, c.ny, c.nz, why)) return fail(s, LBM_EINVAL, why);
   if (!rgba) return fail(s, LBM_EINVAL, "rgba is NULL");
+  if (s->slab) return fail(s, LBM_ENOTSUP, "the headless views read a whole domain");
   if (s->q == 9) return fail(s, LBM_ENOTSUP, "the headless views are 3D");
   // winViewOffset: the view pans with the body under a moving window
   ViewOffset off{{0.f, 0.f, 0.f}};
@@ -497,8 +609,10 @@ int lbm_forces_async(lbm_session *s, double out[6]) {
 
 int lbm_totals(lbm_session *s, double out[8]) {
   if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
-  CK(s, launch_totals(s->q, s->storage, s->f[s->cur], s->n, s->sp.pk, s->tot_partials, s->tot_counter,
-                      s->tot_out, s->stream));
+  // a slab's own planes: past the ghost plane below, n cells apart per population
+  const char *f0 = (const char *)s->f[s->cur] + (s->slab ? s->nxy * s->elem : 0);
+  CK(s, launch_totals(s->q, s->storage, f0, s->cells, s->sp.pk, s->tot_partials, s->tot_counter, s->tot_out,
+                      s->stream, s->n));
   CK(s, cudaMemcpyAsync(s->host_out, s->tot_out, 8 * sizeof(double), cudaMemcpyDeviceToHost,
                         s->stream));
   CK(s, cudaStreamSynchronize(s->stream));

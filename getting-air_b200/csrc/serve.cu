@@ -4,14 +4,28 @@
 // The server owns ONE device arena of `budget` bytes, allocated at creation.
 // A request (a dense lbm_config plus a step count) is admitted when its
 // state -- two f buffers, the mac field and its force scratch -- fits in the
-// arena (first fit, FIFO order); until then it waits in the queue. Every
-// tick advances all resident requests together: per step, one persistent
-// launch per lattice (D2Q9, D3Q19, D3Q27) walks a tile list covering every
-// resident domain and applies the same per-cell update as a dense session
-// (cell3 / cell2), so a request's result is bit-identical whether it runs
-// alone or in a mix. A tick ends when the soonest request completes; finished
-// requests are retired (force read back, memory returned to the arena) and
-// queued ones admitted into the freed space before the next tick.
+// arena (first fit; FIFO or least work first); until then it waits in the
+// queue. A tick advances every resident request by the same number of steps:
+// per step, one persistent launch per (lattice, storage) walks a tile list
+// covering every resident domain of that kind and applies the same per-cell
+// update as a dense session (cell3 / cell2), so a request's result is
+// bit-identical whether it runs alone or in a mix. A tick ends when the
+// soonest request completes.
+//
+// Dense requests of at least kStreamCells cells do not join the tile
+// launches: each runs the dense session's own step (launch_step, the same
+// kernels and force sums as an lbm_session) on a stream of its own, so a
+// large domain gets the tuned dense kernel and the small ones share the
+// tile launches; all of them, the AMR solves included, overlap on the GPU.
+//
+// Ticks are pipelined: lbm_server_poll enqueues the next tick (two tick
+// slots, each with its own staging buffers and completion events) before
+// it waits for the oldest one, so the GPU always has a tick queued while
+// the host retires finished requests (completion by CUDA event, the force
+// read back by an asynchronous copy into pinned memory queued behind the
+// request's last step) and admits new ones (a uniform seed is built on the
+// device; a caller's seed goes up on a separate upload stream). Nothing in
+// a tick waits on the host.
 //
 // A request may also be a 3D two-level AMR solve (lbm_server_submit_amr3d):
 // its hierarchy is built inside its share of the arena
@@ -42,6 +56,9 @@ namespace {
 constexpr int kServeThreads = 256;
 constexpr int kServeCpt = 4;  // cells per thread per tile
 constexpr int kCellsPerTile = kServeThreads * kServeCpt;
+// Dense requests from this size up step on their own stream with the dense
+// session's kernels (64^3 cells: where one domain fills the GPU's launch).
+constexpr int64_t kStreamCells = int64_t(1) << 18;
 
 // Per-domain descriptor: the dense StepParams plus the domain's own buffers.
 struct ServeDom {
@@ -51,8 +68,8 @@ struct ServeDom {
   float *mac;
 };
 
-template <int Q, typename S>
-__global__ void __launch_bounds__(kServeThreads)
+template <int Q, typename S, bool TRT>
+__global__ void __launch_bounds__(kServeThreads, 2)
     serve_step(const ServeDom *__restrict__ doms, const int2 *__restrict__ tiles, int ntiles, int parity,
                int write_mac) {
   __shared__ __align__(16) unsigned char raw[sizeof(ServeDom)];
@@ -73,15 +90,16 @@ __global__ void __launch_bounds__(kServeThreads)
     const int lt = t - d.p.tile0;
     const bool region = d.p.force_on && lt >= d.p.ft0 && lt < d.p.ft1;
     ForceAcc acc;
+    CellWalk w(td.y + threadIdx.x, kServeThreads, nx, ny);
     for (int c = td.y + threadIdx.x; c < end; c += kServeThreads) {
-      const int x = c % nx, r = c / nx;
       CellForce cf;
       if constexpr (Q == 9) {
-        cell2<S>(fin, fout, d.mac, d.p, x, r, region, cf);
+        cell2<S>(fin, fout, d.mac, d.p, w.x, w.y, region, cf);
       } else {
-        cell3<Q, S>(fin, fout, d.mac, d.p, x, r % ny, r / ny, region, cf);
+        cell3<Q, S, TRT>(fin, fout, d.mac, d.p, w.x, w.y, w.z, region, cf);
       }
       if (region) acc.add(cf);
+      w.advance();
     }
     if (region)
       reduce_force<kServeThreads>(acc, d.p.partials, d.p.counter, d.p.ft1 - d.p.ft0, lt - d.p.ft0, d.p.force_out);
@@ -89,10 +107,13 @@ __global__ void __launch_bounds__(kServeThreads)
   }
 }
 
-cudaError_t launch_serve(int q, int storage, int grid, cudaStream_t st, const ServeDom *doms, const int2 *tiles,
-                         int ntiles, int parity, int write_mac) {
-#define SERVE_CASE(QQ, SS)                                                                          \
-  serve_step<QQ, SS><<<grid, kServeThreads, 0, st>>>(doms, tiles, ntiles, parity, write_mac);       \
+cudaError_t launch_serve(int q, int storage, bool trt, int grid, cudaStream_t st, const ServeDom *doms,
+                         const int2 *tiles, int ntiles, int parity, int write_mac) {
+#define SERVE_CASE(QQ, SS)                                                                                   \
+  if (trt && QQ != 9)                                                                                         \
+    serve_step<QQ, SS, true><<<grid, kServeThreads, 0, st>>>(doms, tiles, ntiles, parity, write_mac);        \
+  else                                                                                                        \
+    serve_step<QQ, SS, false><<<grid, kServeThreads, 0, st>>>(doms, tiles, ntiles, parity, write_mac);       \
   break;
   switch (q * 4 + storage) {
     case 9 * 4 + 0: SERVE_CASE(9, float)
@@ -157,12 +178,12 @@ struct Request {
   int64_t id = 0;
   lbm_config cfg{};
   std::vector<float> mac_seed;  // empty: uniform freestream at sponge_u
-  int steps = 0, done = 0;
+  int steps = 0;
+  int enq = 0;                  // steps enqueued (complete once retired)
   double t_submit = 0, t_admit = 0, t_done = 0;
   int64_t off = -1, bytes = 0;
-  char *base = nullptr;  // arena pointer
   void *f[2] = {nullptr, nullptr};
-  int cur = 0;
+  int cur = 0;                  // f buffer current after the enqueued steps
   float *mac = nullptr;
   double *partials = nullptr;
   unsigned *counter = nullptr;
@@ -170,11 +191,36 @@ struct Request {
   int nparts = 0;
   int state = 0;  // 0 queued, 1 resident, 2 finished (resident until released)
   double force[8] = {};
-  // a 3D two-level AMR solve (kind 1): its hierarchy and stream
+  // kind 0: a dense solve in the tile launches; kind 1: a 3D two-level AMR
+  // solve (its hierarchy); kind 2: a dense solve stepped by the dense
+  // session's kernels (its StepParams, and the group sums of its force
+  // partials, two sets of dparts). Kinds 1 and 2 run on their own stream,
+  // with one completion event per tick slot.
   int kind = 0;
   lbm_amr3d_config acfg{};
   lbm_amr3d *amr = nullptr;
-  cudaStream_t amr_stream = nullptr;
+  StepParams sp{};
+  double *groups = nullptr;
+  int dparts = 0;
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+// One tick in flight: its staging (pinned host and device copies of the
+// domain descriptors and tiles), the requests whose last step it holds, the
+// AMR requests it stepped (their ev[slot]), and its event on the server
+// stream (after the dense launches and the force copies).
+struct TickSlot {
+  bool busy = false;
+  int64_t seq = 0;
+  cudaEvent_t ev = nullptr;
+  std::vector<std::pair<int64_t, int>> finishing;  // (id, its row of h_force or -1)
+  std::vector<int64_t> streams;                    // kind 1 and 2 requests stepped
+  ServeDom *h_doms = nullptr, *d_doms = nullptr;
+  int2 *h_tiles = nullptr, *d_tiles = nullptr;
+  int cap_doms = 0, cap_tiles = 0;
+  double *h_force = nullptr;  // pinned, kForceSlots per finishing dense request
+  int cap_force = 0;
 };
 
 // Lattice cells of a request's domain (L0 for an AMR solve).
@@ -185,6 +231,24 @@ int64_t request_bytes(const lbm_config &c, int nparts) {
   const int elem = c.storage == LBM_STORE_FP32 ? 4 : 2;
   auto up = [](int64_t b) { return (b + 255) & ~int64_t(255); };
   return 2 * up((int64_t)c.q * n * elem) + up(n * 16) + up((int64_t)nparts * kForceSlots * 8) + 256 + up(kForceSlots * 8);
+}
+
+// The dense session's step parameters of a kind-2 request (its reach box and
+// force region set as a session sets them) and its number of force partials.
+int streamed_params(const lbm_config &c, StepParams &sp) {
+  fill_step_params(c, (int64_t)c.nx * c.ny * c.nz, 0, sp);
+  return set_body_regions(c, sp, true) ? force_parts(c.q, sp) : 0;
+}
+
+// A kind-2 request: two f buffers, the mac field, two sets of force
+// partials (consecutive steps alternate), their group sums, the ticket and
+// the force.
+int64_t streamed_bytes(const lbm_config &c, int dparts) {
+  const int64_t n = (int64_t)c.nx * c.ny * c.nz;
+  const int elem = c.storage == LBM_STORE_FP32 ? 4 : 2;
+  auto up = [](int64_t b) { return (b + 255) & ~int64_t(255); };
+  return 2 * up((int64_t)c.q * n * elem) + up(n * 16) + up((int64_t)2 * dparts * kForceSlots * 8) +
+         up((int64_t)sum_groups(dparts) * kForceSlots * 8) + 256 + up(kForceSlots * 8);
 }
 
 // Force-region tiles [ft0, ft1) of a domain tiled by kCellsPerTile.
@@ -212,13 +276,12 @@ struct lbm_server {
   char *arena_ptr = nullptr;
   Arena arena;
   std::map<int64_t, Request> reqs;   // by id
-  std::deque<int64_t> queue;         // FIFO of queued ids
-  cudaStream_t stream = nullptr;
-  ServeDom *d_doms = nullptr;
-  int2 *d_tiles = nullptr;
-  int cap_doms = 0, cap_tiles = 0;
-  ServeDom *h_doms = nullptr;        // pinned staging
-  int2 *h_tiles = nullptr;
+  std::deque<int64_t> queue;         // queued ids, in admission order
+  std::deque<int64_t> ready;         // retired, not yet reported by a poll
+  cudaStream_t stream = nullptr;     // the dense ticks
+  cudaStream_t upload = nullptr;     // callers' seeds
+  TickSlot slot[2];
+  int64_t tick_seq = 0;
   int sms = 148;
   int policy = 0;                    // 0 FIFO, 1 shortest work first
   int64_t max_resident_cells = 0;    // 0: no cap besides the budget
@@ -248,26 +311,31 @@ double now_s(const lbm_server *s) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
 }
 
-int ensure_staging(lbm_server *s, int ndoms, int ntiles) {
-  if (ndoms > s->cap_doms) {
-    cudaFree(s->d_doms);
-    cudaFreeHost(s->h_doms);
-    s->d_doms = nullptr;
-    s->h_doms = nullptr;
-    const int cap = std::max(ndoms, 2 * s->cap_doms);
-    SCK(s, cudaMalloc(&s->d_doms, cap * sizeof(ServeDom)));
-    SCK(s, cudaMallocHost(&s->h_doms, cap * sizeof(ServeDom)));
-    s->cap_doms = cap;
-  }
-  if (ntiles > s->cap_tiles) {
-    cudaFree(s->d_tiles);
-    cudaFreeHost(s->h_tiles);
-    s->d_tiles = nullptr;
-    s->h_tiles = nullptr;
-    const int cap = std::max(ntiles, 2 * s->cap_tiles);
-    SCK(s, cudaMalloc(&s->d_tiles, (size_t)cap * sizeof(int2)));
-    SCK(s, cudaMallocHost(&s->h_tiles, (size_t)cap * sizeof(int2)));
-    s->cap_tiles = cap;
+template <typename T> int grow_pair(lbm_server *s, T **h, T **d, int &cap, int need) {
+  if (need <= cap) return LBM_OK;
+  const int c = std::max({need, 2 * cap, 64});
+  cudaFree(*d);
+  if (*h) cudaFreeHost(*h);
+  *d = nullptr;
+  *h = nullptr;
+  cap = 0;
+  SCK(s, cudaMalloc(d, (size_t)c * sizeof(T)));
+  SCK(s, cudaMallocHost(h, (size_t)c * sizeof(T)));
+  cap = c;
+  return LBM_OK;
+}
+
+int ensure_staging(lbm_server *s, TickSlot &t, int ndoms, int ntiles, int nforce) {
+  int rc = grow_pair(s, &t.h_doms, &t.d_doms, t.cap_doms, ndoms);
+  if (!rc) rc = grow_pair(s, &t.h_tiles, &t.d_tiles, t.cap_tiles, ntiles);
+  if (rc) return rc;
+  if (nforce > t.cap_force) {
+    const int c = std::max({nforce, 2 * t.cap_force, 16});
+    if (t.h_force) cudaFreeHost(t.h_force);
+    t.h_force = nullptr;
+    t.cap_force = 0;
+    SCK(s, cudaMallocHost(&t.h_force, (size_t)c * kForceSlots * sizeof(double)));
+    t.cap_force = c;
   }
   return LBM_OK;
 }
@@ -288,8 +356,9 @@ int admit_amr(lbm_server *s, Request &r, bool &ok) {
     s->arena.release(off, bytes);
     return sfail(s, rc, lbm_amr3d_last_error(nullptr));
   }
-  SCK(s, cudaStreamCreateWithFlags(&r.amr_stream, cudaStreamNonBlocking));
-  lbm_amr3d_set_stream(r.amr, r.amr_stream);
+  SCK(s, cudaStreamCreateWithFlags(&r.own, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) SCK(s, cudaEventCreateWithFlags(&r.ev[k], cudaEventDisableTiming));
+  lbm_amr3d_set_stream(r.amr, r.own);
   const int64_t n = request_cells(r);
   std::vector<float> seed;
   const float *src = r.mac_seed.empty() ? nullptr : r.mac_seed.data();
@@ -316,46 +385,75 @@ int admit_amr(lbm_server *s, Request &r, bool &ok) {
 int admit(lbm_server *s, Request &r, bool &ok) {
   if (r.kind == 1) return admit_amr(s, r, ok);
   ok = false;
-  StepParams tmp{};
-  fill_step_params(r.cfg, 1, 0, tmp);
-  const int nparts = force_tiles(r.cfg, tmp);
-  const int64_t bytes = request_bytes(r.cfg, nparts);
+  const int64_t n = request_cells(r);
+  int nparts = 0;
+  int64_t bytes = 0;
+  if (r.kind == 2) {
+    r.dparts = streamed_params(r.cfg, r.sp);
+    bytes = streamed_bytes(r.cfg, r.dparts);
+  } else {
+    StepParams tmp{};
+    fill_step_params(r.cfg, 1, 0, tmp);
+    nparts = force_tiles(r.cfg, tmp);
+    bytes = request_bytes(r.cfg, nparts);
+  }
   const int64_t off = s->arena.alloc(bytes);
   if (off < 0) return LBM_OK;
   r.off = off;
   r.bytes = bytes;
   r.nparts = nparts;
   char *p = s->arena_ptr + off;
-  const int64_t n = (int64_t)r.cfg.nx * r.cfg.ny * r.cfg.nz;
   const int elem = r.cfg.storage == LBM_STORE_FP32 ? 4 : 2;
   auto up = [](int64_t b) { return (b + 255) & ~int64_t(255); };
   const int64_t fb = up((int64_t)r.cfg.q * n * elem);
   r.f[0] = p; p += fb;
   r.f[1] = p; p += fb;
   r.mac = (float *)p; p += up(n * 16);
-  r.partials = (double *)p; p += up((int64_t)nparts * kForceSlots * 8);
+  if (r.kind == 2) {
+    r.partials = (double *)p; p += up((int64_t)2 * r.dparts * kForceSlots * 8);
+    r.groups = (double *)p; p += up((int64_t)sum_groups(r.dparts) * kForceSlots * 8);
+  } else {
+    r.partials = (double *)p; p += up((int64_t)nparts * kForceSlots * 8);
+  }
   r.counter = (unsigned *)p; p += 256;
   r.force_out = (double *)p;
   r.cur = 0;
-  // Seed: the caller's macroscopic field, else the uniform freestream at
-  // sponge_u with rho = 1 - |u|^2 / (2 cs^2) (d3-scenarios.mjs seedMacro3).
-  std::vector<float> seed;
-  const float *src = r.mac_seed.empty() ? nullptr : r.mac_seed.data();
-  if (!src) {
-    const float ux = r.cfg.sponge_u[0], uy = r.cfg.sponge_u[1], uz = r.cfg.q == 9 ? 0.f : r.cfg.sponge_u[2];
-    const float rho = 1.0f - (ux * ux + uy * uy + uz * uz) * 1.5f;
-    seed.resize(4 * n);
-    for (int64_t k = 0; k < n; ++k) {
-      seed[4 * k] = rho; seed[4 * k + 1] = ux; seed[4 * k + 2] = uy; seed[4 * k + 3] = uz;
-    }
-    src = seed.data();
+  cudaStream_t st = s->stream;
+  if (r.kind == 2) {
+    SCK(s, cudaStreamCreateWithFlags(&r.own, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) SCK(s, cudaEventCreateWithFlags(&r.ev[k], cudaEventDisableTiming));
+    r.sp.partials = r.partials;
+    r.sp.groups = r.groups;
+    r.sp.counter = r.counter;
+    r.sp.force_out = r.force_out;
+    st = r.own;
   }
-  SCK(s, cudaMemcpyAsync(r.mac, src, n * 16, cudaMemcpyHostToDevice, s->stream));
-  SCK(s, launch_init_eq(r.cfg.q, r.cfg.storage, r.mac, r.f[0], n, make_pack(r.cfg), s->stream));
-  SCK(s, cudaMemsetAsync(r.counter, 0, 4, s->stream));
-  SCK(s, cudaMemsetAsync(r.force_out, 0, kForceSlots * 8, s->stream));
-  // The seed must be on the device before `seed` goes out of scope.
-  SCK(s, cudaStreamSynchronize(s->stream));
+  // Seed: the caller's macroscopic field, else the uniform freestream at
+  // sponge_u with rho = 1 - |u|^2 / (2 cs^2) (d3-scenarios.mjs seedMacro3),
+  // built on the device. A caller's field goes up on a stream no tick uses
+  // (the upload stream, which the server stream then waits for, or the
+  // request's own): a pageable copy waits for its stream and returns once
+  // the host buffer is staged, so neither waits for a tick in flight.
+  const Pack pk = make_pack(r.cfg);
+  if (!r.mac_seed.empty()) {
+    cudaStream_t us = r.kind == 2 ? r.own : s->upload;
+    cudaError_t e = cudaMemcpyAsync(r.mac, r.mac_seed.data(), n * 16, cudaMemcpyHostToDevice, us);
+    if (!e) e = launch_init_eq(r.cfg.q, r.cfg.storage, r.mac, r.f[0], n, pk, us);
+    if (!e && r.kind != 2) {
+      cudaEvent_t upe = nullptr;
+      e = cudaEventCreateWithFlags(&upe, cudaEventDisableTiming);
+      if (!e) e = cudaEventRecord(upe, s->upload);
+      if (!e) e = cudaStreamWaitEvent(s->stream, upe, 0);
+      if (upe) cudaEventDestroy(upe);
+    }
+    if (e) return sfail(s, LBM_ECUDA, std::string("seed: ") + cudaGetErrorString(e));
+  } else {
+    const float ux = r.cfg.sponge_u[0], uy = r.cfg.sponge_u[1], uz = r.cfg.q == 9 ? 0.f : r.cfg.sponge_u[2];
+    const float rho_u[4] = {1.0f - (ux * ux + uy * uy + uz * uz) * 1.5f, ux, uy, uz};
+    SCK(s, launch_init_uniform(r.cfg.q, r.cfg.storage, rho_u, r.mac, r.f[0], n, pk, st));
+  }
+  SCK(s, cudaMemsetAsync(r.counter, 0, 4, st));
+  SCK(s, cudaMemsetAsync(r.force_out, 0, kForceSlots * 8, st));
   r.mac_seed.clear();
   r.mac_seed.shrink_to_fit();
   r.state = 1;
@@ -364,72 +462,219 @@ int admit(lbm_server *s, Request &r, bool &ok) {
   return LBM_OK;
 }
 
-// Runs `k` steps of every resident, unfinished request.
-int run_steps(lbm_server *s, const std::vector<Request *> &act, int k) {
-  // the AMR solves first: k macro-steps each, queued on their own streams
-  for (Request *r : act) {
-    if (r->kind != 1) continue;
-    const int rc = lbm_amr3d_step(r->amr, k);
-    if (rc) return sfail(s, rc, lbm_amr3d_last_error(r->amr));
+// k steps of a kind-2 request on its own stream: lbm_step's sequence (each
+// step's force partials summed by the next step's first blocks, the last
+// step's by the sum launch after it).
+int step_streamed(lbm_server *s, Request &r, int k) {
+  const int64_t half = (int64_t)r.dparts * kForceSlots;
+  const int parts = r.sp.force_on ? r.dparts : 0;
+  for (int j = 0; j < k; ++j) {
+    StepParams &sp = r.sp;
+    sp.write_mac = (j == k - 1);
+    sp.partials = r.partials + (j & 1) * half;
+    sp.defer_force = j < k - 1;
+    sp.prev_parts = j > 0 ? parts : 0;
+    sp.prev_partials = r.partials + ((j + 1) & 1) * half;
+    SCK(s, launch_step(r.cfg.q, r.cfg.storage, r.f[r.cur], r.f[1 - r.cur], r.mac, sp, r.own));
+    r.cur = 1 - r.cur;
   }
-  for (int q : {9, 19, 27})
-    for (int st = 0; st <= 2; ++st) {
-      std::vector<Request *> group;
-      for (Request *r : act)
-        if (r->kind == 0 && r->cfg.q == q && r->cfg.storage == st) group.push_back(r);
-      if (group.empty()) continue;
-      int ntiles = 0;
-      for (Request *r : group) {
-        const int64_t n = (int64_t)r->cfg.nx * r->cfg.ny * r->cfg.nz;
-        ntiles += (int)((n + kCellsPerTile - 1) / kCellsPerTile);
-      }
-      int rc = ensure_staging(s, (int)group.size(), ntiles);
-      if (rc) return rc;
-      int t = 0;
-      for (size_t d = 0; d < group.size(); ++d) {
-        Request &r = *group[d];
-        const int64_t n = (int64_t)r.cfg.nx * r.cfg.ny * r.cfg.nz;
-        ServeDom &sd = s->h_doms[d];
-        std::memset(&sd, 0, sizeof(sd));
-        fill_step_params(r.cfg, n, 0, sd.p);
-        force_tiles(r.cfg, sd.p);
-        sd.p.tile0 = t;
-        sd.p.partials = r.partials;
-        sd.p.counter = r.counter;
-        sd.p.force_out = r.force_out;
-        sd.fa = r.f[r.cur];
-        sd.fb = r.f[1 - r.cur];
-        sd.mac = r.mac;
-        const int nt = (int)((n + kCellsPerTile - 1) / kCellsPerTile);
-        for (int j = 0; j < nt; ++j) s->h_tiles[t++] = make_int2((int)d, j * kCellsPerTile);
-      }
-      SCK(s, cudaMemcpyAsync(s->d_doms, s->h_doms, group.size() * sizeof(ServeDom), cudaMemcpyHostToDevice,
-                             s->stream));
-      SCK(s, cudaMemcpyAsync(s->d_tiles, s->h_tiles, (size_t)t * sizeof(int2), cudaMemcpyHostToDevice, s->stream));
-      const int grid = std::min(t, 8 * s->sms);
-      for (int j = 0; j < k; ++j) SCK(s, launch_serve(q, st, grid, s->stream, s->d_doms, s->d_tiles, t, j & 1, j == k - 1));
-      for (Request *r : group) {
-        r->done += k;
-        if (k & 1) r->cur = 1 - r->cur;
-        s->lattice_updates += (int64_t)k * r->cfg.nx * r->cfg.ny * r->cfg.nz;
-      }
-      // The staging buffers are rewritten by the next group: wait for the copies.
-      SCK(s, cudaStreamSynchronize(s->stream));
+  r.sp.partials = r.partials;
+  r.sp.defer_force = 0;
+  r.sp.prev_parts = 0;
+  return LBM_OK;
+}
+
+// Enqueues one tick into slot `si`: k steps of every resident request with
+// steps left, k = the fewest left (at most max_steps). Returns with nothing
+// enqueued when no request has steps left.
+int enqueue_tick(lbm_server *s, int si, int max_steps) {
+  TickSlot &t = s->slot[si];
+  std::vector<Request *> act;
+  int k = max_steps;
+  for (auto &kv : s->reqs)
+    if (kv.second.state == 1 && kv.second.enq < kv.second.steps) {
+      act.push_back(&kv.second);
+      k = std::min(k, kv.second.steps - kv.second.enq);
     }
+  if (act.empty()) return LBM_OK;
+  t.finishing.clear();
+  t.streams.clear();
+  int ndoms = 0, ntiles = 0, nforce = 0;
   for (Request *r : act) {
-    if (r->kind != 1) continue;
-    SCK(s, cudaStreamSynchronize(r->amr_stream));
-    r->done += k;
-    s->lattice_updates += (int64_t)k * lbm_amr3d_cell_updates(r->amr);
+    if (r->kind == 0) {
+      ++ndoms;
+      ntiles += (int)((request_cells(*r) + kCellsPerTile - 1) / kCellsPerTile);
+    }
+    nforce += r->kind != 1 && r->enq + k == r->steps;
+  }
+  int rc = ensure_staging(s, t, ndoms, ntiles, nforce);
+  if (rc) return rc;
+  int fi = 0;
+  // the solves on their own streams: AMR macro-steps, or the dense step
+  for (Request *r : act) {
+    if (r->kind == 0) continue;
+    if (r->kind == 1) {
+      rc = lbm_amr3d_step(r->amr, k);
+      if (rc) return sfail(s, rc, lbm_amr3d_last_error(r->amr));
+    } else {
+      rc = step_streamed(s, *r, k);
+      if (rc) return rc;
+    }
+    if (r->enq + k == r->steps) {
+      int row = -1;
+      if (r->kind == 2) {
+        row = fi++;
+        SCK(s, cudaMemcpyAsync(t.h_force + (size_t)kForceSlots * row, r->force_out, kForceSlots * sizeof(double),
+                               cudaMemcpyDeviceToHost, r->own));
+      }
+      t.finishing.emplace_back(r->id, row);
+    }
+    SCK(s, cudaEventRecord(r->ev[si], r->own));
+    t.streams.push_back(r->id);
+  }
+  // the tile launches: one descriptor and tile list per (lattice, storage,
+  // collision) group, all groups staged together and uploaded once
+  struct Group { int q, st; bool trt; int dom0, ndom, tile0, ntile; };
+  std::vector<Group> groups;
+  int d = 0, tt = 0;
+  for (int q : {9, 19, 27})
+    for (int st = 0; st <= 2; ++st)
+      for (int trt = 0; trt <= 1; ++trt) {
+        Group g{q, st, trt == 1, d, 0, tt, 0};
+        for (Request *r : act) {
+          if (r->kind != 0 || r->cfg.q != q || r->cfg.storage != st || (r->cfg.trt != 0) != (trt == 1)) continue;
+          const int64_t n = request_cells(*r);
+          ServeDom &sd = t.h_doms[d];
+          std::memset(&sd, 0, sizeof(sd));
+          fill_step_params(r->cfg, n, 0, sd.p);
+          force_tiles(r->cfg, sd.p);
+          sd.p.tile0 = tt - g.tile0;
+          sd.p.partials = r->partials;
+          sd.p.counter = r->counter;
+          sd.p.force_out = r->force_out;
+          sd.fa = r->f[r->cur];
+          sd.fb = r->f[1 - r->cur];
+          sd.mac = r->mac;
+          const int nt = (int)((n + kCellsPerTile - 1) / kCellsPerTile);
+          for (int j = 0; j < nt; ++j) t.h_tiles[tt++] = make_int2(d - g.dom0, j * kCellsPerTile);
+          ++d;
+        }
+        g.ndom = d - g.dom0;
+        g.ntile = tt - g.tile0;
+        if (g.ndom) groups.push_back(g);
+      }
+  if (ndoms) {
+    SCK(s, cudaMemcpyAsync(t.d_doms, t.h_doms, (size_t)ndoms * sizeof(ServeDom), cudaMemcpyHostToDevice, s->stream));
+    SCK(s, cudaMemcpyAsync(t.d_tiles, t.h_tiles, (size_t)ntiles * sizeof(int2), cudaMemcpyHostToDevice, s->stream));
+  }
+  for (int j = 0; j < k; ++j)
+    for (const Group &g : groups)
+      SCK(s, launch_serve(g.q, g.st, g.trt, std::min(g.ntile, 8 * s->sms), s->stream, t.d_doms + g.dom0,
+                          t.d_tiles + g.tile0, g.ntile, j & 1, j == k - 1));
+  // the last step's force of each tile request that finishes in this tick
+  for (Request *r : act) {
+    if (r->kind != 0 || r->enq + k != r->steps) continue;
+    const int row = fi++;
+    SCK(s, cudaMemcpyAsync(t.h_force + (size_t)kForceSlots * row, r->force_out, kForceSlots * sizeof(double),
+                           cudaMemcpyDeviceToHost, s->stream));
+    t.finishing.emplace_back(r->id, row);
+  }
+  SCK(s, cudaEventRecord(t.ev, s->stream));
+  for (Request *r : act) {
+    r->enq += k;
+    if (r->kind == 0) {
+      if (k & 1) r->cur = 1 - r->cur;
+      s->lattice_updates += (int64_t)k * request_cells(*r);
+    } else if (r->kind == 2) {
+      s->lattice_updates += (int64_t)k * request_cells(*r);  // step_streamed moved cur
+    } else {
+      s->lattice_updates += (int64_t)k * lbm_amr3d_cell_updates(r->amr);
+    }
+  }
+  t.busy = true;
+  t.seq = ++s->tick_seq;
+  return LBM_OK;
+}
+
+// Whether slot si's tick has finished (block: wait for it).
+int tick_done(lbm_server *s, int si, bool block, bool &done) {
+  TickSlot &t = s->slot[si];
+  done = false;
+  std::vector<cudaEvent_t> evs{t.ev};
+  for (int64_t id : t.streams) evs.push_back(s->reqs[id].ev[si]);
+  for (cudaEvent_t e : evs) {
+    const cudaError_t r = block ? cudaEventSynchronize(e) : cudaEventQuery(e);
+    if (r == cudaErrorNotReady) return LBM_OK;
+    if (r != cudaSuccess) return sfail(s, LBM_ECUDA, std::string("tick: ") + cudaGetErrorString(r));
+  }
+  done = true;
+  return LBM_OK;
+}
+
+// Retires the requests whose last step slot si's (finished) tick held.
+int retire_tick(lbm_server *s, int si) {
+  TickSlot &t = s->slot[si];
+  for (const auto &fr : t.finishing) {
+    Request &r = s->reqs[fr.first];
+    if (r.kind == 1) {
+      const int rc = lbm_amr3d_forces(r.amr, r.force);
+      if (rc) return sfail(s, rc, lbm_amr3d_last_error(r.amr));
+    } else {
+      std::memcpy(r.force, t.h_force + (size_t)kForceSlots * fr.second, kForceSlots * sizeof(double));
+    }
+    r.state = 2;
+    r.t_done = now_s(s);
+    s->ready.push_back(fr.first);
+  }
+  t.finishing.clear();
+  t.streams.clear();
+  t.busy = false;
+  return LBM_OK;
+}
+
+// Finishes the busy ticks, oldest first: those already done, or (block)
+// the oldest one whatever its state.
+int complete_ticks(lbm_server *s, bool block_oldest) {
+  for (int pass = 0; pass < 2; ++pass) {
+    int si = -1;
+    for (int k = 0; k < 2; ++k)
+      if (s->slot[k].busy && (si < 0 || s->slot[k].seq < s->slot[si].seq)) si = k;
+    if (si < 0) return LBM_OK;
+    bool done = false;
+    int rc = tick_done(s, si, block_oldest && pass == 0, done);
+    if (rc) return rc;
+    if (!done) return LBM_OK;
+    rc = retire_tick(s, si);
+    if (rc) return rc;
   }
   return LBM_OK;
 }
 
+// Releases what a request holds outside the arena: an AMR hierarchy's
+// handle, its own stream and events.
 void drop_amr(Request &r) {
   if (r.amr) lbm_amr3d_destroy(r.amr);
-  if (r.amr_stream) cudaStreamDestroy(r.amr_stream);
+  if (r.own) {
+    cudaStreamSynchronize(r.own);
+    cudaStreamDestroy(r.own);
+  }
+  for (cudaEvent_t &e : r.ev)
+    if (e) {
+      cudaEventDestroy(e);
+      e = nullptr;
+    }
   r.amr = nullptr;
-  r.amr_stream = nullptr;
+  r.own = nullptr;
+}
+
+void free_slot(TickSlot &t) {
+  cudaFree(t.d_doms);
+  cudaFree(t.d_tiles);
+  if (t.h_doms) cudaFreeHost(t.h_doms);
+  if (t.h_tiles) cudaFreeHost(t.h_tiles);
+  if (t.h_force) cudaFreeHost(t.h_force);
+  if (t.ev) cudaEventDestroy(t.ev);
+  t = TickSlot{};
 }
 
 }  // namespace
@@ -444,8 +689,13 @@ int lbm_server_create(int64_t budget_bytes, lbm_server **out) {
   s->budget = budget_bytes;
   cudaError_t e = cudaMalloc(&s->arena_ptr, budget_bytes);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking);
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&s->slot[k].ev, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     cudaFree(s->arena_ptr);
+    for (TickSlot &t : s->slot) free_slot(t);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->upload) cudaStreamDestroy(s->upload);
     delete s;
     return sfail(nullptr, e == cudaErrorMemoryAllocation ? LBM_ENOMEM : LBM_ECUDA,
                  std::string("server arena: ") + cudaGetErrorString(e));
@@ -462,13 +712,12 @@ int lbm_server_create(int64_t budget_bytes, lbm_server **out) {
 void lbm_server_destroy(lbm_server *s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->upload) cudaStreamSynchronize(s->upload);
   for (auto &kv : s->reqs) drop_amr(kv.second);
   cudaFree(s->arena_ptr);
-  cudaFree(s->d_doms);
-  cudaFree(s->d_tiles);
-  if (s->h_doms) cudaFreeHost(s->h_doms);
-  if (s->h_tiles) cudaFreeHost(s->h_tiles);
+  for (TickSlot &t : s->slot) free_slot(t);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->upload) cudaStreamDestroy(s->upload);
   delete s;
 }
 
@@ -482,13 +731,21 @@ int lbm_server_submit(lbm_server *s, int64_t id, const lbm_config *cfg, const fl
     return sfail(s, LBM_ENOTSUP, "the moving window runs in dense sessions and 3D AMR");
   if (steps < 1) return sfail(s, LBM_EINVAL, "steps must be >= 1");
   if (s->reqs.count(id)) return sfail(s, LBM_EINVAL, "request id already in use");
-  StepParams tmp{};
-  fill_step_params(*cfg, 1, 0, tmp);
-  const int64_t bytes = request_bytes(*cfg, force_tiles(*cfg, tmp));
+  const int kind = (int64_t)cfg->nx * cfg->ny * cfg->nz >= kStreamCells ? 2 : 0;
+  int64_t bytes = 0;
+  if (kind == 2) {
+    StepParams sp{};
+    bytes = streamed_bytes(*cfg, streamed_params(*cfg, sp));
+  } else {
+    StepParams tmp{};
+    fill_step_params(*cfg, 1, 0, tmp);
+    bytes = request_bytes(*cfg, force_tiles(*cfg, tmp));
+  }
   if (bytes > s->budget)
     return sfail(s, LBM_ENOSPC, "request needs " + std::to_string(bytes) + " bytes, more than the whole budget");
   Request r;
   r.id = id;
+  r.kind = kind;
   r.cfg = *cfg;
   r.steps = steps;
   r.t_submit = now_s(s);
@@ -534,7 +791,10 @@ int lbm_server_submit_amr3d(lbm_server *s, int64_t id, const lbm_amr3d_config *c
 int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done, int *n_done) {
   if (!s || max_steps < 1) return s ? sfail(s, LBM_EINVAL, "max_steps must be >= 1") : LBM_EINVAL;
   if (n_done) *n_done = 0;
-  // 1. admit: FIFO while the head fits, or the least total work first;
+  // 1. retire what the finished ticks completed (no waiting)
+  int rc = complete_ticks(s, false);
+  if (rc) return rc;
+  // 2. admit: FIFO while the head fits, or the least total work first;
   // the resident-cell cap keeps the GPU busy without making every request
   // share it (continuous batching's latency cost)
   int64_t resident = 0;
@@ -553,50 +813,43 @@ int lbm_server_poll(lbm_server *s, int max_steps, lbm_result *done, int max_done
     Request &r = s->reqs[s->queue.front()];
     if (capped(r)) break;
     bool ok = false;
-    int rc = admit(s, r, ok);
+    rc = admit(s, r, ok);
     if (rc) return rc;
     if (!ok) break;
     resident += request_cells(r);
     s->queue.pop_front();
   }
-  // 2. one tick: every resident unfinished request, up to the soonest finish
-  std::vector<Request *> act;
-  int k = max_steps;
-  for (auto &kv : s->reqs)
-    if (kv.second.state == 1) {
-      act.push_back(&kv.second);
-      k = std::min(k, kv.second.steps - kv.second.done);
-    }
-  if (!act.empty()) {
-    int rc = run_steps(s, act, k);
+  // 3. fill the free tick slots (oldest first), so that a tick is queued
+  // behind the one the host is about to wait for
+  for (int n = 0; n < 2; ++n) {
+    int si = -1;
+    for (int k = 0; k < 2; ++k)
+      if (!s->slot[k].busy) si = k;
+    if (si < 0) break;
+    const int64_t before = s->tick_seq;
+    rc = enqueue_tick(s, si, max_steps);
+    if (rc) return rc;
+    if (s->tick_seq == before) break;  // nothing left to step
+  }
+  // 4. nothing to report yet: wait for the oldest tick in flight
+  if (s->ready.empty()) {
+    rc = complete_ticks(s, true);
     if (rc) return rc;
   }
-  // 3. retire the finished ones
   int nd = 0;
-  for (Request *r : act) {
-    if (r->done < r->steps) continue;
-    if (done && nd >= max_done) break;  // the rest retire on the next poll
-    if (r->kind == 1) {
-      const int rc = lbm_amr3d_forces(r->amr, r->force);
-      if (rc) return sfail(s, rc, lbm_amr3d_last_error(r->amr));
-    } else {
-      SCK(s, cudaMemcpy(r->force, r->force_out, kForceSlots * 8, cudaMemcpyDeviceToHost));
-    }
-    r->state = 2;
-    r->t_done = now_s(s);
-    if (done && nd < max_done) {
-      lbm_result &o = done[nd];
-      o.id = r->id;
-      o.status = 0;
-      o.steps = r->done;
-      for (int j = 0; j < 6; ++j) o.forces[j] = r->force[j];
-      o.submit_s = r->t_submit;
-      o.admit_s = r->t_admit;
-      o.done_s = r->t_done;
-    }
-    ++nd;
+  while (!s->ready.empty() && done && nd < max_done) {
+    const Request &r = s->reqs[s->ready.front()];
+    s->ready.pop_front();
+    lbm_result &o = done[nd++];
+    o.id = r.id;
+    o.status = 0;
+    o.steps = r.enq;
+    for (int j = 0; j < 6; ++j) o.forces[j] = r.force[j];
+    o.submit_s = r.t_submit;
+    o.admit_s = r.t_admit;
+    o.done_s = r.t_done;
   }
-  if (n_done) *n_done = std::min(nd, max_done);
+  if (n_done) *n_done = nd;
   return LBM_OK;
 }
 
@@ -614,17 +867,15 @@ int lbm_server_read(lbm_server *s, int64_t id, float *f, float *mac) {
     if (rc) return sfail(s, rc, lbm_amr3d_last_error(r.amr));
     return LBM_OK;
   }
+  // a retired request's work is complete; its own stream (kind 2) is idle
+  cudaStream_t st = r.kind == 2 ? r.own : s->stream;
   if (f) {
-    if (r.cfg.storage == LBM_STORE_FP32) {
-      SCK(s, cudaMemcpyAsync(f, r.f[r.cur], (size_t)r.cfg.q * n * 4, cudaMemcpyDeviceToHost, s->stream));
-    } else {
-      // Unpack into the spare buffer's space (as f32 it may not fit): unpack
-      // plane groups through the mac field, which is overwritten by it.
+    if (r.cfg.storage != LBM_STORE_FP32)
       return sfail(s, LBM_ENOTSUP, "reading packed-storage f from the server is not supported; read mac");
-    }
+    SCK(s, cudaMemcpyAsync(f, r.f[r.cur], (size_t)r.cfg.q * n * 4, cudaMemcpyDeviceToHost, st));
   }
-  if (mac) SCK(s, cudaMemcpyAsync(mac, r.mac, n * 16, cudaMemcpyDeviceToHost, s->stream));
-  SCK(s, cudaStreamSynchronize(s->stream));
+  if (mac) SCK(s, cudaMemcpyAsync(mac, r.mac, n * 16, cudaMemcpyDeviceToHost, st));
+  SCK(s, cudaStreamSynchronize(st));
   return LBM_OK;
 }
 
@@ -636,8 +887,10 @@ int lbm_server_release(lbm_server *s, int64_t id) {
   if (it->second.state == 0) {
     s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), id), s->queue.end());
   } else {
+    // retired: its last tick is complete, no queued work reads its memory
     drop_amr(it->second);
     s->arena.release(it->second.off, it->second.bytes);
+    s->ready.erase(std::remove(s->ready.begin(), s->ready.end(), id), s->ready.end());
   }
   s->reqs.erase(it);
   return LBM_OK;

@@ -42,7 +42,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define LBM_ABI_VERSION 1
+#define LBM_ABI_VERSION 2
 
 typedef enum {
   LBM_OK = 0,
@@ -114,7 +114,14 @@ typedef struct {
                              body, a sponge and no wall on the axis          */
   int32_t win_anchor[3];  /* WIN_AX/AY/AZ: the cell the body sits in within
                              the window, the floor of its initial centre    */
-  int32_t reserved[1];    /* zero                                            */
+  int32_t trt;            /* two-relaxation-time collision (3D dense, batch,
+                             server; plans/TRT.md sec 8.0): the odd part of
+                             every direction pair relaxes at omega_- with
+                             tau_- = 1/2 + trt_lambda / (tau - 1/2), the even
+                             part at 1/tau as in BGK. 0 = BGK             */
+  float trt_lambda;       /* the magic parameter Lambda (3/16 in the
+                             reference's ?lambda= default); with trt = 1 it
+                             must be > 0                                   */
 } lbm_config;
 
 typedef struct lbm_session lbm_session;
@@ -282,6 +289,31 @@ int lbm_sync(lbm_session *s);
 
 /* Bytes of device memory the session holds. */
 int64_t lbm_device_bytes(const lbm_session *s);
+
+/* ---- z-slabs: one domain split across GPUs ---------------------------------
+ * No counterpart in the reference (one page steps one domain). A slab
+ * session holds planes [z0, z0 + nz_local) of the 3D domain `cfg` describes
+ * (one per GPU, one process per GPU): its physics -- body, walls, sponge,
+ * force region -- is the whole domain's, at the domain's own coordinates,
+ * and its cells are stored between a ghost plane below and one above. Every
+ * step needs the populations that cross its z faces from the neighbouring
+ * slabs (periodic in z: the last slab's upper neighbour is the first):
+ *   lbm_slab_pack(s, send_lo, send_hi)   its first plane's ez = -1 and last
+ *                                        plane's ez = +1 populations into
+ *                                        caller device buffers of
+ *                                        lbm_slab_halo_bytes(s) each;
+ *   exchange: send_lo to the slab below (its recv_hi), send_hi to the slab
+ *             above (its recv_lo) -- over NCCL or peer copies, by the caller;
+ *   lbm_slab_unpack(s, recv_lo, recv_hi) into the ghost planes;
+ *   lbm_step(s, 1).
+ * A slab's f, mac and totals cover its own planes; its lbm_forces is its
+ * share of the body force (the slabs' shares sum to the domain's). Slabs
+ * take no moving window, free body or headless view. The result of a step
+ * is the whole-domain step's, bit for bit, cell by cell. */
+int lbm_create_slab(const lbm_config *cfg, int z0, int nz_local, lbm_session **out);
+int64_t lbm_slab_halo_bytes(const lbm_session *s);
+int lbm_slab_pack(lbm_session *s, void *send_lo, void *send_hi);
+int lbm_slab_unpack(lbm_session *s, const void *recv_lo, const void *recv_hi);
 
 /* ---- allocation-free stepping --------------------------------------------
  * No counterpart in the reference: added for callers that cannot call
@@ -626,6 +658,11 @@ float lbm_f16_bits_to_f32(uint16_t h);
 /* AMR host rules of amr2d.mjs, as pure functions. */
 /* tauAtLevel (card-params.mjs:188): tau_m = 2 tau_{m-1} - 1/2. */
 double lbm_tau_at_level(double tau0, int m);
+/* The TRT pair (plans/TRT.md sec 8.1, d3-trt.mjs tauMinusOf / lambdaOf on
+ * the reference's TRT branch): tau_- = 1/2 + Lambda / (tau_+ - 1/2), and
+ * Lambda = (tau_+ - 1/2)(tau_- - 1/2). */
+double lbm_trt_tau_minus(double tau_plus, double lambda);
+double lbm_trt_lambda(double tau_plus, double tau_minus);
 /* Post-collision coarse->fine and fine->coarse non-equilibrium factors,
  * 0.5 (tf-1)/(tc-1) and 2 (tc-1)/(tf-1) (amr2d.mjs:136-141). */
 double lbm_dc_rescale_c2f(double tau_coarse, double tau_fine);
@@ -649,6 +686,11 @@ int lbm_active_slot_list(const int32_t *slot_to_block, int nslots, int32_t *out)
  * m >= 2 and the parents of all 9 periodic neighbours. Returns the number of
  * blocks added. */
 int lbm_cascade21(uint8_t **want, int levels, int nbx1, int nby1);
+/* The same closure on the device (amr_cascade.wgsl:114-157 completeQuads and
+ * balance, one deepest-first sweep of launches on cuda_stream): the masks
+ * are copied in, closed and copied back; returns the number of blocks added,
+ * or a negative status. Blocks until done. */
+int lbm_cascade21_device(uint8_t **want, int levels, int nbx1, int nby1, void *cuda_stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -34,7 +34,7 @@ class Config(C.Structure):
                 ("chi_eps", C.c_float), ("sponge_w", C.c_float),
                 ("sponge_axis", C.c_int32 * 3), ("sponge_u", C.c_float * 3),
                 ("body", Body), ("storage", C.c_int32), ("window", C.c_int32 * 3),
-                ("win_anchor", C.c_int32 * 3), ("reserved", C.c_int32 * 1)]
+                ("win_anchor", C.c_int32 * 3), ("trt", C.c_int32), ("trt_lambda", C.c_float)]
 
 
 def config_default(q: int, dims) -> Config:

@@ -118,6 +118,11 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
   const Win win = window_of(c);
   const R CS2 = R(1) / R(3);
   const R OMEGA = R(1) / R(c.tau);
+  // TRT (plans/TRT.md sec 8.0(1)-(2)): OMEGA_M = 1 / tau_- with
+  // tau_- = 1/2 + Lambda / (tau - 1/2) formed in double on the host, the
+  // odd part of each direction relaxing at OMEGA_M in the delta form
+  const double tau_m = 0.5 + (double)c.trt_lambda / ((double)c.tau - 0.5);
+  const R DW = c.trt ? R(1.0 / tau_m) - OMEGA : R(0);
   const R FX = R(c.force[0]), FY = R(c.force[1]), FZ = R(c.force[2]);
   const R SUX = R(c.sponge_u[0]), SUY = R(c.sponge_u[1]), SUZ = R(c.sponge_u[2]);
 #pragma omp parallel for collapse(2) schedule(static)
@@ -189,6 +194,13 @@ void step3(const lbm_config &c, const std::vector<R> &fin, std::vector<R> &fout,
                     ((ezf - uz) * R(3) + t2 * ezf) * Fz;
             R Si = (R(1) - R(0.5) * OMEGA) * w * dot;
             R fc = f[i] - OMEGA * (f[i] - feq) + Si;
+            if (c.trt) {
+              // f_minus = (f_i - f_opp)/2, feq_minus = 3 w rho e.u, S_minus = 3 w e.F
+              const R fminus = R(0.5) * (f[i] - f[T.opp[i]]);
+              const R feqminus = R(3) * w * rho * eu;
+              const R sminus = R(3) * w * (exf * Fx + eyf * Fy + ezf * Fz);
+              fc = fc - DW * (fminus - feqminus) - R(0.5) * DW * sminus;
+            }
             R euf = exf * SUX + eyf * SUY + ezf * SUZ;
             R ft = w * (R(1) + R(3) * euf + R(4.5) * euf * euf - R(1.5) * ufar);
             o = fc * (R(1) - sw) + ft * sw;

@@ -29,15 +29,15 @@ def test_library_exports_symbol(lbm, sym):
 
 
 def test_abi_version(lbm):
-    assert lbm.lib.lbm_abi_version() == 1
+    assert lbm.lib.lbm_abi_version() == 2
     assert b"sm_100a" in lbm.lib.lbm_version()
 
 
 def test_config_struct_size_matches_header(lbm):
     # lbm_config = 4 ints + tau + 3 floats + 3 ints + 2 floats + 5 ints + 2 floats
-    # + 3 ints + 3 floats + lbm_body(19*4) + storage + 7 reserved
+    # + 3 ints + 3 floats + lbm_body(19*4) + storage + window[3] + win_anchor[3] + trt + trt_lambda
     assert C.sizeof(lbm.Body) == 19 * 4
-    assert C.sizeof(lbm.Config) == (4 + 1 + 3 + 3 + 2 + 5 + 2 + 3 + 3) * 4 + 19 * 4 + 8 * 4
+    assert C.sizeof(lbm.Config) == (4 + 1 + 3 + 3 + 2 + 5 + 2 + 3 + 3) * 4 + 19 * 4 + 9 * 4
 
 
 @pytest.mark.parametrize("bad, msg", [

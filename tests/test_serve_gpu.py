@@ -196,3 +196,40 @@ def test_shortest_work_first_with_a_resident_cap(lbm):
         alone.close()
         srv.release(r["id"])
     srv.close()
+
+
+def test_large_requests_on_their_own_streams_equal_sessions(lbm):
+    """Dense requests of 64^3 cells and up run the dense session's own step
+    on their own streams beside the tile launches of the small ones: f, mac
+    and the force are the session's, bit for bit (the same kernels and the
+    same force-sum order)."""
+    from getting_air_b200 import scenarios as sc
+    reqs = sc.serving_stream(count=5, seed=21, nmin=24, nmax=80, steps=(20, 50))
+    big = [dict(r, dims=(64, 64, 64)) for r in reqs[:1]]
+    big[0]["kw"] = dict(big[0]["kw"], body=dict(big[0]["kw"]["body"], centre=(21, 32, 32)))
+    reqs = big + reqs[1:]
+    cfgs = {r["id"]: lbm.config_from(r["q"], r["dims"], **r["kw"]) for r in reqs}
+    assert sum(int(np.prod(r["dims"])) >= 1 << 18 for r in reqs) >= 1
+    srv = lbm.Server(4 << 30)
+    for r in reqs:
+        srv.submit(r["id"], cfgs[r["id"]], r["steps"])
+    got = drain(srv, [r["id"] for r in reqs])
+    for r in reqs:
+        cfg = cfgs[r["id"]]
+        f, mac = srv.read(r["id"], cfg)
+        alone = lbm.Solver(cfg)
+        ux, uy, uz = (np.float32(v) for v in cfg.sponge_u)
+        rho = np.float32(1) - (ux * ux + uy * uy + uz * uz) * np.float32(1.5)
+        alone.init_macro(np.tile(np.array([rho, ux, uy, uz], np.float32), (int(np.prod(r["dims"])), 1)))
+        alone.step(r["steps"])
+        assert np.array_equal(f, alone.read_f()), r["id"]
+        assert np.array_equal(mac, alone.read_mac()), r["id"]
+        want = np.array(alone.forces())
+        if int(np.prod(r["dims"])) >= 1 << 18:
+            assert np.array_equal(np.array(got[r["id"]]["forces"]), want), r["id"]
+        else:
+            assert np.allclose(got[r["id"]]["forces"], want, rtol=1e-10, atol=1e-12 * max(np.abs(want).max(), 1e-30))
+        alone.close()
+        srv.release(r["id"])
+    assert srv.stats()["bytes_used"] == 0
+    srv.close()
