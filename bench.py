@@ -395,11 +395,39 @@ def time_amr3d(lbm, steps, warmup, world):
     return out
 
 
-# The served form admits the least work first, with about one of the largest
+def time_amr3d_served_request(lbm, steps, warmup):
+    """The largest two-level AMR request of the served stream (a 180^3
+    rounded box, RB = 4, blocks within 2 cells refined) stepped alone as a
+    session: CUDA events around `steps` graph-launched macro-steps."""
+    import torch
+    from getting_air_b200 import scenarios as sc
+    reqs = [r for r in sc.serving_stream(count=48, seed=2024, rate=200.0, amr_frac=0.25) if r["levels"] == 2]
+    r = max(reqs, key=lambda x: int(np.prod(x["dims"])) * x["steps"])
+    a = lbm.Amr3D(sc.serving_config(lbm, r))
+    stream = torch.cuda.Stream()
+    a.set_stream(stream.cuda_stream)
+    a.init_macro(sc.uniform_macro(int(np.prod(r["dims"])), (0.05, 0.0, 0.0)))
+    a.step(max(warmup, 3))
+    a.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    a.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"request": {"id": r["id"], "q": r["q"], "dims": list(r["dims"]), "body": r["kw"]["body"]["shape"]},
+           "tiles": a.slots, "ms_per_macro_step": ms, "cell_updates_per_macro_step": a.cell_updates(),
+           "mlups": a.cell_updates() / (ms * 1e-3) / 1e6}
+    a.close()
+    return out
+
+
+# The served form admits the least work first, with about two of the largest
 # (192^3) requests' worth of cells resident: enough to keep the GPU busy, so
 # short requests do not share it with every long one. Measured on this
-# stream: p50 2.9 s against 10.3 s with no cap, at 4 % less throughput.
-SERVE_RESIDENT_CELLS = 8 << 20
+# stream (pipelined ticks): 7.7 GLUPS at p50 3.2 s, against 7.9 GLUPS at
+# p50 8.8 s with no cap.
+SERVE_RESIDENT_CELLS = 16 << 20
 
 
 def time_served(lbm, world, count=48, budget_gb=48, policy="sjf", max_resident_cells=SERVE_RESIDENT_CELLS):
@@ -666,6 +694,8 @@ def run_form(args):
         out = time_amr(lbm, args.steps, args.warmup, world)
     elif args.form == "amr3d_sphere":
         out = time_amr3d(lbm, args.steps, args.warmup, world)
+    elif args.form == "amr3d_served":
+        out = time_amr3d_served_request(lbm, args.steps, args.warmup)
     else:
         out = dict(zip(("served", "served_plain"), time_served(lbm, world)))
     print(json.dumps({"form": args.form, "steps": args.steps, "warmup": args.warmup, **out}))
@@ -681,7 +711,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--form", choices=("fp32", "fp16", "bf16", "d3q27_fp32", "d3q27_fp16", "batched", "amr2d_cylinder",
-                                       "amr3d_sphere", "served", "accuracy"),
+                                       "amr3d_sphere", "amr3d_served", "served", "accuracy"),
                     help="run one of the side forms alone (for profiling) and print its JSON line")
     ap.add_argument("--dims", type=str, default=None,
                     help="with --form fp32/fp16/bf16: a smaller sphere domain NX,NY,NZ (profiling captures)")

@@ -241,6 +241,8 @@ def _load() -> C.CDLL:
         "lbm_amr3d_manage_now": ([P], I),
         "lbm_amr2d_refine_round": ([P], I),
         "lbm_amr2d_set_auto_refine": ([P, I], I),
+        "lbm_amr2d_set_fused": ([P, I], I),
+        "lbm_amr2d_fused": ([P], I),
         "lbm_amr3d_device_bytes": ([C.POINTER(Amr3DConfig), P, C.POINTER(C.c_int64)], I),
         "lbm_amr3d_create_in": ([C.POINTER(Amr3DConfig), P, P, C.c_int64, C.POINTER(P)], I),
         "lbm_server_submit_amr3d": ([P, C.c_int64, C.POINTER(Amr3DConfig), F, I], I),
@@ -866,6 +868,14 @@ class Amr2D:
 
     def set_auto_refine(self, on: bool):
         self._check(lib.lbm_amr2d_set_auto_refine(self._h, int(bool(on))))
+
+    def set_fused(self, on: bool):
+        """One cooperative launch per macro-step (on) or six launches (off)."""
+        self._check(lib.lbm_amr2d_set_fused(self._h, int(bool(on))))
+
+    @property
+    def fused(self) -> bool:
+        return bool(lib.lbm_amr2d_fused(self._h))
 
     def forces(self):
         out = np.zeros(4, np.float64)

@@ -286,6 +286,32 @@ __device__ void interp_cell(const AmrParams &p, const float *__restrict__ f0, fl
   }
 }
 
+// One ring cell of tile `s` (block bx, by): the same-level neighbour's
+// interior cell when that neighbour is refined, else root interpolation.
+__device__ __forceinline__ void fill_ring_cell(const AmrParams &p, const float *__restrict__ f0,
+                                               float *__restrict__ f1, int s, int bx, int by, int fx, int fy) {
+  const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
+  const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
+  const int G = p.G, RB2 = p.RB2;
+  const bool inX = fx >= G && fx < G + RB2, inY = fy >= G && fy < G + RB2;
+  int ns, nfx = fx, nfy = fy;
+  if (inY && fx < G) { ns = p.blockSlot[by * p.NBX + bxm]; nfx = fx + RB2; }
+  else if (inY && fx >= G + RB2) { ns = p.blockSlot[by * p.NBX + bxp]; nfx = fx - RB2; }
+  else if (inX && fy < G) { ns = p.blockSlot[bym * p.NBX + bx]; nfy = fy + RB2; }
+  else if (inX && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bx]; nfy = fy - RB2; }
+  else if (fx < G && fy < G) { ns = p.blockSlot[bym * p.NBX + bxm]; nfx = fx + RB2; nfy = fy + RB2; }
+  else if (fx >= G + RB2 && fy < G) { ns = p.blockSlot[bym * p.NBX + bxp]; nfx = fx - RB2; nfy = fy + RB2; }
+  else if (fx < G && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bxm]; nfx = fx + RB2; nfy = fy - RB2; }
+  else { ns = p.blockSlot[byp * p.NBX + bxp]; nfx = fx - RB2; nfy = fy - RB2; }
+  if (ns >= 0) {
+    const int64_t dst = pcell(p, s, fx, fy), src = pcell(p, ns, nfx, nfy);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f1[i * p.N1 + dst] = f1[i * p.N1 + src];
+  } else {
+    interp_cell(p, f0, f1, s, bx, by, fx, fy);
+  }
+}
+
 // mode 0: ring of every active tile (same-level neighbour copy, else root
 // interpolation); mode 1: every cell of the tiles activated this round.
 __global__ void __launch_bounds__(kChunk)
@@ -297,8 +323,6 @@ __global__ void __launch_bounds__(kChunk)
     const int s = p.activeList[k];
     if (mode == 1 && !p.newly[s]) continue;
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
-    const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
-    const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
     const int G = p.G, RB2 = p.RB2, FB = p.FB;
     for (int c = c0 + threadIdx.x; c < c1; c += kChunk) {
       const int fx = c % FB, fy = c / FB;
@@ -308,22 +332,7 @@ __global__ void __launch_bounds__(kChunk)
         continue;
       }
       if (inX && inY) continue;
-      int ns, nfx = fx, nfy = fy;
-      if (inY && fx < G) { ns = p.blockSlot[by * p.NBX + bxm]; nfx = fx + RB2; }
-      else if (inY && fx >= G + RB2) { ns = p.blockSlot[by * p.NBX + bxp]; nfx = fx - RB2; }
-      else if (inX && fy < G) { ns = p.blockSlot[bym * p.NBX + bx]; nfy = fy + RB2; }
-      else if (inX && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bx]; nfy = fy - RB2; }
-      else if (fx < G && fy < G) { ns = p.blockSlot[bym * p.NBX + bxm]; nfx = fx + RB2; nfy = fy + RB2; }
-      else if (fx >= G + RB2 && fy < G) { ns = p.blockSlot[bym * p.NBX + bxp]; nfx = fx - RB2; nfy = fy + RB2; }
-      else if (fx < G && fy >= G + RB2) { ns = p.blockSlot[byp * p.NBX + bxm]; nfx = fx + RB2; nfy = fy - RB2; }
-      else { ns = p.blockSlot[byp * p.NBX + bxp]; nfx = fx - RB2; nfy = fy - RB2; }
-      if (ns >= 0) {
-        const int64_t dst = pcell(p, s, fx, fy), src = pcell(p, ns, nfx, nfy);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) f1[i * p.N1 + dst] = f1[i * p.N1 + src];
-      } else {
-        interp_cell(p, f0, f1, s, bx, by, fx, fy);
-      }
+      fill_ring_cell(p, f0, f1, s, bx, by, fx, fy);
     }
   }
 }
@@ -333,150 +342,222 @@ __global__ void __launch_bounds__(kChunk)
 // that neighbour is refined, else from this tile's ring), BGK + Guo at
 // tau_f with the chi penalty on this level's band, sponge, SOLID_EQ. Every
 // cell of the tile, ring included, collides (COLLIDE_RING = 1).
+__device__ __forceinline__ void substep_cell(const AmrParams &p, const float *__restrict__ fin,
+                                             float *__restrict__ fout, float2 *__restrict__ vel1, int s, int bx,
+                                             int by, int fx, int fy) {
+  const float Wf = (float)p.W, Hf = (float)p.H;
+  const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
+  const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
+  const int G = p.G, RB2 = p.RB2, FB = p.FB;
+  const int offX = fx <= G ? -1 : (fx + 1 >= G + RB2 ? 1 : 0);
+  const int offY = fy <= G ? -1 : (fy + 1 >= G + RB2 ? 1 : 0);
+  const int cxb = offX > 0 ? bxp : (offX < 0 ? bxm : bx);
+  const int cyb = offY > 0 ? byp : (offY < 0 ? bym : by);
+  const int nbrX = offX ? p.blockSlot[by * p.NBX + cxb] : -1;
+  const int nbrY = offY ? p.blockSlot[cyb * p.NBX + bx] : -1;
+  const int nbrXY = (offX && offY) ? p.blockSlot[cyb * p.NBX + cxb] : -1;
+  const int64_t cell = pcell(p, s, fx, fy);
+  const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
+  float wx = fmodf(px, Wf); if (wx < 0.f) wx += Wf;
+  float wy = fmodf(py, Hf); if (wy < 0.f) wy += Hf;
+  const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
+  const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
+  const float phi = phi2(px, py, p.body, Wf, Hf);
+  const bool near = p.bb && phi < 2.0f;  // a link is at most sqrt(2)/2 root cells long here
+  float f[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int ex = L9::ex(i), ey = L9::ey(i);
+    if (near && phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
+      const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+      f[i] = __ldg(fin + L9::opp(i) * p.N1 + cell) + corr;
+      continue;
+    }
+    int sx = fx - ex, sy = fy - ey, src = s;
+    const int ox = (sx < G || sx >= G + RB2) ? offX : 0;
+    const int oy = (sy < G || sy >= G + RB2) ? offY : 0;
+    const int ns = (ox && oy) ? nbrXY : (ox ? nbrX : (oy ? nbrY : -1));
+    if (ns >= 0) { src = ns; sx -= ox * RB2; sy -= oy * RB2; }
+    sx = min(max(sx, 0), FB - 1);
+    sy = min(max(sy, 0), FB - 1);
+    f[i] = __ldg(fin + i * p.N1 + pcell(p, src, sx, sy));
+  }
+  float rho = 0.f, uxs = 0.f, uys = 0.f;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    rho += f[i];
+    uxs += f[i] * (float)L9::ex(i);
+    uys += f[i] * (float)L9::ey(i);
+  }
+  const float den = fmaxf(rho, 1e-6f);
+  uxs /= den;
+  uys /= den;
+  const float chi = p.bb ? 0.f : chi_from_phi(phi, p.eps_f);
+  const float Fx = rho * chi * (usx - uxs) + p.fx;
+  const float Fy = rho * chi * (usy - uys) + p.fy;
+  const float ux = uxs + Fx / (2.0f * den), uy = uys + Fy / (2.0f * den);
+  const float usq = ux * ux + uy * uy;
+  vel1[cell] = make_float2(ux, uy);
+  if (p.explode && !(fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2)) {
+    // explode/coalesce: the ring advects without colliding (COLLIDE_RING = 0)
+#pragma unroll
+    for (int i = 0; i < 9; ++i) fout[i * p.N1 + cell] = f[i];
+    return;
+  }
+  const float dx = fminf(wx, Wf - 1.0f - wx), dy = fminf(wy, Hf - 1.0f - wy);
+  const float sw = sponge_weight(fminf(dx, dy), p.sponge_w);
+  const bool solid = p.solid_eq && p.bb && phi < 0.f;
+  const float omg = p.omega_f, sfac = 1.0f - 0.5f * omg;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const float exf = (float)L9::ex(i), eyf = (float)L9::ey(i), w = L9::w(i);
+    float o;
+    if (solid) {
+      o = feq9(1.0f, usx, usy, i);
+    } else {
+      const float eu = exf * ux + eyf * uy;
+      const float fe = w * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
+      const float t2 = (exf * ux + eyf * uy) * 9.0f;
+      const float Si = sfac * w * (((exf - ux) * 3.0f + t2 * exf) * Fx + ((eyf - uy) * 3.0f + t2 * eyf) * Fy);
+      const float fc = f[i] - omg * (f[i] - fe) + Si;
+      o = fc * (1.0f - sw) + p.ftarget[i] * sw;
+    }
+    fout[i * p.N1 + cell] = o;
+  }
+}
+
 __global__ void __launch_bounds__(kChunk)
     amr_substep(const float *__restrict__ fin, float *__restrict__ fout, float2 *__restrict__ vel1,
                 const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
-  const float Wf = (float)p.W, Hf = (float)p.H;
   const int FB2 = p.FB * p.FB, nch = (FB2 + kChunk - 1) / kChunk;
   for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
     const int k = w / nch, c0 = (w % nch) * kChunk, c1 = min(c0 + kChunk, FB2);
     const int s = p.activeList[k];
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
-    const int bxm = (bx + p.NBX - 1) % p.NBX, bxp = (bx + 1) % p.NBX;
-    const int bym = (by + p.NBY - 1) % p.NBY, byp = (by + 1) % p.NBY;
-    const int G = p.G, RB2 = p.RB2, FB = p.FB;
-    for (int c = c0 + threadIdx.x; c < c1; c += kChunk) {
-      const int fx = c % FB, fy = c / FB;
-      const int offX = fx <= G ? -1 : (fx + 1 >= G + RB2 ? 1 : 0);
-      const int offY = fy <= G ? -1 : (fy + 1 >= G + RB2 ? 1 : 0);
-      const int cxb = offX > 0 ? bxp : (offX < 0 ? bxm : bx);
-      const int cyb = offY > 0 ? byp : (offY < 0 ? bym : by);
-      const int nbrX = offX ? p.blockSlot[by * p.NBX + cxb] : -1;
-      const int nbrY = offY ? p.blockSlot[cyb * p.NBX + bx] : -1;
-      const int nbrXY = (offX && offY) ? p.blockSlot[cyb * p.NBX + cxb] : -1;
-      const int64_t cell = pcell(p, s, fx, fy);
-      const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
-      float wx = fmodf(px, Wf); if (wx < 0.f) wx += Wf;
-      float wy = fmodf(py, Hf); if (wy < 0.f) wy += Hf;
-      const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
-      const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
-      const float phi = phi2(px, py, p.body, Wf, Hf);
-      const bool near = p.bb && phi < 2.0f;  // a link is at most sqrt(2)/2 root cells long here
-      float f[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        const int ex = L9::ex(i), ey = L9::ey(i);
-        if (near && phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
-          const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
-          f[i] = __ldg(fin + L9::opp(i) * p.N1 + cell) + corr;
-          continue;
-        }
-        int sx = fx - ex, sy = fy - ey, src = s;
-        const int ox = (sx < G || sx >= G + RB2) ? offX : 0;
-        const int oy = (sy < G || sy >= G + RB2) ? offY : 0;
-        const int ns = (ox && oy) ? nbrXY : (ox ? nbrX : (oy ? nbrY : -1));
-        if (ns >= 0) { src = ns; sx -= ox * RB2; sy -= oy * RB2; }
-        sx = min(max(sx, 0), FB - 1);
-        sy = min(max(sy, 0), FB - 1);
-        f[i] = __ldg(fin + i * p.N1 + pcell(p, src, sx, sy));
-      }
-      float rho = 0.f, uxs = 0.f, uys = 0.f;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        rho += f[i];
-        uxs += f[i] * (float)L9::ex(i);
-        uys += f[i] * (float)L9::ey(i);
-      }
-      const float den = fmaxf(rho, 1e-6f);
-      uxs /= den;
-      uys /= den;
-      const float chi = p.bb ? 0.f : chi_from_phi(phi, p.eps_f);
-      const float Fx = rho * chi * (usx - uxs) + p.fx;
-      const float Fy = rho * chi * (usy - uys) + p.fy;
-      const float ux = uxs + Fx / (2.0f * den), uy = uys + Fy / (2.0f * den);
-      const float usq = ux * ux + uy * uy;
-      vel1[cell] = make_float2(ux, uy);
-      if (p.explode && !(fx >= G && fx < G + RB2 && fy >= G && fy < G + RB2)) {
-        // explode/coalesce: the ring advects without colliding (COLLIDE_RING = 0)
-#pragma unroll
-        for (int i = 0; i < 9; ++i) fout[i * p.N1 + cell] = f[i];
-        continue;
-      }
-      const float dx = fminf(wx, Wf - 1.0f - wx), dy = fminf(wy, Hf - 1.0f - wy);
-      const float sw = sponge_weight(fminf(dx, dy), p.sponge_w);
-      const bool solid = p.solid_eq && p.bb && phi < 0.f;
-      const float omg = p.omega_f, sfac = 1.0f - 0.5f * omg;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        const float exf = (float)L9::ex(i), eyf = (float)L9::ey(i), w = L9::w(i);
-        float o;
-        if (solid) {
-          o = feq9(1.0f, usx, usy, i);
-        } else {
-          const float eu = exf * ux + eyf * uy;
-          const float fe = w * rho * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * usq);
-          const float t2 = (exf * ux + eyf * uy) * 9.0f;
-          const float Si = sfac * w * (((exf - ux) * 3.0f + t2 * exf) * Fx + ((eyf - uy) * 3.0f + t2 * eyf) * Fy);
-          const float fc = f[i] - omg * (f[i] - fe) + Si;
-          o = fc * (1.0f - sw) + p.ftarget[i] * sw;
-        }
-        fout[i * p.N1 + cell] = o;
-      }
-    }
+    for (int c = c0 + threadIdx.x; c < c1; c += kChunk) substep_cell(p, fin, fout, vel1, s, bx, by, c % p.FB, c / p.FB);
   }
 }
 
-// 4-child restriction into the root (common_average.wgsl averageCell).
+// 4-child restriction into the root (common_average.wgsl averageCell): root
+// cell c (of RB x RB) of tile s's block.
+__device__ __forceinline__ void average_cell(const AmrParams &p, const float *__restrict__ f1, float *__restrict__ f0,
+                                             int s, int bx, int by, int c) {
+  const int lx = c % p.RB, ly = c / p.RB;
+  const int fx0 = p.G + 2 * lx, fy0 = p.G + 2 * ly;
+  const int64_t ch[4] = {pcell(p, s, fx0, fy0), pcell(p, s, fx0 + 1, fy0), pcell(p, s, fx0, fy0 + 1),
+                         pcell(p, s, fx0 + 1, fy0 + 1)};
+  float fneq_sum[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) fneq_sum[i] = 0.f;
+  float rs = 0.f, rxs = 0.f, rys = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float f[9], rho = 0.f, ux = 0.f, uy = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      f[i] = __ldg(f1 + i * p.N1 + ch[q]);
+      rho += f[i];
+      ux += f[i] * (float)L9::ex(i);
+      uy += f[i] * (float)L9::ey(i);
+    }
+    ux /= fmaxf(rho, 1e-6f);
+    uy /= fmaxf(rho, 1e-6f);
+    rs += rho;
+    rxs += rho * ux;
+    rys += rho * uy;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) fneq_sum[i] += f[i] - feq9(rho, ux, uy, i);
+  }
+  const float ra = rs * 0.25f, den = fmaxf(rs, 1e-6f);
+  const float uxa = rxs / den, uya = rys / den;
+  const int64_t pc = (int64_t)(by * p.RB + ly) * p.W + (bx * p.RB + lx);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) f0[i * p.N0 + pc] = feq9(ra, uxa, uya, i) + p.resc_f2c * (fneq_sum[i] * 0.25f);
+}
+
 __global__ void __launch_bounds__(64)
     amr_average(const float *__restrict__ f1, float *__restrict__ f0, const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
   for (int k = blockIdx.x; k < n; k += gridDim.x) {
     const int s = p.activeList[k];
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
-    for (int c = threadIdx.x; c < p.RB * p.RB; c += 64) {
-      const int lx = c % p.RB, ly = c / p.RB;
-      const int fx0 = p.G + 2 * lx, fy0 = p.G + 2 * ly;
-      const int64_t ch[4] = {pcell(p, s, fx0, fy0), pcell(p, s, fx0 + 1, fy0), pcell(p, s, fx0, fy0 + 1),
-                             pcell(p, s, fx0 + 1, fy0 + 1)};
-      float fneq_sum[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) fneq_sum[i] = 0.f;
-      float rs = 0.f, rxs = 0.f, rys = 0.f;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        float f[9], rho = 0.f, ux = 0.f, uy = 0.f;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-          f[i] = __ldg(f1 + i * p.N1 + ch[q]);
-          rho += f[i];
-          ux += f[i] * (float)L9::ex(i);
-          uy += f[i] * (float)L9::ey(i);
-        }
-        ux /= fmaxf(rho, 1e-6f);
-        uy /= fmaxf(rho, 1e-6f);
-        rs += rho;
-        rxs += rho * ux;
-        rys += rho * uy;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) fneq_sum[i] += f[i] - feq9(rho, ux, uy, i);
-      }
-      const float ra = rs * 0.25f, den = fmaxf(rs, 1e-6f);
-      const float uxa = rxs / den, uya = rys / den;
-      const int64_t pc = (int64_t)(by * p.RB + ly) * p.W + (bx * p.RB + lx);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) f0[i * p.N0 + pc] = feq9(ra, uxa, uya, i) + p.resc_f2c * (fneq_sum[i] * 0.25f);
-    }
+    for (int c = threadIdx.x; c < p.RB * p.RB; c += 64) average_cell(p, f1, f0, s, bx, by, c);
   }
 }
 
-// Finest-level force (amr_force1.wgsl forceCell): interior cells of every
-// active tile, momentum exchange or penalty weighted by dx = 1/2, one FP64
-// partial per tile and a deterministic last-block sum.
+// Finest-level force (amr_force1.wgsl forceCell): this thread's share of
+// the interior cells of tile s (cells threadIdx.x, + kPoolThreads, ...),
+// momentum exchange or penalty weighted by dx = 1/2.
+__device__ __forceinline__ void force_tile_acc(const AmrParams &p, const float *__restrict__ f1, int s, int bx, int by,
+                                               ForceAcc &acc) {
+  const float Wf = (float)p.W, Hf = (float)p.H;
+  for (int c = threadIdx.x; c < p.RB2 * p.RB2; c += kPoolThreads) {
+    const int fx = p.G + c % p.RB2, fy = p.G + c / p.RB2;
+    const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
+    const float phi = phi2(px, py, p.body, Wf, Hf);
+    const int64_t cell = pcell(p, s, fx, fy);
+    const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
+    const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
+    float fxb = 0.f, fyb = 0.f, tz = 0.f;
+    if (p.bb) {
+      if (phi >= 0.f && phi < 2.0f) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          const int ex = L9::ex(i), ey = L9::ey(i);
+          if (phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
+            const float fo = __ldg(f1 + L9::opp(i) * p.N1 + cell);
+            const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+            fxb += -(float)ex * (2.f * fo + corr) * 0.5f;
+            fyb += -(float)ey * (2.f * fo + corr) * 0.5f;
+          }
+        }
+        tz = rx * fyb - ry * fxb;
+      }
+    } else {
+      const float chi = chi_from_phi(phi, p.eps_f);
+      if (chi >= 1e-6f) {
+        float rho = 0.f, ux = 0.f, uy = 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+          const int sx0 = fx - L9::ex(i), sy0 = fy - L9::ey(i);
+          const int sx = min(max(sx0, 0), p.FB - 1), sy = min(max(sy0, 0), p.FB - 1);
+          int64_t src = pcell(p, s, sx, sy);
+          if (p.explode) {
+            // RING_FREE_FORCE: sources past the interior resolve as the step's do
+            const int ox = sx0 >= p.G + p.RB2 ? 1 : (sx0 < p.G ? -1 : 0);
+            const int oy = sy0 >= p.G + p.RB2 ? 1 : (sy0 < p.G ? -1 : 0);
+            if (ox || oy) {
+              const int ns = p.blockSlot[((by + oy + p.NBY) % p.NBY) * p.NBX + (bx + ox + p.NBX) % p.NBX];
+              if (ns >= 0) src = pcell(p, ns, sx0 - ox * p.RB2, sy0 - oy * p.RB2);
+            }
+          }
+          const float v = __ldg(f1 + i * p.N1 + src);
+          rho += v;
+          ux += v * (float)L9::ex(i);
+          uy += v * (float)L9::ey(i);
+        }
+        ux /= fmaxf(rho, 1e-6f);
+        uy /= fmaxf(rho, 1e-6f);
+        const float Fx = rho * chi * (usx - ux), Fy = rho * chi * (usy - uy);
+        fxb = -Fx * 0.5f;
+        fyb = -Fy * 0.5f;
+        tz = rx * fyb - ry * fxb;
+      }
+    }
+    CellForce cf;
+    cf.fx = fxb;
+    cf.fy = fyb;
+    cf.tz = tz;
+    acc.add(cf);
+  }
+}
+
+// The force of every active tile: one FP64 partial per tile and a
+// deterministic last-block sum.
 __global__ void __launch_bounds__(kPoolThreads)
     amr_force(const float *__restrict__ f1, const __grid_constant__ AmrParams p) {
   const int n = p.counts[1];
-  const float Wf = (float)p.W, Hf = (float)p.H;
   if (n == 0) {
     if (blockIdx.x == 0 && threadIdx.x < 4) p.force_out[threadIdx.x] = 0.0;
     return;
@@ -485,68 +566,161 @@ __global__ void __launch_bounds__(kPoolThreads)
     const int s = p.activeList[k];
     const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
     ForceAcc acc;
-    for (int c = threadIdx.x; c < p.RB2 * p.RB2; c += kPoolThreads) {
-      const int fx = p.G + c % p.RB2, fy = p.G + c / p.RB2;
-      const float px = pool_pos(p, bx, fx), py = pool_pos(p, by, fy);
-      const float phi = phi2(px, py, p.body, Wf, Hf);
-      const int64_t cell = pcell(p, s, fx, fy);
-      const float rx = wrap_delta(px - p.body.cx, Wf), ry = wrap_delta(py - p.body.cy, Hf);
-      const float usx = p.body.vx - p.body.wz * ry, usy = p.body.vy + p.body.wz * rx;
-      float fxb = 0.f, fyb = 0.f, tz = 0.f;
-      if (p.bb) {
-        if (phi >= 0.f && phi < 2.0f) {
-#pragma unroll
-          for (int i = 0; i < 9; ++i) {
-            const int ex = L9::ex(i), ey = L9::ey(i);
-            if (phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
-              const float fo = __ldg(f1 + L9::opp(i) * p.N1 + cell);
-              const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
-              fxb += -(float)ex * (2.f * fo + corr) * 0.5f;
-              fyb += -(float)ey * (2.f * fo + corr) * 0.5f;
-            }
-          }
-          tz = rx * fyb - ry * fxb;
-        }
-      } else {
-        const float chi = chi_from_phi(phi, p.eps_f);
-        if (chi >= 1e-6f) {
-          float rho = 0.f, ux = 0.f, uy = 0.f;
-#pragma unroll
-          for (int i = 0; i < 9; ++i) {
-            const int sx0 = fx - L9::ex(i), sy0 = fy - L9::ey(i);
-            const int sx = min(max(sx0, 0), p.FB - 1), sy = min(max(sy0, 0), p.FB - 1);
-            int64_t src = pcell(p, s, sx, sy);
-            if (p.explode) {
-              // RING_FREE_FORCE: sources past the interior resolve as the step's do
-              const int ox = sx0 >= p.G + p.RB2 ? 1 : (sx0 < p.G ? -1 : 0);
-              const int oy = sy0 >= p.G + p.RB2 ? 1 : (sy0 < p.G ? -1 : 0);
-              if (ox || oy) {
-                const int ns = p.blockSlot[((by + oy + p.NBY) % p.NBY) * p.NBX + (bx + ox + p.NBX) % p.NBX];
-                if (ns >= 0) src = pcell(p, ns, sx0 - ox * p.RB2, sy0 - oy * p.RB2);
-              }
-            }
-            const float v = __ldg(f1 + i * p.N1 + src);
-            rho += v;
-            ux += v * (float)L9::ex(i);
-            uy += v * (float)L9::ey(i);
-          }
-          ux /= fmaxf(rho, 1e-6f);
-          uy /= fmaxf(rho, 1e-6f);
-          const float Fx = rho * chi * (usx - ux), Fy = rho * chi * (usy - uy);
-          fxb = -Fx * 0.5f;
-          fyb = -Fy * 0.5f;
-          tz = rx * fyb - ry * fxb;
-        }
-      }
-      CellForce cf;
-      cf.fx = fxb;
-      cf.fy = fyb;
-      cf.tz = tz;
-      acc.add(cf);
-    }
+    force_tile_acc(p, f1, s, bx, by, acc);
     reduce_force<kPoolThreads>(acc, p.partials, p.counter, n, k, p.force_out);
     __syncthreads();
   }
+}
+
+// ---- the interp macro-step as one cooperative launch -----------------------
+// The six launches of a macro-step (force, ring fill, root step, two
+// substeps, restriction) are latency-bound: 64 tiles are 25,600 pool cells,
+// and each launch mostly waits on a chain of dependent loads and on its own
+// start and drain. Here one launch of resident blocks runs them as phases
+// separated by grid barriers:
+//   0  force partials of every tile | ring fill | root step   (independent)
+//   1  force sum (block 0) | substep a -> b
+//   2  substep b -> a
+//   3  restriction into the root
+// Every cell goes through the same device function as in the separate
+// kernels (fill_ring_cell, cell2, substep_cell, average_cell,
+// force_tile_acc, the same block tree and fixed-order partial sum), so the
+// result is theirs to the bit. 256-thread blocks: the force tree must see
+// amr_force's thread mapping.
+
+struct MacroArgs {
+  const float *f0in;
+  float *f0out;
+  float *mac;
+  float *f1a, *f1b;
+  float2 *vel1;
+  unsigned *bar;  // arrivals, generation
+  int *bar_err;
+  unsigned nblocks;
+};
+
+// About a second of polling (2^22 waits of ~256 ns) before a barrier gives
+// up, flags the error and lets its block go on: the launch then ends (its
+// result void, reported by lbm_amr2d_sync as LBM_ETIMEDOUT) instead of
+// holding the GPU. A cooperative launch has every block resident, so a
+// healthy barrier releases within microseconds.
+constexpr unsigned long long kBarrierSpins = 1ull << 22;
+
+__device__ __forceinline__ void grid_barrier(unsigned *bar, int *err, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);  // re-armed before the release
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (*gen == g) {
+        if (++spins > kBarrierSpins) {
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(256);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPoolThreads)
+    amr_macro_fused(const __grid_constant__ AmrParams p, const __grid_constant__ StepParams rp,
+                    const __grid_constant__ MacroArgs m) {
+  __shared__ double sm[kForceSlots * (kPoolThreads / 32)];
+  const int n = p.counts[1];
+  const int FB = p.FB, FB2 = FB * FB, nch = (FB2 + kPoolThreads - 1) / kPoolThreads;
+  const int nroot = (int)((p.N0 + kPoolThreads - 1) / kPoolThreads);
+  // 0: force partials (time t, pool), ring fill (from the root at t), root step
+  for (int w = blockIdx.x; w < n + n * nch + nroot; w += gridDim.x) {
+    if (w < n) {
+      const int s = p.activeList[w];
+      const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+      ForceAcc acc;
+      force_tile_acc(p, m.f1a, s, bx, by, acc);
+      double v[kForceSlots];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v[k] = acc.v[k];
+      v[6] = acc.bad;
+      v[7] = 0.0;
+      block_sum<kForceSlots, kPoolThreads>(v, sm);
+      if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < kForceSlots; ++k) p.partials[(int64_t)w * kForceSlots + k] = v[k];
+      __syncthreads();
+    } else if (w < n + n * nch) {
+      const int k = (w - n) / nch, c = ((w - n) % nch) * kPoolThreads + threadIdx.x;
+      if (c < FB2) {
+        const int s = p.activeList[k];
+        const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+        const int fx = c % FB, fy = c / FB;
+        const bool inX = fx >= p.G && fx < p.G + p.RB2, inY = fy >= p.G && fy < p.G + p.RB2;
+        if (!(inX && inY)) fill_ring_cell(p, m.f0in, m.f1a, s, bx, by, fx, fy);
+      }
+    } else {
+      const int c = (w - n - n * nch) * kPoolThreads + threadIdx.x;
+      if (c < p.N0) {
+        CellForce cf;
+        cell2<float>(m.f0in, m.f0out, m.mac, rp, c % p.W, c / p.W, false, cf);
+      }
+    }
+  }
+  grid_barrier(m.bar, m.bar_err, m.nblocks);
+  // 1: the force of this macro-step, and substep a -> b
+  if (blockIdx.x == 0) {
+    if (n == 0) {
+      if (threadIdx.x < 4) p.force_out[threadIdx.x] = 0.0;
+    } else if (threadIdx.x < 32) {
+      sum_partials_warp<kForceSlots>(p.partials, n, p.force_out);
+    }
+  }
+  for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
+    const int k = w / nch, c = (w % nch) * kPoolThreads + threadIdx.x;
+    if (c >= FB2) continue;
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    substep_cell(p, m.f1a, m.f1b, m.vel1, s, bx, by, c % FB, c / FB);
+  }
+  grid_barrier(m.bar, m.bar_err, m.nblocks);
+  // 2: substep b -> a
+  for (int w = blockIdx.x; w < n * nch; w += gridDim.x) {
+    const int k = w / nch, c = (w % nch) * kPoolThreads + threadIdx.x;
+    if (c >= FB2) continue;
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    substep_cell(p, m.f1b, m.f1a, m.vel1, s, bx, by, c % FB, c / FB);
+  }
+  grid_barrier(m.bar, m.bar_err, m.nblocks);
+  // 3: restriction of the pool into the root at t + 1
+  const int RR = p.RB * p.RB, nrr = (RR + kPoolThreads - 1) / kPoolThreads;
+  for (int w = blockIdx.x; w < n * nrr; w += gridDim.x) {
+    const int k = w / nrr, c = (w % nrr) * kPoolThreads + threadIdx.x;
+    if (c >= RR) continue;
+    const int s = p.activeList[k];
+    const int bid = p.slotToBlock[s], bx = bid % p.NBX, by = bid / p.NBX;
+    average_cell(p, m.f1a, m.f0out, s, bx, by, c);
+  }
+}
+
+// Blocks of the fused macro-step's cooperative launch on the current device
+// (every one resident), or 0 where it cannot run: the explode interface, or
+// a device without cooperative launches.
+int fused_blocks(const AmrParams &p) {
+  int dev = 0, sms = 0, coop = 0, per_sm = 0;
+  if (p.explode || cudaGetDevice(&dev) != cudaSuccess) return 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  const bool ok = coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amr_macro_fused, kPoolThreads, 0) ==
+                              cudaSuccess;
+  cudaGetLastError();
+  return ok ? per_sm * sms : 0;
 }
 
 // ---- explode / coalesce interface ------------------------------------------------
@@ -694,6 +868,11 @@ struct lbm_amr2d {
   double *host = nullptr;
   int *host_counts = nullptr;
   int grid_slots = 0;
+  // the fused macro-step: resident blocks of one cooperative launch (0: off)
+  // and its grid barrier's state and timeout flag
+  int fused_grid = 0;
+  unsigned *bar = nullptr;
+  int *bar_err = nullptr;
   std::string err;
 };
 
@@ -725,6 +904,7 @@ void release_amr(lbm_amr2d *a) {
   cudaFree(p.blockSlot); cudaFree(p.slotToBlock); cudaFree(p.parentSlot); cudaFree(p.freeList);
   cudaFree(p.counts); cudaFree(p.activeList); cudaFree(p.want); cudaFree(p.newly); cudaFree(p.crit);
   cudaFree(p.partials); cudaFree(p.counter); cudaFree(p.force_out);
+  cudaFree(a->bar); cudaFree(a->bar_err);
   if (a->host) cudaFreeHost(a->host);
   if (a->host_counts) cudaFreeHost(a->host_counts);
   if (a->own) cudaStreamDestroy(a->own);
@@ -756,8 +936,8 @@ int validate_amr(const lbm_amr2d_config *c, std::string &why) {
 int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
   AmrParams &p = a->p;
   const int g = a->grid_slots;
-  amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
   if (p.explode) {
+    amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
     // amr2d-gpu.mjs:1096-1124 S_AdvanceExplode: the L0 step runs LAST
     amr_explode<<<g, kChunk, 0, st>>>(a->f0[from], a->f1[0], p);
     amr_substep<<<g, kChunk, 0, st>>>(a->f1[0], a->f1[1], a->vel1, p);
@@ -771,6 +951,24 @@ int macro_launches(lbm_amr2d *a, cudaStream_t st, int from) {
     ACK(a, cudaGetLastError());
     return LBM_OK;
   }
+  if (a->fused_grid > 0) {
+    StepParams rp = a->root;
+    rp.write_mac = 1;
+    const MacroArgs m{a->f0[from], a->f0[1 - from], (float *)a->mac, a->f1[0], a->f1[1], a->vel1, a->bar,
+                      a->bar_err, (unsigned)a->fused_grid};
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(a->fused_grid);
+    lc.blockDim = dim3(kPoolThreads);
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    ACK(a, cudaLaunchKernelEx(&lc, amr_macro_fused, p, rp, m));
+    return LBM_OK;
+  }
+  amr_force<<<g, kPoolThreads, 0, st>>>(a->f1[0], p);
   amr_fill<<<g, kChunk, 0, st>>>(a->f0[from], a->f1[0], 0, p);
   StepParams rp = a->root;
   rp.write_mac = 1;
@@ -808,6 +1006,12 @@ int build_graph(lbm_amr2d *a, int from) {
   if (e == cudaSuccess && rc == LBM_OK) e = cudaGraphInstantiate(&a->graph[from], g, 0);
   if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cs);
+  if ((rc || e != cudaSuccess) && a->fused_grid > 0) {
+    // a cooperative kernel node this driver will not capture: the six launches
+    cudaGetLastError();
+    a->fused_grid = 0;
+    return build_graph(a, from);
+  }
   if (rc) return rc;
   if (e != cudaSuccess) return afail(a, LBM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   return LBM_OK;
@@ -902,6 +1106,7 @@ int lbm_amr2d_create(const lbm_amr2d_config *cfg, lbm_amr2d **out) {
   AM(p.freeList, (p.S / 4) * 4); AM(p.counts, 2 * 4); AM(p.activeList, p.S * 4);
   AM(p.want, p.NBX * p.NBY * 4); AM(p.newly, p.S * 4); AM(p.crit, p.NBX * p.NBY * 4);
   AM(p.partials, (size_t)p.S * kForceSlots * 8); AM(p.counter, 4); AM(p.force_out, kForceSlots * 8);
+  AM(a->bar, 2 * sizeof(unsigned)); AM(a->bar_err, sizeof(int));
 #undef AM
   if ((e = cudaMallocHost(&a->host, 16 * sizeof(double)))) return bail(e, "cudaMallocHost");
   if ((e = cudaMallocHost(&a->host_counts, 4 * sizeof(int)))) return bail(e, "cudaMallocHost");
@@ -922,6 +1127,9 @@ int lbm_amr2d_create(const lbm_amr2d_config *cfg, lbm_amr2d **out) {
   cudaMemset(a->f1[0], 0, 9 * p.N1 * 4);
   cudaMemset(a->f1[1], 0, 9 * p.N1 * 4);
   cudaMemset(a->mac, 0, p.N0 * 16);
+  cudaMemset(a->bar, 0, 2 * sizeof(unsigned));
+  cudaMemset(a->bar_err, 0, sizeof(int));
+  a->fused_grid = fused_blocks(p);
   if ((e = cudaDeviceSynchronize())) return bail(e, "initialise");
   *out = a;
   return LBM_OK;
@@ -1006,6 +1214,20 @@ int lbm_amr2d_set_auto_refine(lbm_amr2d *a, int on) {
   return LBM_OK;
 }
 
+int lbm_amr2d_set_fused(lbm_amr2d *a, int on) {
+  if (!a) return LBM_EINVAL;
+  ACK(a, cudaStreamSynchronize(a->stream));
+  for (auto &g : a->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  a->fused_grid = on ? fused_blocks(a->p) : 0;
+  return LBM_OK;
+}
+
+int lbm_amr2d_fused(const lbm_amr2d *a) { return a ? (a->fused_grid > 0 ? 1 : 0) : 0; }
+
 int lbm_amr2d_forces(lbm_amr2d *a, double out[4]) {
   if (!a || !out) return a ? afail(a, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
   ACK(a, cudaMemcpyAsync(a->host, a->p.force_out, kForceSlots * 8, cudaMemcpyDeviceToHost, a->stream));
@@ -1043,6 +1265,14 @@ int64_t lbm_amr2d_cell_updates(const lbm_amr2d *a) {
 int lbm_amr2d_sync(lbm_amr2d *a) {
   if (!a) return LBM_EINVAL;
   ACK(a, cudaStreamSynchronize(a->stream));
+  if (a->fused_grid > 0) {
+    int flag = 0;
+    ACK(a, cudaMemcpy(&flag, a->bar_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      cudaMemset(a->bar_err, 0, sizeof(int));
+      return afail(a, LBM_ETIMEDOUT, "a grid barrier of the fused macro-step timed out; its results are void");
+    }
+  }
   return LBM_OK;
 }
 

@@ -80,6 +80,28 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm) {
   }
 }
 
+// The fixed-order sum of nparts partials by one warp (lane = threadIdx.x):
+// lane l adds partials l, l + 32, ... in order, then a shuffle tree; lane 0
+// writes out. Every caller that sums the same partials this way gets the
+// same bits.
+template <int NV>
+__device__ __forceinline__ void sum_partials_warp(const double *partials, int nparts, double *out) {
+  const int lane = threadIdx.x & 31;
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+  for (int j = lane; j < nparts; j += 32)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(int64_t)j * NV + k]);
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = acc[k];
+}
+
 // Writes this block's partial (thread 0 holds it), and if this block is the
 // last of `nparts` to do so, sums all partials in a fixed order into `out`
 // and re-arms the ticket counter for the next step. Only warp 0 takes part:
@@ -101,21 +123,8 @@ __device__ bool finish_sum(const double (&v)[NV], double *partials, unsigned int
   }
   if (!__shfl_sync(0xffffffffu, last, 0)) return false;
   __threadfence();
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-  for (int j = lane; j < nparts; j += 32)
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(int64_t)j * NV + k]);
-#pragma unroll
-  for (int k = 0; k < NV; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = acc[k];
-    *counter = 0u;
-  }
+  sum_partials_warp<NV>(partials, nparts, out);
+  if (lane == 0) *counter = 0u;
   return true;
 }
 

@@ -432,6 +432,16 @@ int lbm_amr2d_step(lbm_amr2d *a, int n);
  * step runs every refine_every macro-steps (setAutoRefine). */
 int lbm_amr2d_refine_round(lbm_amr2d *a);
 int lbm_amr2d_set_auto_refine(lbm_amr2d *a, int on);
+/* How the interp interface's macro-step runs: one cooperative launch whose
+ * phases (force partials, ring fill and root step; substep; substep;
+ * restriction) are separated by grid barriers (on, the default where the
+ * device takes cooperative launches), or six launches (off). Both give the
+ * same bits. lbm_amr2d_fused reports which is in use. A barrier that waits
+ * longer than about a second gives up: lbm_amr2d_sync then returns
+ * LBM_ETIMEDOUT. No counterpart in the reference (its macro-step is the six
+ * dispatches). */
+int lbm_amr2d_set_fused(lbm_amr2d *a, int on);
+int lbm_amr2d_fused(const lbm_amr2d *a);
 /* Drag/lift/torque of the last macro-step, FP64: {fx, fy, tz, nonfinite}. */
 int lbm_amr2d_forces(lbm_amr2d *a, double out[4]);
 /* Level-1 topology: block_slot[nbx*nby], slot_to_block[max_slots],

@@ -170,3 +170,31 @@ def test_manual_refine_rounds_equal_automatic_ones(lbm):
     assert np.array_equal(f0, f1)
     assert np.array_equal(t0["block_slot"], t1["block_slot"]) and np.array_equal(t0["active"], t1["active"])
     assert np.array_equal(F0, F1)
+
+
+@pytest.mark.parametrize("bounceback", [False, True])
+def test_fused_macro_step_equals_six_launches(lbm, oracle, bounceback):
+    """The interp macro-step as one cooperative launch (the default) gives the
+    six-launch form's bits: root and pool populations and velocity, force,
+    topology, over 40 macro-steps and three refine rounds."""
+    s, cfg = make(lbm, bounceback=bounceback)
+    out = []
+    for fused in (True, False):
+        a = lbm.Amr2D(cfg)
+        a.set_fused(fused)
+        assert a.fused == fused
+        a.write_root(s["f"], s["vel"])
+        a.step(40)
+        a.sync()
+        f0, v0 = a.read_root()
+        f1, v1 = a.read_pool()
+        out.append((f0, v0, f1, v1, a.forces(), a.topology()))
+        a.close()
+    (f0a, v0a, f1a, v1a, Fa, ta), (f0b, v0b, f1b, v1b, Fb, tb) = out
+    assert np.array_equal(f0a, f0b) and np.array_equal(v0a, v0b)
+    fb2 = (cfg.rb * 2 + 4) ** 2
+    idx = np.concatenate([np.arange(k * fb2, (k + 1) * fb2) for k in ta["active"]])
+    assert np.array_equal(f1a.reshape(9, -1)[:, idx], f1b.reshape(9, -1)[:, idx])
+    assert np.array_equal(v1a[idx], v1b[idx])
+    assert np.array_equal(Fa, Fb)
+    assert np.array_equal(ta["block_slot"], tb["block_slot"]) and np.array_equal(ta["active"], tb["active"])
