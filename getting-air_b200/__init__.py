@@ -239,6 +239,8 @@ def _load() -> C.CDLL:
         "lbm_amr3d_pool_stats": ([P, C.POINTER(C.c_int32)], I),
         "lbm_amr3d_block_q": ([P, C.c_float, C.POINTER(C.c_float)], I),
         "lbm_amr3d_manage_now": ([P], I),
+        "lbm_amr3d_set_links": ([P, I], I),
+        "lbm_amr3d_links": ([P], I),
         "lbm_amr2d_refine_round": ([P], I),
         "lbm_amr2d_set_auto_refine": ([P, I], I),
         "lbm_amr2d_set_fused": ([P, I], I),
@@ -1080,6 +1082,15 @@ class Amr3D:
     def manage_now(self):
         """One decision of the dynamic manager before the next macro-step."""
         self._check(lib.lbm_amr3d_manage_now(self._h))
+
+    def set_links(self, on: bool):
+        """The bounce-back link table on (the default) or off: the same bits
+        either way, off evaluates the body's distance in every step."""
+        self._check(lib.lbm_amr3d_set_links(self._h, 1 if on else 0))
+
+    @property
+    def links(self) -> bool:
+        return bool(lib.lbm_amr3d_links(self._h))
 
     def block_q(self, lead: float = 0.0) -> np.ndarray:
         """Per-block max Q-criterion of the L0 velocity, box dilated by `lead`."""

@@ -194,6 +194,62 @@ __global__ void __launch_bounds__(kTileMaxThreads)
   macp[t.cell] = make_float4(rho, mx / den, my / den, mz / den);
 }
 
+// ---- bounce-back link table -------------------------------------------------
+// With bounce-back, a pool cell's treatment of the body depends only on its
+// position and the body's pose: whether it lies inside (phi < 0), whether a
+// fine link from it can end inside (phi < 1: a fine link is sqrt(3)/2 L0
+// units long and phi is 1-Lipschitz), and which of its Q pull sources do.
+// Deciding the sources costs Q - 1 distance evaluations per near cell (a
+// rotation and a box distance for a rounded box), which dominated the
+// substeps of a large hierarchy. Between changes of the body (lbm_amr3d_set_body)
+// and of the tiles (the manager), the codes are constant, so they are kept
+// in a table of one word per pool cell and rebuilt on those events: bits
+// 0 .. Q-1 the solid sources, kLinkNear, kLinkSolid. The table and the
+// direct evaluation share link_code, so a step reads the same bits either way.
+constexpr uint32_t kLinkNear = 1u << 29;
+constexpr uint32_t kLinkSolid = 1u << 30;
+
+template <int Q>
+__device__ __forceinline__ uint32_t link_code(const Amr3Params &p, const TileCell &t, float phi) {
+  uint32_t code = phi < 0.f ? kLinkSolid : 0u;
+  if (phi < 1.0f) {
+    code |= kLinkNear;
+    if (phi < -0.87f) {
+      // deeper than a link's length plus rounding: every source is solid
+      code |= (1u << Q) - 1u;
+    } else {
+      // the rest direction's source is the cell itself; for a ring cell its
+      // regular pull would read the neighbour tile, so it is decided like
+      // any other link. One rolled loop: one out-of-line SDF call site.
+      code |= phi < 0.f ? 1u : 0u;
+#pragma unroll 1
+      for (int i = 1; i < Q; ++i) {
+        const V3 sp = {f2c(t.fx - c_dirs.ex[i], t.bx * p.rb), f2c(t.fy - c_dirs.ey[i], t.by * p.rb),
+                       f2c(t.fz - c_dirs.ez[i], t.bz * p.rb)};
+        if (phi3(sp, p.c.body, p.c.win) < 0.f) code |= 1u << i;
+      }
+    }
+  }
+  return code;
+}
+
+__device__ __forceinline__ V3 tile_pos(const Amr3Params &p, const TileCell &t) {
+  return {f2c(t.fx, t.bx * p.rb), f2c(t.fy, t.by * p.rb), f2c(t.fz, t.bz * p.rb)};
+}
+
+// Every cell (ring included) of every live tile, or of the tiles flagged in
+// only_new (the manager's grants).
+template <int Q>
+__global__ void __launch_bounds__(kListThreads)
+    amr3_links(const __grid_constant__ Amr3Params p, uint32_t *__restrict__ links, const uint32_t *__restrict__ cells,
+               const unsigned char *__restrict__ only_new) {
+  TileCell t;
+  __shared__ int nb27[27];
+  if (!list_cell(p, cells, 0, p.T3, nb27, t)) return;
+  if (only_new && !only_new[t.slot]) return;
+  links[t.cell] = link_code<Q>(p, t, phi3(tile_pos(p, t), p.c.body, p.c.win));
+}
+
 // ---- explode ------------------------------------------------------------
 template <int Q>
 __global__ void __launch_bounds__(kListThreads)
@@ -292,18 +348,20 @@ __global__ void __launch_bounds__(kListThreads)
       oa[a][k] = (sa < G || sa >= G + RB2) ? off : 0;
     }
   }
-  const V3 pos = {f2c(t.fx, b[0] * p.rb), f2c(t.fy, b[1] * p.rb), f2c(t.fz, b[2] * p.rb)};
-  float phi = 1e30f;
+  const V3 pos = tile_pos(p, t);
+  const bool bb = c.has_body && c.bb;
+  float phi = 1e30f;  // the penalty's chi reads it; bounce-back reads the link code
   V3 us = {0.f, 0.f, 0.f};
+  uint32_t code = 0;
   if (c.has_body) {
-    phi = phi3(pos, c.body, c.win);
+    if (!bb) phi = phi3(pos, c.body, c.win);
+    else code = p.links ? __ldg(p.links + t.cell) : link_code<Q>(p, t, phi3(pos, c.body, c.win));
     us = body_velocity3(pos, c.body, c.win);
   }
-  const bool bb = c.has_body && c.bb;
   const bool in_tile = interior(p, t.fx) && interior(p, t.fy) && interior(p, t.fz);
   // A cell that collides inside the body (SOLID_EQ) is held at feq(1, u_body),
   // whatever it pulls: write that and skip the pull.
-  if ((in_tile || p.collide_ring) && c.solid_eq && bb && phi < 0.f) {
+  if ((in_tile || p.collide_ring) && c.solid_eq && (code & kLinkSolid)) {
     const float ussq = us.x * us.x + us.y * us.y + us.z * us.z;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -313,34 +371,15 @@ __global__ void __launch_bounds__(kListThreads)
     if (p.write_mac) macp[t.cell] = make_float4(1.f, us.x, us.y, us.z);
     return;
   }
-  // a fine link is sqrt(3)/2 L0 units long and phi is 1-Lipschitz
-  const bool near = bb && phi < 1.0f;
+  const bool near = code & kLinkNear;
   float rhoW = 1.f;
-  if (near && c.rho_w_local && phi < 2.f) {
+  if (near && c.rho_w_local) {
     float s = 0.f;
 #pragma unroll
     for (int i = 0; i < Q; ++i) s += __ldg(fin + (int64_t)i * p.P + t.cell);
     rhoW = s;
   }
-  // Which links bounce back: the source is inside the body. A rolled loop
-  // (one SDF instance), and none at all where every source must be solid
-  // (deeper than a link's length plus rounding). The rest direction's
-  // source is the cell itself (phi); for a ring cell its regular pull would
-  // read the neighbour tile, so it is decided like any other link.
-  uint32_t solid_links = 0;
-  if (near) {
-    if (phi < -0.87f) {
-      solid_links = (1u << Q) - 1u;
-    } else {
-      solid_links = phi < 0.f ? 1u : 0u;
-#pragma unroll 1
-      for (int i = 1; i < Q; ++i) {
-        const V3 sp = {f2c(t.fx - c_dirs.ex[i], b[0] * p.rb), f2c(t.fy - c_dirs.ey[i], b[1] * p.rb),
-                       f2c(t.fz - c_dirs.ez[i], b[2] * p.rb)};
-        if (phi3(sp, c.body, c.win) < 0.f) solid_links |= 1u << i;
-      }
-    }
-  }
+  const uint32_t solid_links = code & ((1u << Q) - 1u);
   // One load per direction, its address chosen without a branch (the
   // cell's own opposite population for a solid link, else the pull
   // source), so that all Q loads are in flight together rather than one
@@ -688,14 +727,13 @@ __global__ void __launch_bounds__(kTileThreads)
           for (int i = 0; i < Q; ++i) s += __ldg(fp + (int64_t)i * p.P + cell);
           rhoW = s;
         }
-        // solid sources from one rolled SDF loop (the cell itself, phi >= 0
-        // here, is not one)
-        uint32_t solid = 0;
-#pragma unroll 1
-        for (int i = 1; i < Q; ++i) {
-          const V3 sp = {f2c(fx - c_dirs.ex[i], b[0] * p.rb), f2c(fy - c_dirs.ey[i], b[1] * p.rb),
-                         f2c(fz - c_dirs.ez[i], b[2] * p.rb)};
-          if (phi3(sp, c.body, c.win) < 0.f) solid |= 1u << i;
+        // the solid sources (the cell itself, phi >= 0 here, is not one)
+        uint32_t solid;
+        if (p.links) {
+          solid = __ldg(p.links + cell) & ((1u << Q) - 2u);
+        } else {
+          const TileCell t = {slot, b[0], b[1], b[2], fx, fy, fz, cell};
+          solid = link_code<Q>(p, t, phi) & ((1u << Q) - 2u);
         }
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -1043,6 +1081,7 @@ struct lbm_amr3d {
   cudaGraphExec_t manage_graph[2] = {nullptr, nullptr};
   bool carved = false;          // device memory carved from a caller's block
   uint32_t *d_cells = nullptr;  // tile cells: interior (RB2^3) then ring, packed x | y << 8 | z << 16
+  uint32_t *d_links = nullptr;  // bounce-back link code per pool cell (bounce-back bodies only)
   float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
   float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
@@ -1074,6 +1113,14 @@ cudaError_t launch_interp(lbm_amr3d *a, const float *fc, int ring_only, const un
   const dim3 g = tile_grid(a);
   AMR3_DISPATCH(a->q,
                 amr3_interp<Q><<<g, tile_block(a), 0, a->stream>>>(fc, a->fp[0], a->p, ring_only, only_new));
+}
+
+// The link table of every live tile, or of the tiles in only_new; nothing
+// when the table is off.
+cudaError_t launch_links(lbm_amr3d *a, const unsigned char *only_new) {
+  if (!a->p.slots || !a->p.links) return cudaSuccess;
+  const dim3 gl((a->p.T3 + kListThreads - 1) / kListThreads, a->p.slots);
+  AMR3_DISPATCH(a->q, amr3_links<Q><<<gl, kListThreads, 0, a->stream>>>(a->p, a->d_links, a->d_cells, only_new));
 }
 
 // One decision of the manager before the macro-step from L0 parity `cp`
@@ -1110,6 +1157,7 @@ cudaError_t launch_manage(lbm_amr3d *a, int cp) {
                                            a->d_slot_new, a->d_iface_flag, a->d_want, p.nbx, p.nby, p.nbz,
                                            a->capacity);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launch_links(a, a->d_slot_new)) != cudaSuccess) return e;
   return launch_interp(a, a->fc[cp], 0, a->d_slot_new);
 }
 
@@ -1248,7 +1296,7 @@ void release(lbm_amr3d *a) {
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
                     (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux,
-                    (void *)a->d_block_q, (void *)a->d_cells})
+                    (void *)a->d_block_q, (void *)a->d_cells, (void *)a->d_links})
     if (!a->carved) cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
@@ -1387,6 +1435,8 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     if ((e = mem.take(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "slots");
     if ((e = mem.take(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "iface");
     if ((e = mem.take(&a->d_cells, (size_t)p.T3 * sizeof(uint32_t)))) return bail(e, "cell list");
+    if (r.has_body && r.use_bounceback && (e = mem.take(&a->d_links, (size_t)p.P * sizeof(uint32_t))))
+      return bail(e, "link table");
     if (a->dynamic) {
       if ((e = mem.take(&a->d_want, nb))) return bail(e, "want");
       if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
@@ -1465,6 +1515,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   p.partials = a->partials;
   p.counter = a->counter;
   p.force_out = a->force_out;
+  p.links = a->d_links;  // filled when the hierarchy is seeded
   *out = a;
   return LBM_OK;
 }
@@ -1521,6 +1572,7 @@ int lbm_amr3d_init_macro(lbm_amr3d *a, const float *mac) {
   for (int k = 0; k < 2; ++k)
     ACK(a, launch_init_eq(a->q, LBM_STORE_FP32, a->macc, a->fc[k], a->p.N, a->sp.pk, a->stream));
   ACK(a, launch_interp(a, a->fc[0], 0, nullptr));
+  ACK(a, launch_links(a, nullptr));
   ACK(a, launch_moments(a));
   ACK(a, cudaStreamSynchronize(a->stream));
   a->cp = 0;
@@ -1582,8 +1634,20 @@ int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body) {
   a->sp.swept_band = tmp.swept_band;
   a->p.c = a->sp;
   destroy_graphs(a);
+  if (a->seeded) ACK(a, launch_links(a, nullptr));
   return LBM_OK;
 }
+
+int lbm_amr3d_set_links(lbm_amr3d *a, int on) {
+  if (!a) return LBM_EINVAL;
+  ACK(a, cudaStreamSynchronize(a->stream));
+  destroy_graphs(a);
+  a->p.links = on ? a->d_links : nullptr;
+  if (a->seeded) ACK(a, launch_links(a, nullptr));
+  return LBM_OK;
+}
+
+int lbm_amr3d_links(const lbm_amr3d *a) { return a && a->p.links ? 1 : 0; }
 
 int lbm_amr3d_block_q(lbm_amr3d *a, float lead, float *block_q) {
   if (!a || !block_q) return a ? afail(a, LBM_EINVAL, "block_q is NULL") : LBM_EINVAL;

@@ -40,6 +40,7 @@ struct Amr3Params {
   unsigned int *counter;
   double *force_out;
   StepParams c;                 // L0 physics (body, forcing, sponge, far field)
+  const uint32_t *links;        // bounce-back link code per pool cell (pinned body), or NULL
 };
 
 int amr3_validate(const lbm_amr3d_config *c, std::string &why);

@@ -550,6 +550,17 @@ int lbm_amr3d_set_body(lbm_amr3d *a, const lbm_body *body);
 /* One decision of the dynamic manager now, before the next macro-step
  * (the step runs them every manage_every macro-steps from manage_start). */
 int lbm_amr3d_manage_now(lbm_amr3d *a);
+/* The bounce-back link table (bounce-back bodies): one 32-bit code per pool
+ * cell -- which pull sources lie inside the body, whether the cell is near
+ * or inside it -- built when the hierarchy is seeded, after set_body and for
+ * the tiles each decision grants, and read by the substeps and the pool
+ * force instead of evaluating the body's distance at every cell and link
+ * source. On by default; off evaluates them each step. The results are the
+ * same bits either way. Returns LBM_OK (a hierarchy without a bounce-back
+ * body has no table, and both calls leave it off). No counterpart in the
+ * reference, which evaluates the distance in its step shader. */
+int lbm_amr3d_set_links(lbm_amr3d *a, int on);
+int lbm_amr3d_links(const lbm_amr3d *a);
 /* {slots in use, refusals (pool exhausted), lowest free count seen, decisions}. */
 int lbm_amr3d_pool_stats(lbm_amr3d *a, int32_t out[4]);
 /* Per-block max Q-criterion of the L0 velocity of the last macro-step, over

@@ -445,3 +445,79 @@ def test_manual_manager_decisions_equal_scheduled_ones(lbm):
     assert np.array_equal(b0, b1)
     assert np.array_equal(f0, f1)
     assert np.array_equal(F0, F1)
+
+
+def _spinning_box(q, iface):
+    th = 0.35
+    axis = np.array([0.3, 0.5, 0.81])
+    axis /= np.linalg.norm(axis)
+    quat = (math.cos(th), *(axis * math.sin(th)))
+    body = dict(shape="roundbox", centre=(17.3, 15.8, 16.2), a=5.0, b=3.0, c=2.5, r=0.8, quat=quat,
+                w=(0.0, 0.0, 0.002))
+    kw = dict(tau=0.6, has_body=1, use_bounceback=1, sponge_w=4.0, sponge_u=(0.04, 0.0, 0.0),
+              force=(1e-6, 0.0, 0.0), body=body)
+    return (48, 32, 32), kw
+
+
+@pytest.mark.parametrize("q,iface", [(19, 0), (27, 0), (19, 1)])
+def test_link_table_equals_direct_evaluation(lbm, q, iface):
+    """The bounce-back link table against evaluating the body's distance in
+    every step (a rotated, spinning rounded box, so the table carries solid
+    cells, partial link sets and a nonzero wall velocity): the same bits in
+    L0, the tiles and the force."""
+    from getting_air_b200 import scenarios as sc
+    dims, kw = _spinning_box(q, iface)
+    runs = []
+    for on in (True, False):
+        a = lbm.Amr3D(lbm.amr3d_config(q, dims, refine="body", margin=2.0, iface=iface, **kw))
+        assert a.links
+        a.init_macro(sc.uniform_macro(int(np.prod(dims)), (0.04, 0.0, 0.0)))
+        a.set_links(on)
+        assert a.links == on
+        a.step(12)
+        fc, mc = a.read_coarse()
+        fp, mp = a.read_pool()
+        runs.append((fc, mc, fp, mp, a.forces()))
+        a.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+    assert abs(runs[0][4][0]) > 0
+
+
+def test_link_table_follows_the_body_and_the_manager(lbm):
+    """A towed sphere under the dynamic manager: set_body rebuilds the table
+    and every decision fills it for the tiles it grants, so the run equals
+    the one without a table bit for bit."""
+    from getting_air_b200 import scenarios as sc
+    dims = (40, 24, 24)
+    body = dict(shape="sphere", centre=(10.3, 11.8, 12.1), a=3.0, v=(0.25, 0.0, 0.0))
+    c = lbm.amr3d_config(19, dims, refine="body", margin=2.0, dynamic=1, manage_every=4, slot_headroom=2.0,
+                         tau=0.62, has_body=1, use_bounceback=1, body=body)
+    runs = []
+    for on in (True, False):
+        a = lbm.Amr3D(c)
+        a.init_macro(sc.uniform_macro(int(np.prod(dims)), (0.03, 0.0, 0.0)))
+        a.set_links(on)
+        cx = body["centre"][0]
+        for _ in range(6):
+            a.step(4)
+            cx += 1.0
+            a.set_body(lbm.make_body("sphere", (cx, 11.8, 12.1), a=3.0, v=(0.25, 0.0, 0.0)))
+        a.step(2)
+        fc, mc = a.read_coarse()
+        fp, mp = a.read_pool()
+        runs.append((fc, mc, fp, mp, a.forces(), a.topology()["block_slot"]))
+        st = a.pool_stats()
+        a.close()
+    for x, y in zip(*runs):
+        assert np.array_equal(x, y)
+    assert st["decisions"] == 7  # macro-steps 0, 4, ..., 24
+
+
+def test_no_link_table_without_bounce_back(lbm):
+    case = CASES["roundbox-penalty"]
+    a = lbm.Amr3D(lbm.amr3d_config(19, case["dims"], refine="body", **case["kw"]))
+    assert not a.links
+    a.set_links(True)
+    assert not a.links
+    a.close()
