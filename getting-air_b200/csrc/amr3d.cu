@@ -61,6 +61,7 @@ __device__ __forceinline__ bool interior(const Amr3Params &p, int j) { return j 
 struct TileCell {
   int slot, bx, by, bz, fx, fy, fz;
   int64_t cell;
+  int k;  // position in the tile's cell list (cell-list kernels)
 };
 
 // Tile kernels run one CTA per (fz, slot) with an FB x FB thread block, so a
@@ -113,7 +114,8 @@ __device__ __forceinline__ bool list_cell(const Amr3Params &p, const uint32_t *_
   __syncthreads();
   const int k = blockIdx.x * kListThreads + threadIdx.x;
   if (k >= count) return false;
-  const uint32_t c = __ldg(cells + first + k);
+  t.k = first + k;
+  const uint32_t c = __ldg(cells + t.k);
   t.fx = c & 0xff; t.fy = (c >> 8) & 0xff; t.fz = c >> 16;
   t.cell = (int64_t)t.slot * p.T3 + (t.fz * p.FB + t.fy) * p.FB + t.fx;
   return true;
@@ -332,22 +334,6 @@ __global__ void __launch_bounds__(kListThreads)
   __shared__ int nb27[27];
   if (!list_cell(p, cells, 0, count, nb27, t)) return;
   const StepParams &c = p.c;
-  const int G = kAmrGhost, RB2 = p.RB2, FB = p.FB;
-  const int b[3] = {t.bx, t.by, t.bz};
-  const int fi[3] = {t.fx, t.fy, t.fz};
-  // Per axis and per e in {-1, 0, +1}: the neighbour step of the source --
-  // toward the tile edge this cell sits at, when the source leaves the
-  // interior (DIRECT_GHOST reads the neighbour's interior there).
-  int oa[3][3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const int off = fi[a] <= G ? -1 : (fi[a] + 1 >= G + RB2 ? 1 : 0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int sa = fi[a] - (k - 1);
-      oa[a][k] = (sa < G || sa >= G + RB2) ? off : 0;
-    }
-  }
   const V3 pos = tile_pos(p, t);
   const bool bb = c.has_body && c.bb;
   float phi = 1e30f;  // the penalty's chi reads it; bounce-back reads the link code
@@ -381,34 +367,21 @@ __global__ void __launch_bounds__(kListThreads)
   }
   const uint32_t solid_links = code & ((1u << Q) - 1u);
   // One load per direction, its address chosen without a branch (the
-  // cell's own opposite population for a solid link, else the pull
-  // source), so that all Q loads are in flight together rather than one
-  // round trip per solid link.
+  // cell's own opposite population for a solid link, else the pull source
+  // from the pull table), so that all Q loads are in flight together.
+  const int slot_base = t.slot * p.T3;
+  const uint32_t *pw = p.pulls + t.k;
   float f[Q];
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    const uint32_t w = __ldg(pw + i * p.T3);
+    const int ns = nb27[w & 31u];
+    const int off = ns >= 0 ? ns * p.T3 + (int)((w >> 5) & 0x1fffu) : slot_base + (int)(w >> 18);
     const bool solid = (solid_links >> i) & 1u;
-    int s[3] = {t.fx - e[0], t.fy - e[1], t.fz - e[2]};
-    const int o0 = oa[0][e[0] + 1], o1 = oa[1][e[1] + 1], o2 = oa[2][e[2] + 1];
-    int src = t.slot;
-    if (o0 | o1 | o2) {
-      const int ns = nb27[(o2 + 1) * 9 + (o1 + 1) * 3 + (o0 + 1)];
-      if (ns >= 0) {
-        src = ns;
-        s[0] -= o0 * RB2;
-        s[1] -= o1 * RB2;
-        s[2] -= o2 * RB2;
-      } else {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) s[a] = min(max(s[a], 0), FB - 1);
-      }
-    }
-    const int64_t pull = (int64_t)i * p.P + (int64_t)src * p.T3 + (s[2] * FB + s[1]) * FB + s[0];
-    const float v = __ldg(fin + (solid ? (int64_t)L::opp(i) * p.P + t.cell : pull));
+    const float v = __ldg(solid ? fin + (int64_t)L::opp(i) * p.P + t.cell : fin + (int64_t)i * p.P + off);
     if (solid) {
-      const float corr =
-          2.f * L::w(i) * rhoW * ((float)e[0] * us.x + (float)e[1] * us.y + (float)e[2] * us.z) / kCS2;
+      const float corr = 2.f * L::w(i) * rhoW *
+                         ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
       f[i] = v + corr;
     } else {
       f[i] = v;
@@ -1082,6 +1055,7 @@ struct lbm_amr3d {
   bool carved = false;          // device memory carved from a caller's block
   uint32_t *d_cells = nullptr;  // tile cells: interior (RB2^3) then ring, packed x | y << 8 | z << 16
   uint32_t *d_links = nullptr;  // bounce-back link code per pool cell (bounce-back bodies only)
+  uint32_t *d_pulls = nullptr;  // substep pull sources per (direction, cell list position)
   float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
   float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
@@ -1296,7 +1270,7 @@ void release(lbm_amr3d *a) {
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
                     (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux,
-                    (void *)a->d_block_q, (void *)a->d_cells, (void *)a->d_links})
+                    (void *)a->d_block_q, (void *)a->d_cells, (void *)a->d_links, (void *)a->d_pulls})
     if (!a->carved) cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
@@ -1327,6 +1301,38 @@ const char *lbm_amr3d_last_error(const lbm_amr3d *a) { return a ? a->err.c_str()
 }  // extern "C"
 
 namespace {
+
+// The substep's pull sources, the same for every tile: per direction i and
+// cell list position k, a word of the neighbour slot the source lies in (its
+// index in the CTA's 3 x 3 x 3 table; 13 = this tile), bits 0-4; the source
+// cell in that tile, bits 5-17; and the cell of this tile it clamps to when
+// that neighbour is not refined, bits 18-30 (T3 <= 20^3 < 2^13). DIRECT_GHOST
+// (common_d3_amr_step1.wgsl): a source past the interior, toward the tile
+// edge the cell sits at, is read from the refined neighbour's interior, else
+// from this tile's ring.
+std::vector<uint32_t> pull_table(int q, int FB, int RB2, const std::vector<uint32_t> &cl) {
+  const int G = kAmrGhost, n = (int)cl.size();
+  std::vector<uint32_t> t((size_t)q * n);
+  for (int k = 0; k < n; ++k) {
+    const int fi[3] = {(int)(cl[k] & 0xff), (int)((cl[k] >> 8) & 0xff), (int)(cl[k] >> 16)};
+    for (int i = 0; i < q; ++i) {
+      const int e[3] = {detail::ex27(i), detail::ey27(i), detail::ez27(i)};
+      int o[3], sh[3], sc[3];
+      for (int a = 0; a < 3; ++a) {
+        const int edge = fi[a] <= G ? -1 : (fi[a] + 1 >= G + RB2 ? 1 : 0);
+        const int sa = fi[a] - e[a];
+        o[a] = (sa < G || sa >= G + RB2) ? edge : 0;
+        sh[a] = sa - o[a] * RB2;
+        sc[a] = std::min(std::max(sa, 0), FB - 1);
+      }
+      const uint32_t nb = (uint32_t)((o[2] + 1) * 9 + (o[1] + 1) * 3 + (o[0] + 1));
+      const uint32_t ls = (uint32_t)((sh[2] * FB + sh[1]) * FB + sh[0]);
+      const uint32_t lc = (uint32_t)((sc[2] * FB + sc[1]) * FB + sc[0]);
+      t[(size_t)i * n + k] = nb | ls << 5 | lc << 18;
+    }
+  }
+  return t;
+}
 
 // Builds the hierarchy with its device memory from `mem`; with mem.measure
 // nothing touches the GPU and *bytes receives the device bytes it needs.
@@ -1435,6 +1441,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     if ((e = mem.take(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "slots");
     if ((e = mem.take(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "iface");
     if ((e = mem.take(&a->d_cells, (size_t)p.T3 * sizeof(uint32_t)))) return bail(e, "cell list");
+    if ((e = mem.take(&a->d_pulls, (size_t)a->q * p.T3 * sizeof(uint32_t)))) return bail(e, "pull table");
     if (r.has_body && r.use_bounceback && (e = mem.take(&a->d_links, (size_t)p.P * sizeof(uint32_t))))
       return bail(e, "link table");
     if (a->dynamic) {
@@ -1479,6 +1486,8 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
             if ((in(x) && in(y) && in(z)) == (pass == 0)) cl.push_back(x | (y << 8) | (z << 16));
           }
     cudaMemcpyAsync(a->d_cells, cl.data(), cl.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, a->own);
+    const std::vector<uint32_t> pt = pull_table(a->q, p.FB, p.RB2, cl);
+    cudaMemcpyAsync(a->d_pulls, pt.data(), pt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, a->own);
   }
   if (a->dynamic) {
     std::vector<unsigned char> flag(nb, 0);
@@ -1516,6 +1525,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   p.counter = a->counter;
   p.force_out = a->force_out;
   p.links = a->d_links;  // filled when the hierarchy is seeded
+  p.pulls = a->d_pulls;
   *out = a;
   return LBM_OK;
 }

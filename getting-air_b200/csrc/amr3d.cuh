@@ -41,6 +41,7 @@ struct Amr3Params {
   double *force_out;
   StepParams c;                 // L0 physics (body, forcing, sponge, far field)
   const uint32_t *links;        // bounce-back link code per pool cell (pinned body), or NULL
+  const uint32_t *pulls;        // substep pull sources per (direction, tile cell list position)
 };
 
 int amr3_validate(const lbm_amr3d_config *c, std::string &why);
