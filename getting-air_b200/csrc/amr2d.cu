@@ -369,7 +369,7 @@ __device__ __forceinline__ void substep_cell(const AmrParams &p, const float *__
   for (int i = 0; i < 9; ++i) {
     const int ex = L9::ex(i), ey = L9::ey(i);
     if (near && phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
-      const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+      const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) * kInvCS2;
       f[i] = __ldg(fin + L9::opp(i) * p.N1 + cell) + corr;
       continue;
     }
@@ -507,7 +507,7 @@ __device__ __forceinline__ void force_tile_acc(const AmrParams &p, const float *
           const int ex = L9::ex(i), ey = L9::ey(i);
           if (phi2(pool_pos(p, bx, fx - ex), pool_pos(p, by, fy - ey), p.body, Wf, Hf) < 0.f) {
             const float fo = __ldg(f1 + L9::opp(i) * p.N1 + cell);
-            const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+            const float corr = 2.f * L9::w(i) * ((float)ex * usx + (float)ey * usy) * kInvCS2;
             fxb += -(float)ex * (2.f * fo + corr) * 0.5f;
             fyb += -(float)ey * (2.f * fo + corr) * 0.5f;
           }

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -99,25 +100,38 @@ __constant__ DirTable c_dirs = make_dirs();
 // neighbour table; false for a thread with no cell (after the barrier).
 constexpr int kListThreads = 128;
 
-__device__ __forceinline__ bool list_cell(const Amr3Params &p, const uint32_t *__restrict__ cells, int first,
-                                          int count, int *nb27, TileCell &t) {
+__device__ __forceinline__ bool list_tile(const Amr3Params &p, int *nb27, TileCell &t, bool as_base) {
   t.slot = blockIdx.y;
   const int id = p.slot_to_block[t.slot];
   if (id < 0) return false;  // the whole CTA: a free slot
   t.bx = id % p.nbx; t.by = (id / p.nbx) % p.nby; t.bz = id / (p.nbx * p.nby);
   if (threadIdx.x < 27) {
     const int k = threadIdx.x, dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
-    nb27[k] = k == 13 ? t.slot
-                      : p.block_slot[(wrapi(t.bz + dz, p.nbz) * p.nby + wrapi(t.by + dy, p.nby)) * p.nbx +
-                                     wrapi(t.bx + dx, p.nbx)];
+    const int ns = k == 13 ? t.slot
+                           : p.block_slot[(wrapi(t.bz + dz, p.nbz) * p.nby + wrapi(t.by + dy, p.nby)) * p.nbx +
+                                          wrapi(t.bx + dx, p.nbx)];
+    // as_base: the slot's first pool cell (slot * T3 < P < 2^31)
+    nb27[k] = as_base && ns >= 0 ? ns * p.T3 : ns;
   }
   __syncthreads();
-  const int k = blockIdx.x * kListThreads + threadIdx.x;
-  if (k >= count) return false;
-  t.k = first + k;
-  const uint32_t c = __ldg(cells + t.k);
+  return true;
+}
+
+// The cell at list position pos of the CTA's tile.
+__device__ __forceinline__ void list_at(const Amr3Params &p, const uint32_t *__restrict__ cells, int pos,
+                                        TileCell &t) {
+  t.k = pos;
+  const uint32_t c = __ldg(cells + pos);
   t.fx = c & 0xff; t.fy = (c >> 8) & 0xff; t.fz = c >> 16;
   t.cell = (int64_t)t.slot * p.T3 + (t.fz * p.FB + t.fy) * p.FB + t.fx;
+}
+
+__device__ __forceinline__ bool list_cell(const Amr3Params &p, const uint32_t *__restrict__ cells, int first,
+                                          int count, int *nb27, TileCell &t, bool as_base = false) {
+  if (!list_tile(p, nb27, t, as_base)) return false;
+  const int k = blockIdx.x * kListThreads + threadIdx.x;
+  if (k >= count) return false;
+  list_at(p, cells, first + k, t);
   return true;
 }
 
@@ -324,15 +338,26 @@ __global__ void __launch_bounds__(kListThreads)
 }
 
 // ---- one pool substep ----------------------------------------------------
-template <int Q>
-__global__ void __launch_bounds__(kListThreads)
-    amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
-                 const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells, int count) {
+// Population index i * P + cell, in 32 bits when every index of the pool
+// fits (W32: Q * P < 2^31, the usual case), so that an address is one
+// multiply-add from the buffer's base instead of 64-bit arithmetic.
+template <bool W32> using PoolIdx = std::conditional_t<W32, int, int64_t>;
+
+template <bool W32> struct PoolSink {
+  float *fo;
+  PoolIdx<W32> n;
+  int cell;  // < P < 2^31
+  __device__ __forceinline__ void put(int i, float v) { fo[(PoolIdx<W32>)i * n + cell] = v; }
+};
+
+template <int Q, bool W32>
+__device__ __forceinline__ void substep_cell(const float *__restrict__ fin, float *__restrict__ fout,
+                                             float4 *__restrict__ macp, const Amr3Params &p, const int *nbase,
+                                             const TileCell &t) {
   using L = Lattice<Q>;
-  TileCell t;
-  // the tile's 26 same-level neighbours, loaded once per CTA
-  __shared__ int nb27[27];
-  if (!list_cell(p, cells, 0, count, nb27, t)) return;
+  using I = PoolIdx<W32>;
+  const I P = (I)p.P;
+  const int cell = (int)t.cell;  // < P < 2^31
   const StepParams &c = p.c;
   const V3 pos = tile_pos(p, t);
   const bool bb = c.has_body && c.bb;
@@ -352,7 +377,7 @@ __global__ void __launch_bounds__(kListThreads)
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const float eu = (float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z;
-      fout[(int64_t)i * p.P + t.cell] = L::w(i) * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq);
+      fout[(I)i * P + cell] = L::w(i) * (1.f + 3.f * eu + 4.5f * eu * eu - 1.5f * ussq);
     }
     if (p.write_mac) macp[t.cell] = make_float4(1.f, us.x, us.y, us.z);
     return;
@@ -362,29 +387,40 @@ __global__ void __launch_bounds__(kListThreads)
   if (near && c.rho_w_local) {
     float s = 0.f;
 #pragma unroll
-    for (int i = 0; i < Q; ++i) s += __ldg(fin + (int64_t)i * p.P + t.cell);
+    for (int i = 0; i < Q; ++i) s += __ldg(fin + (I)i * P + cell);
     rhoW = s;
   }
   const uint32_t solid_links = code & ((1u << Q) - 1u);
-  // One load per direction, its address chosen without a branch (the
-  // cell's own opposite population for a solid link, else the pull source
-  // from the pull table), so that all Q loads are in flight together.
-  const int slot_base = t.slot * p.T3;
-  const uint32_t *pw = p.pulls + t.k;
+  // The Q pull loads, addressed from the pull table (four directions per
+  // 128-bit load of it) as 32-bit cell offsets from each plane's base, all
+  // in flight together. A solid link then takes the cell's own opposite
+  // population instead (those loads hit the lines the rho_w sum just read).
+  const int own = nbase[13];
+  constexpr int kW = pull_words(Q);
+  const uint4 *pw = reinterpret_cast<const uint4 *>(p.pulls) + (size_t)t.k * (kW / 4);
   float f[Q];
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const uint32_t w = __ldg(pw + i * p.T3);
-    const int ns = nb27[w & 31u];
-    const int off = ns >= 0 ? ns * p.T3 + (int)((w >> 5) & 0x1fffu) : slot_base + (int)(w >> 18);
-    const bool solid = (solid_links >> i) & 1u;
-    const float v = __ldg(solid ? fin + (int64_t)L::opp(i) * p.P + t.cell : fin + (int64_t)i * p.P + off);
-    if (solid) {
-      const float corr = 2.f * L::w(i) * rhoW *
-                         ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
-      f[i] = v + corr;
-    } else {
-      f[i] = v;
+  for (int j = 0; j < kW / 4; ++j) {
+    const uint4 w4 = __ldg(pw + j);
+    const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = 4 * j + u;
+      if (i < Q) {
+        const int nb = nbase[w[u] & 31u];
+        const int off = nb >= 0 ? nb + (int)((w[u] >> 5) & 0x1fffu) : own + (int)(w[u] >> 18);
+        f[i] = __ldg(fin + (I)i * P + off);
+      }
+    }
+  }
+  if (solid_links) {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      if ((solid_links >> i) & 1u) {
+        const float corr = 2.f * L::w(i) * rhoW *
+                           ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) * kInvCS2;
+        f[i] = __ldg(fin + (I)L::opp(i) * P + cell) + corr;
+      }
     }
   }
   float rho, mx, my, mz;
@@ -397,12 +433,12 @@ __global__ void __launch_bounds__(kListThreads)
   const float Fx = rc * (us.x - uxs) + c.fx, Fy = rc * (us.y - uys) + c.fy, Fz = rc * (us.z - uzs) + c.fz;
   const float hinv = 0.5f * inv;
   const float ux = fmaf(Fx, hinv, uxs), uy = fmaf(Fy, hinv, uys), uz = fmaf(Fz, hinv, uzs);
-  MemSink<float> sink{fout, p.P, (int)t.cell, c.pk};
+  PoolSink<W32> sink{fout, P, cell};
   if (!in_tile && !p.collide_ring) {
     // explode/coalesce: the ring advects and does not collide (COLLIDE_RING = 0)
     if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) fout[(int64_t)i * p.P + t.cell] = f[i];
+    for (int i = 0; i < Q; ++i) fout[(I)i * P + cell] = f[i];
     return;
   }
   float spw = 0.f;
@@ -421,6 +457,20 @@ __global__ void __launch_bounds__(kListThreads)
   }
   collide_store<L, Q>(f, rho, ux, uy, uz, Fx, Fy, Fz, p.omega_f, spw, c.ftarget, sink);
   if (p.write_mac) macp[t.cell] = make_float4(rho, ux, uy, uz);
+}
+
+// One thread per tile cell: CTAs of kListThreads over chunks of the tile's
+// cell list. (A CTA walking several chunks, so that the tile set-up is paid
+// once, held more registers and ran slower: other CTAs hide the set-up.)
+template <int Q, bool W32>
+__global__ void __launch_bounds__(kListThreads, Q == 19 ? (W32 ? 9 : 8) : 6)
+    amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
+                 const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells, int count) {
+  TileCell t;
+  // the tile's 26 same-level neighbours as pool cell bases, once per CTA
+  __shared__ int nbase[27];
+  if (!list_cell(p, cells, 0, count, nbase, t, true)) return;
+  substep_cell<Q, W32>(fin, fout, macp, p, nbase, t);
 }
 
 // ---- coalesce -------------------------------------------------------------
@@ -688,11 +738,16 @@ __global__ void __launch_bounds__(kTileThreads)
     const int fx = kAmrGhost + k % p.RB2, fy = kAmrGhost + (k / p.RB2) % p.RB2, fz = kAmrGhost + k / (p.RB2 * p.RB2);
     const int64_t cell = (int64_t)slot * p.T3 + (fz * p.FB + fy) * p.FB + fx;
     const V3 pos = {f2c(fx, b[0] * p.rb), f2c(fy, b[1] * p.rb), f2c(fz, b[2] * p.rb)};
-    const float phi = phi3(pos, c.body, c.win);
+    // With the link table and no swept-cell term, the cell's code says all
+    // the bounce-back force needs (0 <= phi < 1: near and not solid) and
+    // the distance is not evaluated.
+    const bool coded = c.bb && p.links && !c.swept;
+    const uint32_t code = coded ? __ldg(p.links + cell) : 0u;
+    const float phi = coded ? 0.5f : phi3(pos, c.body, c.win);
     const V3 us = body_velocity3(pos, c.body, c.win);
     float fbx = 0.f, fby = 0.f, fbz = 0.f, fsx = 0.f, fsy = 0.f, fsz = 0.f;
     if (c.bb) {
-      if (phi >= 0.f && phi < 1.0f) {
+      if (coded ? (code & (kLinkNear | kLinkSolid)) == kLinkNear : (phi >= 0.f && phi < 1.0f)) {
         float rhoW = 1.f;
         if (c.rho_w_local && phi < 2.f) {
           float s = 0.f;
@@ -702,7 +757,9 @@ __global__ void __launch_bounds__(kTileThreads)
         }
         // the solid sources (the cell itself, phi >= 0 here, is not one)
         uint32_t solid;
-        if (p.links) {
+        if (coded) {
+          solid = code & ((1u << Q) - 2u);
+        } else if (p.links) {
           solid = __ldg(p.links + cell) & ((1u << Q) - 2u);
         } else {
           const TileCell t = {slot, b[0], b[1], b[2], fx, fy, fz, cell};
@@ -713,7 +770,7 @@ __global__ void __launch_bounds__(kTileThreads)
           if (solid & (1u << i)) {
             const float fo = __ldg(fp + (int64_t)L::opp(i) * p.P + cell);
             const float corr =
-                2.f * L::w(i) * rhoW * ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) / kCS2;
+                2.f * L::w(i) * rhoW * ((float)L::ex(i) * us.x + (float)L::ey(i) * us.y + (float)L::ez(i) * us.z) * kInvCS2;
             const float m = 2.f * fo + corr;
             fbx += -(float)L::ex(i) * m;
             fby += -(float)L::ey(i) * m;
@@ -1141,6 +1198,16 @@ cudaError_t launch_moments(lbm_amr3d *a) {
   AMR3_DISPATCH(a->q, amr3_moments<Q><<<g, tile_block(a), 0, a->stream>>>(a->fp[0], a->macp, a->p));
 }
 
+// A pool substep, with 32-bit population indices when the pool allows.
+template <int Q>
+void launch_substep(dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp, const Amr3Params &p,
+                    const uint32_t *cells) {
+  if ((int64_t)Q * p.P <= INT32_MAX)
+    amr3_substep<Q, true><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+  else
+    amr3_substep<Q, false><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+}
+
 // One macro-step from L0 parity `cp`.
 cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
   Amr3Params p = a->p;
@@ -1172,9 +1239,9 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
       pa.write_mac = 0;
       const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->flux, p, 0);
-      amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa, a->d_cells, p.T3);
+      launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[1], a->flux, p, 1);
-      amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p, a->d_cells, p.T3);
+      launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
       amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
                                                  f2c_rescale);
       if (a->flux && gc)
@@ -1195,8 +1262,8 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
         amr3_explode<Q><<<gr, kListThreads, 0, st>>>(a->fc[cp], a->fp[0], p, a->d_cells, r3i, nring);
         Amr3Params pa = p;
         pa.write_mac = 0;
-        amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[0], a->fp[1], a->macp, pa, a->d_cells, p.T3);
-        amr3_substep<Q><<<gl, kListThreads, 0, st>>>(a->fp[1], a->fp[0], a->macp, p, a->d_cells, p.T3);
+        launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
+        launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
         if (p.n_iface)
           amr3_coalesce<Q><<<p.n_iface, rb3, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
       });
@@ -1302,17 +1369,19 @@ const char *lbm_amr3d_last_error(const lbm_amr3d *a) { return a ? a->err.c_str()
 
 namespace {
 
-// The substep's pull sources, the same for every tile: per direction i and
-// cell list position k, a word of the neighbour slot the source lies in (its
-// index in the CTA's 3 x 3 x 3 table; 13 = this tile), bits 0-4; the source
-// cell in that tile, bits 5-17; and the cell of this tile it clamps to when
-// that neighbour is not refined, bits 18-30 (T3 <= 20^3 < 2^13). DIRECT_GHOST
+// The substep's pull sources, the same for every tile: per cell list
+// position k, pull_words(q) words (Q rounded up to a multiple of 4, so a
+// thread reads its row with 128-bit loads); word i, for direction i, holds
+// the neighbour the source lies in (its index in the CTA's 3 x 3 x 3 table,
+// 13 = this tile) in bits 0-4, the source cell in that tile in bits 5-17,
+// and the cell of this tile it clamps to when that neighbour is not refined
+// in bits 18-30 (T3 <= 20^3 < 2^13). DIRECT_GHOST
 // (common_d3_amr_step1.wgsl): a source past the interior, toward the tile
 // edge the cell sits at, is read from the refined neighbour's interior, else
 // from this tile's ring.
 std::vector<uint32_t> pull_table(int q, int FB, int RB2, const std::vector<uint32_t> &cl) {
-  const int G = kAmrGhost, n = (int)cl.size();
-  std::vector<uint32_t> t((size_t)q * n);
+  const int G = kAmrGhost, n = (int)cl.size(), kw = pull_words(q);
+  std::vector<uint32_t> t((size_t)kw * n, 0u);
   for (int k = 0; k < n; ++k) {
     const int fi[3] = {(int)(cl[k] & 0xff), (int)((cl[k] >> 8) & 0xff), (int)(cl[k] >> 16)};
     for (int i = 0; i < q; ++i) {
@@ -1328,7 +1397,7 @@ std::vector<uint32_t> pull_table(int q, int FB, int RB2, const std::vector<uint3
       const uint32_t nb = (uint32_t)((o[2] + 1) * 9 + (o[1] + 1) * 3 + (o[0] + 1));
       const uint32_t ls = (uint32_t)((sh[2] * FB + sh[1]) * FB + sh[0]);
       const uint32_t lc = (uint32_t)((sc[2] * FB + sc[1]) * FB + sc[0]);
-      t[(size_t)i * n + k] = nb | ls << 5 | lc << 18;
+      t[(size_t)k * kw + i] = nb | ls << 5 | lc << 18;
     }
   }
   return t;
@@ -1387,6 +1456,12 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   a->slot_to_block.resize(a->capacity, -1);
   p.slots = a->capacity;
   p.P = (int64_t)a->capacity * p.T3;
+  if (p.P > INT32_MAX) {
+    // the substep addresses pool cells with 32-bit offsets (2^31 cells of
+    // Q >= 19 populations would be 150+ GB per buffer)
+    delete a;
+    return afail(nullptr, LBM_ENOMEM, "pool of more than 2^31 cells");
+  }
   // interface blocks: covered, or a covered block among the 26 neighbours
   for (int id = 0; id < nb; ++id) {
     const int bx = id % p.nbx, by = (id / p.nbx) % p.nby, bz = id / (p.nbx * p.nby);
@@ -1441,7 +1516,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     if ((e = mem.take(&a->d_slot_to_block, a->capacity * sizeof(int)))) return bail(e, "slots");
     if ((e = mem.take(&a->d_iface, std::max(p.n_iface, 1) * sizeof(int)))) return bail(e, "iface");
     if ((e = mem.take(&a->d_cells, (size_t)p.T3 * sizeof(uint32_t)))) return bail(e, "cell list");
-    if ((e = mem.take(&a->d_pulls, (size_t)a->q * p.T3 * sizeof(uint32_t)))) return bail(e, "pull table");
+    if ((e = mem.take(&a->d_pulls, (size_t)pull_words(a->q) * p.T3 * sizeof(uint32_t)))) return bail(e, "pull table");
     if (r.has_body && r.use_bounceback && (e = mem.take(&a->d_links, (size_t)p.P * sizeof(uint32_t))))
       return bail(e, "link table");
     if (a->dynamic) {

@@ -16,6 +16,8 @@
 namespace lbm {
 
 constexpr int kAmrGhost = 2;
+// words per tile cell in the substep's pull table: Q rounded up to a multiple of 4
+constexpr int pull_words(int q) { return (q + 3) & ~3; }
 constexpr int kTileThreads = 128;    // 1D pool kernels (force, drain, coalesce)
 constexpr int kMaxAmrRb = 8;         // tiles up to FB = 20: FB x FB threads per CTA
 constexpr int kTileMaxThreads = (2 * kMaxAmrRb + 4) * (2 * kMaxAmrRb + 4);

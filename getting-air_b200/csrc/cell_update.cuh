@@ -22,7 +22,11 @@
 
 namespace lbm {
 
-constexpr float kCS2 = 1.0f / 3.0f;
+// 1 / c_s^2. The moving-wall term 2 w_i rho_w (e_i . u_w) / c_s^2 multiplies
+// by it: a division there is an IEEE-rounded divide with a slow-path branch
+// per link, which in the 3D AMR substep (most tile cells near the body) cost
+// a third of the kernel's instructions.
+constexpr float kInvCS2 = 3.0f;
 
 // ---- storage codecs --------------------------------------------------------
 // FP32 planes hold f itself; the 16-bit planes hold (f - off_i) * scale (see
@@ -438,7 +442,7 @@ __device__ __forceinline__ void cell3_core(const S *__restrict__ fi, float (&f)[
         const float fopp = own[L::opp(i)];
         if ((solid >> i) & 1u) {
           const float corr =
-              2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) / kCS2;
+              2.f * L::w(i) * rhoW * ((float)ex * us.x + (float)ey * us.y + (float)ez * us.z) * kInvCS2;
           f[i] = fopp + corr;
           if (phi >= 0.f) {
             const float m = 2.f * fopp + corr;
@@ -709,7 +713,7 @@ __device__ __forceinline__ void cell2_core(const S *__restrict__ fin, float (&f)
       }
       if (solid) {
         const float fopp = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk);
-        const float corr = 2.f * L::w(i) * ((float)ex * usx + (float)ey * usy) / kCS2;
+        const float corr = 2.f * L::w(i) * ((float)ex * usx + (float)ey * usy) * kInvCS2;
         f[i] = fopp + corr;
         if (phi >= 0.f) {
           const float m = 2.f * fopp + corr;
@@ -720,7 +724,7 @@ __device__ __forceinline__ void cell2_core(const S *__restrict__ fin, float (&f)
         const int ysrc = y - ey;
         if (ysrc < 0 || ysrc >= H) {
           const float wu = ysrc < 0 ? p.wall_u0 : p.wall_u1;
-          const float corr = 2.f * L::w(i) * (float)ex * wu / kCS2;
+          const float corr = 2.f * L::w(i) * (float)ex * wu * kInvCS2;
           f[i] = Codec<S>::ld(fi + (int64_t)o * n + cell, o, p.pk) + corr;
         }
       }
