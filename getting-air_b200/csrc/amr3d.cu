@@ -26,6 +26,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -315,8 +316,10 @@ __global__ void __launch_bounds__(kListThreads)
         const int du = b[a] * p.RB2 + fi[a] - kAmrGhost + e[a];
         dv[a] = du >= 0 ? du / 2 : -((1 - du) / 2);
       }
-      const bool into = covered_near(p, nb27, b, dv[0], dv[1], dv[2]) && dg[0] / p.RB2 == b[0] &&
-                        dg[1] / p.RB2 == b[1] && dg[2] / p.RB2 == b[2];
+      // dg / RB2 == b, as a range test on the wrapped (non-negative) dg
+      bool own = true;
+      for (int a = 0; a < 3; ++a) own = own && dg[a] >= b[a] * p.RB2 && dg[a] < (b[a] + 1) * p.RB2;
+      const bool into = covered_near(p, nb27, b, dv[0], dv[1], dv[2]) && own;
       out = into ? __ldg(fc + (int64_t)i * p.N + vc) : 0.f;
     } else {
       const float f = __ldg(fc + (int64_t)i * p.N + vc);
@@ -483,9 +486,14 @@ __device__ __forceinline__ int local_in_tile(const Amr3Params &p, int g, int b, 
   return d + kAmrGhost;
 }
 
-// One CTA per interface block, one thread per L0 cell of it (rb^3 threads);
-// the 3 x 3 x 3 neighbour blocks' slots come from a shared table, so no
-// coverage or slot lookup goes to global memory or divides.
+// One CTA per interface block, SUBS threads per L0 cell of it (rb^3 * SUBS
+// threads, adjacent lanes sharing a cell), each taking every SUBS-th
+// direction. The directions of a cell are independent, and a seam cell's
+// out/in-orphan balance walks 8 children per direction, too long a chain
+// for one thread when a few hundred blocks cannot fill the device; with
+// thousands of blocks one thread per cell (SUBS = 1) keeps its restriction
+// loop unrolled. The 3 x 3 x 3 neighbour blocks' slots come from a shared
+// table, so no coverage or slot lookup goes to global memory or divides.
 __device__ __forceinline__ int rel_block(int q, int b, int nb) {
   int d = q - b;
   if (d > 1) d -= nb;
@@ -493,7 +501,7 @@ __device__ __forceinline__ int rel_block(int q, int b, int nb) {
   return d;
 }
 
-template <int Q>
+template <int Q, int SUBS>
 __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
     amr3_coalesce(const float *__restrict__ fp, float *__restrict__ fc, float4 *__restrict__ macc,
                   const float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
@@ -502,13 +510,17 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
   if (!p.iface && !p.iface_flag[id]) return;  // the whole CTA
   const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
   __shared__ int nb27[27];
+  __shared__ signed char dir[3][27];
   for (int k = threadIdx.x; k < 27; k += blockDim.x) {
     const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
     nb27[k] = p.block_slot[(wrapi(b[2] + dz, p.nbz) * p.nby + wrapi(b[1] + dy, p.nby)) * p.nbx +
                            wrapi(b[0] + dx, p.nbx)];
+    dir[0][k] = (signed char)L::ex(k < Q ? k : 0);
+    dir[1][k] = (signed char)L::ey(k < Q ? k : 0);
+    dir[2][k] = (signed char)L::ez(k < Q ? k : 0);
   }
   __syncthreads();
-  const int l = threadIdx.x;
+  const int l = threadIdx.x / SUBS, sub = threadIdx.x % SUBS;
   const int x = b[0] * p.rb + l % p.rb, y = b[1] * p.rb + (l / p.rb) % p.rb, z = b[2] * p.rb + l / (p.rb * p.rb);
   const int cc[3] = {x, y, z};
   const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
@@ -523,8 +535,8 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
     for (int i = 1; i < Q; ++i) nearc = nearc || covered_near(p, nb27, b, x + L::ex(i), y + L::ey(i), z + L::ez(i));
     if (!nearc) return;
 #pragma unroll 1
-    for (int i = 1; i < Q; ++i) {
-      const int e[3] = {c_dirs.ex[i], c_dirs.ey[i], c_dirs.ez[i]};
+    for (int i = 1 + sub; i < Q; i += SUBS) {
+      const int e[3] = {dir[0][i], dir[1][i], dir[2][i]};
       const int tc[3] = {x + e[0], y + e[1], z + e[2]};
       if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
       float sacc = 0.f, nin = 0.f;
@@ -561,7 +573,7 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
   }
   const int lx0 = kAmrGhost + 2 * (x - b[0] * p.rb), ly0 = kAmrGhost + 2 * (y - b[1] * p.rb),
             lz0 = kAmrGhost + 2 * (z - b[2] * p.rb);
-  if (p.write_mac) {
+  if (p.write_mac && sub == 0) {
     float rs = 0.f, m0 = 0.f, m1 = 0.f, m2 = 0.f;
     for (int q = 0; q < 8; ++q) {
       const float4 m = macp[(int64_t)slot * p.T3 + ((lz0 + ((q >> 2) & 1)) * p.FB + ly0 + ((q >> 1) & 1)) * p.FB +
@@ -573,8 +585,9 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
     macc[cell] = make_float4(rs * 0.125f, m0 * inv, m1 * inv, m2 * inv);
   }
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+  for (int i = sub; i < Q; i += SUBS) {
+    const int e[3] = {SUBS == 1 ? L::ex(i) : dir[0][i], SUBS == 1 ? L::ey(i) : dir[1][i],
+                      SUBS == 1 ? L::ez(i) : dir[2][i]};
     const int tc[3] = {x + e[0], y + e[1], z + e[2]};
     if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
     float sacc = 0.f;
@@ -708,13 +721,37 @@ __global__ void __launch_bounds__(kTileThreads)
 }
 
 // ---- L0 step, skipping covered blocks ------------------------------------
+// With `skip` (the interface flags), the interface blocks are skipped too:
+// that part of the L0 step runs apart, after the coalesce (amr3_coarse_near).
 template <int Q>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     amr3_coarse(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
-                const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby) {
+                const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby,
+                const unsigned char *__restrict__ skip) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
   if (x >= sp.nx) return;
-  if (block_slot[((z / rb) * nby + y / rb) * nbx + x / rb] >= 0) return;
+  const int b = ((z / rb) * nby + y / rb) * nbx + x / rb;
+  if (block_slot[b] >= 0 || (skip && skip[b])) return;
+  CellForce cf;
+  cell3<Q, float>(fin, fout, mac, sp, x, y, z, false, cf);
+}
+
+// The L0 step of the uncovered interface blocks, one CTA of rb^3 threads
+// per interface block: the cells that may pull what the coalesce writes
+// into the time-t buffer (the covered cells and the seam cells next to
+// them, all within one cell of a refined block). Every other cell is at
+// least rb >= 3 cells from a refined block, pulls from one cell away, and
+// steps in amr3_coarse while the tiles advance.
+template <int Q>
+__global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
+    amr3_coarse_near(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
+                     const __grid_constant__ StepParams sp, const __grid_constant__ Amr3Params p) {
+  const int id = p.iface ? p.iface[blockIdx.x] : (int)blockIdx.x;
+  if (!p.iface && !p.iface_flag[id]) return;  // the whole CTA
+  if (p.block_slot[id] >= 0) return;          // covered: the tile restricts into it
+  const int l = threadIdx.x;
+  const int x = (id % p.nbx) * p.rb + l % p.rb, y = ((id / p.nbx) % p.nby) * p.rb + (l / p.rb) % p.rb,
+            z = (id / (p.nbx * p.nby)) * p.rb + l / (p.rb * p.rb);
   CellForce cf;
   cell3<Q, float>(fin, fout, mac, sp, x, y, z, false, cf);
 }
@@ -1113,6 +1150,10 @@ struct lbm_amr3d {
   uint32_t *d_cells = nullptr;  // tile cells: interior (RB2^3) then ring, packed x | y << 8 | z << 16
   uint32_t *d_links = nullptr;  // bounce-back link code per pool cell (bounce-back bodies only)
   uint32_t *d_pulls = nullptr;  // substep pull sources per (direction, cell list position)
+  int coalesce_subs = 1;        // threads per L0 cell in the coalesce
+  cudaStream_t side = nullptr;  // the L0 step away from the interface, beside the tiles' kernels
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int prio_hi = 0;              // the device's highest stream priority
   float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
   float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
@@ -1198,14 +1239,57 @@ cudaError_t launch_moments(lbm_amr3d *a) {
   AMR3_DISPATCH(a->q, amr3_moments<Q><<<g, tile_block(a), 0, a->stream>>>(a->fp[0], a->macp, a->p));
 }
 
+// Threads per L0 cell in the coalesce: doubled up to 8 while the interface
+// blocks' threads still fit the device's resident threads and a CTA's 512.
+int coalesce_subs(const Amr3Params &p, int sms) {
+  const int rb3 = p.rb * p.rb * p.rb;
+  const int64_t resident = (int64_t)sms * 2048;
+  int subs = 1;
+  while (subs < 8 && rb3 * subs * 2 <= kMaxAmrRb * kMaxAmrRb * kMaxAmrRb &&
+         (int64_t)p.n_iface * rb3 * subs * 2 <= resident)
+    subs *= 2;
+  return subs;
+}
+
+// A launch at stream priority `prio` (0: the stream's own). The tiles'
+// kernels of a macro-step run at the device's highest priority while the L0
+// step away from the interface runs beside them, so that each of their
+// short dependent launches starts as soon as its predecessor ends rather
+// than behind the L0 step's tens of thousands of CTAs.
+template <typename... K, typename... A>
+void launch_at(int prio, dim3 g, dim3 b, cudaStream_t st, void (*k)(K...), A &&...args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = g;
+  lc.blockDim = b;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = prio;
+  lc.attrs = at;
+  lc.numAttrs = prio ? 1 : 0;
+  cudaLaunchKernelEx(&lc, k, std::forward<A>(args)...);
+}
+
+template <int Q>
+void launch_coalesce(int prio, cudaStream_t st, const float *fp, float *fc, float4 *macc, const float4 *macp,
+                     const Amr3Params &p, int subs) {
+  const dim3 g(p.n_iface), b(p.rb * p.rb * p.rb * subs);
+  switch (subs) {
+    case 8: launch_at(prio, g, b, st, amr3_coalesce<Q, 8>, fp, fc, macc, macp, p); break;
+    case 4: launch_at(prio, g, b, st, amr3_coalesce<Q, 4>, fp, fc, macc, macp, p); break;
+    case 2: launch_at(prio, g, b, st, amr3_coalesce<Q, 2>, fp, fc, macc, macp, p); break;
+    default: launch_at(prio, g, b, st, amr3_coalesce<Q, 1>, fp, fc, macc, macp, p); break;
+  }
+}
+
 // A pool substep, with 32-bit population indices when the pool allows.
 template <int Q>
-void launch_substep(dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp, const Amr3Params &p,
-                    const uint32_t *cells) {
+void launch_substep(int prio, dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp,
+                    const Amr3Params &p, const uint32_t *cells) {
   if ((int64_t)Q * p.P <= INT32_MAX)
-    amr3_substep<Q, true><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+    launch_at(prio, gl, dim3(kListThreads), st, amr3_substep<Q, true>, fin, fout, macp, p, cells, p.T3);
   else
-    amr3_substep<Q, false><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+    launch_at(prio, gl, dim3(kListThreads), st, amr3_substep<Q, false>, fin, fout, macp, p, cells, p.T3);
 }
 
 // One macro-step from L0 parity `cp`.
@@ -1233,49 +1317,77 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     AMR3_DISPATCH(q, {
       if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
       amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp, a->d_block_slot, p.rb,
-                                                   p.nbx, p.nby);
+                                                   p.nbx, p.nby, nullptr);
       amr3_interp<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p, 1, nullptr);
       Amr3Params pa = p;
       pa.write_mac = 0;
       const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->flux, p, 0);
-      launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
+      launch_substep<Q>(0, gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[1], a->flux, p, 1);
-      launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
+      launch_substep<Q>(0, gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
       amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
                                                  f2c_rescale);
       if (a->flux && gc)
         amr3_reflux<Q><<<gc, kTileThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], (float4 *)a->macc, a->flux, p);
     });
   }
+  StepParams sp = a->sp;
+  sp.write_mac = write_mac ? 1 : 0;
+  const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
+  // The L0 step away from the interface overlaps the tiles' kernels on the
+  // side stream (a fork and a join, parallel branches in the graph); the
+  // interface blocks step after the coalesce. Only for a pool of at least a
+  // quarter of L0's cells: a small pool's kernels are a chain of short,
+  // latency-bound launches, and beside a bandwidth-bound L0 step their
+  // memory latency grows more than the overlap saves (measured on B200: a
+  // 160-tile sphere 0.1704 -> 0.1725 ms per macro-step with the overlap, a
+  // 2262-tile rounded box at 180^3 0.817 -> 0.782 ms).
+  const bool overlap = p.slots && p.n_iface && p.rb >= 3 && a->side && 4 * p.P >= p.N;
+  const int prio = overlap ? a->prio_hi : 0;
+  if (overlap) {
+    if ((e = cudaEventRecord(a->fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(a->side, a->fork, 0)) != cudaSuccess) return e;
+    auto far = [&]() -> cudaError_t {
+      AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, a->side>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
+                                                                        a->d_block_slot, p.rb, p.nbx, p.nby,
+                                                                        a->d_iface_flag));
+    };
+    if ((e = far()) != cudaSuccess) return e;
+  }
   if (p.slots) {
     const dim3 gl((p.T3 + kListThreads - 1) / kListThreads, p.slots);
     const int r3 = p.RB2 * p.RB2 * p.RB2;
     const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
-    const int rb3 = p.rb * p.rb * p.rb;
-    const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
     auto body = [&]() -> cudaError_t {
       AMR3_DISPATCH(q, {
-        if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
+        if (p.c.has_body) launch_at(prio, gf, dim3(kTileThreads), st, amr3_force<Q>, a->fp[0], p);
         const int r3i = p.RB2 * p.RB2 * p.RB2, nring = p.T3 - r3i;
         const dim3 gr((nring + kListThreads - 1) / kListThreads, p.slots);
-        amr3_explode<Q><<<gr, kListThreads, 0, st>>>(a->fc[cp], a->fp[0], p, a->d_cells, r3i, nring);
+        launch_at(prio, gr, dim3(kListThreads), st, amr3_explode<Q>, a->fc[cp], a->fp[0], p, a->d_cells, r3i,
+                  nring);
         Amr3Params pa = p;
         pa.write_mac = 0;
-        launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
-        launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
+        launch_substep<Q>(prio, gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
+        launch_substep<Q>(prio, gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
         if (p.n_iface)
-          amr3_coalesce<Q><<<p.n_iface, rb3, 0, st>>>(a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p);
+          launch_coalesce<Q>(prio, st, a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p, a->coalesce_subs);
       });
     };
     e = body();
     if (e != cudaSuccess) return e;
   }
-  StepParams sp = a->sp;
-  sp.write_mac = write_mac ? 1 : 0;
-  const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
+  if (overlap) {
+    auto near = [&]() -> cudaError_t {
+      AMR3_DISPATCH(q, launch_at(prio, dim3(p.n_iface), dim3(p.rb * p.rb * p.rb), st, amr3_coarse_near<Q>,
+                                 a->fc[cp], a->fc[1 - cp], a->macc, sp, p));
+    };
+    if ((e = near()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(a->join, a->side)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(st, a->join, 0);
+  }
   AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
-                                                                 a->d_block_slot, p.rb, p.nbx, p.nby));
+                                                                 a->d_block_slot, p.rb, p.nbx, p.nby, nullptr));
 }
 
 void destroy_graphs(lbm_amr3d *a) {
@@ -1341,6 +1453,9 @@ void release(lbm_amr3d *a) {
     if (!a->carved) cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
+  if (a->side) cudaStreamDestroy(a->side);
+  if (a->fork) cudaEventDestroy(a->fork);
+  if (a->join) cudaEventDestroy(a->join);
 }
 
 constexpr int kTotBlocks = 296;
@@ -1519,9 +1634,9 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     if ((e = mem.take(&a->d_pulls, (size_t)pull_words(a->q) * p.T3 * sizeof(uint32_t)))) return bail(e, "pull table");
     if (r.has_body && r.use_bounceback && (e = mem.take(&a->d_links, (size_t)p.P * sizeof(uint32_t))))
       return bail(e, "link table");
+    if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
     if (a->dynamic) {
       if ((e = mem.take(&a->d_want, nb))) return bail(e, "want");
-      if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
       if ((e = mem.take(&a->d_slot_new, a->capacity))) return bail(e, "new");
       if ((e = mem.take(&a->d_free_list, nfl * sizeof(int)))) return bail(e, "free list");
       if ((e = mem.take(&a->d_counts, 4 * sizeof(int)))) return bail(e, "counts");
@@ -1542,6 +1657,13 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     return LBM_OK;
   }
   if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
+  if ((e = cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking))) return bail(e, "stream");
+  if ((e = cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming))) return bail(e, "event");
+  if ((e = cudaEventCreateWithFlags(&a->join, cudaEventDisableTiming))) return bail(e, "event");
+  {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) a->prio_hi = greatest;
+  }
   a->stream = a->own;
   for (int k = 0; k < 2; ++k)
     if ((e = cudaMemsetAsync(a->fp[k], 0, fpb, a->own))) return bail(e, "memset pool f");
@@ -1564,15 +1686,19 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     const std::vector<uint32_t> pt = pull_table(a->q, p.FB, p.RB2, cl);
     cudaMemcpyAsync(a->d_pulls, pt.data(), pt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, a->own);
   }
-  if (a->dynamic) {
+  {
+    // interface flags: covered blocks and the blocks touching one (the
+    // dynamic manager rewrites them with each decision)
     std::vector<unsigned char> flag(nb, 0);
     for (int id : a->iface) flag[id] = 1;
+    cudaMemcpyAsync(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice, a->own);
+  }
+  if (a->dynamic) {
     std::vector<int> fl(nfl, 0);
     for (int i = 0; i < nfree; ++i) fl[i] = a->initial + i;
     const int counts[4] = {nfree, 0, nfree, 0};
     cudaMemsetAsync(a->d_want, 0, nb, a->own);
     cudaMemsetAsync(a->d_slot_new, 0, a->capacity, a->own);
-    cudaMemcpyAsync(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice, a->own);
     cudaMemcpyAsync(a->d_free_list, fl.data(), fl.size() * sizeof(int), cudaMemcpyHostToDevice, a->own);
     cudaMemcpyAsync(a->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, a->own);
     if (c->q_abs > 0) {
@@ -1601,6 +1727,12 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   p.force_out = a->force_out;
   p.links = a->d_links;  // filled when the hierarchy is seeded
   p.pulls = a->d_pulls;
+  {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    a->coalesce_subs = coalesce_subs(p, std::max(sms, 1));
+  }
   *out = a;
   return LBM_OK;
 }
