@@ -26,7 +26,6 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
-#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -721,37 +720,13 @@ __global__ void __launch_bounds__(kTileThreads)
 }
 
 // ---- L0 step, skipping covered blocks ------------------------------------
-// With `skip` (the interface flags), the interface blocks are skipped too:
-// that part of the L0 step runs apart, after the coalesce (amr3_coarse_near).
 template <int Q>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     amr3_coarse(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
-                const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby,
-                const unsigned char *__restrict__ skip) {
+                const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby) {
   const int x = blockIdx.x * kStepThreads + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
   if (x >= sp.nx) return;
-  const int b = ((z / rb) * nby + y / rb) * nbx + x / rb;
-  if (block_slot[b] >= 0 || (skip && skip[b])) return;
-  CellForce cf;
-  cell3<Q, float>(fin, fout, mac, sp, x, y, z, false, cf);
-}
-
-// The L0 step of the uncovered interface blocks, one CTA of rb^3 threads
-// per interface block: the cells that may pull what the coalesce writes
-// into the time-t buffer (the covered cells and the seam cells next to
-// them, all within one cell of a refined block). Every other cell is at
-// least rb >= 3 cells from a refined block, pulls from one cell away, and
-// steps in amr3_coarse while the tiles advance.
-template <int Q>
-__global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
-    amr3_coarse_near(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
-                     const __grid_constant__ StepParams sp, const __grid_constant__ Amr3Params p) {
-  const int id = p.iface ? p.iface[blockIdx.x] : (int)blockIdx.x;
-  if (!p.iface && !p.iface_flag[id]) return;  // the whole CTA
-  if (p.block_slot[id] >= 0) return;          // covered: the tile restricts into it
-  const int l = threadIdx.x;
-  const int x = (id % p.nbx) * p.rb + l % p.rb, y = ((id / p.nbx) % p.nby) * p.rb + (l / p.rb) % p.rb,
-            z = (id / (p.nbx * p.nby)) * p.rb + l / (p.rb * p.rb);
+  if (block_slot[((z / rb) * nby + y / rb) * nbx + x / rb] >= 0) return;
   CellForce cf;
   cell3<Q, float>(fin, fout, mac, sp, x, y, z, false, cf);
 }
@@ -762,7 +737,7 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
 // penalty with a tile-clamped gather; FP64 partial per CTA, last-CTA sum.
 template <int Q>
 __global__ void __launch_bounds__(kTileThreads)
-    amr3_force(const float *__restrict__ fp, const __grid_constant__ Amr3Params p) {
+    amr3_force(const float *__restrict__ fp, const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells) {
   using L = Lattice<Q>;
   const StepParams &c = p.c;
   const int r3 = p.RB2 * p.RB2 * p.RB2;
@@ -772,7 +747,9 @@ __global__ void __launch_bounds__(kTileThreads)
   const int id = p.slot_to_block[slot];
   if (k < r3 && id >= 0) {
     const int b[3] = {id % p.nbx, (id / p.nbx) % p.nby, id / (p.nbx * p.nby)};
-    const int fx = kAmrGhost + k % p.RB2, fy = kAmrGhost + (k / p.RB2) % p.RB2, fz = kAmrGhost + k / (p.RB2 * p.RB2);
+    // interior cell k (the cell list holds the interior first, z-, y-, x-major)
+    const uint32_t cl = __ldg(cells + k);
+    const int fx = cl & 0xff, fy = (cl >> 8) & 0xff, fz = cl >> 16;
     const int64_t cell = (int64_t)slot * p.T3 + (fz * p.FB + fy) * p.FB + fx;
     const V3 pos = {f2c(fx, b[0] * p.rb), f2c(fy, b[1] * p.rb), f2c(fz, b[2] * p.rb)};
     // With the link table and no swept-cell term, the cell's code says all
@@ -856,8 +833,16 @@ __global__ void __launch_bounds__(kTileThreads)
   }
   ForceAcc acc;
   acc.add(cf);
-  reduce_force<kTileThreads>(acc, p.partials, p.counter, gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x,
-                             p.force_out);
+  publish_force<kTileThreads>(acc, p.partials, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// The pool force's partials summed in a fixed order (groups of kSumGroup,
+// then the groups), deterministic; a launch of its own, so that the force
+// CTAs publish their partials without a ticket and its fence.
+__global__ void __launch_bounds__(kSumGroup)
+    amr3_force_sum(const double *__restrict__ partials, int nparts, double *__restrict__ groups,
+                   unsigned int *__restrict__ counter, double *__restrict__ out) {
+  sum_partials_grouped<kSumGroup>(partials, nparts, groups, counter, out, blockIdx.x);
 }
 
 // ---- the refinement manager (common_d3_manage.wgsl) ------------------------
@@ -1132,6 +1117,7 @@ struct lbm_amr3d {
   int *d_block_slot = nullptr, *d_slot_to_block = nullptr, *d_iface = nullptr;
   std::vector<int> block_slot, slot_to_block, iface;
   double *partials = nullptr, *force_out = nullptr, *tot_partials = nullptr, *tot_out = nullptr;
+  double *force_groups = nullptr;  // the force partials' group sums
   unsigned int *counter = nullptr, *tot_counter = nullptr;
   double *host_out = nullptr;
   int force_parts = 0;
@@ -1151,9 +1137,6 @@ struct lbm_amr3d {
   uint32_t *d_links = nullptr;  // bounce-back link code per pool cell (bounce-back bodies only)
   uint32_t *d_pulls = nullptr;  // substep pull sources per (direction, cell list position)
   int coalesce_subs = 1;        // threads per L0 cell in the coalesce
-  cudaStream_t side = nullptr;  // the L0 step away from the interface, beside the tiles' kernels
-  cudaEvent_t fork = nullptr, join = nullptr;
-  int prio_hi = 0;              // the device's highest stream priority
   float *d_block_q = nullptr;   // field criterion: per-block max Q (NULL = off)
   float q_refine = 0.f, q_hold = 0.f;
   float4 *flux = nullptr;  // reflux: per L0 cell {dm, dp}
@@ -1251,45 +1234,37 @@ int coalesce_subs(const Amr3Params &p, int sms) {
   return subs;
 }
 
-// A launch at stream priority `prio` (0: the stream's own). The tiles'
-// kernels of a macro-step run at the device's highest priority while the L0
-// step away from the interface runs beside them, so that each of their
-// short dependent launches starts as soon as its predecessor ends rather
-// than behind the L0 step's tens of thousands of CTAs.
-template <typename... K, typename... A>
-void launch_at(int prio, dim3 g, dim3 b, cudaStream_t st, void (*k)(K...), A &&...args) {
-  cudaLaunchConfig_t lc = {};
-  lc.gridDim = g;
-  lc.blockDim = b;
-  lc.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributePriority;
-  at[0].val.priority = prio;
-  lc.attrs = at;
-  lc.numAttrs = prio ? 1 : 0;
-  cudaLaunchKernelEx(&lc, k, std::forward<A>(args)...);
-}
-
 template <int Q>
-void launch_coalesce(int prio, cudaStream_t st, const float *fp, float *fc, float4 *macc, const float4 *macp,
+void launch_coalesce(cudaStream_t st, const float *fp, float *fc, float4 *macc, const float4 *macp,
                      const Amr3Params &p, int subs) {
-  const dim3 g(p.n_iface), b(p.rb * p.rb * p.rb * subs);
+  const int t = p.rb * p.rb * p.rb * subs;
   switch (subs) {
-    case 8: launch_at(prio, g, b, st, amr3_coalesce<Q, 8>, fp, fc, macc, macp, p); break;
-    case 4: launch_at(prio, g, b, st, amr3_coalesce<Q, 4>, fp, fc, macc, macp, p); break;
-    case 2: launch_at(prio, g, b, st, amr3_coalesce<Q, 2>, fp, fc, macc, macp, p); break;
-    default: launch_at(prio, g, b, st, amr3_coalesce<Q, 1>, fp, fc, macc, macp, p); break;
+    case 8: amr3_coalesce<Q, 8><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
+    case 4: amr3_coalesce<Q, 4><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
+    case 2: amr3_coalesce<Q, 2><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
+    default: amr3_coalesce<Q, 1><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
   }
 }
 
 // A pool substep, with 32-bit population indices when the pool allows.
 template <int Q>
-void launch_substep(int prio, dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp,
-                    const Amr3Params &p, const uint32_t *cells) {
+void launch_substep(dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp, const Amr3Params &p,
+                    const uint32_t *cells) {
   if ((int64_t)Q * p.P <= INT32_MAX)
-    launch_at(prio, gl, dim3(kListThreads), st, amr3_substep<Q, true>, fin, fout, macp, p, cells, p.T3);
+    amr3_substep<Q, true><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
   else
-    launch_at(prio, gl, dim3(kListThreads), st, amr3_substep<Q, false>, fin, fout, macp, p, cells, p.T3);
+    amr3_substep<Q, false><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+}
+
+// The pool force at time t and its deterministic sum.
+template <int Q>
+void launch_pool_force(lbm_amr3d *a, const Amr3Params &p, cudaStream_t st) {
+  const int r3 = p.RB2 * p.RB2 * p.RB2;
+  const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
+  amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p, a->d_cells);
+  const int parts = gf.x * gf.y;
+  amr3_force_sum<<<sum_groups(parts), kSumGroup, 0, st>>>(a->partials, parts, a->force_groups, a->counter,
+                                                          a->force_out);
 }
 
 // One macro-step from L0 parity `cp`.
@@ -1315,79 +1290,47 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
     const float tc = a->cfg.root.tau, tf = 2.f * tc - 0.5f;
     const float f2c_rescale = 2.f * (tc - 1.f) / (tf - 1.f);
     AMR3_DISPATCH(q, {
-      if (p.c.has_body) amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p);
+      if (p.c.has_body) launch_pool_force<Q>(a, p, st);
       amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp, a->d_block_slot, p.rb,
-                                                   p.nbx, p.nby, nullptr);
+                                                   p.nbx, p.nby);
       amr3_interp<Q><<<g, tile_block(a), 0, st>>>(a->fc[cp], a->fp[0], p, 1, nullptr);
       Amr3Params pa = p;
       pa.write_mac = 0;
       const int gc = (p.n_iface * rb3 + kTileThreads - 1) / kTileThreads;
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[0], a->flux, p, 0);
-      launch_substep<Q>(0, gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
+      launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
       if (a->flux && gc) amr3_flux<Q><<<gc, kTileThreads, 0, st>>>(a->fp[1], a->flux, p, 1);
-      launch_substep<Q>(0, gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
+      launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
       amr3_drain<Q><<<gd, kTileThreads, 0, st>>>(a->fp[0], a->fc[1 - cp], (float4 *)a->macc, p, nullptr,
                                                  f2c_rescale);
       if (a->flux && gc)
         amr3_reflux<Q><<<gc, kTileThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], (float4 *)a->macc, a->flux, p);
     });
   }
-  StepParams sp = a->sp;
-  sp.write_mac = write_mac ? 1 : 0;
-  const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
-  // The L0 step away from the interface overlaps the tiles' kernels on the
-  // side stream (a fork and a join, parallel branches in the graph); the
-  // interface blocks step after the coalesce. Only for a pool of at least a
-  // quarter of L0's cells: a small pool's kernels are a chain of short,
-  // latency-bound launches, and beside a bandwidth-bound L0 step their
-  // memory latency grows more than the overlap saves (measured on B200: a
-  // 160-tile sphere 0.1704 -> 0.1725 ms per macro-step with the overlap, a
-  // 2262-tile rounded box at 180^3 0.817 -> 0.782 ms).
-  const bool overlap = p.slots && p.n_iface && p.rb >= 3 && a->side && 4 * p.P >= p.N;
-  const int prio = overlap ? a->prio_hi : 0;
-  if (overlap) {
-    if ((e = cudaEventRecord(a->fork, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(a->side, a->fork, 0)) != cudaSuccess) return e;
-    auto far = [&]() -> cudaError_t {
-      AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, a->side>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
-                                                                        a->d_block_slot, p.rb, p.nbx, p.nby,
-                                                                        a->d_iface_flag));
-    };
-    if ((e = far()) != cudaSuccess) return e;
-  }
   if (p.slots) {
     const dim3 gl((p.T3 + kListThreads - 1) / kListThreads, p.slots);
-    const int r3 = p.RB2 * p.RB2 * p.RB2;
-    const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
     auto body = [&]() -> cudaError_t {
       AMR3_DISPATCH(q, {
-        if (p.c.has_body) launch_at(prio, gf, dim3(kTileThreads), st, amr3_force<Q>, a->fp[0], p);
+        if (p.c.has_body) launch_pool_force<Q>(a, p, st);
         const int r3i = p.RB2 * p.RB2 * p.RB2, nring = p.T3 - r3i;
         const dim3 gr((nring + kListThreads - 1) / kListThreads, p.slots);
-        launch_at(prio, gr, dim3(kListThreads), st, amr3_explode<Q>, a->fc[cp], a->fp[0], p, a->d_cells, r3i,
-                  nring);
+        amr3_explode<Q><<<gr, kListThreads, 0, st>>>(a->fc[cp], a->fp[0], p, a->d_cells, r3i, nring);
         Amr3Params pa = p;
         pa.write_mac = 0;
-        launch_substep<Q>(prio, gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
-        launch_substep<Q>(prio, gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
+        launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
+        launch_substep<Q>(gl, st, a->fp[1], a->fp[0], a->macp, p, a->d_cells);
         if (p.n_iface)
-          launch_coalesce<Q>(prio, st, a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p, a->coalesce_subs);
+          launch_coalesce<Q>(st, a->fp[0], a->fc[cp], (float4 *)a->macc, a->macp, p, a->coalesce_subs);
       });
     };
     e = body();
     if (e != cudaSuccess) return e;
   }
-  if (overlap) {
-    auto near = [&]() -> cudaError_t {
-      AMR3_DISPATCH(q, launch_at(prio, dim3(p.n_iface), dim3(p.rb * p.rb * p.rb), st, amr3_coarse_near<Q>,
-                                 a->fc[cp], a->fc[1 - cp], a->macc, sp, p));
-    };
-    if ((e = near()) != cudaSuccess) return e;
-    if ((e = cudaEventRecord(a->join, a->side)) != cudaSuccess) return e;
-    return cudaStreamWaitEvent(st, a->join, 0);
-  }
+  StepParams sp = a->sp;
+  sp.write_mac = write_mac ? 1 : 0;
+  const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
   AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
-                                                                 a->d_block_slot, p.rb, p.nbx, p.nby, nullptr));
+                                                                 a->d_block_slot, p.rb, p.nbx, p.nby));
 }
 
 void destroy_graphs(lbm_amr3d *a) {
@@ -1449,13 +1392,12 @@ void release(lbm_amr3d *a) {
                     (void *)a->partials, (void *)a->force_out, (void *)a->tot_partials, (void *)a->tot_out,
                     (void *)a->counter, (void *)a->tot_counter, (void *)a->d_want, (void *)a->d_slot_new,
                     (void *)a->d_iface_flag, (void *)a->d_free_list, (void *)a->d_counts, (void *)a->flux,
-                    (void *)a->d_block_q, (void *)a->d_cells, (void *)a->d_links, (void *)a->d_pulls})
+                    (void *)a->d_block_q, (void *)a->d_cells, (void *)a->d_links, (void *)a->d_pulls,
+                    (void *)a->force_groups})
     if (!a->carved) cudaFree(ptr);
   if (a->host_out) cudaFreeHost(a->host_out);
   if (a->own) cudaStreamDestroy(a->own);
-  if (a->side) cudaStreamDestroy(a->side);
-  if (a->fork) cudaEventDestroy(a->fork);
-  if (a->join) cudaEventDestroy(a->join);
+
 }
 
 constexpr int kTotBlocks = 296;
@@ -1634,9 +1576,9 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     if ((e = mem.take(&a->d_pulls, (size_t)pull_words(a->q) * p.T3 * sizeof(uint32_t)))) return bail(e, "pull table");
     if (r.has_body && r.use_bounceback && (e = mem.take(&a->d_links, (size_t)p.P * sizeof(uint32_t))))
       return bail(e, "link table");
-    if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
     if (a->dynamic) {
       if ((e = mem.take(&a->d_want, nb))) return bail(e, "want");
+      if ((e = mem.take(&a->d_iface_flag, nb))) return bail(e, "flags");
       if ((e = mem.take(&a->d_slot_new, a->capacity))) return bail(e, "new");
       if ((e = mem.take(&a->d_free_list, nfl * sizeof(int)))) return bail(e, "free list");
       if ((e = mem.take(&a->d_counts, 4 * sizeof(int)))) return bail(e, "counts");
@@ -1646,6 +1588,8 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     a->force_parts = std::max(1, ((r3 + kTileThreads - 1) / kTileThreads) * p.slots);
     if ((e = mem.take(&a->partials, (size_t)a->force_parts * kForceSlots * sizeof(double)))) return bail(e, "partials");
     if ((e = mem.take(&a->force_out, kForceSlots * sizeof(double)))) return bail(e, "force");
+    if ((e = mem.take(&a->force_groups, (size_t)sum_groups(a->force_parts) * kForceSlots * sizeof(double))))
+      return bail(e, "force");
     if ((e = mem.take(&a->counter, sizeof(unsigned int)))) return bail(e, "counter");
     if ((e = mem.take(&a->tot_partials, (size_t)kTotBlocks * 4 * sizeof(double)))) return bail(e, "totals");
     if ((e = mem.take(&a->tot_out, 4 * sizeof(double)))) return bail(e, "totals");
@@ -1657,13 +1601,7 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     return LBM_OK;
   }
   if ((e = cudaStreamCreateWithFlags(&a->own, cudaStreamNonBlocking))) return bail(e, "stream");
-  if ((e = cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking))) return bail(e, "stream");
-  if ((e = cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming))) return bail(e, "event");
-  if ((e = cudaEventCreateWithFlags(&a->join, cudaEventDisableTiming))) return bail(e, "event");
-  {
-    int least = 0, greatest = 0;
-    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) a->prio_hi = greatest;
-  }
+
   a->stream = a->own;
   for (int k = 0; k < 2; ++k)
     if ((e = cudaMemsetAsync(a->fp[k], 0, fpb, a->own))) return bail(e, "memset pool f");
@@ -1686,14 +1624,10 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
     const std::vector<uint32_t> pt = pull_table(a->q, p.FB, p.RB2, cl);
     cudaMemcpyAsync(a->d_pulls, pt.data(), pt.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, a->own);
   }
-  {
-    // interface flags: covered blocks and the blocks touching one (the
-    // dynamic manager rewrites them with each decision)
+  if (a->dynamic) {
     std::vector<unsigned char> flag(nb, 0);
     for (int id : a->iface) flag[id] = 1;
     cudaMemcpyAsync(a->d_iface_flag, flag.data(), nb, cudaMemcpyHostToDevice, a->own);
-  }
-  if (a->dynamic) {
     std::vector<int> fl(nfl, 0);
     for (int i = 0; i < nfree; ++i) fl[i] = a->initial + i;
     const int counts[4] = {nfree, 0, nfree, 0};
