@@ -520,10 +520,9 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
   }
   __syncthreads();
   const int l = threadIdx.x / SUBS, sub = threadIdx.x % SUBS;
-  const int x = b[0] * p.rb + l % p.rb, y = b[1] * p.rb + (l / p.rb) % p.rb, z = b[2] * p.rb + l / (p.rb * p.rb);
-  const int cc[3] = {x, y, z};
-  const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
-  const int nbk[3] = {p.nbx, p.nby, p.nbz};
+  // the cell's position within its block, per axis
+  const int lc[3] = {l % p.rb, (l / p.rb) % p.rb, l / (p.rb * p.rb)};
+  const int x = b[0] * p.rb + lc[0], y = b[1] * p.rb + lc[1], z = b[2] * p.rb + lc[2];
   const int64_t cell = ccell(p, x, y, z);
   const int slot = nb27[13];
   if (slot < 0) {
@@ -538,31 +537,29 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
       const int e[3] = {dir[0][i], dir[1][i], dir[2][i]};
       const int tc[3] = {x + e[0], y + e[1], z + e[2]};
       if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
+      // Child o of the target tc = cell + e, per axis relative to block b
+      // (the neighbour table is b's): its fine source 2 l + e + o (one fine
+      // step upstream, from b's first fine cell) picks the source's block,
+      // the child's coordinate in that tile is the source's plus e, and
+      // the cell's own child o shifted by e lies in L0 cell l + (o + e) / 2
+      // (rounded down), covered or not.
       float sacc = 0.f, nin = 0.f;
       for (int q = 0; q < 8; ++q) {
-        const int o[3] = {q & 1, (q >> 1) & 1, (q >> 2) & 1};
-        int pp[3], qb[3], rel[3];
+        int ks = 0, kc = 0, loc[3];
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
-          // the child of the target and its fine source, one step upstream;
-          // the source's block relative to b from the unwrapped coordinate
-          const int ppu = 2 * tc[a] + o[a], qqu = ppu - e[a];
-          const int d = qqu - b[a] * p.RB2;
-          rel[a] = d < 0 ? -1 : (d >= p.RB2 ? 1 : 0);
-          pp[a] = wrapi(ppu, nf[a]);
-          qb[a] = wrapi(b[a] + rel[a], nbk[a]);
+          const int o = (q >> a) & 1, m = a == 0 ? 1 : (a == 1 ? 3 : 9);
+          const int d = 2 * lc[a] + e[a] + o;
+          const int rel = d < 0 ? -1 : (d >= p.RB2 ? 1 : 0);
+          ks += (rel + 1) * m;
+          loc[a] = d + e[a] - rel * p.RB2 + kAmrGhost;
+          const int r = lc[a] + ((o + e[a]) >> 1);
+          kc += (r < 0 ? 0 : (r >= p.rb ? 2 : 1)) * m;
         }
-        const int qs = nb27[(rel[2] + 1) * 9 + (rel[1] + 1) * 3 + (rel[0] + 1)];
-        if (qs >= 0) {
-          const int lx = local_in_tile(p, pp[0], qb[0], nf[0]), ly = local_in_tile(p, pp[1], qb[1], nf[1]),
-                    lz = local_in_tile(p, pp[2], qb[2], nf[2]);
-          sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)qs * p.T3 + (lz * p.FB + ly) * p.FB + lx);
-        }
-        int ch[3];
-        for (int a = 0; a < 3; ++a) {
-          const int chu = cc[a] * 2 + o[a] + e[a];
-          ch[a] = chu >= 0 ? chu / 2 : -((1 - chu) / 2);
-        }
-        if (covered_near(p, nb27, b, ch[0], ch[1], ch[2])) nin += 1.f;
+        const int qs = nb27[ks];
+        if (qs >= 0)
+          sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)qs * p.T3 + (loc[2] * p.FB + loc[1]) * p.FB + loc[0]);
+        if (nb27[kc] >= 0) nin += 1.f;
       }
       const float own = fc[(int64_t)i * p.N + cell];
       const float net = sacc - nin * own;
@@ -589,11 +586,11 @@ __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
                       SUBS == 1 ? L::ez(i) : dir[2][i]};
     const int tc[3] = {x + e[0], y + e[1], z + e[2]};
     if (covered_near(p, nb27, b, tc[0], tc[1], tc[2])) continue;
+    // the children of tc, in this tile's coordinates (tc is next to the block)
+    const int c0[3] = {2 * (lc[0] + e[0]) + kAmrGhost, 2 * (lc[1] + e[1]) + kAmrGhost, 2 * (lc[2] + e[2]) + kAmrGhost};
     float sacc = 0.f;
     for (int q = 0; q < 8; ++q) {
-      const int lx = local_in_tile(p, tc[0] * 2 + (q & 1), b[0], nf[0]);
-      const int ly = local_in_tile(p, tc[1] * 2 + ((q >> 1) & 1), b[1], nf[1]);
-      const int lz = local_in_tile(p, tc[2] * 2 + ((q >> 2) & 1), b[2], nf[2]);
+      const int lx = c0[0] + (q & 1), ly = c0[1] + ((q >> 1) & 1), lz = c0[2] + ((q >> 2) & 1);
       sacc += __ldg(fp + (int64_t)i * p.P + (int64_t)slot * p.T3 + (lz * p.FB + ly) * p.FB + lx);
     }
     fc[(int64_t)i * p.N + cell] = sacc * 0.125f;
