@@ -267,6 +267,10 @@ __global__ void __launch_bounds__(kListThreads)
 }
 
 // ---- explode ------------------------------------------------------------
+// Which of block b's 3 x 3 x 3 neighbours an L0 coordinate r (relative to
+// b's first cell, one axis) lies in: 0, 1 or 2.
+__device__ __forceinline__ int nb_side(int r, int rb) { return r < 0 ? 0 : (r >= rb ? 2 : 1); }
+
 template <int Q>
 __global__ void __launch_bounds__(kListThreads)
     amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p,
@@ -280,54 +284,64 @@ __global__ void __launch_bounds__(kListThreads)
   const int b[3] = {t.bx, t.by, t.bz};
   const int fi[3] = {t.fx, t.fy, t.fz};
   const int nf[3] = {2 * p.nx, 2 * p.ny, 2 * p.nz};
-  // g: the fine coordinate (wrapped), v: its L0 cell; vu the same unwrapped
-  int g[3], v[3], vu[3];
+  // Per axis: g the fine coordinate (wrapped), v its L0 cell; fr the fine
+  // coordinate from the block's first fine cell and rv = fr / 2 (rounded
+  // down) its L0 cell from the block's first L0 cell. side packs, for
+  // e = -1, 0, +1, the neighbour side (nb_side) of L0 cell rv + e (bits
+  // 2(e+1)) and of the L0 cell holding fine cell fr + e (bits 6 + 2(e+1)).
+  int g[3], v[3], side[3];
   for (int a = 0; a < 3; ++a) {
-    const int gu = b[a] * p.RB2 + fi[a] - kAmrGhost;
-    g[a] = wrapi(gu, nf[a]);
+    const int fr = fi[a] - kAmrGhost;
+    g[a] = wrapi(b[a] * p.RB2 + fr, nf[a]);
     v[a] = g[a] / 2;
-    vu[a] = gu >= 0 ? gu / 2 : -((1 - gu) / 2);
+    const int rv = fr >> 1;
+    side[a] = 0;
+    for (int k = 0; k < 3; ++k)
+      side[a] |= nb_side(rv + k - 1, p.rb) << (2 * k) | nb_side((fr + k - 1) >> 1, p.rb) << (6 + 2 * k);
   }
+  auto sd = [&](int a, int e) { return (side[a] >> (2 * (e + 1))) & 3; };
+  auto sf = [&](int a, int e) { return (side[a] >> (6 + 2 * (e + 1))) & 3; };
   // A ring cell inside a covered L0 cell is never read (DIRECT_GHOST).
-  if (covered_near(p, nb27, b, vu[0], vu[1], vu[2])) return;
-  const int64_t vc = ccell(p, v[0], v[1], v[2]);
+  if (nb27[sd(2, 0) * 9 + sd(1, 0) * 3 + sd(0, 0)] >= 0) return;
+  // L0 cells as 32-bit offsets (N < 2^31)
+  const int vc = (int)ccell(p, v[0], v[1], v[2]);
   bool ok[3];
-  int64_t vm[3], vp[3];
+  int vm[3], vp[3];
   for (int a = 0; a < 3; ++a) {
-    int m[3] = {vu[0], vu[1], vu[2]}, q[3] = {vu[0], vu[1], vu[2]};
+    int k0[3] = {sd(0, 0), sd(1, 0), sd(2, 0)}, k1[3] = {sd(0, 0), sd(1, 0), sd(2, 0)};
+    k0[a] = sd(a, -1);
+    k1[a] = sd(a, 1);
+    ok[a] = nb27[k0[2] * 9 + k0[1] * 3 + k0[0]] < 0 && nb27[k1[2] * 9 + k1[1] * 3 + k1[0]] < 0;
+    int m[3] = {v[0], v[1], v[2]}, q[3] = {v[0], v[1], v[2]};
     m[a] -= 1;
     q[a] += 1;
-    ok[a] = !covered_near(p, nb27, b, m[0], m[1], m[2]) && !covered_near(p, nb27, b, q[0], q[1], q[2]);
-    vm[a] = ccell(p, m[0], m[1], m[2]);
-    vp[a] = ccell(p, q[0], q[1], q[2]);
+    vm[a] = (int)ccell(p, m[0], m[1], m[2]);
+    vp[a] = (int)ccell(p, q[0], q[1], q[2]);
   }
   float d[3];
   for (int a = 0; a < 3; ++a) d[a] = ((float)(g[a] - 2 * v[a]) - 0.5f) * 0.5f;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     const int e[3] = {L::ex(i), L::ey(i), L::ez(i)};
+    const float *plane = fc + (int64_t)i * p.N;
     float out;
-    if (!covered_near(p, nb27, b, vu[0] + e[0], vu[1] + e[1], vu[2] + e[2])) {
+    if (nb27[sd(2, e[2]) * 9 + sd(1, e[1]) * 3 + sd(0, e[0])] < 0) {
       // in-orphan: this child's own one-step destination is in this tile
-      int dg[3], dv[3];
-      for (int a = 0; a < 3; ++a) {
-        dg[a] = wrapi(g[a] + e[a], nf[a]);
-        const int du = b[a] * p.RB2 + fi[a] - kAmrGhost + e[a];
-        dv[a] = du >= 0 ? du / 2 : -((1 - du) / 2);
-      }
-      // dg / RB2 == b, as a range test on the wrapped (non-negative) dg
+      // (its L0 cell covered, and the wrapped fine cell in this block)
       bool own = true;
-      for (int a = 0; a < 3; ++a) own = own && dg[a] >= b[a] * p.RB2 && dg[a] < (b[a] + 1) * p.RB2;
-      const bool into = covered_near(p, nb27, b, dv[0], dv[1], dv[2]) && own;
-      out = into ? __ldg(fc + (int64_t)i * p.N + vc) : 0.f;
+      for (int a = 0; a < 3; ++a) {
+        const int dg = wrapi(g[a] + e[a], nf[a]);
+        own = own && dg >= b[a] * p.RB2 && dg < (b[a] + 1) * p.RB2;
+      }
+      const bool into = nb27[sf(2, e[2]) * 9 + sf(1, e[1]) * 3 + sf(0, e[0])] >= 0 && own;
+      out = into ? __ldg(plane + vc) : 0.f;
     } else {
-      const float f = __ldg(fc + (int64_t)i * p.N + vc);
+      const float f = __ldg(plane + vc);
       if (!p.linear) {
         out = f;
       } else {
         float G[3];
-        for (int a = 0; a < 3; ++a)
-          G[a] = ok[a] ? 0.5f * (__ldg(fc + (int64_t)i * p.N + vp[a]) - __ldg(fc + (int64_t)i * p.N + vm[a])) : 0.f;
+        for (int a = 0; a < 3; ++a) G[a] = ok[a] ? 0.5f * (__ldg(plane + vp[a]) - __ldg(plane + vm[a])) : 0.f;
         // projected orthogonal to e_i, so the two substeps see one state
         const float ee = (float)(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
         const float gd = (G[0] * (float)e[0] + G[1] * (float)e[1] + G[2] * (float)e[2]) / ee;
@@ -1510,6 +1524,12 @@ int amr3_create_impl(const lbm_amr3d_config *c, const uint8_t *block_want, DevCa
   a->slot_to_block.resize(a->capacity, -1);
   p.slots = a->capacity;
   p.P = (int64_t)a->capacity * p.T3;
+  if (p.N > INT32_MAX) {
+    // L0 cells are addressed with 32-bit offsets (2^31 cells of Q >= 19
+    // populations would be 150+ GB per buffer)
+    delete a;
+    return afail(nullptr, LBM_ENOMEM, "L0 grid of more than 2^31 cells");
+  }
   if (p.P > INT32_MAX) {
     // the substep addresses pool cells with 32-bit offsets (2^31 cells of
     // Q >= 19 populations would be 150+ GB per buffer)
