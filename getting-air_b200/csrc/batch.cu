@@ -36,14 +36,17 @@ namespace {
 
 // Register budget for 768 resident threads per SM (85 per thread): the
 // loop over a tile's cells is latency-bound, and occupancy is what hides it.
+// The CTA's share of the tiles: positions k0 .. k1-1 of `order` (tile
+// indices; the identity when NULL), round-robin over the grid.
 template <int Q, typename S, int THREADS>
 __global__ void __launch_bounds__(THREADS, 768 / THREADS)
     batch_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
-               const StepParams *__restrict__ doms, const int2 *__restrict__ tiles, int ntiles,
-               int cells_per_tile, int write_mac) {
+               const StepParams *__restrict__ doms, const int2 *__restrict__ tiles, const int *__restrict__ order,
+               int k0, int k1, int cells_per_tile, int write_mac) {
   __shared__ __align__(16) unsigned char sp_raw[sizeof(StepParams)];
   StepParams &sp = *reinterpret_cast<StepParams *>(sp_raw);
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (int k = k0 + (int)blockIdx.x; k < k1; k += gridDim.x) {
+    const int t = order ? __ldg(order + k) : k;
     const int2 td = __ldg(&tiles[t]);
     const int *src = reinterpret_cast<const int *>(doms + td.x);
     int *dst = reinterpret_cast<int *>(sp_raw);
@@ -91,27 +94,126 @@ __global__ void __launch_bounds__(THREADS, 768 / THREADS)
   }
 }
 
+// One D2Q9 cell of a domain with no body and outside any force region:
+// cell2_core with the tests that cannot fire taken out (no solid link,
+// chi = 0 and u_s = 0, so the Guo force is the body force) and only the
+// moving-wall patch of a wall row kept, the same arithmetic in the same
+// order, so the same bits.
+template <typename S>
+__device__ __forceinline__ void cell2_fluid(const S *__restrict__ fin, float (&f)[9], S *__restrict__ fout,
+                                            float *__restrict__ mac, const StepParams &p, int x, int y) {
+  using L = Lattice<9>;
+  const int W = p.nx, H = p.ny;
+  const int cell = y * W + x;
+  if (p.wall_y && (y == 0 || y == H - 1)) {
+    const S *fi = fin + p.base;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const int ex = L::ex(i), ey = L::ey(i), o = L::opp(i);
+      const int ysrc = y - ey;
+      if (ysrc < 0 || ysrc >= H) {
+        const float wu = ysrc < 0 ? p.wall_u0 : p.wall_u1;
+        const float corr = 2.f * L::w(i) * (float)ex * wu * kInvCS2;
+        f[i] = Codec<S>::ld(fi + (int64_t)o * p.n + cell, o, p.pk) + corr;
+      }
+    }
+  }
+  float rho, mxs, mys, mzs;
+  moments<L, 9>(f, rho, mxs, mys, mzs);
+  const float rhoDen = fmaxf(rho, 1e-6f);
+  const float inv = 1.0f / rhoDen;
+  const float uxs = mxs * inv, uys = mys * inv;
+  const float chi = 0.f, usx = 0.f, usy = 0.f;
+  const float Fx = rho * chi * (usx - uxs) + p.fx;
+  const float Fy = rho * chi * (usy - uys) + p.fy;
+  const float hinv = 0.5f * inv;
+  const float ux = fmaf(Fx, hinv, uxs);
+  const float uy = fmaf(Fy, hinv, uys);
+  float spw = 0.f;
+  if (p.sponge_w > 0.f) {
+    const float dx = fminf((float)x, (float)(W - 1 - x));
+    const float dy = fminf((float)y, (float)(H - 1 - y));
+    spw = sponge_weight_inv(fminf(dx, dy), p.sponge_inv);
+  }
+  MemSink<S> sink{fout + p.base, p.n, cell, p.pk};
+  collide_store<L, 9>(f, rho, ux, uy, 0.f, Fx, Fy, 0.f, p.omega, spw, p.ftarget, sink);
+  if (p.write_mac) reinterpret_cast<float4 *>(mac + 4 * p.base)[cell] = make_float4(rho, ux, uy, 0.f);
+}
+
+// The fluid tiles of a D2Q9 batch (cell2_fluid). Without the bounce-back
+// and force code the update fits 64 registers, and 1024 resident
+// threads per SM keep more loads in flight: the loop is memory-latency
+// bound (measured on B200 for the 512-domain workload: 0.53 ms per step
+// with every tile on the general kernel, 0.48 ms with the lean one).
+// (16-bit storage decodes and encodes each population: it keeps 80
+// registers, 768 threads per SM, where 64 would spill.)
+template <typename S, int THREADS>
+__global__ void __launch_bounds__(THREADS, (sizeof(S) == 4 ? 1024 : 768) / THREADS)
+    batch_step_fluid2(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
+                      const StepParams *__restrict__ doms, const int2 *__restrict__ tiles,
+                      const int *__restrict__ order, int k0, int k1, int cells_per_tile, int write_mac) {
+  __shared__ __align__(16) unsigned char sp_raw[sizeof(StepParams)];
+  StepParams &sp = *reinterpret_cast<StepParams *>(sp_raw);
+  for (int k = k0 + (int)blockIdx.x; k < k1; k += gridDim.x) {
+    const int2 td = __ldg(&tiles[__ldg(order + k)]);
+    const int *src = reinterpret_cast<const int *>(doms + td.x);
+    int *dst = reinterpret_cast<int *>(sp_raw);
+    for (int j = threadIdx.x; j < (int)(sizeof(StepParams) / 4); j += THREADS) dst[j] = __ldg(src + j);
+    __syncthreads();
+    if (threadIdx.x == 0) sp.write_mac = write_mac;
+    __syncthreads();
+    const int nx = sp.nx;
+    const int end = min(td.y + cells_per_tile, nx * sp.ny);
+    // two cells per pass, both gathers issued before either update
+    for (int c = td.y + threadIdx.x; c < end; c += 2 * THREADS) {
+      const int c2 = c + THREADS;
+      const bool two = c2 < end;
+      const int x = c % nx, r = c / nx;
+      const int x2 = two ? c2 % nx : 0, r2 = two ? c2 / nx : 0;
+      float f[9], g[9];
+      gather2<S>(fin + sp.base, sp, x, r, f);
+      if (two) gather2<S>(fin + sp.base, sp, x2, r2, g);
+      cell2_fluid<S>(fin, f, fout, mac, sp, x, r);
+      if (two) cell2_fluid<S>(fin, g, fout, mac, sp, x2, r2);
+    }
+    __syncthreads();
+  }
+}
+
 using BatchFn = void (*)(const void *, void *, float *, const StepParams *, const int2 *, int, int, int);
 
 template <int Q, typename S, int T>
 void launch_batch(dim3 g, cudaStream_t st, const void *fin, void *fout, float *mac, const StepParams *d,
-                  const int2 *tiles, int nt, int cpt, int wm) {
-  batch_step<Q, S, T><<<g, T, 0, st>>>((const S *)fin, (S *)fout, mac, d, tiles, nt, cpt, wm);
+                  const int2 *tiles, const int *order, int k0, int k1, int cpt, int wm, bool fluid) {
+  if constexpr (Q == 9) {
+    if (fluid) {
+      batch_step_fluid2<S, T><<<g, T, 0, st>>>((const S *)fin, (S *)fout, mac, d, tiles, order, k0, k1, cpt, wm);
+      return;
+    }
+  }
+  batch_step<Q, S, T><<<g, T, 0, st>>>((const S *)fin, (S *)fout, mac, d, tiles, order, k0, k1, cpt, wm);
 }
 
 template <int T>
 cudaError_t launch_any(int q, int storage, dim3 g, cudaStream_t st, const void *fin, void *fout, float *mac,
-                       const StepParams *d, const int2 *tiles, int nt, int cpt, int wm) {
+                       const StepParams *d, const int2 *tiles, const int *order, int k0, int k1, int cpt, int wm,
+                       bool fluid) {
   switch (q * 4 + storage) {
-    case 9 * 4 + 0: launch_batch<9, float, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 9 * 4 + 1: launch_batch<9, __half, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 9 * 4 + 2: launch_batch<9, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 19 * 4 + 0: launch_batch<19, float, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 19 * 4 + 1: launch_batch<19, __half, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 19 * 4 + 2: launch_batch<19, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 27 * 4 + 0: launch_batch<27, float, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 27 * 4 + 1: launch_batch<27, __half, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
-    case 27 * 4 + 2: launch_batch<27, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, nt, cpt, wm); break;
+    case 9 * 4 + 0: launch_batch<9, float, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, fluid); break;
+    case 9 * 4 + 1: launch_batch<9, __half, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, fluid); break;
+    case 9 * 4 + 2:
+      launch_batch<9, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, fluid);
+      break;
+    case 19 * 4 + 0: launch_batch<19, float, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false); break;
+    case 19 * 4 + 1: launch_batch<19, __half, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false); break;
+    case 19 * 4 + 2:
+      launch_batch<19, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false);
+      break;
+    case 27 * 4 + 0: launch_batch<27, float, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false); break;
+    case 27 * 4 + 1: launch_batch<27, __half, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false); break;
+    case 27 * 4 + 2:
+      launch_batch<27, __nv_bfloat16, T>(g, st, fin, fout, mac, d, tiles, order, k0, k1, cpt, wm, false);
+      break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -119,14 +221,19 @@ cudaError_t launch_any(int q, int storage, dim3 g, cudaStream_t st, const void *
 
 }  // namespace
 
+// One launch over tile positions k0 .. k1-1 of `order`; `fluid` picks the
+// lean D2Q9 kernel for tiles the host classified as fluid.
 cudaError_t launch_batch_step(int q, int storage, int threads, int ctas, cudaStream_t st, const void *fin,
-                              void *fout, float *mac, const StepParams *doms, const int2 *tiles, int ntiles,
-                              int cells_per_tile, int write_mac) {
+                              void *fout, float *mac, const StepParams *doms, const int2 *tiles, const int *order,
+                              int k0, int k1, int cells_per_tile, int write_mac, bool fluid) {
   dim3 g(ctas);
+  if (k1 <= k0) return cudaSuccess;
   if (threads == 128)
-    return launch_any<128>(q, storage, g, st, fin, fout, mac, doms, tiles, ntiles, cells_per_tile, write_mac);
+    return launch_any<128>(q, storage, g, st, fin, fout, mac, doms, tiles, order, k0, k1, cells_per_tile, write_mac,
+                           fluid);
   if (threads == 256)
-    return launch_any<256>(q, storage, g, st, fin, fout, mac, doms, tiles, ntiles, cells_per_tile, write_mac);
+    return launch_any<256>(q, storage, g, st, fin, fout, mac, doms, tiles, order, k0, k1, cells_per_tile, write_mac,
+                           fluid);
   return cudaErrorInvalidValue;
 }
 
@@ -149,6 +256,8 @@ struct lbm_batch {
   std::vector<StepParams> h_doms;
   int2 *d_tiles = nullptr;
   int ntiles = 0;
+  int *d_order = nullptr;        // tile indices: the general tiles, then the fluid ones
+  int ngeneral = 0;
   double *partials = nullptr;
   int64_t npartials = 0;
   unsigned int *counters = nullptr;
@@ -218,6 +327,19 @@ int retile(lbm_batch *b) {
     }
   }
   if (tiles.size() > 0x7fffffff) return bfail(b, LBM_EINVAL, "too many tiles");
+  // D2Q9 tiles that need none of the bounce-back and force code run the
+  // lean kernel: no body, no force region (walls it handles).
+  std::vector<int> general, fluid;
+  for (int t = 0; t < (int)tiles.size(); ++t) {
+    const StepParams &p = b->h_doms[tiles[t].x];
+    (b->q == 9 && !p.has_body && !p.force_on ? fluid : general).push_back(t);
+  }
+  b->ngeneral = (int)general.size();
+  general.insert(general.end(), fluid.begin(), fluid.end());
+  cudaFree(b->d_order);
+  b->d_order = nullptr;
+  BCK(b, cudaMalloc(&b->d_order, general.size() * sizeof(int)));
+  BCK(b, cudaMemcpy(b->d_order, general.data(), general.size() * sizeof(int), cudaMemcpyHostToDevice));
   cudaFree(b->d_tiles);
   b->d_tiles = nullptr;
   BCK(b, cudaMalloc(&b->d_tiles, tiles.size() * sizeof(int2)));
@@ -239,10 +361,15 @@ int retile(lbm_batch *b) {
   return LBM_OK;
 }
 
+// A step: the general tiles, then the fluid ones (their cells are disjoint;
+// both read the step's input buffer and write its output).
 cudaError_t one_step(lbm_batch *b, cudaStream_t st, int from, int write_mac) {
-  return launch_batch_step(b->q, b->storage, b->threads, b->ctas_per_sm * b->sms, st, b->f[from],
-                           b->f[1 - from], b->mac, b->d_doms, b->d_tiles, b->ntiles, b->threads * b->cpt,
-                           write_mac);
+  const int ctas = b->ctas_per_sm * b->sms, cpt = b->threads * b->cpt;
+  cudaError_t e = launch_batch_step(b->q, b->storage, b->threads, ctas, st, b->f[from], b->f[1 - from], b->mac,
+                                    b->d_doms, b->d_tiles, b->d_order, 0, b->ngeneral, cpt, write_mac, false);
+  if (e != cudaSuccess) return e;
+  return launch_batch_step(b->q, b->storage, b->threads, ctas, st, b->f[from], b->f[1 - from], b->mac, b->d_doms,
+                           b->d_tiles, b->d_order, b->ngeneral, b->ntiles, cpt, write_mac, true);
 }
 
 int build_graph(lbm_batch *b, int from) {
@@ -270,6 +397,7 @@ void release_batch(lbm_batch *b) {
   cudaFree(b->mac);
   cudaFree(b->d_doms);
   cudaFree(b->d_tiles);
+  cudaFree(b->d_order);
   cudaFree(b->partials);
   cudaFree(b->counters);
   cudaFree(b->force_out);

@@ -155,9 +155,10 @@ int totals_blocks();
 cudaError_t launch_totals(int q, int storage, const void *f, int64_t n, const Pack &pk, double *partials,
                           unsigned int *counter, double *out, cudaStream_t st, int64_t stride = 0);
 
-// One step of every domain of a batch (batch.cu).
+// One launch of a batch step over tile positions k0 .. k1-1 of `order`
+// (batch.cu); `fluid` selects the lean D2Q9 kernel.
 cudaError_t launch_batch_step(int q, int storage, int threads, int ctas, cudaStream_t st, const void *fin,
-                              void *fout, float *mac, const StepParams *doms, const int2 *tiles, int ntiles,
-                              int cells_per_tile, int write_mac);
+                              void *fout, float *mac, const StepParams *doms, const int2 *tiles, const int *order,
+                              int k0, int k1, int cells_per_tile, int write_mac, bool fluid);
 
 }  // namespace lbm

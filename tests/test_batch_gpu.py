@@ -100,3 +100,29 @@ def test_batch_packed_storage_matches_dense(lbm, oracle):
     for (f, m), (wf_, wm) in zip(got, want):
         assert np.array_equal(f, wf_)
 
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+def test_batch_d2q9_general_and_lean_tiles_equal_dense(lbm, oracle, storage):
+    """A D2Q9 batch whose tiles split between the two kernels of a step: a
+    cylinder (bounce-back body, sponge, force region: the general kernel)
+    beside a Couette channel with moving walls, a forced channel and a
+    periodic domain in uniform flow (the lean kernel). Each domain's
+    populations and mac equal the same domain stepped alone as a dense
+    session, to the bit, in every storage; the cylinder's force is the same
+    FP64 sum over a different partition of the same cell contributions."""
+    from getting_air_b200 import scenarios as sc
+    cyl = sc.cylinder2d(W=96, H=48, r=6.0)
+    doms = [((96, 48, 1), dict(cyl["kw"]), cyl["mac"]),
+            ((64, 40, 1), dict(tau=0.7, sponge_w=0.0, wall=(0, 1, 0), wall_u=(0.03, -0.02)),
+             sc.uniform_macro(64 * 40)),
+            ((80, 72, 1), dict(tau=0.62, sponge_w=0.0, wall=(0, 1, 0), force=(2e-6, 0.0, 0.0)),
+             sc.uniform_macro(80 * 72)),
+            ((48, 48, 1), dict(tau=0.8, sponge_w=0.0), sc.uniform_macro(48 * 48, (0.02, -0.01, 0.0)))]
+    doms = [(d, dict(kw, storage=storage), m) for d, kw, m in doms]
+    got, want, gf, wf = run_pair(lbm, oracle, 9, doms, 12)
+    for (f, m), (wf_, wm) in zip(got, want):
+        assert np.array_equal(f, wf_)
+        assert np.array_equal(m, wm)
+    assert np.allclose(gf, wf, rtol=1e-10, atol=1e-12 * np.abs(wf).max())
+    assert abs(wf[0][0]) > 0
