@@ -20,7 +20,7 @@ Bounds. FP32 storage computes in f32 with FMAs against the oracle's f64:
 1e-5 in velocity. The 16-bit storages round every population to the
 format's quantum of its deviation from the far-field equilibrium each
 step: FP16 (11 significand bits at scale 2^10) and BF16 (8 bits). Their
-velocity bound is the north star's 1e-3. The drag after 100 steps from an
+velocity bound is 1e-3, the accuracy the packed forms are held to. The drag after 100 steps from an
 impulsive start is a transient sum with heavy cancellation; measured on
 B200: FP32 1.3e-4, FP16 7.9e-4, BF16 2.5e-3 relative (velocity 3.6e-6,
 5.4e-5, 2.3e-4), so the drag bounds below are 1e-3, 1e-2 and 2e-2.

@@ -291,7 +291,7 @@ def test_packed_storage_error_is_bounded(lbm, oracle, storage):
     """16-bit storage holds (f - feq(1, U_far)) * scale: the round trip is
     within the 16-bit quantum of that deviation, and the velocity after 200
     steps stays within the stated bound of the FP64 oracle (1e-4 for FP16,
-    1e-3 for BF16; north_star asks for 1e-3)."""
+    1e-3 for BF16, the packed forms' accuracy target)."""
     from getting_air_b200 import scenarios as sc
     s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40, storage=storage)
     f0 = oracle.init_eq(19, s["mac"], fp32=True).astype(np.float32)
