@@ -597,12 +597,32 @@ int lbm_forces(lbm_session *s, double out[6]) {
   return LBM_OK;
 }
 
+namespace {
+// Six doubles from device memory into pinned host memory the device can
+// address: a one-warp kernel on the stream instead of a copy-engine
+// transfer, whose start and finish between two kernels cost the stream
+// several microseconds (measured on B200 in a loop of one-step calls, each
+// followed by the force readback: 0.135 ms per step with the copy).
+__global__ void copy_force_to_host(const double *__restrict__ src, double *dst) {
+  if (threadIdx.x < 6) dst[threadIdx.x] = src[threadIdx.x];
+}
+}  // namespace
+
 int lbm_forces_async(lbm_session *s, double out[6]) {
   if (!s || !out) return s ? fail(s, LBM_EINVAL, "out is NULL") : LBM_EINVAL;
   if (!s->sp.force_on && !s->free_body) {
     for (int k = 0; k < 6; ++k) out[k] = 0.0;
     return LBM_OK;
   }
+  // Pinned (page-locked) host memory has a device address under unified
+  // addressing; anything else goes through the copy engine as before.
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeHost && at.devicePointer) {
+    copy_force_to_host<<<1, 32, 0, s->stream>>>(s->force_out, (double *)at.devicePointer);
+    CK(s, cudaGetLastError());
+    return LBM_OK;
+  }
+  cudaGetLastError();  // a pageable pointer is no error here
   CK(s, cudaMemcpyAsync(out, s->force_out, 6 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   return LBM_OK;
 }

@@ -274,7 +274,9 @@ int lbm_forces(lbm_session *s, double out[6]);
  * host memory `out` (pinned for a true asynchronous copy) on the session
  * stream and returns without waiting: a caller can record every step's force
  * while the device keeps stepping, then lbm_sync() once. The buffer must
- * stay valid until that sync. */
+ * stay valid until that sync. Pinned memory is written by a small kernel
+ * on the stream (no copy-engine transfer between two steps); pageable
+ * memory by cudaMemcpyAsync. */
 int lbm_forces_async(lbm_session *s, double out[6]);
 
 /* Conserved totals over the current f, FP64 on the device:

@@ -183,19 +183,35 @@ def test_totals_match_oracle(lbm, oracle, q):
 
 
 def test_forces_async_matches_sync(lbm, oracle):
+    # Pinned memory takes the kernel copy, pageable memory the copy engine;
+    # every entry equals the force read synchronously after the same step.
     import torch
     from getting_air_b200 import scenarios as sc
     s = sc.sphere(n=8, dims=(48, 32, 32), u0=0.05, re=40)
-    sol = lbm.Solver.create(19, s["dims"], **s["kw"])
-    sol.init_macro(s["mac"])
-    hist = torch.zeros((5, 6), dtype=torch.float64).pin_memory()
-    for k in range(5):
-        sol.step(1)
-        sol.forces_async(hist[k].data_ptr())
-    sol.sync()
-    assert np.array_equal(hist[4].numpy(), sol.forces())
-    assert not np.array_equal(hist[0].numpy(), hist[4].numpy())
-    sol.close()
+    runs = {}
+    for kind in ("pinned", "pageable", "sync"):
+        sol = lbm.Solver.create(19, s["dims"], **s["kw"])
+        sol.init_macro(s["mac"])
+        if kind == "pinned":
+            t = torch.zeros((5, 6), dtype=torch.float64).pin_memory()
+            hist, ptr = t.numpy(), lambda k: t[k].data_ptr()
+        else:
+            hist = np.zeros((5, 6))
+            ptr = lambda k: hist[k].ctypes.data
+        for k in range(5):
+            sol.step(1)
+            if kind == "sync":
+                hist[k] = sol.forces()
+            else:
+                sol.forces_async(ptr(k))
+        sol.sync()
+        if kind == "pinned":
+            assert np.array_equal(hist[4], sol.forces())
+        runs[kind] = hist.copy()
+        sol.close()
+    assert np.array_equal(runs["pinned"], runs["sync"])
+    assert np.array_equal(runs["pageable"], runs["sync"])
+    assert not np.array_equal(runs["sync"][0], runs["sync"][4])
 
 
 def test_totals_count_nonfinite_cells(lbm, oracle):
