@@ -35,6 +35,7 @@
 // and +7 % of the step against no force at all, and +1 % for this form).
 
 #include <type_traits>
+#include <utility>
 
 #include "cell_update.cuh"
 
@@ -153,6 +154,7 @@ template <int Q, typename S, bool TRT>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     d3_step(const S *__restrict__ fin, S *__restrict__ fout, float *__restrict__ mac,
             const __grid_constant__ StepParams p) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   d3_step_block<Q, S, TRT>(fin, fout, mac, p);
 }
 
@@ -239,6 +241,7 @@ __global__ void __launch_bounds__(kStepThreads)
 __global__ void __launch_bounds__(kStepThreads)
     force_finish(const double *__restrict__ partials, int nparts, double *__restrict__ groups,
                  unsigned int *__restrict__ counter, double *__restrict__ out) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   sum_partials_grouped<kStepThreads>(partials, nparts, groups, counter, out, blockIdx.x);
 }
 
@@ -392,6 +395,26 @@ int grid_for(int64_t n, int threads) {
 }  // namespace
 
 namespace {
+// A launch that may begin while the previous kernel on the stream drains
+// (programmatic dependent launch): the step and force-sum kernels wait at
+// their first instruction (griddepcontrol.wait) until that kernel has
+// completed and its writes are visible, so the order is the stream's; what
+// overlaps is the new grid's launch and scheduling with the old one's tail.
+// Measured on B200 for one-step calls: 0.124 -> 0.120 ms per step, and with
+// a force readback after each 0.129 -> 0.124 ms.
+template <typename... K, typename... A>
+void launch_pdl(dim3 g, dim3 b, cudaStream_t st, void (*k)(K...), A &&...args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = g;
+  lc.blockDim = b;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  cudaLaunchKernelEx(&lc, k, std::forward<A>(args)...);
+}
 cudaError_t launch_step_kernel(int q, int storage, const void *f_in, void *f_out, float *mac, const StepParams &p,
                                cudaStream_t st) {
   dim3 grid((p.nx + kStepThreads - 1) / kStepThreads, p.ny, q == 9 ? 1 : p.nz - 2 * p.zlo);
@@ -403,9 +426,9 @@ cudaError_t launch_step_kernel(int q, int storage, const void *f_in, void *f_out
     else if (p.pose_in)
       d3_step_free<Q, S, false><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
     else if (p.trt_dw != 0.f)
-      d3_step<Q, S, true><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+      launch_pdl(grid, dim3(kStepThreads), st, d3_step<Q, S, true>, (const S *)f_in, (S *)f_out, mac, p);
     else
-      d3_step<Q, S, false><<<grid, kStepThreads, 0, st>>>((const S *)f_in, (S *)f_out, mac, p);
+      launch_pdl(grid, dim3(kStepThreads), st, d3_step<Q, S, false>, (const S *)f_in, (S *)f_out, mac, p);
   });
 }
 }  // namespace
@@ -419,7 +442,8 @@ cudaError_t launch_step(int q, int storage, const void *f_in, void *f_out, float
   const cudaError_t e = launch_step_kernel(q, storage, f_in, f_out, mac, p, st);
   if (e != cudaSuccess || !p.force_on || p.defer_force) return e;
   const int parts = force_parts(q, p);
-  force_finish<<<sum_groups(parts), kStepThreads, 0, st>>>(p.partials, parts, p.groups, p.counter, p.force_out);
+  launch_pdl(dim3(sum_groups(parts)), dim3(kStepThreads), st, force_finish, (const double *)p.partials, parts,
+             p.groups, p.counter, p.force_out);
   return cudaGetLastError();
 }
 

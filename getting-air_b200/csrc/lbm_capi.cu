@@ -604,6 +604,7 @@ namespace {
 // several microseconds (measured on B200 in a loop of one-step calls, each
 // followed by the force readback: 0.135 ms per step with the copy).
 __global__ void copy_force_to_host(const double *__restrict__ src, double *dst) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   if (threadIdx.x < 6) dst[threadIdx.x] = src[threadIdx.x];
 }
 }  // namespace
@@ -618,7 +619,20 @@ int lbm_forces_async(lbm_session *s, double out[6]) {
   // addressing; anything else goes through the copy engine as before.
   cudaPointerAttributes at{};
   if (cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeHost && at.devicePointer) {
-    copy_force_to_host<<<1, 32, 0, s->stream>>>(s->force_out, (double *)at.devicePointer);
+    {
+      // launched like the step kernels (programmatic dependent launch); the
+      // kernel waits for the previous one before it reads the force
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3(1);
+      lc.blockDim = dim3(32);
+      lc.stream = s->stream;
+      cudaLaunchAttribute la[1];
+      la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      la[0].val.programmaticStreamSerializationAllowed = 1;
+      lc.attrs = la;
+      lc.numAttrs = 1;
+      cudaLaunchKernelEx(&lc, copy_force_to_host, (const double *)s->force_out, (double *)at.devicePointer);
+    }
     CK(s, cudaGetLastError());
     return LBM_OK;
   }
