@@ -26,6 +26,7 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -275,6 +276,7 @@ template <int Q>
 __global__ void __launch_bounds__(kListThreads)
     amr3_explode(const float *__restrict__ fc, float *__restrict__ fp, const __grid_constant__ Amr3Params p,
                  const uint32_t *__restrict__ cells, int first, int count) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   using L = Lattice<Q>;
   TileCell t;
   // the ring cells only; coverage of the L0 cells around the tile from the
@@ -482,6 +484,7 @@ template <int Q, bool W32>
 __global__ void __launch_bounds__(kListThreads, Q == 19 ? (W32 ? 9 : 8) : 6)
     amr3_substep(const float *__restrict__ fin, float *__restrict__ fout, float4 *__restrict__ macp,
                  const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells, int count) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   TileCell t;
   // the tile's 26 same-level neighbours as pool cell bases, once per CTA
   __shared__ int nbase[27];
@@ -518,6 +521,7 @@ template <int Q, int SUBS>
 __global__ void __launch_bounds__(kMaxAmrRb * kMaxAmrRb * kMaxAmrRb)
     amr3_coalesce(const float *__restrict__ fp, float *__restrict__ fc, float4 *__restrict__ macc,
                   const float4 *__restrict__ macp, const __grid_constant__ Amr3Params p) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   using L = Lattice<Q>;
   const int id = p.iface ? p.iface[blockIdx.x] : (int)blockIdx.x;
   if (!p.iface && !p.iface_flag[id]) return;  // the whole CTA
@@ -735,6 +739,7 @@ template <int Q>
 __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) / 4 : kStepMinBlocks)
     amr3_coarse(const float *__restrict__ fin, float *__restrict__ fout, float *__restrict__ mac,
                 const __grid_constant__ StepParams sp, const int *__restrict__ block_slot, int rb, int nbx, int nby) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   const int x = blockIdx.x * kStepThreads + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
   if (x >= sp.nx) return;
   if (block_slot[((z / rb) * nby + y / rb) * nbx + x / rb] >= 0) return;
@@ -749,6 +754,7 @@ __global__ void __launch_bounds__(kStepThreads, Q == 27 ? (kStepMinBlocks * 3) /
 template <int Q>
 __global__ void __launch_bounds__(kTileThreads)
     amr3_force(const float *__restrict__ fp, const __grid_constant__ Amr3Params p, const uint32_t *__restrict__ cells) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   using L = Lattice<Q>;
   const StepParams &c = p.c;
   const int r3 = p.RB2 * p.RB2 * p.RB2;
@@ -853,6 +859,7 @@ __global__ void __launch_bounds__(kTileThreads)
 __global__ void __launch_bounds__(kSumGroup)
     amr3_force_sum(const double *__restrict__ partials, int nparts, double *__restrict__ groups,
                    unsigned int *__restrict__ counter, double *__restrict__ out) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // a no-op unless launched by launch_pdl
   sum_partials_grouped<kSumGroup>(partials, nparts, groups, counter, out, blockIdx.x);
 }
 
@@ -1245,15 +1252,34 @@ int coalesce_subs(const Amr3Params &p, int sms) {
   return subs;
 }
 
+// A launch that may begin while the previous kernel on the stream drains
+// (programmatic dependent launch; in a graph, a programmatic edge): the
+// macro-step's kernels wait at their first instruction (griddepcontrol.wait)
+// until the previous one has completed and its writes are visible, so the
+// order is the stream's; the new grid's launch overlaps the old one's tail.
+template <typename... K, typename... A>
+void launch_pdl(dim3 g, dim3 b, cudaStream_t st, void (*k)(K...), A &&...args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = g;
+  lc.blockDim = b;
+  lc.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  cudaLaunchKernelEx(&lc, k, std::forward<A>(args)...);
+}
+
 template <int Q>
 void launch_coalesce(cudaStream_t st, const float *fp, float *fc, float4 *macc, const float4 *macp,
                      const Amr3Params &p, int subs) {
   const int t = p.rb * p.rb * p.rb * subs;
   switch (subs) {
-    case 8: amr3_coalesce<Q, 8><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
-    case 4: amr3_coalesce<Q, 4><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
-    case 2: amr3_coalesce<Q, 2><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
-    default: amr3_coalesce<Q, 1><<<p.n_iface, t, 0, st>>>(fp, fc, macc, macp, p); break;
+    case 8: launch_pdl(dim3(p.n_iface), dim3(t), st, amr3_coalesce<Q, 8>, fp, fc, macc, macp, p); break;
+    case 4: launch_pdl(dim3(p.n_iface), dim3(t), st, amr3_coalesce<Q, 4>, fp, fc, macc, macp, p); break;
+    case 2: launch_pdl(dim3(p.n_iface), dim3(t), st, amr3_coalesce<Q, 2>, fp, fc, macc, macp, p); break;
+    default: launch_pdl(dim3(p.n_iface), dim3(t), st, amr3_coalesce<Q, 1>, fp, fc, macc, macp, p); break;
   }
 }
 
@@ -1262,9 +1288,9 @@ template <int Q>
 void launch_substep(dim3 gl, cudaStream_t st, const float *fin, float *fout, float4 *macp, const Amr3Params &p,
                     const uint32_t *cells) {
   if ((int64_t)Q * p.P <= INT32_MAX)
-    amr3_substep<Q, true><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+    launch_pdl(gl, dim3(kListThreads), st, amr3_substep<Q, true>, fin, fout, macp, p, cells, p.T3);
   else
-    amr3_substep<Q, false><<<gl, kListThreads, 0, st>>>(fin, fout, macp, p, cells, p.T3);
+    launch_pdl(gl, dim3(kListThreads), st, amr3_substep<Q, false>, fin, fout, macp, p, cells, p.T3);
 }
 
 // The pool force at time t and its deterministic sum.
@@ -1272,10 +1298,10 @@ template <int Q>
 void launch_pool_force(lbm_amr3d *a, const Amr3Params &p, cudaStream_t st) {
   const int r3 = p.RB2 * p.RB2 * p.RB2;
   const dim3 gf((r3 + kTileThreads - 1) / kTileThreads, p.slots);
-  amr3_force<Q><<<gf, kTileThreads, 0, st>>>(a->fp[0], p, a->d_cells);
+  launch_pdl(gf, dim3(kTileThreads), st, amr3_force<Q>, (const float *)a->fp[0], p, (const uint32_t *)a->d_cells);
   const int parts = gf.x * gf.y;
-  amr3_force_sum<<<sum_groups(parts), kSumGroup, 0, st>>>(a->partials, parts, a->force_groups, a->counter,
-                                                          a->force_out);
+  launch_pdl(dim3(sum_groups(parts)), dim3(kSumGroup), st, amr3_force_sum, (const double *)a->partials, parts,
+             a->force_groups, a->counter, a->force_out);
 }
 
 // One macro-step from L0 parity `cp`.
@@ -1325,7 +1351,8 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
         if (p.c.has_body) launch_pool_force<Q>(a, p, st);
         const int r3i = p.RB2 * p.RB2 * p.RB2, nring = p.T3 - r3i;
         const dim3 gr((nring + kListThreads - 1) / kListThreads, p.slots);
-        amr3_explode<Q><<<gr, kListThreads, 0, st>>>(a->fc[cp], a->fp[0], p, a->d_cells, r3i, nring);
+        launch_pdl(gr, dim3(kListThreads), st, amr3_explode<Q>, (const float *)a->fc[cp], a->fp[0], p,
+                   (const uint32_t *)a->d_cells, r3i, nring);
         Amr3Params pa = p;
         pa.write_mac = 0;
         launch_substep<Q>(gl, st, a->fp[0], a->fp[1], a->macp, pa, a->d_cells);
@@ -1340,8 +1367,8 @@ cudaError_t launch_macro(lbm_amr3d *a, int cp, bool write_mac) {
   StepParams sp = a->sp;
   sp.write_mac = write_mac ? 1 : 0;
   const dim3 gs((p.nx + kStepThreads - 1) / kStepThreads, p.ny, p.nz);
-  AMR3_DISPATCH(q, amr3_coarse<Q><<<gs, kStepThreads, 0, st>>>(a->fc[cp], a->fc[1 - cp], a->macc, sp,
-                                                                 a->d_block_slot, p.rb, p.nbx, p.nby));
+  AMR3_DISPATCH(q, launch_pdl(gs, dim3(kStepThreads), st, amr3_coarse<Q>, (const float *)a->fc[cp], a->fc[1 - cp],
+                              a->macc, sp, (const int *)a->d_block_slot, p.rb, p.nbx, p.nby));
 }
 
 void destroy_graphs(lbm_amr3d *a) {
