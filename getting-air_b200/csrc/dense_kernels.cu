@@ -110,7 +110,8 @@ __device__ __forceinline__ void d3_step_block(const S *__restrict__ fin, S *__re
   // The fluid path pays for 16-bit storage (issue-bound: 0.1106 against
   // 0.1167 ms per step on the 256x128x128 sphere) but not for FP32, whose
   // step is bound by memory latency and ran 0.1123 against 0.1110 ms with
-  // it: FP32 takes the general path everywhere.
+  // it (D3Q27: 0.1589 against 0.1537 ms): FP32 takes the general path
+  // everywhere.
   const int lo = bx * kStepThreads, hi = min(lo + kStepThreads, p.nx) - 1;
   const int kind = std::is_same<S, float>::value ? kGeneral : block_kind(p, lo, hi, by, zg, region);
   if (kind == kFluid) {
