@@ -521,3 +521,38 @@ def test_no_link_table_without_bounce_back(lbm):
     a.set_links(True)
     assert not a.links
     a.close()
+
+
+@pytest.mark.parametrize("dims,radius", [((80, 80, 80), 12.0), ((96, 96, 96), 18.0)])
+def test_amr3d_mid_size_hierarchies_match_oracle(lbm, oracle, dims, radius):
+    """Hierarchies of a few hundred tiles (730 and 1509 interface blocks):
+    on a 148-SM device the coalesce runs 4 and 2 threads per L0 cell here,
+    against 8 on the small grids above and 1 on the largest served
+    requests. L0, the tiles and the force against the FP64 oracle after 4
+    macro-steps, to the same tolerances as the small grids."""
+    kw = dict(tau=0.6, has_body=1, use_bounceback=1, sponge_w=4.0, sponge_u=(0.04, 0.0, 0.0),
+              body=dict(shape="sphere", centre=(dims[0] / 2 + 0.3, dims[1] / 2 - 0.2, dims[2] / 2 + 0.1),
+                        a=radius))
+    c = lbm.amr3d_config(19, dims, refine="body", margin=2.0, **kw)
+    n = int(np.prod(dims))
+    mac = np.zeros((n, 4), np.float32)
+    mac[:, 0] = 1.0
+    mac[:, 1] = 0.04
+    a = lbm.Amr3D(c)
+    o = oracle.Amr3D(c)
+    assert a.slots == o.slots > 300
+    a.init_macro(mac)
+    o.seed(mac.astype(np.float64))
+    a.step(4)
+    of = o.step(4)
+    gfc, gmac = a.read_coarse()
+    gfp, _ = a.read_pool()
+    ofc, omac, ofp, _ = o.read()
+    assert rel_l2(gfc.astype(np.float64), ofc) <= 2e-6
+    assert rel_l2(gfp.astype(np.float64), ofp) <= 2e-6
+    assert rel_l2(gmac[:, 1:4].astype(np.float64), omac[:, 1:4]) <= 2e-4
+    g = a.forces()
+    scale = max(np.abs(of[-1, :6]).max(), 1e-6)
+    assert np.abs(g - of[-1, :6]).max() <= 1e-3 * scale, (g, of[-1, :6])
+    a.close()
+    o.close()
